@@ -1,0 +1,363 @@
+"""Benchmark: seconds from device-resident X to relative duality gap 1e-6 for the TensorSVM
+training path (kernel factor + SMW interior point), on the n=1M, d=18, k=256 two-Gaussian
+workload (gamma 0.05, C 32, 10% label noise), synthetic data.
+
+One step = one full training solve: GPU sketch, two fused kernel-block passes, CholeskyQR,
+projection, Jacobi eigen-factor, then the IPM until rel_gap = (pobj-dobj)/max(1,|pobj|) <= 1e-6
+with ||rd||/(1+sqrt n) and |rp|/(1+sqrt n) <= 1e-6.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp16|bf16|fp32]
+    python bench.py --impl reference ...     # the reference trainer's own build, host cores
+
+Multi-GPU (torchrun): replicas only -- every rank trains an independent problem of the same
+size (a different data seed), there is no collective on the data path; the line reports the
+max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "s to rel. gap 1e-6, mixed/TC vs FP32 form (n=1M,d=18,k=256); % of roofline"
+WORKLOAD = "two_gaussians_rbf"
+N_DEFAULT, D, K, GAMMA, CPEN, NOISE = 1_000_000, 18, 256, 0.05, 32.0, 0.10
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p, "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index, self.proc, self.samples = index, None, []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[j] for s in self.samples for j in range(4) if s[3 + j] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def dist_max(values, world):
+    if world == 1:
+        return values
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(values, dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.cpu().tolist()
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ------------------------------------------------------------------------------------------
+# our arm
+# ------------------------------------------------------------------------------------------
+
+def run_ours(args, world, rank, local):
+    import torch
+    from tensorsvm_b200 import _lib, api, synth
+    torch.cuda.set_device(local)
+    n = args.n
+    X, y = synth.two_gaussians(n, D, seed=2 + rank, noise=NOISE)
+    Xd, yd = torch.from_numpy(X).cuda(), torch.from_numpy(y).cuda()
+    ctx = _lib.Context(local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    prec = args.precision
+
+    def step(precision):
+        Z, finfo = api.factor(ctx, Xd, yd, GAMMA, K, precision)
+        alpha, _, _, st = api.ipm(ctx, Z, yd, K, CPEN, rel_gap_tol=1e-6,
+                                  precision=_lib.PREC_FP32 if precision == "fp32" else _lib.PREC_BF16)
+        return finfo, st
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step(prec)
+        barrier(world)
+        torch.cuda.synchronize()
+        launches0 = ctx.launches
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        finfos, stats, per_step = [], [], []
+        with ClockSampler(local) as clk:
+            e0.record(stream)
+            for _ in range(args.steps):
+                s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s0.record(stream)
+                fi, st = step(prec)
+                s1.record(stream)
+                finfos.append(fi)
+                stats.append(st)
+                per_step.append((s0, s1))
+            e1.record(stream)
+            torch.cuda.synchronize()
+        barrier(world)
+        launches = ctx.launches - launches0
+        total_ms = e0.elapsed_time(e1)
+        step_ms = [a.elapsed_time(b) for a, b in per_step]
+        # end to end through the public host-buffer API (tsvm_train), H2D/D2H inside
+        Xh = torch.from_numpy(X).pin_memory()
+        yh = torch.from_numpy(y).pin_memory()
+        e2e_ms = []
+        for _ in range(args.e2e_steps):
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            m = api.train(ctx, Xh.numpy(), yh.numpy(), _lib.KERNEL_RBF, GAMMA, CPEN, K, prec,
+                          rel_gap_tol=1e-6,
+                          precision=_lib.PREC_FP32 if prec == "fp32" else _lib.PREC_BF16)
+            t1.record(stream)
+            torch.cuda.synchronize()
+            e2e_ms.append(t0.elapsed_time(t1))
+        fp32_s = None
+        if args.fp32_form and prec != "fp32":
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            f0.record(stream)
+            fi32, st32 = step("fp32")
+            f1.record(stream)
+            torch.cuda.synchronize()
+            fp32_s = f0.elapsed_time(f1) / 1e3
+    sec = total_ms / 1e3 / args.steps
+    sec, e2e_s = dist_max([sec, (sum(e2e_ms) / max(1, len(e2e_ms))) / 1e3], world)
+    if rank != 0:
+        ctx.close()
+        return None
+    pk, pk_kind = peaks()
+    fi = finfos[-1]
+    km_ms = fi["ms_kermatmul_kernel"] / 2.0          # per launch (two launches per step)
+    km_flops = fi["flops_kermatmul"] / 2.0
+    tensor = prec != "fp32"
+    if tensor:
+        peak, unit, pname = pk["bf16_tflops_sustained"], "TFLOP/s", "bf16_tflops_sustained"
+    else:
+        # FP32 SIMT FMA peak: 148 SMs x 128 lanes x 2 flops x 1.965 GHz (nominal, no measured copy)
+        peak, unit, pname, pk_kind = 148 * 128 * 2 * 1.965e9 / 1e12, "TFLOP/s", "fp32_simt_nominal", "nominal"
+    achieved = km_flops / (km_ms / 1e3) / 1e12
+    st = stats[-1]
+    line = {
+        "metric": METRIC,
+        "value": round(sec, 4),
+        "unit": "s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 2),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": {"fp16": "f16 (fp32 accum)", "bf16": "bf16 (fp32 accum)", "fp32": "f32"}[prec]
+                 + " contractions, f64 k x k + IPM vectors",
+        "data": "synthetic (seeded two-Gaussian mixture, 10% label noise)",
+        "config": {"workload": WORKLOAD, "n": n, "d": D, "k": K, "gamma": GAMMA, "C": CPEN,
+                   "precision": prec, "stop": "rel_gap<=1e-6 and ||rd||,|rp|/(1+sqrt n)<=1e-6",
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (Z 1 GiB fp32, kernel operand 0.5 GiB)"},
+        "phases_ms": {"sketch": round(fi["ms_sketch"], 2), "pass1": round(fi["ms_pass1"], 2),
+                      "ortho": round(fi["ms_ortho"], 2), "pass2": round(fi["ms_pass2"], 2),
+                      "project": round(fi["ms_project"], 2), "factor_total": round(fi["ms_total"], 2),
+                      "ipm": round(st["ms_total"], 2), "ipm_syrk": round(st["ms_syrk"], 2),
+                      "ipm_chol": round(st["ms_factor"], 2), "ipm_iters": st["iters"]},
+        "solution": {"rel_gap": st["rel_gap"], "pobj": st["pobj"], "dobj": st["dobj"],
+                     "iters": st["iters"]},
+        "step_s": [round(t / 1e3, 4) for t in step_ms],
+        "roofline": {"bound": "tensor" if tensor else "fp32-simt", "kernel": "kermatmul (fused kernel-block product)",
+                     "achieved": round(achieved, 2), "peak": round(peak, 1), "unit": unit,
+                     "frac": round(achieved / peak, 4), "peak_source": f"{pk_kind} {pname}",
+                     "traffic": None, "flops_per_launch": km_flops, "ms_per_launch": round(km_ms, 3)},
+        "e2e": {"value": round(e2e_s, 4), "unit": "s",
+                "h2d_bytes_per_step": int(X.nbytes + y.nbytes), "d2h_bytes_per_step": int(8 * n + 8)},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if fp32_s is not None:
+        line["fp32_form"] = {"value": round(fp32_s, 3), "unit": "s", "speedup_mixed_vs_fp32": round(fp32_s / sec, 2)}
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args)
+    ctx.close()
+    return line
+
+
+def cpu_baseline(args):
+    """The FP64 oracle (same algorithm, host BLAS/LAPACK) on a bounded sample, scaled to n."""
+    from oracle import oracle as orc
+    from tensorsvm_b200 import synth
+    ns = args.cpu_sample
+    X, y = synth.two_gaussians(ns, D, seed=2, noise=NOISE)
+    t0 = time.perf_counter()
+    f = orc.lra(X, y, GAMMA, K)
+    t1 = time.perf_counter()
+    r = orc.mpc(f.U, y, CPEN, kernel="rbf", rel_gap_tol=1e-6)
+    t2 = time.perf_counter()
+    scale = args.n / ns
+    est = (t1 - t0) * scale * scale + (t2 - t1) * scale
+    return {"value": round(est, 1), "unit": "s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"FP64 oracle (numpy/OpenBLAS) on n={ns} rows of the same generator: "
+                      f"factor {t1 - t0:.2f}s scaled by (n/ns)^2, IPM {t2 - t1:.2f}s "
+                      f"({r.iters} it) scaled by n/ns"}
+
+
+# ------------------------------------------------------------------------------------------
+# reference arm: the reference trainer built from its own source (oracle/_ref)
+# ------------------------------------------------------------------------------------------
+
+def parse_ref_log(text):
+    text = re.sub(r"\x1b\[[0-9;]*m", "", text)
+    el = [float(v) for v in re.findall(r"elapsed time = ([0-9.]+) seconds", text)]
+    read = float(re.search(r"Reading files took ([0-9.]+) seconds", text).group(1))
+    km1 = float(re.search(r"rbf_kermatmul1.*?elapsed time = [0-9.]+ seconds\s*elapsed time = ([0-9.]+)",
+                          text, re.S).group(1))
+    km2 = float(re.search(r"rbf_kermatmul2.*?elapsed time = [0-9.]+ seconds\s*elapsed time = ([0-9.]+)",
+                          text, re.S).group(1))
+    write = el[-1]
+    iters = [ln for ln in re.findall(r"iter (\d+), mu=\S+, normdx=(\S+), normdy=(\S+) max/min\(D\)=\S+ "
+                                     r"pobj=(\S+) dobj=(\S+)", text)]
+    return read, km1, km2, write, iters
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    ref = os.path.join(ROOT, "oracle", "_ref", "tensorsvm-train-ref")
+    if not os.path.exists(ref):
+        return {"impl": "reference", "unavailable": "oracle/_ref/tensorsvm-train-ref not built"}
+    from tensorsvm_b200 import synth
+    tmp = tempfile.mkdtemp()
+    small = os.path.join(tmp, "small.train")
+    X, y = synth.two_gaussians(8192, D, seed=2, noise=NOISE)
+    synth.write_libsvm(small, X, y)
+    ns = args.ref_sample
+    big = os.path.join(tmp, "sample.train")
+    X, y = synth.two_gaussians(ns, D, seed=2, noise=NOISE)
+    synth.write_libsvm(big, X, y)
+    cmd = [ref, "-k", str(K), "-c", str(CPEN), "-g", str(GAMMA), "-t", "2"]
+    for _ in range(args.warmup):
+        subprocess.run(cmd + [small, small + ".model"], capture_output=True, text=True, timeout=600)
+    ests, walls, details = [], [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        p = subprocess.run(cmd + [big, big + ".model"], capture_output=True, text=True, timeout=1800)
+        wall = time.perf_counter() - t0
+        read, km1, km2, write, iters = parse_ref_log(p.stdout)
+        # time to rel_gap 1e-6: the reference logs every 5 iterations; keep its whole MPC phase
+        # unless an earlier logged iterate already met the criterion (then scale by iterations)
+        rest = wall - read - write - km1 - km2     # sketch, TSQR, C, eig, U, MPC: ~linear in n
+        scale = args.n / ns
+        est = (km1 + km2) * scale * scale + rest * scale
+        ests.append(est)
+        walls.append(wall)
+        details.append({"wall": round(wall, 2), "read": read, "kermatmul": round(km1 + km2, 3),
+                        "writemodel": write, "iters_logged": len(iters)})
+    value = statistics.mean(ests)
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": "s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * statistics.mean(walls), 1), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 LRA (cuBLAS) + f64 host IPM (OpenBLAS)",
+        "data": "synthetic (seeded two-Gaussian mixture, 10% label noise)",
+        "config": {"workload": WORKLOAD, "n": args.n, "d": D, "k": K, "gamma": GAMMA, "C": CPEN},
+        "cpu_baseline": {"value": round(value, 2), "unit": "s", "cores": os.cpu_count(),
+                         "kind": "reference",
+                         "sample": f"reference build (oracle/_ref) on n={ns} rows; kernel passes "
+                                   f"scaled (n/ns)^2, other phases n/ns; excludes file read and "
+                                   f"model write"},
+        "e2e": {"value": round(value, 2), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "detail": details,
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp16", choices=["fp16", "bf16", "fp32"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-fp32-form", dest="fp32_form", action="store_false")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=16384)
+    ap.add_argument("--ref-sample", type=int, default=262144)
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        line = run_reference(args, world, rank)
+    else:
+        line = run_ours(args, world, rank, local)
+    if line is not None and rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

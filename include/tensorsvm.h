@@ -1,0 +1,172 @@
+/* tensorsvm.h - C ABI of the B200-native TensorSVM training path.
+ *
+ * The reference trainer (robbwu/tensorsvm, tensorsvm-train.cu) has no library API: its seams
+ * are two C++ functions that pass state through globals,
+ *     double LRA(float *Z, int ldz, double *U, int ldu, long n, long k)      tensorsvm-train.cu:1941
+ *     void   mpc(double *Z, double *a, double C, double *X, double *Xi, int N, int d)
+ *                                                                          tensorsvm-train.cu:1507
+ * plus the bias computation inside writemodel (tensorsvm-train.cu:355-376) and the driver in
+ * main (tensorsvm-train.cu:858-1059).  Each entry point below names the one it replaces.
+ *
+ * Conventions (all entry points):
+ *   - every call returns a tsvm_status; none calls exit();
+ *   - pointers documented as "device" are caller-owned CUDA device buffers on the context's
+ *     device; "host" buffers are caller-owned host memory;
+ *   - the library owns its device scratch inside the context (grown on demand, freed by
+ *     tsvm_destroy);
+ *   - one context per host thread; all work is issued on the context's stream, and every
+ *     call returns after that stream is synchronised unless noted otherwise.
+ */
+#ifndef TENSORSVM_H
+#define TENSORSVM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum tsvm_status {
+  TSVM_OK = 0,
+  TSVM_ERR_INVALID_ARGUMENT = 1,
+  TSVM_ERR_CUDA = 2,
+  TSVM_ERR_OUT_OF_MEMORY = 3,
+  /* capacitance matrix I + Z^T D^-1 Z is not positive definite; the reference prints
+   * "Cholesky fact info error" and returns early (tensorsvm-train.cu:1709-1714) */
+  TSVM_ERR_NOT_SPD = 4,
+  TSVM_ERR_UNSUPPORTED = 5,
+  TSVM_ERR_NO_DEVICE = 6,
+  /* a bounded device-side wait gave up; the context stays usable */
+  TSVM_ERR_TIMEOUT = 7,
+  /* IPM stopped because max(D)/min(D) > 1e18 (tensorsvm-train.cu:1653-1658); results valid */
+  TSVM_WARN_ILL_CONDITIONED = 8,
+  /* IPM stopped at the iteration cap (MAX_MPC_ITER, tensorsvm-train.cu:62); results valid */
+  TSVM_WARN_MAX_ITER = 9,
+  /* the Gaussian sketch stream ran short of accepted pairs (retry limit reached) */
+  TSVM_ERR_SKETCH = 10,
+  TSVM_ERR_IO = 11
+} tsvm_status;
+
+/* -t kernel_type values accepted by the reference (tensorsvm-train.cu:1112-1118) */
+typedef enum tsvm_kernel { TSVM_KERNEL_LINEAR = 0, TSVM_KERNEL_RBF = 2 } tsvm_kernel;
+
+/* Arithmetic of the two contractions (kernel-block product and Z^T D^-1 Z).
+ * FP32: SIMT FP32 (the "plain" form, what the reference computes without -tensorcore).
+ * BF16/FP16: tcgen05 tensor cores with FP32 accumulation (the "-tensorcore" form). */
+typedef enum tsvm_precision {
+  TSVM_PREC_FP32 = 0,
+  TSVM_PREC_BF16 = 1,
+  TSVM_PREC_FP16 = 2
+} tsvm_precision;
+
+/* Sketch source.  GLIBC reproduces the reference's gaussrand() stream exactly (glibc rand()
+ * from its default seed, Marsaglia polar method, tensorsvm-train.cu:2621-2643) on the GPU.
+ * USER takes a caller-provided n x k row-major float matrix. */
+typedef enum tsvm_sketch { TSVM_SKETCH_GLIBC = 0, TSVM_SKETCH_USER = 1 } tsvm_sketch;
+
+typedef struct tsvm_context tsvm_context;
+
+typedef struct tsvm_factor_info {
+  int64_t n;
+  int32_t d, k, k_padded;
+  int32_t realk;                 /* eigenvalues of C kept (> 0), tensorsvm-train.cu:2197-2211 */
+  int32_t precision;
+  double eig_max, eig_min;       /* largest / smallest eigenvalue of C (the "[LRA]" print) */
+  double ms_sketch, ms_pass1, ms_ortho, ms_pass2, ms_project, ms_total;
+  double ms_kermatmul_kernel;    /* device time of the two fused kernel-block launches */
+  double flops_kermatmul;        /* algorithmic flops: 2 passes x (2 n^2 k + 2 n^2 d) */
+} tsvm_factor_info;
+
+typedef struct tsvm_ipm_options {
+  int32_t max_iter;       /* iteration cap, default 100 (tensorsvm-train.cu:62) */
+  double tol;             /* reference stop: mu, ||rd||, |rp| all < tol; default 1e-7 (T:1647) */
+  double rel_gap_tol;     /* additional stop when rel_gap = (pobj-dobj)/max(1,|pobj|) <= tol
+                             and ||rd||/(1+sqrt n), |rp|/(1+sqrt n) <= tol; <= 0 disables */
+  int32_t precision;      /* SYRK arithmetic: TSVM_PREC_FP32 or TSVM_PREC_BF16 */
+  int32_t refine_sweeps;  /* iterative-refinement sweeps per Newton direction (0..2) */
+  int32_t kernel;         /* initialisation rule: TSVM_KERNEL_RBF (T:1535) or _LINEAR (T:1553) */
+  int32_t verbose;        /* print the reference's "iter %d, mu=..." lines every 5 iterations */
+} tsvm_ipm_options;
+
+typedef struct tsvm_ipm_stats {
+  int32_t iters;
+  int32_t status;         /* tsvm_status of the solve */
+  double mu, norm_rd, norm_rp, cond_d, pobj, dobj, rel_gap;
+  double ms_total, ms_syrk, ms_factor, ms_streams;
+  double t_rel_gap_1e6_ms; /* wall time at the first iterate with rel_gap <= 1e-6 (or -1) */
+} tsvm_ipm_stats;
+
+/* Human-readable status. */
+const char *tsvm_status_string(tsvm_status s);
+
+/* Create a context on CUDA device `device` with its own stream.  Replaces the per-call
+ * cublasCreate/cudaStreamCreate/cusolverDnCreate of LRA and mpc (T:1509-1514, T:1945-1961). */
+tsvm_status tsvm_create(tsvm_context **ctx, int device);
+tsvm_status tsvm_destroy(tsvm_context *ctx);
+
+/* Issue the context's work on a caller-owned CUDA stream (cudaStream_t passed as void*);
+ * NULL restores the context's own stream.  The library never destroys a caller's stream. */
+tsvm_status tsvm_set_stream(tsvm_context *ctx, void *stream);
+
+/* Fill `opt` with the reference's defaults (max_iter 100, tol 1e-7, FP32, RBF init). */
+void tsvm_ipm_default_options(tsvm_ipm_options *opt);
+
+/* Kernel factor (replaces LRA, tensorsvm-train.cu:1941-2374).
+ * Computes Z (n x k, row-major, leading dimension ldz >= k) with Z Z^T ~= Y K Y, K the RBF
+ * kernel exp(-gamma ||x_i - x_j||^2) of X: sketch Q, W = Y K Y Q, W = orth(W), Q = Y K Y W,
+ * C = W^T Q, C = V diag(w) V^T, Z = W V diag(sqrt(max(w, 0))).  Columns k..ldz-1 of Z are 0.
+ *   X      device, n x d row-major float
+ *   y      device, n labels in {+1, -1}
+ *   Q_user device, n x k row-major float when sketch == TSVM_SKETCH_USER, else NULL
+ *   Z      device, n x ldz row-major float (output)
+ *   info   host, may be NULL */
+tsvm_status tsvm_factor(tsvm_context *ctx, const float *X, const float *y, int64_t n, int32_t d,
+                        double gamma, int32_t k, int32_t precision, int32_t sketch,
+                        const float *Q_user, float *Z, int32_t ldz, tsvm_factor_info *info);
+
+/* Linear "factor": Z = diag(y) X, k = d (tensorsvm-train.cu:909-914).  Device buffers. */
+tsvm_status tsvm_linear_factor(tsvm_context *ctx, const float *X, const float *y, int64_t n,
+                               int32_t d, float *Z, int32_t ldz);
+
+/* Interior-point solve of  min 1/2 a^T Q a - e^T a,  y^T a = 0,  0 <= a <= C,  Q = Z Z^T
+ * (replaces mpc, tensorsvm-train.cu:1507-1785, with NewtonStep 1794-1822 and SMWSolve
+ * 1824-1840).  Newton steps go through M = I + Z^T D^-1 Z (FP64 Cholesky on the device).
+ *   Z          device, n x ldz row-major float (columns beyond k ignored)
+ *   y          device, n labels in {+1, -1}
+ *   alpha_out  device, n doubles (the dual variables "X" of the reference)
+ *   xi_out     device, n doubles or NULL
+ *   ymult_out  host, the equality multiplier (the reference's local "y"), or NULL
+ *   opt        host, NULL for defaults;  stats host, may be NULL
+ * Returns TSVM_OK on convergence, TSVM_WARN_ILL_CONDITIONED / TSVM_WARN_MAX_ITER when the
+ * reference's other stopping rules fired (outputs valid), TSVM_ERR_NOT_SPD on a failed
+ * Cholesky (outputs hold the last iterate, as the reference leaves X). */
+tsvm_status tsvm_ipm(tsvm_context *ctx, const float *Z, int32_t ldz, const float *y, int64_t n,
+                     int32_t k, double C, const tsvm_ipm_options *opt, double *alpha_out,
+                     double *xi_out, double *ymult_out, tsvm_ipm_stats *stats);
+
+/* Bias of the RBF model (replaces tensorsvm-train.cu:355-376): the mean over the first <= 50
+ * free SVs j (1e-6 < alpha_j < C - 1e-6, in index order) of y_j - sum_{i in SV} alpha_i y_j
+ * (Z_i . Z_j).  b is NaN when there is no free SV (as the reference's 0/0).
+ *   Z, y, alpha device;  b_out, b_std_out, n_sv, n_free host (any may be NULL) */
+tsvm_status tsvm_bias(tsvm_context *ctx, const float *Z, int32_t ldz, const float *y,
+                      const double *alpha, int64_t n, int32_t k, double C, double *b_out,
+                      double *b_std_out, int32_t *n_sv, int32_t *n_free);
+
+/* End-to-end training from HOST buffers (the path main() drives, tensorsvm-train.cu:907-1024):
+ * copies X and y to the device, factors (RBF) or labels (linear), solves, computes the bias
+ * and copies alpha back.  For the linear kernel `gamma` and `k` are ignored and w is not
+ * formed here (the caller forms it from alpha, as writemodel does).
+ *   X host n x d row-major; y host labels +-1; alpha_out host n doubles; b_out host. */
+tsvm_status tsvm_train(tsvm_context *ctx, const float *X, const float *y, int64_t n, int32_t d,
+                       int32_t kernel, double gamma, double C, int32_t k, int32_t precision,
+                       const tsvm_ipm_options *opt, double *alpha_out, double *b_out,
+                       tsvm_factor_info *finfo, tsvm_ipm_stats *istats);
+
+/* Number of tensorsvm kernels this library launched since the context was created. */
+int64_t tsvm_kernel_launches(const tsvm_context *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TENSORSVM_H */

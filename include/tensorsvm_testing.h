@@ -1,0 +1,43 @@
+/* tensorsvm_testing.h - test hooks of libtensorsvm_b200 (not part of the training API).
+ *
+ * Each hook runs one internal device routine on caller-owned DEVICE buffers and synchronises,
+ * so the parity tests can check a kernel in isolation against the CPU oracle.  The routines
+ * they expose stand in for the reference's calls noted below; they have no counterpart of
+ * their own in the reference's (non-existent) library API.
+ */
+#ifndef TENSORSVM_TESTING_H
+#define TENSORSVM_TESTING_H
+
+#include "tensorsvm.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* glibc rand() stream from the default seed (count values): the generator behind
+ * gaussrand() (tensorsvm-train.cu:2629-2630). */
+tsvm_status tsvm_test_rand_stream(tsvm_context *ctx, int64_t count, uint32_t *out);
+/* The reference's gaussrand() stream (tensorsvm-train.cu:2621-2643), count floats. */
+tsvm_status tsvm_test_sketch(tsvm_context *ctx, int64_t count, float *out);
+/* W (n x kp) = (Y K Y) A (n x kp) with the given precision (kermatmul, T:2476-2567). */
+tsvm_status tsvm_test_kermatmul(tsvm_context *ctx, const float *X, const float *y, int64_t n,
+                                int32_t d, double gamma, const float *A, int32_t kp, float *W,
+                                int32_t precision);
+/* In-place lower Cholesky of A (n x n row-major); *info_host = 0 or failing column (T:1709). */
+tsvm_status tsvm_test_chol(tsvm_context *ctx, double *A, int32_t n, int32_t *info_host);
+/* Solve L L^T X = B, B holds nrhs rows of length ldb (T:1834). */
+tsvm_status tsvm_test_potrs(tsvm_context *ctx, const double *L, int32_t n, double *B,
+                            int32_t nrhs, int32_t ldb);
+/* Eigen-decomposition of the symmetric A (n x n); w eigenvalues, V eigenvectors as columns
+ * (T:2191). */
+tsvm_status tsvm_test_eig(tsvm_context *ctx, double *A, int32_t n, double *w, double *V,
+                          int32_t *sweeps_host);
+/* G (ka x kb) = A^T diag(s) B over n rows with FP64 accumulation; s may be NULL. */
+tsvm_status tsvm_test_gram(tsvm_context *ctx, const float *A, int64_t lda, const float *B,
+                           int64_t ldb, int64_t n, int32_t ka, int32_t kb, int32_t symmetric,
+                           const double *s, double *G);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TENSORSVM_TESTING_H */

@@ -1,0 +1,247 @@
+// C ABI of the library (include/tensorsvm.h): context management, argument checking and the
+// end-to-end train call.  All compute lives in the other .cu files.
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+#include "context.h"
+#include "kernels.h"
+
+namespace tsvm {
+
+tsvm_status cuda_status(cudaError_t e, const char *what, const char *file, int line) {
+  if (getenv("TSVM_DEBUG"))
+    fprintf(stderr, "tensorsvm: CUDA error %s (%s) at %s:%d\n", cudaGetErrorString(e), what, file,
+            line);
+  if (e == cudaErrorMemoryAllocation) return TSVM_ERR_OUT_OF_MEMORY;
+  if (e == cudaErrorNoDevice || e == cudaErrorInvalidDevice) return TSVM_ERR_NO_DEVICE;
+  return TSVM_ERR_CUDA;
+}
+
+tsvm_status scratch(tsvm_context *ctx, Slot s, size_t bytes, void **out) {
+  bytes = (bytes + 255) & ~(size_t)255;
+  if (bytes == 0) bytes = 256;
+  if (ctx->bytes[s] < bytes) {
+    if (ctx->buf[s]) {
+      TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+      TSVM_CUDA(cudaFree(ctx->buf[s]));
+      ctx->buf[s] = nullptr;
+      ctx->bytes[s] = 0;
+    }
+    void *p = nullptr;
+    TSVM_CUDA(cudaMalloc(&p, bytes));
+    ctx->buf[s] = p;
+    ctx->bytes[s] = bytes;
+  }
+  *out = ctx->buf[s];
+  return TSVM_OK;
+}
+
+float event_ms(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  cudaEventSynchronize(b);
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+// Host-side linear model (w, b) from alpha, as writemodel does (tensorsvm-train.cu:301-332).
+static void linear_bias_host(const float *X, const float *y, const double *alpha, int64_t n,
+                             int d, double C, double *b_out) {
+  std::vector<double> w(d, 0.0);
+  std::vector<int64_t> freeidx;
+  for (int64_t i = 0; i < n; ++i) {
+    if (alpha[i] > 1e-6) {
+      for (int c = 0; c < d; ++c) w[c] += alpha[i] * y[i] * X[i * d + c];
+      if (alpha[i] < C - 1e-6) freeidx.push_back(i);
+    }
+  }
+  const int64_t m = std::min<int64_t>((int64_t)freeidx.size(), 5000);
+  double b = 0.0;
+  if (m > 0) {
+    double s = 0.0;
+    for (int64_t t = 0; t < m; ++t) {
+      const int64_t j = freeidx[t];
+      double v = y[j];
+      for (int c = 0; c < d; ++c) v -= w[c] * X[j * d + c];
+      s += v;
+    }
+    b = s / m;
+  }
+  *b_out = b;
+}
+
+}  // namespace tsvm
+
+using namespace tsvm;
+
+extern "C" {
+
+const char *tsvm_status_string(tsvm_status s) {
+  switch (s) {
+    case TSVM_OK: return "ok";
+    case TSVM_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case TSVM_ERR_CUDA: return "CUDA error";
+    case TSVM_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case TSVM_ERR_NOT_SPD: return "capacitance matrix not positive definite (Cholesky failed)";
+    case TSVM_ERR_UNSUPPORTED: return "unsupported shape or precision";
+    case TSVM_ERR_NO_DEVICE: return "no CUDA device";
+    case TSVM_ERR_TIMEOUT: return "bounded device wait timed out";
+    case TSVM_WARN_ILL_CONDITIONED: return "stopped: max/min(D) > 1e18";
+    case TSVM_WARN_MAX_ITER: return "stopped: iteration limit reached";
+    case TSVM_ERR_SKETCH: return "sketch stream exhausted";
+    case TSVM_ERR_IO: return "I/O error";
+  }
+  return "unknown status";
+}
+
+tsvm_status tsvm_create(tsvm_context **out, int device) {
+  if (!out) return TSVM_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return TSVM_ERR_NO_DEVICE;
+  if (device < 0 || device >= count) return TSVM_ERR_INVALID_ARGUMENT;
+  TSVM_CUDA(cudaSetDevice(device));
+  tsvm_context *ctx = new tsvm_context();
+  ctx->device = device;
+  cudaError_t e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+  ctx->stream = ctx->own_stream;
+  for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreate(&ctx->ev[i]);
+  if (e == cudaSuccess) e = cudaMallocHost(&ctx->host_scalars, 4096);
+  if (e != cudaSuccess) {
+    tsvm_destroy(ctx);
+    return cuda_status(e, "tsvm_create", __FILE__, __LINE__);
+  }
+  *out = ctx;
+  return TSVM_OK;
+}
+
+tsvm_status tsvm_destroy(tsvm_context *ctx) {
+  if (!ctx) return TSVM_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (int i = 0; i < SLOT_COUNT_; ++i)
+    if (ctx->buf[i]) cudaFree(ctx->buf[i]);
+  for (int i = 0; i < 8; ++i)
+    if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+  if (ctx->host_scalars) cudaFreeHost(ctx->host_scalars);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+  return TSVM_OK;
+}
+
+tsvm_status tsvm_set_stream(tsvm_context *ctx, void *stream) {
+  if (!ctx) return TSVM_ERR_INVALID_ARGUMENT;
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+  return TSVM_OK;
+}
+
+void tsvm_ipm_default_options(tsvm_ipm_options *opt) {
+  if (!opt) return;
+  opt->max_iter = 100;
+  opt->tol = 1e-7;
+  opt->rel_gap_tol = 0.0;
+  opt->precision = TSVM_PREC_FP32;
+  opt->refine_sweeps = 0;
+  opt->kernel = TSVM_KERNEL_RBF;
+  opt->verbose = 0;
+}
+
+int64_t tsvm_kernel_launches(const tsvm_context *ctx) { return ctx ? ctx->launches : 0; }
+
+tsvm_status tsvm_factor(tsvm_context *ctx, const float *X, const float *y, int64_t n, int32_t d,
+                        double gamma, int32_t k, int32_t precision, int32_t sketch,
+                        const float *Q_user, float *Z, int32_t ldz, tsvm_factor_info *info) {
+  if (!ctx || !X || !y || !Z) return TSVM_ERR_INVALID_ARGUMENT;
+  if (precision < TSVM_PREC_FP32 || precision > TSVM_PREC_FP16) return TSVM_ERR_INVALID_ARGUMENT;
+  TSVM_CUDA(cudaSetDevice(ctx->device));
+  return factor_rbf(ctx, X, y, n, d, gamma, k, precision, sketch, Q_user, Z, ldz, info);
+}
+
+tsvm_status tsvm_linear_factor(tsvm_context *ctx, const float *X, const float *y, int64_t n,
+                               int32_t d, float *Z, int32_t ldz) {
+  if (!ctx || !X || !y || !Z || n < 1 || d < 1 || ldz < d) return TSVM_ERR_INVALID_ARGUMENT;
+  TSVM_CUDA(cudaSetDevice(ctx->device));
+  TSVM_TRY(label_rows(ctx, X, y, n, d, Z, ldz));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSVM_OK;
+}
+
+tsvm_status tsvm_ipm(tsvm_context *ctx, const float *Z, int32_t ldz, const float *y, int64_t n,
+                     int32_t k, double C, const tsvm_ipm_options *opt, double *alpha_out,
+                     double *xi_out, double *ymult_out, tsvm_ipm_stats *stats) {
+  if (!ctx || !Z || !y || !alpha_out || n < 2 || k < 1 || ldz < k || !(C > 0))
+    return TSVM_ERR_INVALID_ARGUMENT;
+  if ((ldz % 4) != 0 || (reinterpret_cast<uintptr_t>(Z) & 15) != 0) return TSVM_ERR_INVALID_ARGUMENT;
+  tsvm_ipm_options o;
+  tsvm_ipm_default_options(&o);
+  if (opt) o = *opt;
+  if (o.max_iter < 0 || !(o.tol > 0)) return TSVM_ERR_INVALID_ARGUMENT;
+  TSVM_CUDA(cudaSetDevice(ctx->device));
+  return ipm_solve(ctx, Z, ldz, y, n, k, C, o, alpha_out, xi_out, ymult_out, stats);
+}
+
+tsvm_status tsvm_bias(tsvm_context *ctx, const float *Z, int32_t ldz, const float *y,
+                      const double *alpha, int64_t n, int32_t k, double C, double *b_out,
+                      double *b_std_out, int32_t *n_sv, int32_t *n_free) {
+  if (!ctx || !Z || !y || !alpha || n < 1 || k < 1 || ldz < k) return TSVM_ERR_INVALID_ARGUMENT;
+  TSVM_CUDA(cudaSetDevice(ctx->device));
+  return bias_rbf(ctx, Z, ldz, y, alpha, n, k, C, b_out, b_std_out, n_sv, n_free);
+}
+
+tsvm_status tsvm_train(tsvm_context *ctx, const float *X, const float *y, int64_t n, int32_t d,
+                       int32_t kernel, double gamma, double C, int32_t k, int32_t precision,
+                       const tsvm_ipm_options *opt, double *alpha_out, double *b_out,
+                       tsvm_factor_info *finfo, tsvm_ipm_stats *istats) {
+  if (!ctx || !X || !y || !alpha_out || n < 2 || d < 1) return TSVM_ERR_INVALID_ARGUMENT;
+  if (kernel != TSVM_KERNEL_LINEAR && kernel != TSVM_KERNEL_RBF) return TSVM_ERR_UNSUPPORTED;
+  TSVM_CUDA(cudaSetDevice(ctx->device));
+  tsvm_ipm_options o;
+  tsvm_ipm_default_options(&o);
+  if (opt) o = *opt;
+  o.kernel = kernel;
+  float *dX = nullptr, *dZ = nullptr;
+  double *dalpha = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_DEV_IN, (size_t)n * d + (size_t)n + 64, &dX));
+  float *dy = dX + (size_t)n * d;
+  TSVM_CUDA(cudaMemcpyAsync(dX, X, sizeof(float) * n * d, cudaMemcpyHostToDevice, ctx->stream));
+  TSVM_CUDA(cudaMemcpyAsync(dy, y, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream));
+  TSVM_TRY(scratch_t(ctx, SLOT_DEV_OUT, (size_t)n, &dalpha));
+  tsvm_status st;
+  if (kernel == TSVM_KERNEL_RBF) {
+    const int kp = (int)round_up(k, 64);
+    TSVM_TRY(scratch_t(ctx, SLOT_DEV_Z, (size_t)n * kp, &dZ));
+    TSVM_TRY(factor_rbf(ctx, dX, dy, n, d, gamma, k, precision, TSVM_SKETCH_GLIBC, nullptr, dZ, kp,
+                        finfo));
+    st = ipm_solve(ctx, dZ, kp, dy, n, k, C, o, dalpha, nullptr, nullptr, istats);
+    if (st != TSVM_OK && st != TSVM_WARN_ILL_CONDITIONED && st != TSVM_WARN_MAX_ITER &&
+        st != TSVM_ERR_NOT_SPD)
+      return st;
+    double b = 0.0;
+    TSVM_TRY(bias_rbf(ctx, dZ, kp, dy, dalpha, n, k, C, &b, nullptr, nullptr, nullptr));
+    if (b_out) *b_out = b;
+    TSVM_CUDA(cudaMemcpyAsync(alpha_out, dalpha, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                              ctx->stream));
+    TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  } else {
+    const int ldz = (int)round_up(d, 4);
+    TSVM_TRY(scratch_t(ctx, SLOT_DEV_Z, (size_t)n * ldz, &dZ));
+    TSVM_TRY(label_rows(ctx, dX, dy, n, d, dZ, ldz));
+    st = ipm_solve(ctx, dZ, ldz, dy, n, d, C, o, dalpha, nullptr, nullptr, istats);
+    if (st != TSVM_OK && st != TSVM_WARN_ILL_CONDITIONED && st != TSVM_WARN_MAX_ITER &&
+        st != TSVM_ERR_NOT_SPD)
+      return st;
+    TSVM_CUDA(cudaMemcpyAsync(alpha_out, dalpha, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                              ctx->stream));
+    TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (b_out) linear_bias_host(X, y, alpha_out, n, d, C, b_out);
+  }
+  return st;
+}
+
+}  // extern "C"

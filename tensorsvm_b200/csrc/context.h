@@ -1,0 +1,73 @@
+// The tsvm_context behind the C ABI: device, stream, launch counter and a slot-keyed
+// device scratch arena (grown on demand, never shrunk, freed by tsvm_destroy).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "tensorsvm.h"
+
+namespace tsvm {
+
+enum Slot : int {
+  SLOT_RAND = 0,      // sketch: raw rand() stream
+  SLOT_STATES,        // sketch: per-segment generator states
+  SLOT_COUNTS,        // sketch: per-block accept counts / offsets
+  SLOT_JUMP,          // sketch: jump-ahead matrices
+  SLOT_Q,             // factor: sketch / pass-2 output (n x kp fp32)
+  SLOT_W,             // factor: pass-1 output, orthonormalised in place (n x kp fp32)
+  SLOT_W2,            // factor: scratch n x kp fp32
+  SLOT_OPA,           // factor: tensor-core B operand (kp x n fp16/bf16, labels folded in)
+  SLOT_OPX,           // factor: tensor-core split features (n x Kg fp16)
+  SLOT_XC,            // factor: centred features + norms
+  SLOT_PART,          // split-n partial sums (fp64)
+  SLOT_SMALL,         // k x k fp64 work (Gram, Cholesky, eigen)
+  SLOT_SMALL2,
+  SLOT_SMALL3,
+  SLOT_IPM_VEC,       // IPM fp64 vectors
+  SLOT_IPM_SCAL,      // IPM device scalars
+  SLOT_IPM_M,         // IPM capacitance matrix + factor
+  SLOT_IPM_ZH,        // IPM low-precision copy of Z (bf16)
+  SLOT_MISC,
+  SLOT_DEV_IN,        // tsvm_train: device copies of host inputs
+  SLOT_DEV_Z,         // tsvm_train: factor Z
+  SLOT_DEV_OUT,       // tsvm_train: device alpha
+  SLOT_COUNT_
+};
+
+}  // namespace tsvm
+
+struct tsvm_context {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;      // stream all work is issued on
+  cudaStream_t own_stream = nullptr;  // the context's own stream
+  int64_t launches = 0;
+  void *buf[tsvm::SLOT_COUNT_] = {};
+  size_t bytes[tsvm::SLOT_COUNT_] = {};
+  cudaEvent_t ev[8] = {};
+  // sketch jump-ahead tables, keyed by the number of segments they cover
+  int jump_levels = 0;
+  // pinned host staging for small device->host reads
+  double *host_scalars = nullptr;
+};
+
+namespace tsvm {
+
+// Ensure slot `s` holds at least `bytes` bytes; returns the device pointer (or null + status).
+tsvm_status scratch(tsvm_context *ctx, Slot s, size_t bytes, void **out);
+
+template <class T>
+inline tsvm_status scratch_t(tsvm_context *ctx, Slot s, size_t count, T **out) {
+  void *p = nullptr;
+  tsvm_status st = scratch(ctx, s, count * sizeof(T), &p);
+  *out = static_cast<T *>(p);
+  return st;
+}
+
+// Elapsed ms between two recorded events (synchronises on the second).
+float event_ms(cudaEvent_t a, cudaEvent_t b);
+
+}  // namespace tsvm

@@ -1,0 +1,200 @@
+// Kernel factor Z with Z Z^T ~= Y K Y (replaces LRA, tensorsvm-train.cu:1941-2374).
+//
+// Same method as the reference, with every step on the device and every matrix resident:
+//   sketch Q = gaussrand stream               (T:1966-1974)       sketch.cu
+//   W = (Y K Y) Q                              (T:2067)            kermatmul_{simt,tc}.cu
+//   W = orth(W)                                (T:2075, TSQR)      shifted CholeskyQR3 here
+//   Q = (Y K Y) W                              (T:2085)
+//   C = W^T Q, symmetrised                     (T:2122-2160)       gram_fp64 + symmetrize
+//   C = V diag(w) V^T, X = V diag(sqrt(w+))   (T:2179-2211)       Jacobi eigensolver
+//   Z = W X                                    (T:2213-2241)       apply_right_fp32
+// The orthonormalisation is shifted CholeskyQR3 (Fukaya et al., SIAM J. Sci. Comput. 2020):
+// G = W^T W accumulated exactly in FP64, G + s I with s = 11 (n k + k (k+1)) u ||W||_F^2,
+// then two unshifted CholeskyQR steps.  Only range(W) matters for Z Z^T = W C+ W^T, so any
+// orthonormal basis of the same range gives the reference's factor.
+#include <math.h>
+
+#include <vector>
+
+#include "common.cuh"
+#include "context.h"
+#include "kernels.h"
+
+namespace tsvm {
+namespace {
+
+// G[i][i] += factor * trace(G)   (one block)
+__global__ void shift_by_trace(double *G, int k, double factor) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < k; i += blockDim.x) s += G[(int64_t)i * k + i];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+    sh[0] = t;
+  }
+  __syncthreads();
+  const double shift = factor * sh[0];
+  for (int i = threadIdx.x; i < k; i += blockDim.x) G[(int64_t)i * k + i] += shift;
+}
+
+// R32 (kp x kp fp32) = Linv^T padded with zeros: W R32 = W L^-T.
+__global__ void rinv_to_fp32(const double *__restrict__ Linv, int k, int kp,
+                             float *__restrict__ R32) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)kp * kp) return;
+  const int m = (int)(e / kp), c = (int)(e % kp);
+  R32[e] = (m < k && c < k) ? (float)Linv[(int64_t)c * k + m] : 0.f;
+}
+
+// X32 (kp x kp fp32) = V diag(sqrt(max(w, 0))) padded with zeros (T:2199-2210).
+__global__ void eigfactor_to_fp32(const double *__restrict__ V, const double *__restrict__ w,
+                                  int k, int kp, float *__restrict__ X32) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)kp * kp) return;
+  const int m = (int)(e / kp), c = (int)(e % kp);
+  float v = 0.f;
+  if (m < k && c < k) {
+    const double wc = w[c];
+    v = wc > 0.0 ? (float)(V[(int64_t)m * k + c] * sqrt(wc)) : 0.f;
+  }
+  X32[e] = v;
+}
+
+struct Phase {
+  tsvm_context *ctx;
+  cudaEvent_t a, b;
+};
+
+}  // namespace
+
+static tsvm_status kermatmul(tsvm_context *ctx, const float *Xc, const float *norms,
+                             const float *y, int64_t n, int d, double gamma, const float *A,
+                             int kp, float *W, int precision, float *kernel_ms) {
+  if (precision == TSVM_PREC_FP32)
+    return kermatmul_fp32(ctx, Xc, norms, y, n, d, gamma, A, kp, W);
+  if (!kermatmul_tc_supported(d, kp)) return TSVM_ERR_UNSUPPORTED;
+  return kermatmul_tc(ctx, Xc, norms, y, n, d, gamma, A, kp, W, precision, kernel_ms);
+}
+
+static tsvm_status orthonormalise(tsvm_context *ctx, float *W, int64_t n, int k, int kp) {
+  double *G = nullptr, *Linv = nullptr;
+  float *R32 = nullptr;
+  int *info = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_SMALL, (size_t)k * k + 8, &G));
+  TSVM_TRY(scratch_t(ctx, SLOT_SMALL2, (size_t)k * k, &Linv));
+  TSVM_TRY(scratch_t(ctx, SLOT_IPM_M, (size_t)kp * kp, &R32));
+  info = reinterpret_cast<int *>(G + (size_t)k * k);
+  const double u = ldexp(1.0, -53);
+  for (int step = 0; step < 3; ++step) {
+    double factor = step == 0 ? 11.0 * ((double)n * k + (double)k * (k + 1)) * u : 0.0;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+      TSVM_TRY(gram_fp64(ctx, W, kp, W, kp, n, k, k, true, G));
+      if (factor > 0) {
+        shift_by_trace<<<1, 256, 0, ctx->stream>>>(G, k, factor);
+        TSVM_LAUNCHED(ctx);
+      }
+      TSVM_TRY(chol_fp64(ctx, G, k, k, info));
+      int hinfo = 0;
+      TSVM_CUDA(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+      TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+      if (hinfo == 0) break;
+      if (attempt == 3) return TSVM_ERR_NOT_SPD;
+      factor = factor > 0 ? factor * 100.0 : 11.0 * ((double)n * k + (double)k * (k + 1)) * u;
+    }
+    TSVM_TRY(trinv_lower_fp64(ctx, G, k, k, Linv));
+    rinv_to_fp32<<<(unsigned)ceil_div((int64_t)kp * kp, 256), 256, 0, ctx->stream>>>(Linv, k, kp,
+                                                                                      R32);
+    TSVM_LAUNCHED(ctx);
+    TSVM_TRY(apply_right_fp32(ctx, W, n, kp, R32, W));
+  }
+  return TSVM_OK;
+}
+
+tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_t n, int d,
+                       double gamma, int k, int precision, int sketch, const float *Q_user,
+                       float *Z, int ldz, tsvm_factor_info *info) {
+  if (n < 2 || d < 1 || k < 1 || k > 1000 || ldz < k || !(gamma > 0)) return TSVM_ERR_INVALID_ARGUMENT;
+  if (k > n) return TSVM_ERR_INVALID_ARGUMENT;
+  const int kp = (int)round_up(k, 64);
+  cudaEvent_t *ev = ctx->ev;
+  TSVM_CUDA(cudaEventRecord(ev[0], ctx->stream));
+  float *Xc = nullptr, *Q = nullptr, *W = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_XC, (size_t)n * d + (size_t)n + 64, &Xc));
+  float *norms = Xc + (size_t)n * d;
+  TSVM_TRY(centre_features(ctx, X, n, d, Xc, norms));
+  TSVM_TRY(scratch_t(ctx, SLOT_Q, (size_t)n * kp, &Q));
+  TSVM_TRY(scratch_t(ctx, SLOT_W, (size_t)n * kp, &W));
+  if (sketch == TSVM_SKETCH_GLIBC) {
+    TSVM_TRY(sketch_glibc(ctx, n * (int64_t)k, W));          // stream order = row-major n x k
+    TSVM_TRY(pad_rows(ctx, W, k, n, k, Q, kp));
+  } else if (sketch == TSVM_SKETCH_USER) {
+    if (!Q_user) return TSVM_ERR_INVALID_ARGUMENT;
+    TSVM_TRY(pad_rows(ctx, Q_user, k, n, k, Q, kp));
+  } else {
+    return TSVM_ERR_INVALID_ARGUMENT;
+  }
+  TSVM_CUDA(cudaEventRecord(ev[1], ctx->stream));
+  float km1 = 0.f, km2 = 0.f;
+  TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, Q, kp, W, precision, &km1));
+  TSVM_CUDA(cudaEventRecord(ev[2], ctx->stream));
+  TSVM_TRY(orthonormalise(ctx, W, n, k, kp));
+  TSVM_CUDA(cudaEventRecord(ev[3], ctx->stream));
+  TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, W, kp, Q, precision, &km2));
+  TSVM_CUDA(cudaEventRecord(ev[4], ctx->stream));
+  double *Cm = nullptr, *V = nullptr, *w = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_SMALL, (size_t)k * k + 8, &Cm));
+  TSVM_TRY(scratch_t(ctx, SLOT_SMALL2, (size_t)k * k + (size_t)k, &V));
+  w = V + (size_t)k * k;
+  TSVM_TRY(gram_fp64(ctx, W, kp, Q, kp, n, k, k, false, Cm));
+  TSVM_TRY(small_symmetrize(ctx, Cm, k, k));
+  int sweeps = 0;
+  TSVM_TRY(eig_jacobi_fp64(ctx, Cm, k, k, w, V, &sweeps));
+  float *X32 = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_IPM_M, (size_t)kp * kp, &X32));
+  eigfactor_to_fp32<<<(unsigned)ceil_div((int64_t)kp * kp, 256), 256, 0, ctx->stream>>>(V, w, k,
+                                                                                         kp, X32);
+  TSVM_LAUNCHED(ctx);
+  if (ldz == kp) {
+    TSVM_TRY(apply_right_fp32(ctx, W, n, kp, X32, Z));
+  } else {
+    TSVM_TRY(apply_right_fp32(ctx, W, n, kp, X32, Q));  // Q is free again
+    TSVM_TRY(pad_rows(ctx, Q, kp, n, k, Z, ldz));
+  }
+  TSVM_CUDA(cudaEventRecord(ev[5], ctx->stream));
+  std::vector<double> hw(k);
+  TSVM_CUDA(cudaMemcpyAsync(hw.data(), w, sizeof(double) * k, cudaMemcpyDeviceToHost, ctx->stream));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (info) {
+    info->n = n;
+    info->d = d;
+    info->k = k;
+    info->k_padded = kp;
+    info->precision = precision;
+    int realk = 0;
+    double wmax = -INFINITY, wmin = INFINITY;
+    for (int i = 0; i < k; ++i) {
+      realk += hw[i] > 0.0;
+      wmax = fmax(wmax, hw[i]);
+      wmin = fmin(wmin, hw[i]);
+    }
+    info->realk = realk;
+    info->eig_max = wmax;
+    info->eig_min = wmin;
+    info->ms_sketch = event_ms(ev[0], ev[1]);
+    info->ms_pass1 = event_ms(ev[1], ev[2]);
+    info->ms_ortho = event_ms(ev[2], ev[3]);
+    info->ms_pass2 = event_ms(ev[3], ev[4]);
+    info->ms_project = event_ms(ev[4], ev[5]);
+    info->ms_total = event_ms(ev[0], ev[5]);
+    info->ms_kermatmul_kernel =
+        precision == TSVM_PREC_FP32 ? info->ms_pass1 + info->ms_pass2 : (double)km1 + km2;
+    info->flops_kermatmul = 2.0 * (2.0 * (double)n * n * k + 2.0 * (double)n * n * d);
+  }
+  return TSVM_OK;
+}
+
+}  // namespace tsvm

@@ -1,0 +1,84 @@
+// Internal (non-ABI) entry points shared between the .cu files of the library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "context.h"
+#include "tensorsvm.h"
+
+namespace tsvm {
+
+// ---- sketch.cu -------------------------------------------------------------------------
+// The reference's gaussrand() stream (count floats, contiguous) into Q.
+tsvm_status sketch_glibc(tsvm_context *ctx, int64_t count, float *Q);
+// Raw glibc rand() stream (count values) into out (device).
+tsvm_status glibc_rand_stream(tsvm_context *ctx, int64_t count, uint32_t *out);
+
+// ---- features.cu -----------------------------------------------------------------------
+// Centre X (n x d row-major) by its column means into Xc (n x d), write row norms ||xc||^2.
+tsvm_status centre_features(tsvm_context *ctx, const float *X, int64_t n, int d, float *Xc,
+                            float *norms);
+// Copy src (n x k, leading dim lds) into dst (n x ldd), zero columns k..ldd-1.
+tsvm_status pad_rows(tsvm_context *ctx, const float *src, int64_t lds, int64_t n, int k,
+                     float *dst, int64_t ldd);
+// Z = diag(y) X padded to ldz columns (linear kernel, tensorsvm-train.cu:909-914).
+tsvm_status label_rows(tsvm_context *ctx, const float *X, const float *y, int64_t n, int d,
+                       float *Z, int64_t ldz);
+
+// ---- kermatmul_simt.cu -----------------------------------------------------------------
+// W (n x kp) = (Y K Y) A (n x kp), K_ij = exp(-gamma ||xc_i - xc_j||^2); FP32 SIMT.
+// kp must be a multiple of 64; d <= 64.
+tsvm_status kermatmul_fp32(tsvm_context *ctx, const float *Xc, const float *norms,
+                           const float *y, int64_t n, int d, double gamma, const float *A,
+                           int kp, float *W);
+
+// ---- kermatmul_tc.cu -------------------------------------------------------------------
+bool kermatmul_tc_supported(int d, int kp);
+// Tensor-core (tcgen05) version; precision TSVM_PREC_FP16 or TSVM_PREC_BF16 for P and A.
+tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms, const float *y,
+                         int64_t n, int d, double gamma, const float *A, int kp, float *W,
+                         int precision, float *kernel_ms);
+
+// ---- tallskinny.cu ---------------------------------------------------------------------
+// G (ka x kb, row-major fp64, ldg = kb) = A^T B over n rows; A n x lda fp32, B n x ldb fp32.
+// If symmetric (A == B, ka == kb) only the lower triangle is accumulated and G is mirrored.
+// rowscale (n doubles, may be null) weights row i: G = A^T diag(rowscale) B.
+tsvm_status gram_fp64(tsvm_context *ctx, const float *A, int64_t lda, const float *B,
+                      int64_t ldb, int64_t n, int ka, int kb, bool symmetric, double *G,
+                      const double *rowscale = nullptr);
+// Out (n x kp) = A (n x kp) * R (kp x kp, fp32 row-major). Out may alias A.
+tsvm_status apply_right_fp32(tsvm_context *ctx, const float *A, int64_t n, int kp,
+                             const float *R, float *Out);
+
+// ---- dense.cu (small k x k FP64, single device) ----------------------------------------
+// In-place lower Cholesky of the n x n row-major matrix A (lda); *info_dev receives 0 or the
+// 1-based failing column. Upper triangle is left untouched.
+tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_dev);
+// Solve (L L^T) X = B for nrhs right-hand sides stored as rows of B (nrhs x ldb).
+tsvm_status potrs_fp64(tsvm_context *ctx, const double *L, int n, int lda, double *B, int nrhs,
+                       int ldb);
+// Lower-triangular inverse: Linv = L^-1 (both n x n row-major, lda).
+tsvm_status trinv_lower_fp64(tsvm_context *ctx, const double *L, int n, int lda, double *Linv);
+// Symmetric eigen-decomposition by cyclic Jacobi: A (n x n, lda) is overwritten; w (n) gets
+// the eigenvalues, V (n x n row-major) the eigenvectors as COLUMNS.
+tsvm_status eig_jacobi_fp64(tsvm_context *ctx, double *A, int n, int lda, double *w, double *V,
+                            int *sweeps_out);
+// Elementwise helpers on small matrices (device kernels, defined in dense.cu).
+tsvm_status small_add_diag(tsvm_context *ctx, double *A, int n, int lda, double shift);
+tsvm_status small_symmetrize(tsvm_context *ctx, double *A, int n, int lda);
+
+// ---- ipm.cu ----------------------------------------------------------------------------
+tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y, int64_t n,
+                      int k, double C, const tsvm_ipm_options &opt, double *alpha_out,
+                      double *xi_out, double *ymult_out, tsvm_ipm_stats *stats);
+tsvm_status bias_rbf(tsvm_context *ctx, const float *Z, int ldz, const float *y,
+                     const double *alpha, int64_t n, int k, double C, double *b, double *bstd,
+                     int32_t *nsv, int32_t *nfree);
+
+// ---- factor.cu -------------------------------------------------------------------------
+tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_t n, int d,
+                       double gamma, int k, int precision, int sketch, const float *Q_user,
+                       float *Z, int ldz, tsvm_factor_info *info);
+
+}  // namespace tsvm

@@ -1,0 +1,83 @@
+// Test hooks (include/tensorsvm_testing.h): thin wrappers that run one internal routine and
+// synchronise, so parity tests can check kernels in isolation.
+#include "common.cuh"
+#include "context.h"
+#include "kernels.h"
+#include "tensorsvm_testing.h"
+
+using namespace tsvm;
+
+extern "C" {
+
+tsvm_status tsvm_test_rand_stream(tsvm_context *ctx, int64_t count, uint32_t *out) {
+  if (!ctx || !out || count < 0) return TSVM_ERR_INVALID_ARGUMENT;
+  TSVM_TRY(glibc_rand_stream(ctx, count, out));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSVM_OK;
+}
+
+tsvm_status tsvm_test_sketch(tsvm_context *ctx, int64_t count, float *out) {
+  if (!ctx || !out || count < 0) return TSVM_ERR_INVALID_ARGUMENT;
+  TSVM_TRY(sketch_glibc(ctx, count, out));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSVM_OK;
+}
+
+tsvm_status tsvm_test_kermatmul(tsvm_context *ctx, const float *X, const float *y, int64_t n,
+                                int32_t d, double gamma, const float *A, int32_t kp, float *W,
+                                int32_t precision) {
+  if (!ctx || !X || !y || !A || !W || n < 1 || d < 1 || kp < 1) return TSVM_ERR_INVALID_ARGUMENT;
+  float *Xc = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_XC, (size_t)n * d + (size_t)n + 64, &Xc));
+  float *norms = Xc + (size_t)n * d;
+  TSVM_TRY(centre_features(ctx, X, n, d, Xc, norms));
+  float ms = 0.f;
+  if (precision == TSVM_PREC_FP32) {
+    TSVM_TRY(kermatmul_fp32(ctx, Xc, norms, y, n, d, gamma, A, kp, W));
+  } else {
+    if (!kermatmul_tc_supported(d, kp)) return TSVM_ERR_UNSUPPORTED;
+    TSVM_TRY(kermatmul_tc(ctx, Xc, norms, y, n, d, gamma, A, kp, W, precision, &ms));
+  }
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSVM_OK;
+}
+
+tsvm_status tsvm_test_chol(tsvm_context *ctx, double *A, int32_t n, int32_t *info_host) {
+  if (!ctx || !A || n < 1) return TSVM_ERR_INVALID_ARGUMENT;
+  int *info = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_MISC, 16, &info));
+  TSVM_TRY(chol_fp64(ctx, A, n, n, info));
+  int h = 0;
+  TSVM_CUDA(cudaMemcpyAsync(&h, info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (info_host) *info_host = h;
+  return TSVM_OK;
+}
+
+tsvm_status tsvm_test_potrs(tsvm_context *ctx, const double *L, int32_t n, double *B,
+                            int32_t nrhs, int32_t ldb) {
+  if (!ctx || !L || !B || n < 1 || ldb < n) return TSVM_ERR_INVALID_ARGUMENT;
+  TSVM_TRY(potrs_fp64(ctx, L, n, n, B, nrhs, ldb));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSVM_OK;
+}
+
+tsvm_status tsvm_test_eig(tsvm_context *ctx, double *A, int32_t n, double *w, double *V,
+                          int32_t *sweeps_host) {
+  if (!ctx || !A || !w || !V || n < 1) return TSVM_ERR_INVALID_ARGUMENT;
+  int sweeps = 0;
+  tsvm_status st = eig_jacobi_fp64(ctx, A, n, n, w, V, &sweeps);
+  if (sweeps_host) *sweeps_host = sweeps;
+  return st;
+}
+
+tsvm_status tsvm_test_gram(tsvm_context *ctx, const float *A, int64_t lda, const float *B,
+                           int64_t ldb, int64_t n, int32_t ka, int32_t kb, int32_t symmetric,
+                           const double *s, double *G) {
+  if (!ctx || !A || !B || !G || n < 1) return TSVM_ERR_INVALID_ARGUMENT;
+  TSVM_TRY(gram_fp64(ctx, A, lda, B, ldb, n, ka, kb, symmetric != 0, G, s));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSVM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,115 @@
+"""Kernel-level parity on the GPU (through the C ABI test hooks) against the CPU oracle."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+from tensorsvm_b200 import _lib, synth
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def P(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+@pytest.mark.parametrize("count", [1, 31, 2048, 2049, 3_000_001])
+def test_rand_stream_bit_exact(ctx, count):
+    out = torch.empty(count, dtype=torch.int32, device="cuda")
+    _lib.check(ctx.lib.tsvm_test_rand_stream(ctx.handle, count, P(out)), "rand")
+    got = out.cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, orc.glibc_rand(count))
+
+
+@pytest.mark.parametrize("n,k", [(8192, 32), (1000, 50), (3, 1), (65536, 256)])
+def test_sketch_matches_reference_stream(ctx, n, k):
+    cnt = n * k
+    out = torch.empty(cnt, dtype=torch.float32, device="cuda")
+    _lib.check(ctx.lib.tsvm_test_sketch(ctx.handle, cnt, P(out)), "sketch")
+    got = out.cpu().numpy()
+    ref = orc.polar_sketch(n, k).ravel()
+    # same accept/reject pattern and order; values differ only where log() rounds differently
+    ulp = np.abs(got.view(np.int32).astype(np.int64) - ref.view(np.int32).astype(np.int64))
+    assert ulp.max() <= 2
+    assert np.mean(ulp != 0) < 5e-3
+
+
+@pytest.mark.parametrize("k", [1, 32, 50, 256, 400])
+def test_cholesky_and_solve(ctx, k):
+    rng = np.random.default_rng(k)
+    A = rng.standard_normal((k, k + 5))
+    M = A @ A.T + np.eye(k)
+    L = dev(M.copy())
+    info = ctypes.c_int32(-1)
+    _lib.check(ctx.lib.tsvm_test_chol(ctx.handle, P(L), k, ctypes.byref(info)), "chol")
+    assert info.value == 0
+    Lh = np.tril(L.cpu().numpy())
+    assert np.allclose(Lh, np.linalg.cholesky(M), rtol=1e-10, atol=1e-10)
+    B = rng.standard_normal((2, k))
+    Bd = dev(B.copy())
+    _lib.check(ctx.lib.tsvm_test_potrs(ctx.handle, P(L), k, P(Bd), 2, k), "potrs")
+    assert np.allclose(Bd.cpu().numpy(), np.linalg.solve(M, B.T).T, rtol=1e-8, atol=1e-10)
+
+
+def test_cholesky_reports_indefinite(ctx):
+    M = np.eye(40)
+    M[17, 17] = -1.0
+    L = dev(M)
+    info = ctypes.c_int32(0)
+    _lib.check(ctx.lib.tsvm_test_chol(ctx.handle, P(L), 40, ctypes.byref(info)), "chol")
+    assert info.value == 18
+
+
+@pytest.mark.parametrize("k", [2, 7, 32, 128, 256])
+def test_jacobi_eigensolver(ctx, k):
+    rng = np.random.default_rng(100 + k)
+    A = rng.standard_normal((k, k))
+    S = (A + A.T) / 2
+    S[0, :] *= 1e3  # spread of scales, and one negative direction kept in the spectrum
+    S = (S + S.T) / 2
+    w = torch.empty(k, dtype=torch.float64, device="cuda")
+    V = torch.empty((k, k), dtype=torch.float64, device="cuda")
+    sweeps = ctypes.c_int32(0)
+    _lib.check(ctx.lib.tsvm_test_eig(ctx.handle, P(dev(S.copy())), k, P(w), P(V),
+                                     ctypes.byref(sweeps)), "eig")
+    wh, Vh = w.cpu().numpy(), V.cpu().numpy()
+    assert 0 < sweeps.value < 40
+    assert np.allclose(np.sort(wh), np.linalg.eigvalsh(S), rtol=1e-10, atol=1e-9 * np.abs(S).max())
+    assert np.linalg.norm(Vh @ np.diag(wh) @ Vh.T - S) / np.linalg.norm(S) < 1e-12
+    assert np.linalg.norm(Vh.T @ Vh - np.eye(k)) < 1e-11
+
+
+@pytest.mark.parametrize("sym", [True, False])
+def test_gram_fp64_exact_products(ctx, sym):
+    rng = np.random.default_rng(7)
+    n, ka, kb = 10007, 70, 70 if sym else 33
+    A = rng.standard_normal((n, 72)).astype(np.float32)
+    B = A if sym else rng.standard_normal((n, 36)).astype(np.float32)
+    s = rng.random(n) + 0.5
+    G = torch.empty((ka, kb), dtype=torch.float64, device="cuda")
+    Ad, Bd, sd = dev(A), dev(B), dev(s)
+    _lib.check(ctx.lib.tsvm_test_gram(ctx.handle, P(Ad), 72, P(Bd), B.shape[1], n, ka, kb,
+                                      int(sym), P(sd), P(G)), "gram")
+    ref = (A[:, :ka].astype(np.float64) * s[:, None]).T @ B[:, :kb].astype(np.float64)
+    assert np.allclose(G.cpu().numpy(), ref, rtol=1e-12, atol=1e-9)
+
+
+@pytest.mark.parametrize("n,d,kp", [(3001, 18, 64), (1024, 54, 128), (517, 28, 256), (700, 5, 448)])
+def test_kermatmul_fp32(ctx, n, d, kp):
+    rng = np.random.default_rng(n)
+    X = rng.standard_normal((n, d)).astype(np.float32)
+    y = np.where(rng.random(n) < 0.5, 1.0, -1.0).astype(np.float32)
+    A = rng.standard_normal((n, kp)).astype(np.float32)
+    W = torch.empty((n, kp), dtype=torch.float32, device="cuda")
+    g = 0.05
+    _lib.check(ctx.lib.tsvm_test_kermatmul(ctx.handle, P(dev(X)), P(dev(y)), n, d, g, P(dev(A)), kp,
+                                           P(W), _lib.PREC_FP32), "kermatmul")
+    ref = orc.kermatmul(X, y, g, A)
+    err = np.linalg.norm(W.cpu().numpy() - ref) / np.linalg.norm(ref)
+    assert err < 2e-6, err

@@ -1,0 +1,164 @@
+"""Training-path parity on the GPU: factor vs the oracle's LRA on the same sketch, the IPM vs the
+oracle's mpc on the same Z, bias, and end to end vs the reference's own model files."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import jaccard, ref_fixture, ref_log
+from oracle import oracle as orc
+from tensorsvm_b200 import _lib, api, synth
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.fixture(scope="module")
+def c1():
+    X, y, g, C, k = synth.make("c1")
+    return X, y, g, C, k
+
+
+@pytest.fixture(scope="module")
+def c1_factor(ctx, c1):
+    X, y, g, C, k = c1
+    Z, info = api.factor(ctx, dev(X), dev(y), g, k, "fp32")
+    return Z, info
+
+
+def test_factor_fp32_matches_oracle_lra(c1, c1_factor):
+    X, y, g, C, k = c1
+    Z, info = c1_factor
+    Zh = Z.cpu().numpy()[:, :k].astype(np.float64)
+    assert np.all(Z.cpu().numpy()[:, k:] == 0)
+    f = orc.lra(X, y, g, k)
+    G, Gr = Zh @ Zh.T, f.U @ f.U.T
+    err = np.linalg.norm(G - Gr) / np.linalg.norm(Gr)
+    assert err < 1e-4, err
+    assert info["realk"] == f.realk == k
+    assert abs(info["eig_max"] - f.eigvals[-1]) / f.eigvals[-1] < 1e-5
+
+
+def test_factor_error_vs_exact_kernel(c1, c1_factor):
+    X, y, g, C, k = c1
+    Z, _ = c1_factor
+    Zh = Z.cpu().numpy()[:2048, :k].astype(np.float64)
+    K = orc.rbf_block(X[:2048], X[:2048], y[:2048], y[:2048], g)
+    f = orc.lra(X, y, g, k)
+    e_gpu = np.linalg.norm(K - Zh @ Zh.T) / np.linalg.norm(K)
+    e_orc = np.linalg.norm(K - f.U[:2048] @ f.U[:2048].T) / np.linalg.norm(K)
+    assert abs(e_gpu - e_orc) < 1e-4 * max(1.0, e_orc)
+
+
+def test_ipm_matches_oracle_mpc_on_same_z(ctx, c1, c1_factor):
+    X, y, g, C, k = c1
+    Z, _ = c1_factor
+    alpha, xi, ym, st = api.ipm(ctx, Z, dev(y), k, C, want_xi=True)
+    Zh = Z.cpu().numpy()[:, :k].astype(np.float64)
+    r = orc.mpc(Zh, y, C, kernel="rbf")
+    a = alpha.cpu().numpy()
+    assert st["iters"] == r.iters
+    assert abs(st["pobj"] - r.log[-1][5]) / abs(r.log[-1][5]) < 1e-9
+    assert abs(st["dobj"] - r.log[-1][6]) / abs(r.log[-1][6]) < 1e-9
+    assert np.max(np.abs(a - r.x)) < 1e-4
+    b_gpu, _, nsv, nfree = api.bias(ctx, Z, dev(y), alpha, k, C)
+    b_orc, _ = orc.bias_rbf(Zh, y, r.x, C)
+    assert abs(b_gpu - b_orc) < 1e-6
+    sv, free = orc.sv_sets(a, C)
+    assert (nsv, nfree) == (len(sv), len(free))
+    Xt = synth.make("c1_test")[0]
+    dv_g = orc.decision_values_dense(a, y, X, g, b_gpu, Xt)
+    dv_o = orc.decision_values_dense(r.x, y, X, g, b_orc, Xt)
+    assert np.max(np.abs(dv_g - dv_o)) < 1e-4
+
+
+def test_train_end_to_end_matches_reference(ctx, c1):
+    X, y, g, C, k = c1
+    m = api.train(ctx, X, y, _lib.KERNEL_RBF, g, C, k, "fp32")
+    last = ref_log("ref_c1_rbf")[-1]
+    st = m.ipm_stats
+    assert abs(st["pobj"] - last[5]) / abs(last[5]) < 1e-5
+    assert abs(st["dobj"] - last[6]) / abs(last[6]) < 1e-5
+    idx, coef, rho, _ = ref_fixture("ref_c1_rbf")
+    sv, _ = orc.sv_sets(m.alpha, C)
+    assert jaccard(sv, idx) > 0.99
+    ref_alpha = np.zeros(len(X))
+    ref_alpha[idx] = coef * y[idx]
+    Xt = synth.make("c1_test")[0]
+    dv = orc.decision_values_dense(m.alpha, y, X, g, m.b, Xt)
+    dv_r = orc.decision_values_dense(ref_alpha, y, X, g, -rho, Xt)
+    assert np.mean(np.sign(dv) == np.sign(dv_r)) >= 0.999
+
+
+def test_linear_end_to_end_matches_reference(ctx, c1, tmp_path):
+    X, y, g, C, k = c1
+    m = api.train(ctx, X, y, _lib.KERNEL_LINEAR, 0.0, 1.0, 0, "fp32")
+    r, w, b = orc.train_linear(X, y, 1.0)
+    assert m.ipm_stats["iters"] == r.iters
+    assert np.max(np.abs(m.alpha - r.x)) < 1e-6
+    assert abs(m.b - b) < 1e-7
+    path = tmp_path / "lin.model"
+    api.write_model(str(path), m, X, y, 1, -1)
+    got = path.read_text().split("\n")
+    ref = open(os.path.join(os.path.dirname(__file__), "golden", "ref_c1_lin.model")).read().split("\n")
+    assert got[:6] == ref[:6]
+    assert np.allclose([float(v) for v in got[6:25]], [float(v) for v in ref[6:25]], atol=1e-8)
+
+
+@pytest.mark.parametrize("n,k", [(1000, 50), (777, 33), (64, 8), (2500, 130)])
+def test_ragged_shapes_match_oracle(ctx, n, k):
+    X, y = synth.two_gaussians(n, 7, seed=n)
+    g, C = 0.1, 4.0
+    Z, info = api.factor(ctx, dev(X), dev(y), g, k, "fp32")
+    f = orc.lra(X, y, g, k)
+    Zh = Z.cpu().numpy()[:, :k].astype(np.float64)
+    G, Gr = Zh @ Zh.T, f.U @ f.U.T
+    assert np.linalg.norm(G - Gr) / np.linalg.norm(Gr) < 1e-4
+    alpha, _, _, st = api.ipm(ctx, Z, dev(y), k, C)
+    r = orc.mpc(Zh, y, C, kernel="rbf")
+    assert abs(st["pobj"] - r.log[-1][5]) / max(1.0, abs(r.log[-1][5])) < 1e-8
+    assert np.max(np.abs(alpha.cpu().numpy() - r.x)) < 1e-4 * C
+
+
+def test_rel_gap_stop_and_stats(ctx, c1, c1_factor):
+    X, y, g, C, k = c1
+    Z, _ = c1_factor
+    alpha, _, _, st = api.ipm(ctx, Z, dev(y), k, C, rel_gap_tol=1e-6)
+    assert st["status_code"] == _lib.OK
+    assert st["rel_gap"] <= 1e-6 and st["t_rel_gap_1e6_ms"] > 0
+
+
+def test_ipm_nan_input_reports_not_spd(ctx):
+    X, y = synth.two_gaussians(256, 3, seed=2)
+    Z = torch.zeros((256, 64), dtype=torch.float32, device="cuda")
+    Z[:, :3] = dev(X)
+    Z[5, 1] = float("nan")
+    alpha, _, _, st = api.ipm(ctx, Z, dev(y), 3, 1.0)
+    assert st["status_code"] == _lib.ERR_NOT_SPD
+    assert st["iters"] == 1
+
+
+def test_cli_end_to_end(tmp_path):
+    X, y = synth.two_gaussians(3000, 18, seed=11, noise=0.05)
+    y = -y  # first label -1 becomes POS, as in the reference's remap
+    train = tmp_path / "t.train"
+    synth.write_libsvm(str(train), X, y)
+    model = tmp_path / "t.model"
+    p = subprocess.run([_lib.CLI_PATH, "-k", "32", "-c", "8", "-g", "0.05", "-t", "2", str(train),
+                        str(model)], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stdout + p.stderr
+    m = orc.parse_model(model.read_text())
+    assert m["header"]["label"] == [str(int(y[0])), str(int(-y[0]))]
+    assert m["header"]["kernel_type"] == ["rbf"]
+    yy, pos, neg = orc.remap_labels(y)
+    f, r, b = orc.train_rbf(X, yy, 0.05, 8.0, 32)
+    sv, _ = orc.sv_sets(r.x, 8.0)
+    assert abs(int(m["header"]["total_sv"][0]) - len(sv)) <= 0.01 * len(sv)
+    dv = orc.decision_values(m, X[:500], 18)
+    dv_o = orc.decision_values_dense(r.x, yy, X, 0.05, b, X[:500])
+    assert np.mean(np.sign(dv) == np.sign(dv_o)) >= 0.995
