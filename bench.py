@@ -172,8 +172,7 @@ def run_ours(args, world, rank, local):
             t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             t0.record(stream)
             m = api.train(ctx, Xh.numpy(), yh.numpy(), _lib.KERNEL_RBF, GAMMA, CPEN, K, prec,
-                          rel_gap_tol=1e-6,
-                          precision=_lib.PREC_FP32 if prec == "fp32" else _lib.PREC_BF16)
+                          rel_gap_tol=1e-6)
             t1.record(stream)
             torch.cuda.synchronize()
             e2e_ms.append(t0.elapsed_time(t1))

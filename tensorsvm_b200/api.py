@@ -92,6 +92,7 @@ def train(ctx, X: np.ndarray, y: np.ndarray, kernel: int = _lib.KERNEL_RBF, gamm
     alpha = np.empty(n, dtype=np.float64)
     b = ctypes.c_double()
     finfo, istats = _lib.FactorInfo(), _lib.IpmStats()
+    opts.setdefault("precision", _lib.PREC_FP32 if precision == "fp32" else _lib.PREC_BF16)
     o = _lib.default_options(kernel=kernel, **opts)
     st = ctx.lib.tsvm_train(ctx.handle, X.ctypes.data, y.ctypes.data, n, d, kernel, float(gamma),
                             float(C), k, PRECISIONS[precision], ctypes.byref(o),

@@ -30,6 +30,8 @@ enum Slot : int {
   SLOT_IPM_SCAL,      // IPM device scalars
   SLOT_IPM_M,         // IPM capacitance matrix + factor
   SLOT_IPM_ZH,        // IPM low-precision copy of Z (bf16)
+  SLOT_IPM_PART,      // IPM / bias streaming partial sums (kept apart from SLOT_PART, which the
+                      // Z^T D^-1 Z accumulation may regrow inside the iteration)
   SLOT_MISC,
   SLOT_DEV_IN,        // tsvm_train: device copies of host inputs
   SLOT_DEV_Z,         // tsvm_train: factor Z

@@ -675,7 +675,7 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
   TSVM_TRY(scratch_t(ctx, SLOT_IPM_SCAL, (size_t)kNScal + 8 * (size_t)kz + 64, &sbuf));
   TSVM_TRY(scratch_t(ctx, SLOT_IPM_M, (size_t)k * k, &M));
   double *part = nullptr;
-  TSVM_TRY(scratch_t(ctx, SLOT_PART, (size_t)run.nblk * (2 * kz + 16), &part));
+  TSVM_TRY(scratch_t(ctx, SLOT_IPM_PART, (size_t)run.nblk * (2 * kz + 16), &part));
   run.part_vec = part;
   run.part_s = part + (size_t)run.nblk * 2 * kz;
   run.scal = sbuf;
@@ -941,7 +941,7 @@ tsvm_status bias_rbf(tsvm_context *ctx, const float *Z, int ldz, const float *y,
   const int kz = run.geo.kz;
   double *sbuf = nullptr, *part = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_MISC, (size_t)kNScal + kz + 256, &sbuf));
-  TSVM_TRY(scratch_t(ctx, SLOT_PART, (size_t)run.nblk * (2 * kz + 16), &part));
+  TSVM_TRY(scratch_t(ctx, SLOT_IPM_PART, (size_t)run.nblk * (2 * kz + 16), &part));
   run.part_vec = part;
   run.part_s = part + (size_t)run.nblk * 2 * kz;
   run.scal = sbuf;

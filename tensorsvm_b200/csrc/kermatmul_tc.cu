@@ -1,12 +1,586 @@
-// Tensor-core (tcgen05) fused kernel-block product.  Placeholder until the sm_100a kernel lands.
+// Tensor-core fused kernel-block product for sm_100a: W = (Y K Y) A with tcgen05 + TMEM + TMA.
+//
+// Replaces rbf_kermatmul's XIJ SGEMM + rbf_kergen + K*A SGEMM (tensorsvm-train.cu:2476-2612)
+// with one kernel per 128-row block I of W that streams every 64-row block J of X and A:
+//
+//   S_IJ  = XA_I XB_J^T              tcgen05.mma kind::f16, K = 64, accumulator in TMEM
+//   P_IJ  = exp2(S_IJ)                (exp warpgroups: tcgen05.ld -> ex2 -> f16 -> SMEM)
+//   W_I  += P_IJ AT_J^T              tcgen05.mma kind::f16 (FP16 or BF16), accumulator in TMEM
+//
+// The Gram operands are built so that the MMA directly produces the scaled, negated squared
+// distance: with x~ = xc sqrt(2 gamma log2 e) split as hi + lo (FP16 each) and
+// h + m + l = ||x~||^2 / 2 (FP16 each),
+//   XA_i = [hi_i, lo_i, hi_i, 1, 1, 1, -h_i, -m_i, -l_i, 0...]
+//   XB_j = [hi_j, hi_j, lo_j, -h_j, -m_j, -l_j, 1, 1, 1, 0...]
+//   S_ij = hi.hi + lo.hi + hi.lo - ||x~_i||^2/2 - ||x~_j||^2/2 = -gamma log2(e) ||x_i - x_j||^2
+// to ~2^-22 relative (the FP32 accumulation of exact FP16 products), so the epilogue is a
+// bare ex2.  Labels are folded into AT (AT[c][j] = s y_j A[j][c], s a power of two that keeps
+// FP16 away from its subnormal range) and into the final scaling of W's rows by y_i / s.
+//
+// Warp roles (320 threads): warp 0 TMA producer, warp 1 TMEM allocator + single-thread MMA
+// issuer, warps 2-5 and 6-9 two exp warpgroups that take alternate J blocks (S is double
+// buffered in TMEM: 2 x 64 columns; W uses up to 256 columns).  All waits are bounded: after
+// ~1 s without progress a block records an error and leaves; the host reports
+// TSVM_ERR_TIMEOUT.  No cluster multicast anywhere.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <vector>
+
 #include "common.cuh"
 #include "context.h"
 #include "kernels.h"
 
 namespace tsvm {
-bool kermatmul_tc_supported(int, int) { return false; }
-tsvm_status kermatmul_tc(tsvm_context *, const float *, const float *, const float *, int64_t, int,
-                         double, const float *, int, float *, int, float *) {
-  return TSVM_ERR_UNSUPPORTED;
+namespace {
+
+constexpr int kBM = 128;          // rows of W per CTA (TMEM lanes)
+constexpr int kBJ = 64;           // J block (K of the second MMA, N of the Gram)
+constexpr int kKG = 64;           // Gram K (split features + norms, zero padded)
+constexpr int kStages = 3;        // TMA ring depth
+constexpr int kThreadsTC = 320;
+constexpr int kMaxSlab = 256;     // columns of W per launch (MMA N <= 256)
+
+constexpr uint32_t kXaBytes = kBM * kKG * 2;       // 16 KB
+constexpr uint32_t kXbBytes = kBJ * kKG * 2;       //  8 KB
+constexpr uint32_t kAtBytesMax = kMaxSlab * kBJ * 2;  // 32 KB (kpw rows x 128 B)
+constexpr uint32_t kPBytes = kBM * kBJ * 2;        // 16 KB
+
+struct SmemLayout {
+  // all operand tiles are 1024-byte aligned (128B swizzle atoms)
+  uint32_t xa, xb[kStages], at[kStages], p[2], bars, total;
+};
+
+__host__ __device__ constexpr uint32_t align1k(uint32_t v) { return (v + 1023u) & ~1023u; }
+
+__host__ __device__ inline SmemLayout smem_layout(int kpw) {
+  SmemLayout L{};
+  uint32_t off = 0;
+  L.xa = off;
+  off += kXaBytes;
+  for (int s = 0; s < kStages; ++s) {
+    L.xb[s] = off;
+    off += kXbBytes;
+    L.at[s] = off;
+    off = align1k(off + (uint32_t)kpw * kBJ * 2);
+  }
+  for (int b = 0; b < 2; ++b) {
+    L.p[b] = off;
+    off += kPBytes;
+  }
+  L.bars = off;
+  off += 256;
+  L.total = off;
+  return L;
 }
+
+// ---------------------------------------------------------------------------------------
+// PTX helpers (sm_100a)
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t su32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ uint64_t gtimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: returns false (and raises the block's abort flag) after ~1 s without progress,
+// or as soon as another thread of the block has aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t deadline = gtimer() + 1000000000ull;
+  for (uint32_t spin = 1;; ++spin) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((spin & 63) == 0) {
+      if (*abort) return false;
+      if (gtimer() > deadline) {
+        *abort = 1;
+        return false;
+      }
+    }
+  }
+}
+__device__ __forceinline__ void tma_load_2d(const CUtensorMap *map, uint32_t bar, uint32_t dst,
+                                            int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+      "l"(map), "r"(bar), "r"(x), "r"(y)
+      : "memory");
+}
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// SMEM matrix descriptor, K-major operand with the 128-byte swizzle: rows of 128 B, 8-row
+// (1024 B) swizzle atoms stacked at SBO = 1024 B; LBO unused for this mode (1); version 1.
+__device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr & 0x3FFFFu) >> 4);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(1024u >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+// Instruction descriptor, kind::f16, D = F32, A/B K-major, fmt 0 = F16, 1 = BF16.
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N, uint32_t fmt) {
+  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void umma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc,
+                                     uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ float ex2(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+template <bool BF16>
+__device__ __forceinline__ uint32_t pack2(float lo, float hi) {
+  if constexpr (BF16) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t *>(&v);
+  } else {
+    __half2 v = __floats2half2_rn(lo, hi);
+    return *reinterpret_cast<uint32_t *>(&v);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// The fused kernel.  grid.x = row blocks of 128; slab = columns [c0, c0 + kpw) of W.
+// ---------------------------------------------------------------------------------------
+template <bool BF16>
+__global__ void __launch_bounds__(kThreadsTC, 1)
+kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
+                    const __grid_constant__ CUtensorMap map_xb,
+                    const __grid_constant__ CUtensorMap map_at, const float *__restrict__ y,
+                    const float *__restrict__ inv_scale, int64_t n, int ntiles, int c0, int kpw,
+                    float *__restrict__ W, int64_t ldw, int *__restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  // 1024-align the dynamic shared window
+  const uint32_t raw = su32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t *sbase = smem_raw + (base - raw);
+  const SmemLayout L = smem_layout(kpw);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sbase + L.bars);
+  // barrier slots
+  const uint32_t b_full = su32(bars + 0);            // [kStages]
+  const uint32_t b_empty = su32(bars + kStages);     // [kStages]
+  const uint32_t b_sfull = su32(bars + 2 * kStages); // [2]
+  const uint32_t b_sempty = b_sfull + 16;            // [2]
+  const uint32_t b_pfull = b_sfull + 32;             // [2]
+  const uint32_t b_pempty = b_sfull + 48;            // [2]
+  const uint32_t b_wfull = b_sfull + 64;
+  const uint32_t b_xafull = b_sfull + 72;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kStages + 10);
+  volatile int *abort = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t i0 = (int64_t)blockIdx.x * kBM;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(b_full + 8 * s, 1);
+      mbar_init(b_empty + 8 * s, 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(b_sfull + 8 * b, 1);
+      mbar_init(b_sempty + 8 * b, 128);
+      mbar_init(b_pfull + 8 * b, 128);
+      mbar_init(b_pempty + 8 * b, 1);
+    }
+    mbar_init(b_wfull, 1);
+    mbar_init(b_xafull, 1);
+    *abort = 0;
+    fence_barrier_init();
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     su32(tmem_slot)),
+                 "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t t_s = tmem;          // S buffers: columns [0, 128)
+  const uint32_t t_w = tmem + 128;    // W accumulator: columns [128, 128 + kpw)
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      asm volatile("prefetch.tensormap [%0];" ::"l"(&map_xa) : "memory");
+      asm volatile("prefetch.tensormap [%0];" ::"l"(&map_xb) : "memory");
+      asm volatile("prefetch.tensormap [%0];" ::"l"(&map_at) : "memory");
+      mbar_expect_tx(b_xafull, kXaBytes);
+      tma_load_2d(&map_xa, b_xafull, base + L.xa, 0, (int)i0);
+      const uint32_t stage_bytes = kXbBytes + (uint32_t)kpw * kBJ * 2;
+      for (int t = 0; t < ntiles; ++t) {
+        const int st = t % kStages, use = t / kStages;
+        if (!mbar_wait(b_empty + 8 * st, (use & 1) ^ 1, abort)) break;
+        mbar_expect_tx(b_full + 8 * st, stage_bytes);
+        tma_load_2d(&map_xb, b_full + 8 * st, base + L.xb[st], 0, t * kBJ);
+        tma_load_2d(&map_at, b_full + 8 * st, base + L.at[st], t * kBJ, c0);
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      constexpr uint32_t idg = idesc_f16(kBM, kBJ, 0);           // Gram: FP16 always
+      const uint32_t id2 = idesc_f16(kBM, kpw, BF16 ? 1u : 0u);  // P AT^T
+      bool ok = mbar_wait(b_xafull, 0, abort);
+      for (int t = 0; ok && t <= ntiles; ++t) {
+        if (t < ntiles) {
+          const int st = t % kStages, use = t / kStages, b = t & 1, ub = t >> 1;
+          if (!mbar_wait(b_full + 8 * st, use & 1, abort)) break;
+          if (!mbar_wait(b_sempty + 8 * b, (ub & 1) ^ 1, abort)) break;
+          tc_fence_after();
+#pragma unroll
+          for (int kk = 0; kk < kKG / 16; ++kk)
+            umma(t_s + b * kBJ, desc_sw128(base + L.xa + kk * 32),
+                 desc_sw128(base + L.xb[st] + kk * 32), idg, kk > 0 ? 1u : 0u);
+          umma_commit(b_sfull + 8 * b);
+        }
+        if (t > 0) {
+          const int tp = t - 1, bp = tp & 1, ubp = tp >> 1, stp = tp % kStages;
+          if (!mbar_wait(b_pfull + 8 * bp, ubp & 1, abort)) break;
+          tc_fence_after();
+#pragma unroll
+          for (int kk = 0; kk < kBJ / 16; ++kk)
+            umma(t_w, desc_sw128(base + L.p[bp] + kk * 32), desc_sw128(base + L.at[stp] + kk * 32),
+                 id2, (tp > 0 || kk > 0) ? 1u : 0u);
+          umma_commit(b_pempty + 8 * bp);
+          umma_commit(b_empty + 8 * stp);
+        }
+      }
+      umma_commit(b_wfull);
+    }
+  } else {
+    // ---------------- exp warpgroups ----------------
+    const int g = (warp - 2) >> 2;        // warpgroup 0: warps 2-5, 1: warps 6-9
+    const int q = warp & 3;               // TMEM lane quarter this warp may access
+    const int row = q * 32 + lane;        // row of the 128-row block (TMEM lane)
+    const uint32_t lane_off = (uint32_t)(q * 32) << 16;
+    const uint32_t prow = (uint32_t)row * 128u;
+    const uint32_t sw = (uint32_t)(row & 7);
+    for (int t = g; t < ntiles; t += 2) {
+      const int b = g, ub = t >> 1;
+      if (!mbar_wait(b_sfull + 8 * b, ub & 1, abort)) break;
+      tc_fence_after();
+      uint32_t s0[32], s1[32];
+      tmem_ld32(t_s + b * kBJ + lane_off, s0);
+      tmem_ld32(t_s + b * kBJ + 32 + lane_off, s1);
+      tmem_wait_ld();
+      tc_fence_before();
+      mbar_arrive(b_sempty + 8 * b);
+      uint32_t pk[32];
+#pragma unroll
+      for (int c = 0; c < 16; ++c)
+        pk[c] = pack2<BF16>(ex2(__uint_as_float(s0[2 * c])), ex2(__uint_as_float(s0[2 * c + 1])));
+#pragma unroll
+      for (int c = 0; c < 16; ++c)
+        pk[16 + c] =
+            pack2<BF16>(ex2(__uint_as_float(s1[2 * c])), ex2(__uint_as_float(s1[2 * c + 1])));
+      if (!mbar_wait(b_pempty + 8 * b, (ub & 1) ^ 1, abort)) break;
+      const uint32_t pbase = base + L.p[b] + prow;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const uint32_t addr = pbase + (((uint32_t)u ^ sw) << 4);
+        asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(pk[4 * u]),
+                     "r"(pk[4 * u + 1]), "r"(pk[4 * u + 2]), "r"(pk[4 * u + 3])
+                     : "memory");
+      }
+      fence_async_smem();
+      mbar_arrive(b_pfull + 8 * b);
+    }
+    // ---------------- epilogue: W rows of this block, half of the slab per warpgroup -----
+    if (mbar_wait(b_wfull, 0, abort)) {
+      tc_fence_after();
+      const int64_t gi = i0 + row;
+      const float sc = gi < n ? y[gi] * inv_scale[0] : 0.f;
+      const int half = kpw / 2;
+      for (int cc = g * half; cc < (g + 1) * half; cc += 32) {
+        uint32_t v[32];
+        tmem_ld32(t_w + cc + lane_off, v);
+        tmem_wait_ld();
+        if (gi < n) {
+          float4 *dst = reinterpret_cast<float4 *>(W + gi * ldw + c0 + cc);
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            dst[j] = make_float4(__uint_as_float(v[4 * j]) * sc, __uint_as_float(v[4 * j + 1]) * sc,
+                                 __uint_as_float(v[4 * j + 2]) * sc,
+                                 __uint_as_float(v[4 * j + 3]) * sc);
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (threadIdx.x == 0 && *abort) atomicExch(err, 1);
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Operand preparation
+// ---------------------------------------------------------------------------------------
+// XA/XB rows (n_pad x 64 FP16) from centred features: see the file comment for the layout.
+__global__ void prep_gram_operands(const float *__restrict__ Xc, int64_t n, int64_t n_pad, int d,
+                                   double scale, __half *__restrict__ XA, __half *__restrict__ XB) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_pad) return;
+  __half *a = XA + i * kKG, *b = XB + i * kKG;
+  for (int c = 0; c < kKG; ++c) {
+    a[c] = __float2half_rn(0.f);
+    b[c] = __float2half_rn(0.f);
+  }
+  if (i >= n) return;
+  double nn = 0.0;
+  for (int c = 0; c < d; ++c) {
+    const double xt = (double)Xc[i * d + c] * scale;
+    nn += xt * xt;
+    const __half hi = __float2half_rn((float)xt);
+    const __half lo = __float2half_rn((float)(xt - (double)__half2float(hi)));
+    a[c] = hi;
+    a[d + c] = lo;
+    a[2 * d + c] = hi;
+    b[c] = hi;
+    b[d + c] = hi;
+    b[2 * d + c] = lo;
+  }
+  const double v = 0.5 * nn;
+  const __half h = __float2half_rn((float)v);
+  const double r1 = v - (double)__half2float(h);
+  const __half m = __float2half_rn((float)r1);
+  const __half l = __float2half_rn((float)(r1 - (double)__half2float(m)));
+  const __half one = __float2half_rn(1.f);
+  const int o = 3 * d;
+  a[o + 0] = one; a[o + 1] = one; a[o + 2] = one;
+  a[o + 3] = __hneg(h); a[o + 4] = __hneg(m); a[o + 5] = __hneg(l);
+  b[o + 0] = __hneg(h); b[o + 1] = __hneg(m); b[o + 2] = __hneg(l);
+  b[o + 3] = one; b[o + 4] = one; b[o + 5] = one;
+}
+
+__global__ void sumsq_partial(const float *__restrict__ A, int64_t count, double *__restrict__ part) {
+  __shared__ double sh[8];
+  double s = 0.0;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < count;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const double v = A[e];
+    s += v * v;
+  }
+  double v1[1] = {s};
+  block_sum<1>(v1, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = v1[0];
+}
+
+// s = 2^round(-log2(rms)): puts the operand's RMS near 1 in FP16/BF16.
+__global__ void choose_scale(const double *__restrict__ part, int nb, int64_t count,
+                             float *__restrict__ scale) {
+  if (threadIdx.x != 0) return;
+  double s = 0.0;
+  for (int b = 0; b < nb; ++b) s += part[b];
+  const double rms = sqrt(s / (double)(count > 0 ? count : 1));
+  int e = 0;
+  if (rms > 0.0 && isfinite(rms)) e = (int)lrint(-log2(rms));
+  if (e > 60) e = 60;
+  if (e < -60) e = -60;
+  scale[0] = ldexpf(1.f, e);
+  scale[1] = ldexpf(1.f, -e);  // inverse, applied in the epilogue
+}
+
+// AT[c][j] = s * y_j * A[j][c] for c < kp, j < n; zeros for j in [n, n_pad).  32x32 tiles.
+template <typename T>
+__global__ void prep_at(const float *__restrict__ A, const float *__restrict__ y, int64_t n,
+                        int64_t n_pad, int kp, const float *__restrict__ scale, T *__restrict__ AT) {
+  __shared__ float tile[32][33];
+  const int64_t j0 = (int64_t)blockIdx.x * 32;
+  const int c0 = blockIdx.y * 32;
+  const float s = scale[0];
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int64_t j = j0 + r;
+    const int c = c0 + threadIdx.x;
+    float v = 0.f;
+    if (j < n && c < kp) v = A[j * kp + c] * y[j] * s;
+    tile[r][threadIdx.x] = v;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int c = c0 + r;
+    const int64_t j = j0 + threadIdx.x;
+    if (c < kp && j < n_pad) {
+      if constexpr (sizeof(T) == 2 && std::is_same<T, __half>::value)
+        AT[(int64_t)c * n_pad + j] = __float2half_rn(tile[threadIdx.x][r]);
+      else
+        AT[(int64_t)c * n_pad + j] = __float2bfloat16_rn(tile[threadIdx.x][r]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// 2D row-major map over a [rows][cols] 2-byte matrix, box [box_rows][box_cols], 128B swizzle.
+bool make_map(CUtensorMap *map, const void *ptr, CUtensorMapDataType dt, uint64_t cols,
+              uint64_t rows, uint32_t box_cols, uint32_t box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {cols, rows};
+  const cuuint64_t strides[1] = {cols * 2};
+  const cuuint32_t box[2] = {box_cols, box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  return fn(map, dt, 2, const_cast<void *>(ptr), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+bool kermatmul_tc_supported(int d, int kp) {
+  return d >= 1 && 3 * d + 6 <= kKG && kp >= 64 && kp % 64 == 0 && encode_fn() != nullptr;
+}
+
+tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms, const float *y,
+                         int64_t n, int d, double gamma, const float *A, int kp, float *W,
+                         int precision, float *kernel_ms) {
+  (void)norms;
+  if (!kermatmul_tc_supported(d, kp)) return TSVM_ERR_UNSUPPORTED;
+  const bool bf16 = precision == TSVM_PREC_BF16;
+  const int64_t n_pad = round_up(n, kBM);
+  // operands
+  __half *XA = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_OPX, (size_t)2 * n_pad * kKG, &XA));
+  __half *XB = XA + (size_t)n_pad * kKG;
+  uint16_t *AT = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_OPA, (size_t)kp * n_pad, &AT));
+  double *part = nullptr;
+  const int nb = ctx->num_sms * 2;
+  TSVM_TRY(scratch_t(ctx, SLOT_MISC, (size_t)nb + 16, &part));
+  float *scale = reinterpret_cast<float *>(part + nb);
+  int *err = reinterpret_cast<int *>(scale + 4);
+  const double xscale = sqrt(2.0 * gamma * 1.4426950408889634);
+  prep_gram_operands<<<(unsigned)ceil_div(n_pad, 256), 256, 0, ctx->stream>>>(Xc, n, n_pad, d,
+                                                                              xscale, XA, XB);
+  TSVM_LAUNCHED(ctx);
+  sumsq_partial<<<nb, 256, 0, ctx->stream>>>(A, n * (int64_t)kp, part);
+  TSVM_LAUNCHED(ctx);
+  choose_scale<<<1, 32, 0, ctx->stream>>>(part, nb, n * (int64_t)kp, scale);
+  TSVM_LAUNCHED(ctx);
+  const dim3 tgrid((unsigned)(n_pad / 32), (unsigned)ceil_div(kp, 32));
+  if (bf16)
+    prep_at<__nv_bfloat16><<<tgrid, dim3(32, 8), 0, ctx->stream>>>(
+        A, y, n, n_pad, kp, scale, reinterpret_cast<__nv_bfloat16 *>(AT));
+  else
+    prep_at<__half><<<tgrid, dim3(32, 8), 0, ctx->stream>>>(A, y, n, n_pad, kp, scale,
+                                                           reinterpret_cast<__half *>(AT));
+  TSVM_LAUNCHED(ctx);
+  TSVM_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
+
+  CUtensorMap mxa, mxb;
+  if (!make_map(&mxa, XA, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, kKG, n_pad, 64, kBM) ||
+      !make_map(&mxb, XB, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, kKG, n_pad, 64, kBJ))
+    return TSVM_ERR_CUDA;
+  const int ntiles = (int)(n_pad / kBJ);
+  cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
+  TSVM_CUDA(cudaEventRecord(e0, ctx->stream));
+  for (int c0 = 0; c0 < kp; c0 += kMaxSlab) {
+    const int kpw = kp - c0 < kMaxSlab ? kp - c0 : kMaxSlab;
+    CUtensorMap mat;
+    if (!make_map(&mat, AT, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
+                  n_pad, kp, kBJ, kpw))
+      return TSVM_ERR_CUDA;
+    const SmemLayout L = smem_layout(kpw);
+    const size_t smem = L.total + 1024;
+    auto kern = bf16 ? kermatmul_tc_kernel<true> : kermatmul_tc_kernel<false>;
+    TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<(unsigned)(n_pad / kBM), kThreadsTC, smem, ctx->stream>>>(mxa, mxb, mat, y, scale + 1, n,
+                                                                     ntiles, c0, kpw, W, kp, err);
+    TSVM_LAUNCHED(ctx);
+  }
+  TSVM_CUDA(cudaEventRecord(e1, ctx->stream));
+  int herr = 0;
+  TSVM_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (kernel_ms) *kernel_ms = event_ms(e0, e1);
+  if (herr) return TSVM_ERR_TIMEOUT;
+  return TSVM_OK;
+}
+
 }  // namespace tsvm

@@ -35,8 +35,10 @@ def test_sketch_matches_reference_stream(ctx, n, k):
     got = out.cpu().numpy()
     ref = orc.polar_sketch(n, k).ravel()
     # same accept/reject pattern and order; values differ only where log() rounds differently
+    # (a 1-ulp log difference grows to a few ulp through the division, sqrt and product)
+    assert np.array_equal(np.sign(got), np.sign(ref))
     ulp = np.abs(got.view(np.int32).astype(np.int64) - ref.view(np.int32).astype(np.int64))
-    assert ulp.max() <= 2
+    assert ulp.max() <= 4
     assert np.mean(ulp != 0) < 5e-3
 
 
@@ -76,8 +78,8 @@ def test_jacobi_eigensolver(ctx, k):
     w = torch.empty(k, dtype=torch.float64, device="cuda")
     V = torch.empty((k, k), dtype=torch.float64, device="cuda")
     sweeps = ctypes.c_int32(0)
-    _lib.check(ctx.lib.tsvm_test_eig(ctx.handle, P(dev(S.copy())), k, P(w), P(V),
-                                     ctypes.byref(sweeps)), "eig")
+    Sd = dev(S.copy())
+    _lib.check(ctx.lib.tsvm_test_eig(ctx.handle, P(Sd), k, P(w), P(V), ctypes.byref(sweeps)), "eig")
     wh, Vh = w.cpu().numpy(), V.cpu().numpy()
     assert 0 < sweeps.value < 40
     assert np.allclose(np.sort(wh), np.linalg.eigvalsh(S), rtol=1e-10, atol=1e-9 * np.abs(S).max())
@@ -108,8 +110,43 @@ def test_kermatmul_fp32(ctx, n, d, kp):
     A = rng.standard_normal((n, kp)).astype(np.float32)
     W = torch.empty((n, kp), dtype=torch.float32, device="cuda")
     g = 0.05
-    _lib.check(ctx.lib.tsvm_test_kermatmul(ctx.handle, P(dev(X)), P(dev(y)), n, d, g, P(dev(A)), kp,
+    Xd, yd, Ad = dev(X), dev(y), dev(A)   # keep the device copies alive across the call
+    _lib.check(ctx.lib.tsvm_test_kermatmul(ctx.handle, P(Xd), P(yd), n, d, g, P(Ad), kp,
                                            P(W), _lib.PREC_FP32), "kermatmul")
     ref = orc.kermatmul(X, y, g, A)
     err = np.linalg.norm(W.cpu().numpy() - ref) / np.linalg.norm(ref)
     assert err < 2e-6, err
+
+
+@pytest.mark.parametrize("prec,tol", [(_lib.PREC_FP16, 2e-3), (_lib.PREC_BF16, 1.5e-2)])
+@pytest.mark.parametrize("n,d,kp", [(3001, 18, 64), (517, 12, 256), (1000, 18, 448), (300, 3, 128)])
+def test_kermatmul_tensor_core(ctx, n, d, kp, prec, tol):
+    rng = np.random.default_rng(n + kp)
+    X = rng.standard_normal((n, d)).astype(np.float32)
+    y = np.where(rng.random(n) < 0.5, 1.0, -1.0).astype(np.float32)
+    A = rng.standard_normal((n, kp)).astype(np.float32)
+    W = torch.empty((n, kp), dtype=torch.float32, device="cuda")
+    g = 0.05
+    Xd, yd, Ad = dev(X), dev(y), dev(A)
+    _lib.check(ctx.lib.tsvm_test_kermatmul(ctx.handle, P(Xd), P(yd), n, d, g, P(Ad), kp,
+                                           P(W), prec), "kermatmul_tc")
+    ref = orc.kermatmul(X, y, g, A)
+    err = np.linalg.norm(W.cpu().numpy() - ref) / np.linalg.norm(ref)
+    assert err < tol, err
+
+
+def test_kermatmul_tensor_core_distance_precision(ctx):
+    # the split-FP16 Gram must resolve close pairs: K near 1 for near-duplicate rows
+    rng = np.random.default_rng(5)
+    n, d, kp = 1024, 18, 64
+    base = rng.standard_normal((n // 2, d)).astype(np.float32) * 3.0
+    X = np.concatenate([base, base + 1e-3 * rng.standard_normal(base.shape).astype(np.float32)])
+    y = np.ones(n, dtype=np.float32)
+    A = np.zeros((n, kp), dtype=np.float32)
+    A[np.arange(n), np.arange(n) % kp] = 1.0
+    W = torch.empty((n, kp), dtype=torch.float32, device="cuda")
+    Xd, yd, Ad = dev(X), dev(y), dev(A)
+    _lib.check(ctx.lib.tsvm_test_kermatmul(ctx.handle, P(Xd), P(yd), n, d, 0.5, P(Ad), kp, P(W),
+                                           _lib.PREC_FP16), "kermatmul_tc")
+    ref = orc.kermatmul(X, y, 0.5, A)
+    assert np.max(np.abs(W.cpu().numpy() - ref)) < 2e-3 * np.max(np.abs(ref))
