@@ -153,6 +153,23 @@ tsvm_status tsvm_bias(tsvm_context *ctx, const float *Z, int32_t ldz, const floa
                       const double *alpha, int64_t n, int32_t k, double C, double *b_out,
                       double *b_std_out, int32_t *n_sv, int32_t *n_free);
 
+/* Allocation-free variant of tsvm_bias, for callers that must not let a library allocate
+ * device memory (a serving process whose HBM is pre-partitioned by its own pool, a host
+ * framework that forbids plug-in allocations, or a process that has already committed all
+ * device memory).  It has no counterpart in the reference, whose bias loop runs on the host.
+ * It needs no tsvm_context and calls no allocator: its scratch is a fixed ~2.4 MB static
+ * device array (resident on each device that loads the library until exit).
+ *   Z, y, alpha  device inputs as for tsvm_bias, on the current device
+ *   out          device, 4 doubles: b, b_std, number of SVs, number of free SVs
+ *   stream       cudaStream_t (void*), NULL for the legacy default stream; the call is
+ *                asynchronous on it
+ * Limits: k <= 1024, otherwise TSVM_ERR_INVALID_ARGUMENT.  The first call on each device
+ * looks up the array's device address (cudaGetSymbolAddress) with that device current; make
+ * it before any stream capture.  All calls share the array: calls that overlap on the GPU
+ * race and must be ordered by the caller. */
+tsvm_status tsvm_bias_noalloc(const float *Z, int32_t ldz, const float *y, const double *alpha,
+                              int64_t n, int32_t k, double C, double *out, void *stream);
+
 /* End-to-end training from HOST buffers (the path main() drives, tensorsvm-train.cu:907-1024):
  * copies X and y to the device, factors (RBF) or labels (linear), solves, computes the bias
  * and copies alpha back.  For the linear kernel `gamma` and `k` are ignored and w is not

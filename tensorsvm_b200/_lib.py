@@ -38,8 +38,8 @@ SKETCH_USER = 1
 EXPORTS = [
     "tsvm_status_string", "tsvm_create", "tsvm_destroy", "tsvm_set_stream",
     "tsvm_ipm_default_options",
-    "tsvm_factor", "tsvm_linear_factor", "tsvm_ipm", "tsvm_bias", "tsvm_train",
-    "tsvm_kernel_launches",
+    "tsvm_factor", "tsvm_linear_factor", "tsvm_ipm", "tsvm_bias", "tsvm_bias_noalloc",
+    "tsvm_train", "tsvm_kernel_launches",
 ]
 TEST_EXPORTS = [
     "tsvm_test_rand_stream", "tsvm_test_sketch", "tsvm_test_kermatmul", "tsvm_test_chol",
@@ -108,6 +108,8 @@ def load() -> ctypes.CDLL:
     lib.tsvm_bias.restype = ctypes.c_int
     lib.tsvm_bias.argtypes = [P, P, I32, P, P, I64, I32, D, ctypes.POINTER(D), ctypes.POINTER(D),
                               ctypes.POINTER(I32), ctypes.POINTER(I32)]
+    lib.tsvm_bias_noalloc.restype = ctypes.c_int
+    lib.tsvm_bias_noalloc.argtypes = [P, I32, P, P, I64, I32, D, P, P]
     lib.tsvm_train.restype = ctypes.c_int
     lib.tsvm_train.argtypes = [P, P, P, I64, I32, I32, D, D, I32, I32, ctypes.POINTER(IpmOptions),
                                P, ctypes.POINTER(D), ctypes.POINTER(FactorInfo),
