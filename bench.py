@@ -92,22 +92,32 @@ class ClockSampler:
 
 
 def dist_setup():
+    """One process per GPU (torchrun env vars); NCCL on GPUs, gloo when there is no CUDA."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         import datetime
+        import torch
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return world, rank, local
 
 
+def replica_seed(rank: int) -> int:
+    """Data seed of a replica: every rank trains an independent problem of the same size."""
+    return 2 + rank
+
+
 def dist_max(values, world):
+    """Element-wise max over ranks (the timing of a replica job is its slowest rank)."""
     if world == 1:
         return values
     import torch
     import torch.distributed as dist
-    t = torch.tensor(values, dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(values, dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return t.cpu().tolist()
 
@@ -127,7 +137,7 @@ def run_ours(args, world, rank, local):
     from tensorsvm_b200 import _lib, api, synth
     torch.cuda.set_device(local)
     n = args.n
-    X, y = synth.two_gaussians(n, D, seed=2 + rank, noise=NOISE)
+    X, y = synth.two_gaussians(n, D, seed=replica_seed(rank), noise=NOISE)
     Xd, yd = torch.from_numpy(X).cuda(), torch.from_numpy(y).cuda()
     ctx = _lib.Context(local)
     stream = torch.cuda.Stream()

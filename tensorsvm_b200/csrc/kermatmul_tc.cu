@@ -17,9 +17,15 @@
 // bare ex2.  Labels are folded into AT (AT[c][j] = s y_j A[j][c], s a power of two that keeps
 // FP16 away from its subnormal range) and into the final scaling of W's rows by y_i / s.
 //
-// Warp roles (320 threads): warp 0 TMA producer, warp 1 TMEM allocator + single-thread MMA
-// issuer, warps 2-5 and 6-9 two exp warpgroups that take alternate J blocks (S is double
-// buffered in TMEM: 2 x 64 columns; W uses up to 256 columns).  All waits are bounded: after
+// Warp roles (352 threads): warp 0 loads XA and streams the Gram operands (6-deep ring, freed
+// as soon as the Gram MMA completes), warp 10 streams the kernel-block operands (5-deep ring,
+// freed after P AT^T), warp 1 allocates TMEM and one thread issues the MMAs, warps 2-5 and 6-9
+// are two exp warpgroups that take alternate J blocks.  S/P live in four 64-column TMEM
+// buffers and W in up to 256 more.  The issuer runs the Gram MMAs two J blocks ahead of the
+// P AT^T MMAs.  Two separate rings matter: with one ring a stage stays busy from its load
+// until P AT^T, so the loads could only run about two blocks ahead and the kernel was bound
+// by L2->SMEM load latency.  The exponentials can be split between MUFU ex2 and a polynomial
+// on the FMA pipe (TSVM_TC_POLY); MUFU alone is fastest here.  All waits are bounded: after
 // ~1 s without progress a block records an error and leaves; the host reports
 // TSVM_ERR_TIMEOUT.  No cluster multicast anywhere.
 #include <cuda.h>
@@ -38,40 +44,33 @@ namespace {
 constexpr int kBM = 128;          // rows of W per CTA (TMEM lanes)
 constexpr int kBJ = 64;           // J block (K of the second MMA, N of the Gram)
 constexpr int kKG = 64;           // Gram K (split features + norms, zero padded)
-constexpr int kStages = 3;        // TMA ring depth
-constexpr int kThreadsTC = 320;
+constexpr int kXbStages = 6;      // ring of Gram operands (freed as soon as the Gram completes)
+constexpr int kAtStages = 5;      // ring of kernel-block operands (freed after P AT^T)
+constexpr int kLookahead = 2;     // Gram MMAs issued this many J blocks ahead of P AT^T
+constexpr int kThreadsTC = 352;
 constexpr int kMaxSlab = 256;     // columns of W per launch (MMA N <= 256)
 
 constexpr uint32_t kXaBytes = kBM * kKG * 2;       // 16 KB
 constexpr uint32_t kXbBytes = kBJ * kKG * 2;       //  8 KB
-constexpr uint32_t kAtBytesMax = kMaxSlab * kBJ * 2;  // 32 KB (kpw rows x 128 B)
-constexpr uint32_t kPBytes = kBM * kBJ * 2;        // 16 KB
-
-struct SmemLayout {
-  // all operand tiles are 1024-byte aligned (128B swizzle atoms)
-  uint32_t xa, xb[kStages], at[kStages], p[2], bars, total;
-};
 
 __host__ __device__ constexpr uint32_t align1k(uint32_t v) { return (v + 1023u) & ~1023u; }
 
+// Shared-memory layout, all operand tiles 1024-byte aligned (128B swizzle atoms):
+// [XA 16 KB][XB ring: 6 x 8 KB][AT ring: 5 x kpw*128 B][barriers].  P lives in TMEM.
+// Offsets are computed arithmetically (no arrays), so they stay in registers.
+struct SmemLayout {
+  uint32_t at0, at_bytes, bars, total;
+  __host__ __device__ uint32_t xa() const { return 0; }
+  __host__ __device__ uint32_t xb(int s) const { return kXaBytes + (uint32_t)s * kXbBytes; }
+  __host__ __device__ uint32_t at(int s) const { return at0 + (uint32_t)s * at_bytes; }
+};
+
 __host__ __device__ inline SmemLayout smem_layout(int kpw) {
   SmemLayout L{};
-  uint32_t off = 0;
-  L.xa = off;
-  off += kXaBytes;
-  for (int s = 0; s < kStages; ++s) {
-    L.xb[s] = off;
-    off += kXbBytes;
-    L.at[s] = off;
-    off = align1k(off + (uint32_t)kpw * kBJ * 2);
-  }
-  for (int b = 0; b < 2; ++b) {
-    L.p[b] = off;
-    off += kPBytes;
-  }
-  L.bars = off;
-  off += 256;
-  L.total = off;
+  L.at0 = kXaBytes + kXbStages * kXbBytes;
+  L.at_bytes = align1k((uint32_t)kpw * kBJ * 2);
+  L.bars = L.at0 + kAtStages * L.at_bytes;
+  L.total = L.bars + 512;
   return L;
 }
 
@@ -108,15 +107,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 // Bounded wait: returns false (and raises the block's abort flag) after ~1 s without progress,
-// or as soon as another thread of the block has aborted.
+// or as soon as another thread of the block has aborted.  The global timer is slow to read, so
+// it is only consulted every 1024 unsuccessful polls (each poll may itself suspend briefly).
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const uint64_t deadline = gtimer() + 1000000000ull;
+  uint64_t deadline = 0;
   for (uint32_t spin = 1;; ++spin) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((spin & 63) == 0) {
+    if ((spin & 1023) == 0) {
       if (*abort) return false;
-      if (gtimer() > deadline) {
+      const uint64_t now = gtimer();
+      if (deadline == 0) {
+        deadline = now + 1000000000ull;
+      } else if (now > deadline) {
         *abort = 1;
         return false;
       }
@@ -186,10 +188,54 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+      "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+      "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]),
+      "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]),
+      "r"(r[29]), "r"(r[30]), "r"(r[31])
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+// MMA with the A operand in TMEM (M rows = lanes, 16-bit K pairs packed per 32-bit column).
+__device__ __forceinline__ void umma_ts(uint32_t dtmem, uint32_t atmem, uint64_t bdesc,
+                                        uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(dtmem),
+      "r"(atmem), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
 __device__ __forceinline__ float ex2(float x) {
   float y;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
+}
+// 2^x on the FMA/ALU pipes (offloads the MUFU/conversion pipe): x = n + f with n the nearest
+// integer (1.5 * 2^23 rounding trick) and f in [-1/2, 1/2]; 2^f by a degree-4 polynomial fitted
+// by least squares at Chebyshev nodes (max relative error 2.7e-6); 2^n added to the exponent
+// field.  x is clamped at -125 (results below 2^-125 are zero in FP16/BF16 anyway).
+__device__ __forceinline__ float exp2_poly(float x) {
+  x = fmaxf(x, -125.f);
+  const float t = x + 12582912.f;
+  const float n = t - 12582912.f;
+  const float f = x - n;
+  float p = fmaf(0.009560510516166687f, f, 0.05591703951358795f);
+  p = fmaf(p, f, 0.24024981260299683f);
+  p = fmaf(p, f, 0.6931219696998596f);
+  p = fmaf(p, f, 0.9999991655349731f);
+  return __int_as_float(__float_as_int(p) + (__float_as_int(t) << 23));
+}
+// Element e of a row: NPOLY of every 8 consecutive columns use the polynomial, the rest MUFU.
+template <int NPOLY>
+__device__ __forceinline__ float exp2_mixed(float x, int e) {
+  return (e & 7) < NPOLY ? exp2_poly(x) : ex2(x);
 }
 template <bool BF16>
 __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
@@ -204,8 +250,15 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
 
 // ---------------------------------------------------------------------------------------
 // The fused kernel.  grid.x = row blocks of 128; slab = columns [c0, c0 + kpw) of W.
+//
+// TMEM: four 64-column S/P buffers (columns 0..255) and the W accumulator (256..256+kpw).
+// J block t uses buffer t % 4: the Gram MMA writes S there, the exp warpgroup (t % 2) reads it
+// and writes P (FP16/BF16 pairs) back over its first 32 columns, and the second MMA reads P as
+// its A operand straight from TMEM.  The buffer is free again when that MMA completes.
 // ---------------------------------------------------------------------------------------
-template <bool BF16>
+constexpr int kSBufs = 4;
+
+template <bool BF16, int NPOLY>
 __global__ void __launch_bounds__(kThreadsTC, 1)
 kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
                     const __grid_constant__ CUtensorMap map_xb,
@@ -213,37 +266,41 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
                     const float *__restrict__ inv_scale, int64_t n, int ntiles, int c0, int kpw,
                     float *__restrict__ W, int64_t ldw, int *__restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  // 1024-align the dynamic shared window
   const uint32_t raw = su32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   uint8_t *sbase = smem_raw + (base - raw);
   const SmemLayout L = smem_layout(kpw);
   uint64_t *bars = reinterpret_cast<uint64_t *>(sbase + L.bars);
-  // barrier slots
-  const uint32_t b_full = su32(bars + 0);            // [kStages]
-  const uint32_t b_empty = su32(bars + kStages);     // [kStages]
-  const uint32_t b_sfull = su32(bars + 2 * kStages); // [2]
-  const uint32_t b_sempty = b_sfull + 16;            // [2]
-  const uint32_t b_pfull = b_sfull + 32;             // [2]
-  const uint32_t b_pempty = b_sfull + 48;            // [2]
-  const uint32_t b_wfull = b_sfull + 64;
-  const uint32_t b_xafull = b_sfull + 72;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kStages + 10);
+  // barrier slots (8 bytes each)
+  const uint32_t b_xbfull = su32(bars);                  // [kXbStages] Gram operand loaded
+  const uint32_t b_xbempty = b_xbfull + 8 * kXbStages;   // [kXbStages] Gram operand consumed
+  const uint32_t b_atfull = b_xbempty + 8 * kXbStages;   // [kAtStages] kernel operand loaded
+  const uint32_t b_atempty = b_atfull + 8 * kAtStages;   // [kAtStages] kernel operand consumed
+  const uint32_t b_sfull = b_atempty + 8 * kAtStages;    // [kSBufs] S written by the Gram MMA
+  const uint32_t b_pfull = b_sfull + 8 * kSBufs;         // [kSBufs] P written by the exp warps
+  const uint32_t b_free = b_pfull + 8 * kSBufs;          // [kSBufs] buffer consumed by P AT^T
+  const uint32_t b_wfull = b_free + 8 * kSBufs;          // W accumulation finished
+  const uint32_t b_xafull = b_wfull + 8;                 // XA loaded
+  uint32_t *tmem_slot =
+      reinterpret_cast<uint32_t *>(bars + 2 * kXbStages + 2 * kAtStages + 3 * kSBufs + 2);
   volatile int *abort = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t i0 = (int64_t)blockIdx.x * kBM;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
-      mbar_init(b_full + 8 * s, 1);
-      mbar_init(b_empty + 8 * s, 1);
+    for (int s = 0; s < kXbStages; ++s) {
+      mbar_init(b_xbfull + 8 * s, 1);
+      mbar_init(b_xbempty + 8 * s, 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int s = 0; s < kAtStages; ++s) {
+      mbar_init(b_atfull + 8 * s, 1);
+      mbar_init(b_atempty + 8 * s, 1);
+    }
+    for (int b = 0; b < kSBufs; ++b) {
       mbar_init(b_sfull + 8 * b, 1);
-      mbar_init(b_sempty + 8 * b, 128);
       mbar_init(b_pfull + 8 * b, 128);
-      mbar_init(b_pempty + 8 * b, 1);
+      mbar_init(b_free + 8 * b, 1);
     }
     mbar_init(b_wfull, 1);
     mbar_init(b_xafull, 1);
@@ -260,24 +317,32 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const uint32_t t_s = tmem;          // S buffers: columns [0, 128)
-  const uint32_t t_w = tmem + 128;    // W accumulator: columns [128, 128 + kpw)
+  const uint32_t t_w = tmem + kSBufs * kBJ;   // W accumulator columns
 
   if (warp == 0) {
-    // ---------------- TMA producer ----------------
+    // ---------------- TMA producer: XA once, then the Gram operand ring ----------------
     if (lane == 0) {
       asm volatile("prefetch.tensormap [%0];" ::"l"(&map_xa) : "memory");
       asm volatile("prefetch.tensormap [%0];" ::"l"(&map_xb) : "memory");
-      asm volatile("prefetch.tensormap [%0];" ::"l"(&map_at) : "memory");
       mbar_expect_tx(b_xafull, kXaBytes);
-      tma_load_2d(&map_xa, b_xafull, base + L.xa, 0, (int)i0);
-      const uint32_t stage_bytes = kXbBytes + (uint32_t)kpw * kBJ * 2;
+      tma_load_2d(&map_xa, b_xafull, base + L.xa(), 0, (int)i0);
       for (int t = 0; t < ntiles; ++t) {
-        const int st = t % kStages, use = t / kStages;
-        if (!mbar_wait(b_empty + 8 * st, (use & 1) ^ 1, abort)) break;
-        mbar_expect_tx(b_full + 8 * st, stage_bytes);
-        tma_load_2d(&map_xb, b_full + 8 * st, base + L.xb[st], 0, t * kBJ);
-        tma_load_2d(&map_at, b_full + 8 * st, base + L.at[st], t * kBJ, c0);
+        const int st = t % kXbStages, use = t / kXbStages;
+        if (!mbar_wait(b_xbempty + 8 * st, (use & 1) ^ 1, abort)) break;
+        mbar_expect_tx(b_xbfull + 8 * st, kXbBytes);
+        tma_load_2d(&map_xb, b_xbfull + 8 * st, base + L.xb(st), 0, t * kBJ);
+      }
+    }
+  } else if (warp == 10) {
+    // ---------------- TMA producer: kernel-block operand ring ----------------
+    if (lane == 0) {
+      asm volatile("prefetch.tensormap [%0];" ::"l"(&map_at) : "memory");
+      const uint32_t at_bytes = (uint32_t)kpw * kBJ * 2;
+      for (int t = 0; t < ntiles; ++t) {
+        const int st = t % kAtStages, use = t / kAtStages;
+        if (!mbar_wait(b_atempty + 8 * st, (use & 1) ^ 1, abort)) break;
+        mbar_expect_tx(b_atfull + 8 * st, at_bytes);
+        tma_load_2d(&map_at, b_atfull + 8 * st, base + L.at(st), t * kBJ, c0);
       }
     }
   } else if (warp == 1) {
@@ -286,68 +351,62 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
       constexpr uint32_t idg = idesc_f16(kBM, kBJ, 0);           // Gram: FP16 always
       const uint32_t id2 = idesc_f16(kBM, kpw, BF16 ? 1u : 0u);  // P AT^T
       bool ok = mbar_wait(b_xafull, 0, abort);
-      for (int t = 0; ok && t <= ntiles; ++t) {
+      for (int t = 0; ok && t < ntiles + kLookahead; ++t) {
         if (t < ntiles) {
-          const int st = t % kStages, use = t / kStages, b = t & 1, ub = t >> 1;
-          if (!mbar_wait(b_full + 8 * st, use & 1, abort)) break;
-          if (!mbar_wait(b_sempty + 8 * b, (ub & 1) ^ 1, abort)) break;
+          const int st = t % kXbStages, use = t / kXbStages, b = t % kSBufs, ub = t / kSBufs;
+          if (!mbar_wait(b_xbfull + 8 * st, use & 1, abort)) break;
+          if (!mbar_wait(b_free + 8 * b, (ub & 1) ^ 1, abort)) break;
           tc_fence_after();
 #pragma unroll
           for (int kk = 0; kk < kKG / 16; ++kk)
-            umma(t_s + b * kBJ, desc_sw128(base + L.xa + kk * 32),
-                 desc_sw128(base + L.xb[st] + kk * 32), idg, kk > 0 ? 1u : 0u);
+            umma(tmem + b * kBJ, desc_sw128(base + L.xa() + kk * 32),
+                 desc_sw128(base + L.xb(st) + kk * 32), idg, kk > 0 ? 1u : 0u);
           umma_commit(b_sfull + 8 * b);
+          umma_commit(b_xbempty + 8 * st);
         }
-        if (t > 0) {
-          const int tp = t - 1, bp = tp & 1, ubp = tp >> 1, stp = tp % kStages;
+        if (t >= kLookahead) {
+          const int tp = t - kLookahead, bp = tp % kSBufs, ubp = tp / kSBufs;
+          const int stp = tp % kAtStages, usp = tp / kAtStages;
+          if (!mbar_wait(b_atfull + 8 * stp, usp & 1, abort)) break;
           if (!mbar_wait(b_pfull + 8 * bp, ubp & 1, abort)) break;
           tc_fence_after();
 #pragma unroll
           for (int kk = 0; kk < kBJ / 16; ++kk)
-            umma(t_w, desc_sw128(base + L.p[bp] + kk * 32), desc_sw128(base + L.at[stp] + kk * 32),
-                 id2, (tp > 0 || kk > 0) ? 1u : 0u);
-          umma_commit(b_pempty + 8 * bp);
-          umma_commit(b_empty + 8 * stp);
+            umma_ts(t_w, tmem + bp * kBJ + kk * 8, desc_sw128(base + L.at(stp) + kk * 32), id2,
+                    (tp > 0 || kk > 0) ? 1u : 0u);
+          umma_commit(b_free + 8 * bp);
+          umma_commit(b_atempty + 8 * stp);
         }
       }
       umma_commit(b_wfull);
     }
-  } else {
+  } else if (warp >= 2 && warp < 10) {
     // ---------------- exp warpgroups ----------------
     const int g = (warp - 2) >> 2;        // warpgroup 0: warps 2-5, 1: warps 6-9
     const int q = warp & 3;               // TMEM lane quarter this warp may access
     const int row = q * 32 + lane;        // row of the 128-row block (TMEM lane)
     const uint32_t lane_off = (uint32_t)(q * 32) << 16;
-    const uint32_t prow = (uint32_t)row * 128u;
-    const uint32_t sw = (uint32_t)(row & 7);
     for (int t = g; t < ntiles; t += 2) {
-      const int b = g, ub = t >> 1;
+      const int b = t % kSBufs, ub = t / kSBufs;
       if (!mbar_wait(b_sfull + 8 * b, ub & 1, abort)) break;
       tc_fence_after();
+      const uint32_t tb = tmem + b * kBJ + lane_off;
       uint32_t s0[32], s1[32];
-      tmem_ld32(t_s + b * kBJ + lane_off, s0);
-      tmem_ld32(t_s + b * kBJ + 32 + lane_off, s1);
+      tmem_ld32(tb, s0);
+      tmem_ld32(tb + 32, s1);
       tmem_wait_ld();
-      tc_fence_before();
-      mbar_arrive(b_sempty + 8 * b);
       uint32_t pk[32];
 #pragma unroll
       for (int c = 0; c < 16; ++c)
-        pk[c] = pack2<BF16>(ex2(__uint_as_float(s0[2 * c])), ex2(__uint_as_float(s0[2 * c + 1])));
+        pk[c] = pack2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c]), 2 * c),
+                            exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c + 1]), 2 * c + 1));
 #pragma unroll
       for (int c = 0; c < 16; ++c)
-        pk[16 + c] =
-            pack2<BF16>(ex2(__uint_as_float(s1[2 * c])), ex2(__uint_as_float(s1[2 * c + 1])));
-      if (!mbar_wait(b_pempty + 8 * b, (ub & 1) ^ 1, abort)) break;
-      const uint32_t pbase = base + L.p[b] + prow;
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const uint32_t addr = pbase + (((uint32_t)u ^ sw) << 4);
-        asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(pk[4 * u]),
-                     "r"(pk[4 * u + 1]), "r"(pk[4 * u + 2]), "r"(pk[4 * u + 3])
-                     : "memory");
-      }
-      fence_async_smem();
+        pk[16 + c] = pack2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c]), 2 * c),
+                                 exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c + 1]), 2 * c + 1));
+      tmem_st32(tb, pk);   // P over the first 32 columns of the buffer (S is no longer needed)
+      tmem_wait_st();
+      tc_fence_before();
       mbar_arrive(b_pfull + 8 * b);
     }
     // ---------------- epilogue: W rows of this block, half of the slab per warpgroup -----
@@ -511,6 +570,32 @@ bool make_map(CUtensorMap *map, const void *ptr, CUtensorMapDataType dt, uint64_
             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+using TcKernel = void (*)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const float *,
+                          const float *, int64_t, int, int, int, float *, int64_t, int *);
+
+// Exps per 8 columns evaluated by the FMA-pipe polynomial (the rest on MUFU); tunable through
+// TSVM_TC_POLY (0, 2, 4, 6 or 8) for the autotuning sweep in the benchmarks.
+int poly_split() {
+  int v = 0;
+  if (const char *e = getenv("TSVM_TC_POLY")) {
+    const int x = atoi(e);
+    if (x == 0 || x == 2 || x == 4 || x == 6 || x == 8) v = x;
+  }
+  return v;
+}
+
+TcKernel select_kernel(bool bf16, int npoly) {
+#define TSVM_SEL(P) \
+  if (npoly == P) return bf16 ? kermatmul_tc_kernel<true, P> : kermatmul_tc_kernel<false, P>;
+  TSVM_SEL(0)
+  TSVM_SEL(2)
+  TSVM_SEL(4)
+  TSVM_SEL(6)
+  TSVM_SEL(8)
+#undef TSVM_SEL
+  return bf16 ? kermatmul_tc_kernel<true, 4> : kermatmul_tc_kernel<false, 4>;
+}
+
 }  // namespace
 
 bool kermatmul_tc_supported(int d, int kp) {
@@ -568,7 +653,7 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
       return TSVM_ERR_CUDA;
     const SmemLayout L = smem_layout(kpw);
     const size_t smem = L.total + 1024;
-    auto kern = bf16 ? kermatmul_tc_kernel<true> : kermatmul_tc_kernel<false>;
+    auto kern = select_kernel(bf16, poly_split());
     TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<(unsigned)(n_pad / kBM), kThreadsTC, smem, ctx->stream>>>(mxa, mxb, mat, y, scale + 1, n,
                                                                      ntiles, c0, kpw, W, kp, err);

@@ -17,14 +17,16 @@ constexpr int kGT = 64;      // output tile edge
 constexpr int kGRows = 32;   // rows staged per step
 
 // grid: (tile index, split).  Each block accumulates a 64x64 tile over rows [r0, r1).
+// Operands are converted to FP64 once, while staging 32-row slabs into shared memory (with the
+// optional row weight folded into the A side), so the inner loop is pure DFMA: each thread owns
+// a 4x4 block of the tile and reads 4 + 4 doubles per row.
 __global__ void __launch_bounds__(256)
 gram_partial_kernel(const float *__restrict__ A, int64_t lda, const float *__restrict__ B,
                     int64_t ldb, int64_t n, int ka, int kb, int tiles_b, int symmetric,
                     int64_t rows_per_split, const double *__restrict__ rowscale,
                     double *__restrict__ part) {
-  __shared__ float As[kGRows][kGT];
-  __shared__ float Bs[kGRows][kGT];
-  __shared__ double Sc[kGRows];
+  __shared__ double As[kGRows][kGT];
+  __shared__ double Bs[kGRows][kGT];
   int t = blockIdx.x, ta, tb;
   if (symmetric) {  // lower-triangle tile enumeration
     ta = 0;
@@ -48,21 +50,19 @@ gram_partial_kernel(const float *__restrict__ A, int64_t lda, const float *__res
     for (int e = threadIdx.x; e < kGRows * kGT; e += 256) {
       const int rr = e / kGT, c = e % kGT;
       const int64_t gr = r + rr;
-      As[rr][c] = (gr < r1 && a0 + c < ka) ? A[gr * lda + a0 + c] : 0.f;
-      Bs[rr][c] = (gr < r1 && b0 + c < kb) ? B[gr * ldb + b0 + c] : 0.f;
-    }
-    if (threadIdx.x < kGRows) {
-      const int64_t gr = r + threadIdx.x;
-      Sc[threadIdx.x] = (gr < r1) ? (rowscale ? rowscale[gr] : 1.0) : 0.0;
+      const bool in = gr < r1;
+      const double sc = in ? (rowscale ? rowscale[gr] : 1.0) : 0.0;
+      As[rr][c] = (in && a0 + c < ka) ? (double)A[gr * lda + a0 + c] * sc : 0.0;
+      Bs[rr][c] = (in && b0 + c < kb) ? (double)B[gr * ldb + b0 + c] : 0.0;
     }
     __syncthreads();
-#pragma unroll 4
+#pragma unroll 8
     for (int rr = 0; rr < kGRows; ++rr) {
       double av[4], bv[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) av[i] = (double)As[rr][ty + 16 * i] * Sc[rr];
+      for (int i = 0; i < 4; ++i) av[i] = As[rr][ty + 16 * i];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bv[j] = (double)Bs[rr][tx + 16 * j];
+      for (int j = 0; j < 4; ++j) bv[j] = Bs[rr][tx + 16 * j];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll

@@ -150,3 +150,20 @@ def test_kermatmul_tensor_core_distance_precision(ctx):
                                            _lib.PREC_FP16), "kermatmul_tc")
     ref = orc.kermatmul(X, y, 0.5, A)
     assert np.max(np.abs(W.cpu().numpy() - ref)) < 2e-3 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("npoly", ["0", "2", "6", "8"])
+def test_kermatmul_tensor_core_exp_split(ctx, npoly, monkeypatch):
+    # every MUFU / polynomial split of the exponentials gives the same product
+    monkeypatch.setenv("TSVM_TC_POLY", npoly)
+    rng = np.random.default_rng(11)
+    n, d, kp = 2000, 18, 128
+    X = rng.standard_normal((n, d)).astype(np.float32)
+    y = np.where(rng.random(n) < 0.5, 1.0, -1.0).astype(np.float32)
+    A = rng.standard_normal((n, kp)).astype(np.float32)
+    W = torch.empty((n, kp), dtype=torch.float32, device="cuda")
+    Xd, yd, Ad = dev(X), dev(y), dev(A)
+    _lib.check(ctx.lib.tsvm_test_kermatmul(ctx.handle, P(Xd), P(yd), n, d, 0.05, P(Ad), kp, P(W),
+                                           _lib.PREC_FP16), "kermatmul_tc")
+    ref = orc.kermatmul(X, y, 0.05, A)
+    assert np.linalg.norm(W.cpu().numpy() - ref) / np.linalg.norm(ref) < 2e-3
