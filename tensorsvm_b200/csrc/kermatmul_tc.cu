@@ -17,15 +17,16 @@
 // bare ex2.  Labels are folded into AT (AT[c][j] = s y_j A[j][c], s a power of two that keeps
 // FP16 away from its subnormal range) and into the final scaling of W's rows by y_i / s.
 //
-// Warp roles (352 threads): warp 0 loads XA and streams the Gram operands (6-deep ring, freed
+// Warp roles (384 threads): warp 0 loads XA and streams the Gram operands (6-deep ring, freed
 // as soon as the Gram MMA completes), warp 10 streams the kernel-block operands (5-deep ring,
-// freed after P AT^T), warp 1 allocates TMEM and one thread issues the MMAs, warps 2-5 and 6-9
-// are two exp warpgroups that take alternate J blocks.  S/P live in four 64-column TMEM
-// buffers and W in up to 256 more.  The issuer runs the Gram MMAs two J blocks ahead of the
-// P AT^T MMAs.  Two separate rings matter: with one ring a stage stays busy from its load
-// until P AT^T, so the loads could only run about two blocks ahead and the kernel was bound
-// by L2->SMEM load latency.  The exponentials can be split between MUFU ex2 and a polynomial
-// on the FMA pipe (TSVM_TC_POLY); MUFU alone is fastest here.  All waits are bounded: after
+// freed after P AT^T), warp 1 allocates TMEM and issues the Gram MMAs, warp 11 issues the
+// P AT^T MMAs, warps 2-5 and 6-9 are two exp warpgroups that take alternate J blocks.  S/P live
+// in four 64-column TMEM buffers and W in up to 256 more.  Issuing is split over two threads
+// because one thread issuing everything (each barrier wait and each tcgen05 instruction costs
+// tens of cycles in a single thread) could not keep the tensor pipe busy; each issuer works
+// from precomputed descriptors and incremental ring counters.  The exponentials can be split
+// between MUFU ex2 and a polynomial on the FMA pipe (TSVM_TC_POLY); MUFU alone is fastest
+// here.  All waits are bounded: after
 // ~1 s without progress a block records an error and leaves; the host reports
 // TSVM_ERR_TIMEOUT.  No cluster multicast anywhere.
 #include <cuda.h>
@@ -46,8 +47,7 @@ constexpr int kBJ = 64;           // J block (K of the second MMA, N of the Gram
 constexpr int kKG = 64;           // Gram K (split features + norms, zero padded)
 constexpr int kXbStages = 6;      // ring of Gram operands (freed as soon as the Gram completes)
 constexpr int kAtStages = 5;      // ring of kernel-block operands (freed after P AT^T)
-constexpr int kLookahead = 2;     // Gram MMAs issued this many J blocks ahead of P AT^T
-constexpr int kThreadsTC = 352;
+constexpr int kThreadsTC = 384;
 constexpr int kMaxSlab = 256;     // columns of W per launch (MMA N <= 256)
 
 constexpr uint32_t kXaBytes = kBM * kKG * 2;       // 16 KB
@@ -326,11 +326,13 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
       asm volatile("prefetch.tensormap [%0];" ::"l"(&map_xb) : "memory");
       mbar_expect_tx(b_xafull, kXaBytes);
       tma_load_2d(&map_xa, b_xafull, base + L.xa(), 0, (int)i0);
+      int st = 0;
+      uint32_t ph = 0;
       for (int t = 0; t < ntiles; ++t) {
-        const int st = t % kXbStages, use = t / kXbStages;
-        if (!mbar_wait(b_xbempty + 8 * st, (use & 1) ^ 1, abort)) break;
+        if (!mbar_wait(b_xbempty + 8 * st, ph ^ 1, abort)) break;
         mbar_expect_tx(b_xbfull + 8 * st, kXbBytes);
         tma_load_2d(&map_xb, b_xbfull + 8 * st, base + L.xb(st), 0, t * kBJ);
+        if (++st == kXbStages) { st = 0; ph ^= 1; }
       }
     }
   } else if (warp == 10) {
@@ -338,45 +340,59 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
     if (lane == 0) {
       asm volatile("prefetch.tensormap [%0];" ::"l"(&map_at) : "memory");
       const uint32_t at_bytes = (uint32_t)kpw * kBJ * 2;
+      int st = 0;
+      uint32_t ph = 0;
       for (int t = 0; t < ntiles; ++t) {
-        const int st = t % kAtStages, use = t / kAtStages;
-        if (!mbar_wait(b_atempty + 8 * st, (use & 1) ^ 1, abort)) break;
+        if (!mbar_wait(b_atempty + 8 * st, ph ^ 1, abort)) break;
         mbar_expect_tx(b_atfull + 8 * st, at_bytes);
         tma_load_2d(&map_at, b_atfull + 8 * st, base + L.at(st), t * kBJ, c0);
+        if (++st == kAtStages) { st = 0; ph ^= 1; }
       }
     }
   } else if (warp == 1) {
-    // ---------------- MMA issuer ----------------
+    // ---------------- Gram MMA issuer: S_t = XA XB_t^T into buffer t % 4 ----------------
     if (lane == 0) {
-      constexpr uint32_t idg = idesc_f16(kBM, kBJ, 0);           // Gram: FP16 always
-      const uint32_t id2 = idesc_f16(kBM, kpw, BF16 ? 1u : 0u);  // P AT^T
+      constexpr uint32_t idg = idesc_f16(kBM, kBJ, 0);  // Gram: FP16 always
+      const uint64_t dxa = desc_sw128(base + L.xa());
+      const uint64_t dxb0 = desc_sw128(base + L.xb(0));
       bool ok = mbar_wait(b_xafull, 0, abort);
-      for (int t = 0; ok && t < ntiles + kLookahead; ++t) {
-        if (t < ntiles) {
-          const int st = t % kXbStages, use = t / kXbStages, b = t % kSBufs, ub = t / kSBufs;
-          if (!mbar_wait(b_xbfull + 8 * st, use & 1, abort)) break;
-          if (!mbar_wait(b_free + 8 * b, (ub & 1) ^ 1, abort)) break;
-          tc_fence_after();
+      int st = 0, b = 0;
+      uint32_t sph = 0, bph = 0;  // ring / buffer phase parities
+      for (int t = 0; ok && t < ntiles; ++t) {
+        if (!mbar_wait(b_xbfull + 8 * st, sph, abort)) break;
+        if (!mbar_wait(b_free + 8 * b, bph ^ 1, abort)) break;
+        tc_fence_after();
+        const uint64_t dxb = dxb0 + (uint64_t)((st * kXbBytes) >> 4);
 #pragma unroll
-          for (int kk = 0; kk < kKG / 16; ++kk)
-            umma(tmem + b * kBJ, desc_sw128(base + L.xa() + kk * 32),
-                 desc_sw128(base + L.xb(st) + kk * 32), idg, kk > 0 ? 1u : 0u);
-          umma_commit(b_sfull + 8 * b);
-          umma_commit(b_xbempty + 8 * st);
-        }
-        if (t >= kLookahead) {
-          const int tp = t - kLookahead, bp = tp % kSBufs, ubp = tp / kSBufs;
-          const int stp = tp % kAtStages, usp = tp / kAtStages;
-          if (!mbar_wait(b_atfull + 8 * stp, usp & 1, abort)) break;
-          if (!mbar_wait(b_pfull + 8 * bp, ubp & 1, abort)) break;
-          tc_fence_after();
+        for (int kk = 0; kk < kKG / 16; ++kk)
+          umma(tmem + b * kBJ, dxa + 2 * kk, dxb + 2 * kk, idg, kk > 0 ? 1u : 0u);
+        umma_commit(b_sfull + 8 * b);
+        umma_commit(b_xbempty + 8 * st);
+        if (++st == kXbStages) { st = 0; sph ^= 1; }
+        if (++b == kSBufs) { b = 0; bph ^= 1; }
+      }
+    }
+  } else if (warp == 11) {
+    // ---------------- P AT^T issuer: W += P_t AT_t^T, P from TMEM ----------------
+    if (lane == 0) {
+      const uint32_t id2 = idesc_f16(kBM, kpw, BF16 ? 1u : 0u);
+      const uint64_t dat0 = desc_sw128(base + L.at(0));
+      const uint32_t at_step = L.at_bytes >> 4;
+      int st = 0, b = 0;
+      uint32_t sph = 0, bph = 0;
+      for (int t = 0; t < ntiles; ++t) {
+        if (!mbar_wait(b_atfull + 8 * st, sph, abort)) break;
+        if (!mbar_wait(b_pfull + 8 * b, bph, abort)) break;
+        tc_fence_after();
+        const uint64_t dat = dat0 + (uint64_t)(st * at_step);
+        const uint32_t ap = tmem + b * kBJ;
 #pragma unroll
-          for (int kk = 0; kk < kBJ / 16; ++kk)
-            umma_ts(t_w, tmem + bp * kBJ + kk * 8, desc_sw128(base + L.at(stp) + kk * 32), id2,
-                    (tp > 0 || kk > 0) ? 1u : 0u);
-          umma_commit(b_free + 8 * bp);
-          umma_commit(b_atempty + 8 * stp);
-        }
+        for (int kk = 0; kk < kBJ / 16; ++kk)
+          umma_ts(t_w, ap + kk * 8, dat + 2 * kk, id2, (t > 0 || kk > 0) ? 1u : 0u);
+        umma_commit(b_free + 8 * b);
+        umma_commit(b_atempty + 8 * st);
+        if (++st == kAtStages) { st = 0; sph ^= 1; }
+        if (++b == kSBufs) { b = 0; bph ^= 1; }
       }
       umma_commit(b_wfull);
     }
@@ -386,9 +402,10 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
     const int q = warp & 3;               // TMEM lane quarter this warp may access
     const int row = q * 32 + lane;        // row of the 128-row block (TMEM lane)
     const uint32_t lane_off = (uint32_t)(q * 32) << 16;
+    int b = g;
+    uint32_t bph = 0;
     for (int t = g; t < ntiles; t += 2) {
-      const int b = t % kSBufs, ub = t / kSBufs;
-      if (!mbar_wait(b_sfull + 8 * b, ub & 1, abort)) break;
+      if (!mbar_wait(b_sfull + 8 * b, bph, abort)) break;
       tc_fence_after();
       const uint32_t tb = tmem + b * kBJ + lane_off;
       uint32_t s0[32], s1[32];
@@ -408,6 +425,8 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
       tmem_wait_st();
       tc_fence_before();
       mbar_arrive(b_pfull + 8 * b);
+      b += 2;
+      if (b >= kSBufs) { b -= kSBufs; bph ^= 1; }
     }
     // ---------------- epilogue: W rows of this block, half of the slab per warpgroup -----
     if (mbar_wait(b_wfull, 0, abort)) {
