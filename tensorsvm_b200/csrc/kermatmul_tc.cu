@@ -1,7 +1,8 @@
 // Tensor-core fused kernel-block product for sm_100a: W = (Y K Y) A with tcgen05 + TMEM + TMA.
 //
 // Replaces rbf_kermatmul's XIJ SGEMM + rbf_kergen + K*A SGEMM (tensorsvm-train.cu:2476-2612)
-// with one kernel per 128-row block I of W that streams every 64-row block J of X and A:
+// with one persistent kernel whose CTAs take the 128-row blocks I of W in turn; for each it
+// streams every 64-row block J of X and A:
 //
 //   S_IJ  = XA_I XB_J^T              tcgen05.mma kind::f16, K = 64, accumulator in TMEM
 //   P_IJ  = exp2(S_IJ)                (exp warpgroups: tcgen05.ld -> ex2 -> f16 -> SMEM)
@@ -17,7 +18,7 @@
 // bare ex2.  Labels are folded into AT (AT[c][j] = s y_j A[j][c], s a power of two that keeps
 // FP16 away from its subnormal range) and into the final scaling of W's rows by y_i / s.
 //
-// Warp roles (384 threads): warp 0 loads XA and streams the Gram operands (6-deep ring, freed
+// Warp roles (384 threads): warp 0 loads XA per row block and streams the Gram operands (6-deep ring, freed
 // as soon as the Gram MMA completes), warp 10 streams the kernel-block operands (5-deep ring,
 // freed after P AT^T), warp 1 allocates TMEM and issues the Gram MMAs, warp 11 issues the
 // P AT^T MMAs, warps 2-5 and 6-9 are two exp warpgroups that take alternate J blocks.  S/P live
@@ -136,9 +137,6 @@ __device__ __forceinline__ void tma_load_2d(const CUtensorMap *map, uint32_t bar
 __device__ __forceinline__ void fence_barrier_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
-__device__ __forceinline__ void fence_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
 __device__ __forceinline__ void tc_fence_before() {
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 }
@@ -249,12 +247,19 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
 }
 
 // ---------------------------------------------------------------------------------------
-// The fused kernel.  grid.x = row blocks of 128; slab = columns [c0, c0 + kpw) of W.
+// The fused kernel, persistent: grid.x <= SM count, CTA c takes the 128-row blocks c, c + G,
+// c + 2G, ... (G = gridDim.x) in turn, and every CTA walks the J blocks in the same order, so
+// the CTAs of one round read the same XB/AT tiles at about the same time and those come from
+// L2 (one CTA per row block, launched in waves, spreads the CTAs over all of J and the ~0.6 GiB
+// operand set at n = 1M misses L2).  slab = columns [c0, c0 + kpw) of W.
 //
 // TMEM: four 64-column S/P buffers (columns 0..255) and the W accumulator (256..256+kpw).
-// J block t uses buffer t % 4: the Gram MMA writes S there, the exp warpgroup (t % 2) reads it
-// and writes P (FP16/BF16 pairs) back over its first 32 columns, and the second MMA reads P as
-// its A operand straight from TMEM.  The buffer is free again when that MMA completes.
+// Flat J block T (counted over all row blocks of the CTA) uses buffer T % 4: the Gram MMA
+// writes S there, the exp warpgroup (T % 2) reads it and writes P (FP16/BF16 pairs) back over
+// its first 32 columns, and the second MMA reads P as its A operand straight from TMEM.  The
+// buffer is free again when that MMA completes.  XA and W are single-buffered: the next row
+// block's XA is loaded once the last Gram MMA of the previous one completed (xaempty), and its
+// first P AT^T MMA waits for the epilogue to have read W out of TMEM (wempty).
 // ---------------------------------------------------------------------------------------
 constexpr int kSBufs = 4;
 
@@ -263,8 +268,8 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
 kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
                     const __grid_constant__ CUtensorMap map_xb,
                     const __grid_constant__ CUtensorMap map_at, const float *__restrict__ y,
-                    const float *__restrict__ inv_scale, int64_t n, int ntiles, int c0, int kpw,
-                    float *__restrict__ W, int64_t ldw, int *__restrict__ err) {
+                    const float *__restrict__ inv_scale, int64_t n, int nrb, int ntiles, int kp,
+                    int c0, int kpw, float *__restrict__ W, int64_t ldw, int *__restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   const uint32_t raw = su32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -279,14 +284,16 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
   const uint32_t b_sfull = b_atempty + 8 * kAtStages;    // [kSBufs] S written by the Gram MMA
   const uint32_t b_pfull = b_sfull + 8 * kSBufs;         // [kSBufs] P written by the exp warps
   const uint32_t b_free = b_pfull + 8 * kSBufs;          // [kSBufs] buffer consumed by P AT^T
-  const uint32_t b_wfull = b_free + 8 * kSBufs;          // W accumulation finished
-  const uint32_t b_xafull = b_wfull + 8;                 // XA loaded
+  const uint32_t b_wfull = b_free + 8 * kSBufs;          // W accumulation of a row block done
+  const uint32_t b_wempty = b_wfull + 8;                 // W read out by the epilogue
+  const uint32_t b_xafull = b_wempty + 8;                // XA loaded
+  const uint32_t b_xaempty = b_xafull + 8;               // last Gram MMA of a row block done
   uint32_t *tmem_slot =
-      reinterpret_cast<uint32_t *>(bars + 2 * kXbStages + 2 * kAtStages + 3 * kSBufs + 2);
+      reinterpret_cast<uint32_t *>(bars + 2 * kXbStages + 2 * kAtStages + 3 * kSBufs + 4);
   volatile int *abort = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t i0 = (int64_t)blockIdx.x * kBM;
+  const int G = gridDim.x;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kXbStages; ++s) {
@@ -303,7 +310,9 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
       mbar_init(b_free + 8 * b, 1);
     }
     mbar_init(b_wfull, 1);
+    mbar_init(b_wempty, 256);
     mbar_init(b_xafull, 1);
+    mbar_init(b_xaempty, 1);
     *abort = 0;
     fence_barrier_init();
   }
@@ -320,19 +329,23 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
   const uint32_t t_w = tmem + kSBufs * kBJ;   // W accumulator columns
 
   if (warp == 0) {
-    // ---------------- TMA producer: XA once, then the Gram operand ring ----------------
+    // ---------------- TMA producer: XA per row block, then its Gram operand ring ----------
     if (lane == 0) {
       asm volatile("prefetch.tensormap [%0];" ::"l"(&map_xa) : "memory");
       asm volatile("prefetch.tensormap [%0];" ::"l"(&map_xb) : "memory");
-      mbar_expect_tx(b_xafull, kXaBytes);
-      tma_load_2d(&map_xa, b_xafull, base + L.xa(), 0, (int)i0);
       int st = 0;
       uint32_t ph = 0;
-      for (int t = 0; t < ntiles; ++t) {
-        if (!mbar_wait(b_xbempty + 8 * st, ph ^ 1, abort)) break;
-        mbar_expect_tx(b_xbfull + 8 * st, kXbBytes);
-        tma_load_2d(&map_xb, b_xbfull + 8 * st, base + L.xb(st), 0, t * kBJ);
-        if (++st == kXbStages) { st = 0; ph ^= 1; }
+      bool ok = true;
+      for (int rb = blockIdx.x, r = 0; ok && rb < nrb; rb += G, ++r) {
+        if (r > 0 && !mbar_wait(b_xaempty, (r - 1) & 1, abort)) break;
+        mbar_expect_tx(b_xafull, kXaBytes);
+        tma_load_2d(&map_xa, b_xafull, base + L.xa(), 0, rb * kBM);
+        for (int t = 0; t < ntiles; ++t) {
+          if (!mbar_wait(b_xbempty + 8 * st, ph ^ 1, abort)) { ok = false; break; }
+          mbar_expect_tx(b_xbfull + 8 * st, kXbBytes);
+          tma_load_2d(&map_xb, b_xbfull + 8 * st, base + L.xb(st), 0, t * kBJ);
+          if (++st == kXbStages) { st = 0; ph ^= 1; }
+        }
       }
     }
   } else if (warp == 10) {
@@ -342,98 +355,117 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
       const uint32_t at_bytes = (uint32_t)kpw * kBJ * 2;
       int st = 0;
       uint32_t ph = 0;
-      for (int t = 0; t < ntiles; ++t) {
-        if (!mbar_wait(b_atempty + 8 * st, ph ^ 1, abort)) break;
-        mbar_expect_tx(b_atfull + 8 * st, at_bytes);
-        tma_load_2d(&map_at, b_atfull + 8 * st, base + L.at(st), t * kBJ, c0);
-        if (++st == kAtStages) { st = 0; ph ^= 1; }
+      bool ok = true;
+      for (int rb = blockIdx.x; ok && rb < nrb; rb += G) {
+        for (int t = 0; t < ntiles; ++t) {
+          if (!mbar_wait(b_atempty + 8 * st, ph ^ 1, abort)) { ok = false; break; }
+          mbar_expect_tx(b_atfull + 8 * st, at_bytes);
+          tma_load_2d(&map_at, b_atfull + 8 * st, base + L.at(st), 0, t * kp + c0);
+          if (++st == kAtStages) { st = 0; ph ^= 1; }
+        }
       }
     }
   } else if (warp == 1) {
-    // ---------------- Gram MMA issuer: S_t = XA XB_t^T into buffer t % 4 ----------------
+    // ---------------- Gram MMA issuer: S_T = XA XB_t^T into buffer T % 4 ----------------
     if (lane == 0) {
       constexpr uint32_t idg = idesc_f16(kBM, kBJ, 0);  // Gram: FP16 always
       const uint64_t dxa = desc_sw128(base + L.xa());
       const uint64_t dxb0 = desc_sw128(base + L.xb(0));
-      bool ok = mbar_wait(b_xafull, 0, abort);
       int st = 0, b = 0;
       uint32_t sph = 0, bph = 0;  // ring / buffer phase parities
-      for (int t = 0; ok && t < ntiles; ++t) {
-        if (!mbar_wait(b_xbfull + 8 * st, sph, abort)) break;
-        if (!mbar_wait(b_free + 8 * b, bph ^ 1, abort)) break;
-        tc_fence_after();
-        const uint64_t dxb = dxb0 + (uint64_t)((st * kXbBytes) >> 4);
+      bool ok = true;
+      for (int rb = blockIdx.x, r = 0; ok && rb < nrb; rb += G, ++r) {
+        if (!mbar_wait(b_xafull, r & 1, abort)) break;
+        for (int t = 0; t < ntiles; ++t) {
+          if (!mbar_wait(b_xbfull + 8 * st, sph, abort) ||
+              !mbar_wait(b_free + 8 * b, bph ^ 1, abort)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint64_t dxb = dxb0 + (uint64_t)((st * kXbBytes) >> 4);
 #pragma unroll
-        for (int kk = 0; kk < kKG / 16; ++kk)
-          umma(tmem + b * kBJ, dxa + 2 * kk, dxb + 2 * kk, idg, kk > 0 ? 1u : 0u);
-        umma_commit(b_sfull + 8 * b);
-        umma_commit(b_xbempty + 8 * st);
-        if (++st == kXbStages) { st = 0; sph ^= 1; }
-        if (++b == kSBufs) { b = 0; bph ^= 1; }
+          for (int kk = 0; kk < kKG / 16; ++kk)
+            umma(tmem + b * kBJ, dxa + 2 * kk, dxb + 2 * kk, idg, kk > 0 ? 1u : 0u);
+          umma_commit(b_sfull + 8 * b);
+          umma_commit(b_xbempty + 8 * st);
+          if (++st == kXbStages) { st = 0; sph ^= 1; }
+          if (++b == kSBufs) { b = 0; bph ^= 1; }
+        }
+        if (ok) umma_commit(b_xaempty);
       }
     }
   } else if (warp == 11) {
-    // ---------------- P AT^T issuer: W += P_t AT_t^T, P from TMEM ----------------
+    // ---------------- P AT^T issuer: W += P_T AT_t^T, P from TMEM ----------------
     if (lane == 0) {
       const uint32_t id2 = idesc_f16(kBM, kpw, BF16 ? 1u : 0u);
       const uint64_t dat0 = desc_sw128(base + L.at(0));
       const uint32_t at_step = L.at_bytes >> 4;
       int st = 0, b = 0;
       uint32_t sph = 0, bph = 0;
-      for (int t = 0; t < ntiles; ++t) {
-        if (!mbar_wait(b_atfull + 8 * st, sph, abort)) break;
-        if (!mbar_wait(b_pfull + 8 * b, bph, abort)) break;
+      bool ok = true;
+      for (int rb = blockIdx.x, r = 0; ok && rb < nrb; rb += G, ++r) {
+        if (r > 0 && !mbar_wait(b_wempty, (r - 1) & 1, abort)) break;
         tc_fence_after();
-        const uint64_t dat = dat0 + (uint64_t)(st * at_step);
-        const uint32_t ap = tmem + b * kBJ;
+        for (int t = 0; t < ntiles; ++t) {
+          if (!mbar_wait(b_atfull + 8 * st, sph, abort) ||
+              !mbar_wait(b_pfull + 8 * b, bph, abort)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint64_t dat = dat0 + (uint64_t)(st * at_step);
+          const uint32_t ap = tmem + b * kBJ;
 #pragma unroll
-        for (int kk = 0; kk < kBJ / 16; ++kk)
-          umma_ts(t_w, ap + kk * 8, dat + 2 * kk, id2, (t > 0 || kk > 0) ? 1u : 0u);
-        umma_commit(b_free + 8 * b);
-        umma_commit(b_atempty + 8 * st);
-        if (++st == kAtStages) { st = 0; sph ^= 1; }
-        if (++b == kSBufs) { b = 0; bph ^= 1; }
+          for (int kk = 0; kk < kBJ / 16; ++kk)
+            umma_ts(t_w, ap + kk * 8, dat + 2 * kk, id2, (t > 0 || kk > 0) ? 1u : 0u);
+          umma_commit(b_free + 8 * b);
+          umma_commit(b_atempty + 8 * st);
+          if (++st == kAtStages) { st = 0; sph ^= 1; }
+          if (++b == kSBufs) { b = 0; bph ^= 1; }
+        }
+        if (ok) umma_commit(b_wfull);
       }
-      umma_commit(b_wfull);
     }
   } else if (warp >= 2 && warp < 10) {
-    // ---------------- exp warpgroups ----------------
+    // ---------------- exp warpgroups, then the epilogue of each row block ----------------
     const int g = (warp - 2) >> 2;        // warpgroup 0: warps 2-5, 1: warps 6-9
     const int q = warp & 3;               // TMEM lane quarter this warp may access
     const int row = q * 32 + lane;        // row of the 128-row block (TMEM lane)
     const uint32_t lane_off = (uint32_t)(q * 32) << 16;
-    int b = g;
-    uint32_t bph = 0;
-    for (int t = g; t < ntiles; t += 2) {
-      if (!mbar_wait(b_sfull + 8 * b, bph, abort)) break;
-      tc_fence_after();
-      const uint32_t tb = tmem + b * kBJ + lane_off;
-      uint32_t s0[32], s1[32];
-      tmem_ld32(tb, s0);
-      tmem_ld32(tb + 32, s1);
-      tmem_wait_ld();
-      uint32_t pk[32];
+    const int half = kpw / 2;
+    bool ok = true;
+    for (int rb = blockIdx.x, r = 0; ok && rb < nrb; rb += G, ++r) {
+      const uint32_t T0 = (uint32_t)r * (uint32_t)ntiles;   // flat index of the first J block
+      for (uint32_t T = T0 + ((T0 & 1u) != (uint32_t)g ? 1u : 0u); T < T0 + (uint32_t)ntiles;
+           T += 2) {
+        const uint32_t b = T & (kSBufs - 1);
+        if (!mbar_wait(b_sfull + 8 * b, (T / kSBufs) & 1u, abort)) { ok = false; break; }
+        tc_fence_after();
+        const uint32_t tb = tmem + b * kBJ + lane_off;
+        uint32_t s0[32], s1[32];
+        tmem_ld32(tb, s0);
+        tmem_ld32(tb + 32, s1);
+        tmem_wait_ld();
+        uint32_t pk[32];
 #pragma unroll
-      for (int c = 0; c < 16; ++c)
-        pk[c] = pack2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c]), 2 * c),
-                            exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c + 1]), 2 * c + 1));
+        for (int c = 0; c < 16; ++c)
+          pk[c] = pack2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c]), 2 * c),
+                              exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c + 1]), 2 * c + 1));
 #pragma unroll
-      for (int c = 0; c < 16; ++c)
-        pk[16 + c] = pack2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c]), 2 * c),
-                                 exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c + 1]), 2 * c + 1));
-      tmem_st32(tb, pk);   // P over the first 32 columns of the buffer (S is no longer needed)
-      tmem_wait_st();
-      tc_fence_before();
-      mbar_arrive(b_pfull + 8 * b);
-      b += 2;
-      if (b >= kSBufs) { b -= kSBufs; bph ^= 1; }
-    }
-    // ---------------- epilogue: W rows of this block, half of the slab per warpgroup -----
-    if (mbar_wait(b_wfull, 0, abort)) {
+        for (int c = 0; c < 16; ++c)
+          pk[16 + c] = pack2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c]), 2 * c),
+                                   exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c + 1]), 2 * c + 1));
+        tmem_st32(tb, pk);   // P over the first 32 columns of the buffer (S is no longer needed)
+        tmem_wait_st();
+        tc_fence_before();
+        mbar_arrive(b_pfull + 8 * b);
+      }
+      // epilogue: W rows of this block, half of the slab per warpgroup
+      if (!ok || !mbar_wait(b_wfull, r & 1, abort)) break;
       tc_fence_after();
-      const int64_t gi = i0 + row;
+      const int64_t gi = (int64_t)rb * kBM + row;
       const float sc = gi < n ? y[gi] * inv_scale[0] : 0.f;
-      const int half = kpw / 2;
       for (int cc = g * half; cc < (g + 1) * half; cc += 32) {
         uint32_t v[32];
         tmem_ld32(t_w + cc + lane_off, v);
@@ -447,6 +479,8 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
                                  __uint_as_float(v[4 * j + 3]) * sc);
         }
       }
+      tc_fence_before();
+      mbar_arrive(b_wempty);
     }
   }
   tc_fence_before();
@@ -526,7 +560,11 @@ __global__ void choose_scale(const double *__restrict__ part, int nb, int64_t co
   scale[1] = ldexpf(1.f, -e);  // inverse, applied in the epilogue
 }
 
-// AT[c][j] = s * y_j * A[j][c] for c < kp, j < n; zeros for j in [n, n_pad).  32x32 tiles.
+// AT in J-block-major order: AT[t][c][jl] = s * y_j * A[j][c] with j = 64 t + jl, for c < kp,
+// j < n, and zeros for j in [n, n_pad).  Each J block's kernel-block operand is one contiguous
+// kp x 128-byte slab, so a TMA box touches one or two pages; with the plain [kp][n] layout a box
+// spans kp rows 2n bytes apart (256 pages at n = 1M), which overruns the address-translation
+// caches.  32x32 transpose tiles.
 template <typename T>
 __global__ void prep_at(const float *__restrict__ A, const float *__restrict__ y, int64_t n,
                         int64_t n_pad, int kp, const float *__restrict__ scale, T *__restrict__ AT) {
@@ -546,10 +584,11 @@ __global__ void prep_at(const float *__restrict__ A, const float *__restrict__ y
     const int c = c0 + r;
     const int64_t j = j0 + threadIdx.x;
     if (c < kp && j < n_pad) {
+      const int64_t o = ((j / kBJ) * kp + c) * kBJ + (j % kBJ);
       if constexpr (sizeof(T) == 2 && std::is_same<T, __half>::value)
-        AT[(int64_t)c * n_pad + j] = __float2half_rn(tile[threadIdx.x][r]);
+        AT[o] = __float2half_rn(tile[threadIdx.x][r]);
       else
-        AT[(int64_t)c * n_pad + j] = __float2bfloat16_rn(tile[threadIdx.x][r]);
+        AT[o] = __float2bfloat16_rn(tile[threadIdx.x][r]);
     }
   }
 }
@@ -590,7 +629,7 @@ bool make_map(CUtensorMap *map, const void *ptr, CUtensorMapDataType dt, uint64_
 }
 
 using TcKernel = void (*)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const float *,
-                          const float *, int64_t, int, int, int, float *, int64_t, int *);
+                          const float *, int64_t, int, int, int, int, int, float *, int64_t, int *);
 
 // Exps per 8 columns evaluated by the FMA-pipe polynomial (the rest on MUFU); tunable through
 // TSVM_TC_POLY (0, 2, 4, 6 or 8) for the autotuning sweep in the benchmarks.
@@ -662,20 +701,22 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
       !make_map(&mxb, XB, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, kKG, n_pad, 64, kBJ))
     return TSVM_ERR_CUDA;
   const int ntiles = (int)(n_pad / kBJ);
+  const int nrb = (int)(n_pad / kBM);
+  const unsigned grid = (unsigned)(nrb < ctx->num_sms ? nrb : ctx->num_sms);
   cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
   TSVM_CUDA(cudaEventRecord(e0, ctx->stream));
   for (int c0 = 0; c0 < kp; c0 += kMaxSlab) {
     const int kpw = kp - c0 < kMaxSlab ? kp - c0 : kMaxSlab;
     CUtensorMap mat;
     if (!make_map(&mat, AT, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
-                  n_pad, kp, kBJ, kpw))
+                  kBJ, (uint64_t)ntiles * kp, kBJ, kpw))
       return TSVM_ERR_CUDA;
     const SmemLayout L = smem_layout(kpw);
     const size_t smem = L.total + 1024;
     auto kern = select_kernel(bf16, poly_split());
     TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<(unsigned)(n_pad / kBM), kThreadsTC, smem, ctx->stream>>>(mxa, mxb, mat, y, scale + 1, n,
-                                                                     ntiles, c0, kpw, W, kp, err);
+    kern<<<grid, kThreadsTC, smem, ctx->stream>>>(mxa, mxb, mat, y, scale + 1, n, nrb, ntiles, kp,
+                                                  c0, kpw, W, kp, err);
     TSVM_LAUNCHED(ctx);
   }
   TSVM_CUDA(cudaEventRecord(e1, ctx->stream));
