@@ -83,8 +83,12 @@ typedef struct tsvm_ipm_options {
   double tol;             /* reference stop: mu, ||rd||, |rp| all < tol; default 1e-7 (T:1647) */
   double rel_gap_tol;     /* additional stop when rel_gap = (pobj-dobj)/max(1,|pobj|) <= tol
                              and ||rd||/(1+sqrt n), |rp|/(1+sqrt n) <= tol; <= 0 disables */
-  int32_t precision;      /* SYRK arithmetic: TSVM_PREC_FP32 or TSVM_PREC_BF16 */
-  int32_t refine_sweeps;  /* iterative-refinement sweeps per Newton direction (0..2) */
+  int32_t precision;      /* capacitance matrix M = I + Z^T D^-1 Z: TSVM_PREC_FP32 sums it
+                             exactly in FP64 (the reference's DSYRK); TSVM_PREC_BF16 or _FP16
+                             uses the tensor-core SYRK of a BF16 hi+lo split (FP32 accumulate)
+                             for the rows with small weight, FP64 for the rest (k <= 256) */
+  int32_t refine_sweeps;  /* mixed precision: refinement sweeps of every capacitance solve
+                             against the exact operator (1..2; 0 means 1) */
   int32_t kernel;         /* initialisation rule: TSVM_KERNEL_RBF (T:1535) or _LINEAR (T:1553) */
   int32_t verbose;        /* print the reference's "iter %d, mu=..." lines every 5 iterations */
 } tsvm_ipm_options;
@@ -95,6 +99,11 @@ typedef struct tsvm_ipm_stats {
   double mu, norm_rd, norm_rp, cond_d, pobj, dobj, rel_gap;
   double ms_total, ms_syrk, ms_factor, ms_streams;
   double t_rel_gap_1e6_ms; /* wall time at the first iterate with rel_gap <= 1e-6 (or -1) */
+  /* Mixed-precision capacitance matrix (precision BF16/FP16): 1 if used; iterations redone
+   * with more rows summed exactly; rows summed exactly in FP64 per iteration (max, mean); the
+   * largest relative residual of an unrefined capacitance solve. */
+  int32_t mixed_syrk, syrk_retries, exact_rows_max;
+  double exact_rows_mean, refine_res_max;
 } tsvm_ipm_stats;
 
 /* Human-readable status. */

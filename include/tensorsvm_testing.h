@@ -37,6 +37,13 @@ tsvm_status tsvm_test_gram(tsvm_context *ctx, const float *A, int64_t lda, const
                            int64_t ldb, int64_t n, int32_t ka, int32_t kb, int32_t symmetric,
                            const double *s, double *G);
 
+/* M (k x k fp64) = I + Z^T diag(dinv) Z by the mixed-precision path of the IPM: rows with
+ * dinv <= tau through the tensor-core SYRK of a `ways`-term (2 or 3) BF16 split, the others
+ * exactly in FP64; *exact_rows receives their count.  k <= 256. */
+tsvm_status tsvm_test_syrk_mixed(tsvm_context *ctx, const float *Z, int32_t ldz, int64_t n,
+                                 int32_t k, const double *dinv, double tau, int32_t ways,
+                                 double *M, int32_t *exact_rows);
+
 #ifdef __cplusplus
 }
 #endif

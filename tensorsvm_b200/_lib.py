@@ -43,7 +43,7 @@ EXPORTS = [
 ]
 TEST_EXPORTS = [
     "tsvm_test_rand_stream", "tsvm_test_sketch", "tsvm_test_kermatmul", "tsvm_test_chol",
-    "tsvm_test_potrs", "tsvm_test_eig", "tsvm_test_gram",
+    "tsvm_test_potrs", "tsvm_test_eig", "tsvm_test_gram", "tsvm_test_syrk_mixed",
 ]
 
 
@@ -72,7 +72,10 @@ class IpmStats(ctypes.Structure):
                 ("pobj", ctypes.c_double), ("dobj", ctypes.c_double),
                 ("rel_gap", ctypes.c_double), ("ms_total", ctypes.c_double),
                 ("ms_syrk", ctypes.c_double), ("ms_factor", ctypes.c_double),
-                ("ms_streams", ctypes.c_double), ("t_rel_gap_1e6_ms", ctypes.c_double)]
+                ("ms_streams", ctypes.c_double), ("t_rel_gap_1e6_ms", ctypes.c_double),
+                ("mixed_syrk", ctypes.c_int32), ("syrk_retries", ctypes.c_int32),
+                ("exact_rows_max", ctypes.c_int32), ("exact_rows_mean", ctypes.c_double),
+                ("refine_res_max", ctypes.c_double)]
 
 
 _lib = None
@@ -125,6 +128,7 @@ def load() -> ctypes.CDLL:
         "tsvm_test_potrs": [P, P, I32, P, I32, I32],
         "tsvm_test_eig": [P, P, I32, P, P, ctypes.POINTER(I32)],
         "tsvm_test_gram": [P, P, I64, P, I64, I64, I32, I32, I32, P, P],
+        "tsvm_test_syrk_mixed": [P, P, I32, I64, I32, P, D, I32, P, ctypes.POINTER(I32)],
     }.items():
         fn = getattr(lib, name)
         fn.restype = ctypes.c_int

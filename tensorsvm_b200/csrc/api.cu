@@ -147,7 +147,7 @@ void tsvm_ipm_default_options(tsvm_ipm_options *opt) {
   opt->tol = 1e-7;
   opt->rel_gap_tol = 0.0;
   opt->precision = TSVM_PREC_FP32;
-  opt->refine_sweeps = 0;
+  opt->refine_sweeps = 1;
   opt->kernel = TSVM_KERNEL_RBF;
   opt->verbose = 0;
 }

@@ -29,7 +29,10 @@ enum Slot : int {
   SLOT_IPM_VEC,       // IPM fp64 vectors
   SLOT_IPM_SCAL,      // IPM device scalars
   SLOT_IPM_M,         // IPM capacitance matrix + factor
-  SLOT_IPM_ZH,        // IPM low-precision copy of Z (bf16)
+  SLOT_SYRK_OP,       // IPM: BF16 split operand of the tensor-core SYRK
+  SLOT_SYRK_PART,     // IPM: per-CTA FP32 partial Gram matrices of the tensor-core SYRK
+  SLOT_SYRK_CNT,      // IPM: per-block counts of the exactly summed (large-weight) rows
+  SLOT_IPM_IDX,       // IPM: indices of the exactly summed rows
   SLOT_IPM_PART,      // IPM / bias streaming partial sums (kept apart from SLOT_PART, which the
                       // Z^T D^-1 Z accumulation may regrow inside the iteration)
   SLOT_MISC,

@@ -30,7 +30,7 @@ enum ScalarIdx : int {
   I_C = 0, I_N, I_Y, I_MU, I_RP, I_DMAX, I_DMIN, I_COND, I_SUMX, I_SUMXI,
   I_NORMRD, I_XQX, I_POBJ, I_DOBJ, I_RELGAP,
   I_ATR7, I_ATB, I_DYA, I_ALPHA_AFF, I_MUAFF, I_SIGMA, I_ATR7C, I_DYC, I_ALPHA,
-  I_E2SUM, I_E2SQ, I_INFO, I_COUNT
+  I_E2SUM, I_E2SQ, I_INFO, I_RESMAX, I_RESPREV, I_COUNT
 };
 constexpr int kNScal = 32;
 
@@ -476,6 +476,144 @@ vec_kernel(int64_t n, Op op, const double *__restrict__ scal, double *__restrict
   if (NS + NM > 0) block_partials<NS, NM>(sums, mins, part_s, vsh);
 }
 
+// Refinement pass: w_r = Z^T D^-1 (Z g_r) for R vectors g_r (kz apart) in one read of Z.  Per
+// row the dot products z . g_r are reduced over the LPR lanes that hold the row, scaled by
+// dinv, and accumulated into the lanes' column sums (FP64, block partials as in zt_kernel).
+template <int R, int LPR, int CPL>
+__global__ void __launch_bounds__(kThreads)
+zgz_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n,
+           const double *__restrict__ dinv, const double *__restrict__ g, int kz,
+           double *__restrict__ part_vec) {
+  constexpr int RPW = 32 / LPR;
+  constexpr int NC = CPL * 4;
+  extern __shared__ double zsh[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int slot = lane / LPR, sl = lane % LPR;
+  double gr[NC][R], acc[NC][R];
+#pragma unroll
+  for (int c = 0; c < CPL; ++c)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int col = 4 * (sl + c * LPR) + q;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        gr[4 * c + q][r] = col < k ? g[r * kz + col] : 0.0;
+        acc[4 * c + q][r] = 0.0;
+      }
+    }
+  const int64_t gw = (int64_t)blockIdx.x * kWarps + warp;
+  const int64_t stride = (int64_t)gridDim.x * kWarps * 32;
+  for (int64_t base = gw * 32; base < n; base += stride) {
+#pragma unroll 2
+    for (int step = 0; step < 32 / RPW; ++step) {
+      const int64_t row = base + step * RPW + slot;
+      if (row < n) {
+        const float4 *zr = reinterpret_cast<const float4 *>(Z + row * ldz);
+        float4 z[CPL];
+        double d[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) d[r] = 0.0;
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) {
+          const int gq = sl + c * LPR;
+          z[c] = 4 * gq < k ? __ldg(zr + gq) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            d[r] = fma((double)z[c].x, gr[4 * c + 0][r], d[r]);
+            d[r] = fma((double)z[c].y, gr[4 * c + 1][r], d[r]);
+            d[r] = fma((double)z[c].z, gr[4 * c + 2][r], d[r]);
+            d[r] = fma((double)z[c].w, gr[4 * c + 3][r], d[r]);
+          }
+        }
+        const double di = dinv[row];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+#pragma unroll
+          for (int o = LPR / 2; o > 0; o >>= 1) d[r] += __shfl_xor_sync(0xffffffffu, d[r], o);
+          d[r] *= di;
+        }
+#pragma unroll
+        for (int c = 0; c < CPL; ++c)
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            acc[4 * c + 0][r] = fma((double)z[c].x, d[r], acc[4 * c + 0][r]);
+            acc[4 * c + 1][r] = fma((double)z[c].y, d[r], acc[4 * c + 1][r]);
+            acc[4 * c + 2][r] = fma((double)z[c].z, d[r], acc[4 * c + 2][r]);
+            acc[4 * c + 3][r] = fma((double)z[c].w, d[r], acc[4 * c + 3][r]);
+          }
+      }
+    }
+  }
+  const int ncol = LPR * NC;
+  double *red = zsh;  // [kWarps*RPW][R][ncol]
+#pragma unroll
+  for (int c = 0; c < CPL; ++c)
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+        red[((warp * RPW + slot) * R + r) * ncol + 4 * (sl + c * LPR) + q] = acc[4 * c + q][r];
+  __syncthreads();
+  for (int e = threadIdx.x; e < R * kz; e += kThreads) {
+    const int r = e / kz, col = e % kz;
+    double sum = 0.0;
+    if (col < ncol)
+      for (int ws = 0; ws < kWarps * RPW; ++ws) sum += red[(ws * R + r) * ncol + col];
+    part_vec[(int64_t)blockIdx.x * R * kz + e] = sum;
+  }
+}
+
+// c = h0 - (g + w) (the residual h0 - M g of the capacitance solve, M g = g + Z^T D^-1 Z g);
+// with `record`, the relative residual max_r ||c_r|| / ||h0_r|| goes into I_RESMAX, and a value
+// above 0.5 (refinement cannot be trusted to converge) marks the iteration as failed.
+__global__ void refine_resid_kernel(const double *__restrict__ h0, const double *__restrict__ g,
+                                    const double *__restrict__ w, double *__restrict__ c, int R,
+                                    int kz, int k, double *__restrict__ sc, int *__restrict__ info,
+                                    int record) {
+  __shared__ double red[2][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double worst = 0.0;
+  for (int r = 0; r < R; ++r) {
+    double sc2 = 0.0, sh2 = 0.0;
+    for (int e = threadIdx.x; e < kz; e += blockDim.x) {
+      const int i = r * kz + e;
+      const double v = e < k ? h0[i] - (g[i] + w[i]) : 0.0;
+      c[i] = v;
+      sc2 += v * v;
+      sh2 += h0[i] * h0[i];
+    }
+    sc2 = warp_sum(sc2);
+    sh2 = warp_sum(sh2);
+    if (lane == 0) {
+      red[0][warp] = sc2;
+      red[1][warp] = sh2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double a = 0.0, b = 0.0;
+      for (int j = 0; j < (int)(blockDim.x >> 5); ++j) {
+        a += red[0][j];
+        b += red[1][j];
+      }
+      const double rel = b > 0.0 ? sqrt(a / b) : 0.0;
+      worst = fmax(worst, isfinite(rel) ? rel : INFINITY);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && record) {
+    sc[I_RESMAX] = fmax(sc[I_RESMAX], worst);
+    if (!(worst <= 0.5)) {
+      *info = -1;
+      sc[I_INFO] = -1.0;
+    }
+  }
+}
+
+__global__ void kvec_add(double *__restrict__ g, const double *__restrict__ c, int count) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < count) g[e] += c[e];
+}
+
 // Sum block partials in fixed order; the last block also reduces the scalars and runs the
 // scalar stage of the iteration.
 __global__ void finalize_kernel(const double *__restrict__ part_vec, int nblk, int nvec,
@@ -512,6 +650,8 @@ __global__ void finalize_kernel(const double *__restrict__ part_vec, int nblk, i
       sc[I_E2SQ] = red[1];
       break;
     case ST_BEGIN:
+      sc[I_RESPREV] = sc[I_RESMAX];
+      sc[I_RESMAX] = 0.0;
       sc[I_MU] = red[0] / (2.0 * n);
       sc[I_SUMX] = red[1];
       sc[I_SUMXI] = red[2];
@@ -591,6 +731,7 @@ struct Runner {
   double *scal;       // device scalars
   double *part_vec, *part_s;
   int *info;
+  const double *dinv;
 
   template <class Op, int LPR, int CPL>
   tsvm_status zt_launch(const Op &op, double *out_vec, int stage) {
@@ -636,6 +777,46 @@ struct Runner {
     }
     return TSVM_ERR_UNSUPPORTED;
   }
+  template <int R, int LPR, int CPL>
+  tsvm_status zgz_launch(const double *g, double *w) {
+    constexpr int RPW = 32 / LPR;
+    const size_t smem_red = sizeof(double) * (size_t)kWarps * RPW * R * LPR * CPL * 4;
+    auto kern = zgz_kernel<R, LPR, CPL>;
+    if (smem_red > 48 * 1024)
+      TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem_red));
+    kern<<<nblk, kThreads, smem_red, ctx->stream>>>(Z, ldz, k, n, dinv, g, geo.kz, part_vec);
+    TSVM_LAUNCHED(ctx);
+    return finalize(R * geo.kz, w, 0, 0, ST_NONE);
+  }
+  template <int R>
+  tsvm_status zgz(const double *g, double *w) {
+    switch (geo.lpr * 10 + geo.cpl) {
+      case 81: return zgz_launch<R, 8, 1>(g, w);
+      case 161: return zgz_launch<R, 16, 1>(g, w);
+      case 321: return zgz_launch<R, 32, 1>(g, w);
+      case 322: return zgz_launch<R, 32, 2>(g, w);
+      case 324: return zgz_launch<R, 32, 4>(g, w);
+      case 328: return zgz_launch<R, 32, 8>(g, w);
+    }
+    return TSVM_ERR_UNSUPPORTED;
+  }
+  // Iterative refinement of the capacitance solve M g = h0 against the exact M (M~ factored in
+  // M_fac): per sweep one pass over Z for w = Z^T D^-1 Z g, then g += M~^-1 (h0 - g - w).
+  template <int R>
+  tsvm_status refine(const double *M_fac, const double *h0, double *g, double *w, double *c,
+                     int sweeps) {
+    for (int sweep = 0; sweep < sweeps; ++sweep) {
+      TSVM_TRY(zgz<R>(g, w));
+      refine_resid_kernel<<<1, 256, 0, ctx->stream>>>(h0, g, w, c, R, geo.kz, k, scal, info,
+                                                        sweep == 0 ? 1 : 0);
+      TSVM_LAUNCHED(ctx);
+      TSVM_TRY(potrs_fp64(ctx, M_fac, k, k, c, R, geo.kz));
+      kvec_add<<<(unsigned)ceil_div(R * geo.kz, 256), 256, 0, ctx->stream>>>(g, c, R * geo.kz);
+      TSVM_LAUNCHED(ctx);
+    }
+    return TSVM_OK;
+  }
   template <class Op>
   tsvm_status vec(const Op &op, int stage) {
     vec_kernel<Op><<<nblk, kThreads, 0, ctx->stream>>>(n, op, scal, part_s);
@@ -672,7 +853,7 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
 
   double *vecbuf = nullptr, *sbuf = nullptr, *M = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_IPM_VEC, (size_t)11 * n, &vecbuf));
-  TSVM_TRY(scratch_t(ctx, SLOT_IPM_SCAL, (size_t)kNScal + 8 * (size_t)kz + 64, &sbuf));
+  TSVM_TRY(scratch_t(ctx, SLOT_IPM_SCAL, (size_t)kNScal + 10 * (size_t)kz + 64, &sbuf));
   TSVM_TRY(scratch_t(ctx, SLOT_IPM_M, (size_t)k * k, &M));
   double *part = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_IPM_PART, (size_t)run.nblk * (2 * kz + 16), &part));
@@ -681,7 +862,11 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
   run.scal = sbuf;
   double *q = sbuf + kNScal;          // kz
   double *h = q + kz;                  // 2 x kz (right-hand sides, then solutions)
-  run.info = reinterpret_cast<int *>(h + 2 * kz + 4 * kz);
+  double *h0 = h + 2 * kz;             // 2 x kz copy of the right-hand sides (refinement)
+  double *wv = h0 + 2 * kz;            // 2 x kz  Z^T D^-1 Z g
+  double *cv = wv + 2 * kz;            // 2 x kz  residual / correction
+  run.info = reinterpret_cast<int *>(cv + 2 * kz);   // [0] Cholesky/refinement status,
+  int *big_count = run.info + 1;                     // [1] rows summed exactly in FP64
 
   Vecs V;
   V.x = vecbuf;
@@ -696,6 +881,24 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
   V.ds = V.dx + n;
   V.dxi = V.ds + n;
   V.a = y;
+  run.dinv = V.dinv;
+
+  // Mixed-precision capacitance matrix: tensor-core SYRK of the rows with dinv <= tau, exact
+  // FP64 sum of the others, refinement of every solve against the exact operator.  tau adapts
+  // to the refinement residual of the previous iteration.
+  const bool mixed = opt.precision != TSVM_PREC_FP32 && syrk_tc_supported(k) && k >= 32;
+  const int sweeps = mixed ? std::max(1, std::min(2, (int)opt.refine_sweeps)) : 0;
+  double tau = 64.0;
+  int64_t *big_idx = nullptr;
+  double *G64 = nullptr;
+  if (mixed) {
+    TSVM_TRY(scratch_t(ctx, SLOT_IPM_IDX, (size_t)n + 8, &big_idx));
+    TSVM_TRY(scratch_t(ctx, SLOT_SMALL3, (size_t)k * k, &G64));
+  }
+  int host_info[2] = {0, 0};
+  int64_t exact_rows_sum = 0;
+  int exact_rows_max = 0, syrk_retries = 0, mixed_iters = 0;
+  double res_max = 0.0;
 
   double hsc[kNScal] = {0};
   hsc[I_C] = C;
@@ -750,6 +953,9 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
     TSVM_TRY(run.zw(ResidOp{V, 0.0}, q, ST_RESID));
     TSVM_CUDA(cudaMemcpyAsync(ctx->host_scalars, run.scal, sizeof(double) * kNScal,
                               cudaMemcpyDeviceToHost, ctx->stream));
+    if (mixed)
+      TSVM_CUDA(cudaMemcpyAsync(host_info, run.info, sizeof(host_info), cudaMemcpyDeviceToHost,
+                                ctx->stream));
     TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
     memcpy(sc, ctx->host_scalars, sizeof(sc));
     if (pending_events) {
@@ -757,13 +963,33 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
       ms_factor += event_ms(ev_syrk1, ev_chol1);
       pending_events = false;
     }
-    if (iter > 0 && sc[I_INFO] != 0.0) {  // Cholesky failed in the previous iteration
-      if (opt.verbose)
-        printf("Cholesky fact info error %d; solver becomes unstable. Terminate.\n",
-               (int)sc[I_INFO]);
-      result = TSVM_ERR_NOT_SPD;
-      break;
+    bool retry = false;
+    if (mixed && iter > 0) {  // bookkeeping of the previous iteration's mixed SYRK
+      exact_rows_sum += host_info[1];
+      exact_rows_max = std::max(exact_rows_max, host_info[1]);
+      ++mixed_iters;
+      if (sc[I_INFO] == 0.0) res_max = std::max(res_max, sc[I_RESPREV]);
     }
+    if (iter > 0 && sc[I_INFO] != 0.0) {  // Cholesky (or refinement) failed last iteration
+      if (mixed && tau > 0.0) {
+        // the step was not taken: redo the iteration with more rows summed exactly
+        ++syrk_retries;
+        tau = tau > 1e-6 ? tau / 64.0 : 0.0;
+        retry = true;
+        if (opt.verbose) printf("mixed SYRK: retry with tau=%.3e\n", tau);
+      } else {
+        if (opt.verbose)
+          printf("Cholesky fact info error %d; solver becomes unstable. Terminate.\n",
+                 (int)sc[I_INFO]);
+        result = TSVM_ERR_NOT_SPD;
+        break;
+      }
+    } else if (mixed && iter > 0) {
+      const double r = sc[I_RESPREV];
+      if (r > 1e-4) tau /= 8.0;
+      else if (r < 1e-6 && tau < 1e30) tau *= 2.0;
+    }
+    (void)retry;
     const double mu = sc[I_MU], nrd = sc[I_NORMRD], nrp = fabs(sc[I_RP]), cond = sc[I_COND];
     if (t_gap < 0 && sc[I_RELGAP] <= 1e-6) {
       const double scale = 1.0 + sqrt((double)n);
@@ -801,21 +1027,35 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
     }
     // M = I + Z^T D^-1 Z (FP64 accumulation), Cholesky (T:1674-1714)
     TSVM_CUDA(cudaEventRecord(ev_syrk0, ctx->stream));
-    TSVM_TRY(gram_fp64(ctx, Z, ldz, Z, ldz, n, k, k, true, M, V.dinv));
-    TSVM_TRY(small_add_diag(ctx, M, k, k, 1.0));
+    if (mixed) {
+      TSVM_TRY(big_rows(ctx, V.dinv, n, tau, big_idx, big_count));
+      TSVM_TRY(gram_fp64_rows(ctx, Z, ldz, n, k, big_idx, big_count, V.dinv, G64));
+      TSVM_TRY(syrk_capacitance_tc(ctx, Z, ldz, n, k, V.dinv, tau, 2, G64, M));
+    } else {
+      TSVM_TRY(gram_fp64(ctx, Z, ldz, Z, ldz, n, k, k, true, M, V.dinv));
+      TSVM_TRY(small_add_diag(ctx, M, k, k, 1.0));
+    }
     TSVM_CUDA(cudaEventRecord(ev_syrk1, ctx->stream));
     TSVM_TRY(chol_fp64(ctx, M, k, k, run.info));
     TSVM_CUDA(cudaEventRecord(ev_chol1, ctx->stream));
     pending_events = true;
     // predictor: r7 = SMW(r5), b = SMW(a) in one pair of passes
     TSVM_TRY(run.zt(SmwRhs2Op{V}, h, ST_NONE));
+    if (sweeps)
+      TSVM_CUDA(cudaMemcpyAsync(h0, h, sizeof(double) * 2 * kz, cudaMemcpyDeviceToDevice,
+                                ctx->stream));
     TSVM_TRY(potrs_fp64(ctx, M, k, k, h, 2, kz));
+    if (sweeps) TSVM_TRY(run.refine<2>(M, h0, h, wv, cv, sweeps));
     TSVM_TRY(run.zw(SmwBack2Op{V}, h, ST_DYA));
     TSVM_TRY(run.vec(AffineOp{V, C, 0.0}, ST_ALPHA_AFF));
     TSVM_TRY(run.vec(MuAffOp{V, C, 0.0}, ST_SIGMA));
     // corrector
     TSVM_TRY(run.zt(CorrRhsOp{V, C, 0.0}, h, ST_NONE));
+    if (sweeps)
+      TSVM_CUDA(cudaMemcpyAsync(h0, h, sizeof(double) * kz, cudaMemcpyDeviceToDevice,
+                                ctx->stream));
     TSVM_TRY(potrs_fp64(ctx, M, k, k, h, 1, kz));
+    if (sweeps) TSVM_TRY(run.refine<1>(M, h0, h, wv, cv, sweeps));
     TSVM_TRY(run.zw(CorrBackOp{V}, h, ST_DYC));
     TSVM_TRY(run.vec(CombineOp{V, C, 0.0, 0.0}, ST_ALPHA));
     TSVM_TRY(run.vec(UpdateOp{V, 0.0, true}, ST_NONE));
@@ -848,6 +1088,11 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
     stats->ms_factor = ms_factor;
     stats->ms_streams = stats->ms_total - ms_syrk - ms_factor;
     stats->t_rel_gap_1e6_ms = t_gap;
+    stats->mixed_syrk = mixed ? 1 : 0;
+    stats->syrk_retries = syrk_retries;
+    stats->exact_rows_max = exact_rows_max;
+    stats->exact_rows_mean = mixed_iters ? (double)exact_rows_sum / mixed_iters : 0.0;
+    stats->refine_res_max = res_max;
   }
   return result;
 }

@@ -47,6 +47,11 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
 tsvm_status gram_fp64(tsvm_context *ctx, const float *A, int64_t lda, const float *B,
                       int64_t ldb, int64_t n, int ka, int kb, bool symmetric, double *G,
                       const double *rowscale = nullptr);
+// G (k x k, fp64) = sum over the rows listed in rowidx[0 .. *count_dev) of rowscale[i] a_i a_i^T
+// (count read on the device, at most n_max rows).
+tsvm_status gram_fp64_rows(tsvm_context *ctx, const float *A, int64_t lda, int64_t n_max, int k,
+                           const int64_t *rowidx, const int *count_dev, const double *rowscale,
+                           double *G);
 // Out (n x kp) = A (n x kp) * R (kp x kp, fp32 row-major). Out may alias A.
 tsvm_status apply_right_fp32(tsvm_context *ctx, const float *A, int64_t n, int kp,
                              const float *R, float *Out);
@@ -67,6 +72,18 @@ tsvm_status eig_jacobi_fp64(tsvm_context *ctx, double *A, int n, int lda, double
 // Elementwise helpers on small matrices (device kernels, defined in dense.cu).
 tsvm_status small_add_diag(tsvm_context *ctx, double *A, int n, int lda, double shift);
 tsvm_status small_symmetrize(tsvm_context *ctx, double *A, int n, int lda);
+
+// ---- syrk_tc.cu ------------------------------------------------------------------------
+bool syrk_tc_supported(int k);
+// idx[0 .. *count_dev) = the rows with dinv > tau, in increasing order.
+tsvm_status big_rows(tsvm_context *ctx, const double *dinv, int64_t n, double tau, int64_t *idx,
+                     int *count_dev);
+// M (k x k, fp64, full) = I + G64 + sum over rows with dinv <= tau of dinv_j z_j z_j^T, the
+// latter from a `ways`-term BF16 split on the tensor cores with FP32 accumulation.  G64 may be
+// null.  A timed-out tensor-core launch leaves NaN in M (the Cholesky then reports failure).
+tsvm_status syrk_capacitance_tc(tsvm_context *ctx, const float *Z, int ldz, int64_t n, int k,
+                                const double *dinv, double tau, int ways, const double *G64,
+                                double *M);
 
 // ---- ipm.cu ----------------------------------------------------------------------------
 tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y, int64_t n,

@@ -1,0 +1,355 @@
+// Mixed-precision Gram of the SMW capacitance matrix, M = I + Z^T D^-1 Z, on the tensor cores.
+//
+// Replaces the DSYRK of mpc (tensorsvm-train.cu:1674-1697, FP64 on host or cublasDsyrk).  Rows
+// are split by their weight dinv_j = 1/D_j:
+//   * rows with dinv_j <= tau: z~_j = sqrt(dinv_j) z_j is split into WAYS BF16 terms
+//     (hi = bf16(z~), lo = bf16(z~ - hi), ...) and G_tc = sum_{a+b<WAYS} P_a^T P_b is
+//     accumulated by tcgen05 MMAs in FP32 (TMEM), per CTA over a contiguous range of rows;
+//   * rows with dinv_j > tau (in late iterations the free support vectors, whose weights grow
+//     like 1/mu and would dominate the FP32 rounding) are gathered in index order and summed
+//     exactly in FP64 (gram_fp64_rows);
+// and M = I + G_tc + G_64 is reduced in FP64 in a fixed order.  The IPM refines every SMW
+// solve against the exact operator (one extra pass over Z) and adapts tau from the observed
+// residual, so M only has to be a good preconditioner.
+//
+// TC kernel: persistent CTAs (one per SM), each streams its row chunks of 64 rows; per chunk
+// WAYS tiles [KP rows][64 cols] BF16, K-major with the 128-byte swizzle, arrive by TMA and
+// feed 128 x N x 16 MMAs for the lower block strips (rows 0-127 x cols 0-127, rows 128-255 x
+// cols 0-255).  Warp 0 issues TMA, warp 1 owns TMEM and issues MMAs, warps 2-5 drain the
+// FP32 accumulators to per-CTA partials.  All waits are bounded.
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "context.h"
+#include "kernels.h"
+#include "tc_common.cuh"
+
+namespace tsvm {
+namespace {
+
+using namespace tc;
+
+constexpr int kSJ = 64;              // rows of Z per chunk (MMA K of one chunk, 4 x 16)
+constexpr int kSyrkThreads = 192;
+
+template <int WAYS, int KP>
+struct SyrkCfg {
+  static constexpr uint32_t kTile = KP * kSJ * 2;          // bytes of one part tile
+  static constexpr uint32_t kStage = WAYS * kTile;
+  static constexpr int kStages = (200 * 1024) / kStage > 4 ? 4 : (200 * 1024) / kStage;
+  static constexpr int kSegs = KP / 128;                   // 128-row strips of the output
+  static constexpr uint32_t kTmemCols = KP == 256 ? 512 : 128;
+  static constexpr uint32_t kBars = kStages * kStage;      // barrier area offset
+  static constexpr uint32_t kSmem = kBars + 256 + 1024;    // + alignment slack
+};
+
+// parts[w][t][c][jl] (BF16): WAYS-term split of sqrt(dinv_j) Z[j][c], j = 64 t + jl; zero for
+// rows with dinv_j > tau, rows j >= n and columns c >= k.  grid (T, KP / 32), block (32, 8).
+template <int WAYS>
+__global__ void __launch_bounds__(256)
+syrk_prep(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, int64_t T, int KP,
+          const double *__restrict__ dinv, double tau, __nv_bfloat16 *__restrict__ parts) {
+  __shared__ float tile[kSJ][33];
+  __shared__ float wrow[kSJ];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+  const int64_t t = blockIdx.x;
+  const int c0 = blockIdx.y * 32;
+  if (tid < kSJ) {
+    const int64_t j = t * kSJ + tid;
+    float w = 0.f;
+    if (j < n) {
+      const double d = dinv[j];
+      if (d <= tau) w = (float)sqrt(d);
+    }
+    wrow[tid] = w;
+  }
+  __syncthreads();
+  for (int r = ty; r < kSJ; r += 8) {
+    const int64_t j = t * kSJ + r;
+    const int c = c0 + tx;
+    float v = 0.f;
+    const float w = wrow[r];
+    if (w != 0.f && c < k) v = Z[j * ldz + c] * w;
+    tile[r][tx] = v;
+  }
+  __syncthreads();
+  const size_t part_stride = (size_t)T * KP * kSJ;
+  for (int cc = ty; cc < 32; cc += 8) {
+    const int c = c0 + cc;
+    float v0 = tile[2 * tx][cc], v1 = tile[2 * tx + 1][cc];
+    __nv_bfloat162 *dst =
+        reinterpret_cast<__nv_bfloat162 *>(parts + ((size_t)t * KP + c) * kSJ) + tx;
+#pragma unroll
+    for (int w = 0; w < WAYS; ++w) {
+      const __nv_bfloat162 h = __floats2bfloat162_rn(v0, v1);
+      dst[w * part_stride / 2] = h;
+      v0 -= __low2float(h);
+      v1 -= __high2float(h);
+    }
+  }
+}
+
+template <int WAYS, int KP>
+__global__ void __launch_bounds__(kSyrkThreads, 1)
+syrk_tc_kernel(const __grid_constant__ CUtensorMap map, int T, float *__restrict__ part,
+               int *__restrict__ err) {
+  using Cfg = SyrkCfg<WAYS, KP>;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  const uint32_t raw = su32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t *sbase = smem_raw + (base - raw);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sbase + Cfg::kBars);
+  const uint32_t b_full = su32(bars);                    // [kStages]
+  const uint32_t b_empty = b_full + 8 * Cfg::kStages;    // [kStages]
+  const uint32_t b_done = b_empty + 8 * Cfg::kStages;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * Cfg::kStages + 1);
+  volatile int *abort = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int G = gridDim.x;
+  const int t0 = (int)((int64_t)T * blockIdx.x / G), t1 = (int)((int64_t)T * (blockIdx.x + 1) / G);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < Cfg::kStages; ++s) {
+      mbar_init(b_full + 8 * s, 1);
+      mbar_init(b_empty + 8 * s, 1);
+    }
+    mbar_init(b_done, 1);
+    *abort = 0;
+    fence_barrier_init();
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     su32(tmem_slot)),
+                 "r"(Cfg::kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      asm volatile("prefetch.tensormap [%0];" ::"l"(&map) : "memory");
+      int st = 0;
+      uint32_t ph = 0;
+      for (int t = t0; t < t1; ++t) {
+        if (!mbar_wait(b_empty + 8 * st, ph ^ 1, abort)) break;
+        mbar_expect_tx(b_full + 8 * st, Cfg::kStage);
+        const uint32_t dst = base + st * Cfg::kStage;
+#pragma unroll
+        for (int w = 0; w < WAYS; ++w)
+          tma_load_2d(&map, b_full + 8 * st, dst + w * Cfg::kTile, 0, (w * T + t) * KP);
+        if (++st == Cfg::kStages) { st = 0; ph ^= 1; }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint64_t d0 = desc_sw128(base);
+      int st = 0;
+      uint32_t ph = 0;
+      bool first = true, ok = true;
+      for (int t = t0; t < t1; ++t) {
+        if (!mbar_wait(b_full + 8 * st, ph, abort)) { ok = false; break; }
+        tc_fence_after();
+        const uint64_t ds = d0 + (uint64_t)((st * Cfg::kStage) >> 4);
+#pragma unroll
+        for (int a = 0; a < WAYS; ++a)
+#pragma unroll
+          for (int b = 0; a + b < WAYS; ++b)
+#pragma unroll
+            for (int mb = 0; mb < Cfg::kSegs; ++mb) {
+              const uint32_t idesc = idesc_f16(128, (mb + 1) * 128, 1u);
+              const uint64_t da = ds + (uint64_t)((a * Cfg::kTile + mb * 128 * 128) >> 4);
+              const uint64_t db = ds + (uint64_t)((b * Cfg::kTile) >> 4);
+              const uint32_t dt = tmem + (mb == 0 ? 0u : 128u);
+#pragma unroll
+              for (int kk = 0; kk < kSJ / 16; ++kk)
+                umma(dt, da + 2 * kk, db + 2 * kk, idesc,
+                     (first && a == 0 && b == 0 && kk == 0) ? 0u : 1u);
+            }
+        first = false;
+        umma_commit(b_empty + 8 * st);
+        if (++st == Cfg::kStages) { st = 0; ph ^= 1; }
+      }
+      if (ok) umma_commit(b_done);
+    }
+  } else {
+    // epilogue: warps 2-5, lane quarter q = warp % 4
+    const int q = warp & 3;
+    const uint32_t lane_off = (uint32_t)(q * 32) << 16;
+    const bool have = t1 > t0;
+    if (!have || mbar_wait(b_done, 0, abort)) {
+      tc_fence_after();
+      float *P = part + (size_t)blockIdx.x * KP * KP;
+#pragma unroll
+      for (int mb = 0; mb < Cfg::kSegs; ++mb) {
+        const int r = mb * 128 + q * 32 + lane;
+        const uint32_t tcol = tmem + (mb == 0 ? 0u : 128u);
+        for (int c0 = 0; c0 < (mb + 1) * 128; c0 += 32) {
+          uint32_t v[32];
+          if (have) {
+            tmem_ld32(tcol + c0 + lane_off, v);
+            tmem_wait_ld();
+          } else {
+#pragma unroll
+            for (int i = 0; i < 32; ++i) v[i] = 0u;
+          }
+          float4 *dst = reinterpret_cast<float4 *>(P + (size_t)r * KP + c0);
+#pragma unroll
+          for (int i = 0; i < 8; ++i)
+            dst[i] = make_float4(__uint_as_float(v[4 * i]), __uint_as_float(v[4 * i + 1]),
+                                 __uint_as_float(v[4 * i + 2]), __uint_as_float(v[4 * i + 3]));
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (threadIdx.x == 0 && *abort) atomicExch(err, 1);
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(Cfg::kTmemCols));
+  }
+}
+
+// M[r][c] = M[c][r] = (r == c) + G64[r][c] + sum_g part[g][r][c] (FP64, CTA order), r >= c.
+// A timed-out tensor-core launch (err set) poisons M with NaN.
+__global__ void syrk_reduce(const float *__restrict__ part, int G, int KP, int k,
+                            const double *__restrict__ G64, const int *__restrict__ err,
+                            double *__restrict__ M) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)k * k) return;
+  const int r = (int)(e / k), c = (int)(e % k);
+  if (c > r) return;
+  double s = 0.0;
+  for (int g = 0; g < G; ++g) s += (double)part[((size_t)g * KP + r) * KP + c];
+  if (G64) s += G64[(size_t)r * k + c];
+  if (r == c) s += 1.0;
+  if (*err) s = NAN;
+  M[(size_t)r * k + c] = s;
+  M[(size_t)c * k + r] = s;
+}
+
+// Rows with dinv > tau, in index order: per-block counts over contiguous row ranges, then each
+// block writes its rows at the prefix offset.  count_out[0] = total.
+__global__ void __launch_bounds__(256)
+big_rows_count(const double *__restrict__ dinv, int64_t n, double tau, int *__restrict__ counts) {
+  __shared__ int wsum[8];
+  const int64_t rows = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t r0 = (int64_t)blockIdx.x * rows, r1 = min(n, r0 + rows);
+  int c = 0;
+  for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) c += dinv[i] > tau ? 1 : 0;
+  c = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int s = 0;
+    for (int w = 0; w < 8; ++w) s += wsum[w];
+    counts[blockIdx.x] = s;
+  }
+}
+
+__global__ void __launch_bounds__(256)
+big_rows_index(const double *__restrict__ dinv, int64_t n, double tau,
+               const int *__restrict__ counts, int64_t *__restrict__ idx,
+               int *__restrict__ count_out) {
+  __shared__ int wcnt[8];
+  __shared__ int base_sh;
+  const int64_t rows = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t r0 = (int64_t)blockIdx.x * rows, r1 = min(n, r0 + rows);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    int s = 0;
+    for (int b = 0; b < (int)blockIdx.x; ++b) s += counts[b];
+    base_sh = s;
+    if (blockIdx.x == gridDim.x - 1) count_out[0] = s + counts[blockIdx.x];
+  }
+  __syncthreads();
+  int base = base_sh;
+  for (int64_t b0 = r0; b0 < r1; b0 += blockDim.x) {
+    const int64_t i = b0 + threadIdx.x;
+    const bool f = i < r1 && dinv[i] > tau;
+    const unsigned bal = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) wcnt[warp] = __popc(bal);
+    __syncthreads();
+    int off = base;
+    for (int w = 0; w < warp; ++w) off += wcnt[w];
+    off += __popc(bal & ((1u << lane) - 1u));
+    if (f) idx[off] = i;
+    int tot = 0;
+    for (int w = 0; w < 8; ++w) tot += wcnt[w];
+    __syncthreads();
+    base += tot;
+  }
+}
+
+template <int WAYS, int KP>
+tsvm_status launch_syrk_tc(tsvm_context *ctx, const CUtensorMap &map, int T, int G, float *part,
+                           int *err) {
+  using Cfg = SyrkCfg<WAYS, KP>;
+  auto kern = syrk_tc_kernel<WAYS, KP>;
+  TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)Cfg::kSmem));
+  kern<<<G, kSyrkThreads, Cfg::kSmem, ctx->stream>>>(map, T, part, err);
+  TSVM_LAUNCHED(ctx);
+  return TSVM_OK;
+}
+
+}  // namespace
+
+bool syrk_tc_supported(int k) { return k >= 1 && k <= 256 && tc::encode_fn() != nullptr; }
+
+tsvm_status big_rows(tsvm_context *ctx, const double *dinv, int64_t n, double tau, int64_t *idx,
+                     int *count_dev) {
+  const int nb = ctx->num_sms * 4;
+  int *counts = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_SYRK_CNT, (size_t)nb, &counts));
+  big_rows_count<<<nb, 256, 0, ctx->stream>>>(dinv, n, tau, counts);
+  TSVM_LAUNCHED(ctx);
+  big_rows_index<<<nb, 256, 0, ctx->stream>>>(dinv, n, tau, counts, idx, count_dev);
+  TSVM_LAUNCHED(ctx);
+  return TSVM_OK;
+}
+
+tsvm_status syrk_capacitance_tc(tsvm_context *ctx, const float *Z, int ldz, int64_t n, int k,
+                                const double *dinv, double tau, int ways, const double *G64,
+                                double *M) {
+  if (!syrk_tc_supported(k) || (ways != 2 && ways != 3)) return TSVM_ERR_UNSUPPORTED;
+  const int KP = k <= 128 ? 128 : 256;
+  const int64_t T = ceil_div(n, (int64_t)kSJ);
+  if ((int64_t)ways * T * KP > (int64_t)INT32_MAX) return TSVM_ERR_UNSUPPORTED;
+  __nv_bfloat16 *parts = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_SYRK_OP, (size_t)ways * T * KP * kSJ, &parts));
+  const int G = (int)std::min<int64_t>(ctx->num_sms, T);
+  float *part = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_SYRK_PART, (size_t)G * KP * KP + 64, &part));
+  int *err = reinterpret_cast<int *>(part + (size_t)G * KP * KP);
+  TSVM_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
+  const dim3 pgrid((unsigned)T, (unsigned)(KP / 32));
+  if (ways == 2)
+    syrk_prep<2><<<pgrid, dim3(32, 8), 0, ctx->stream>>>(Z, ldz, k, n, T, KP, dinv, tau, parts);
+  else
+    syrk_prep<3><<<pgrid, dim3(32, 8), 0, ctx->stream>>>(Z, ldz, k, n, T, KP, dinv, tau, parts);
+  TSVM_LAUNCHED(ctx);
+  CUtensorMap map;
+  if (!tc::make_map(&map, parts, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, kSJ, (uint64_t)ways * T * KP,
+                    kSJ, KP))
+    return TSVM_ERR_CUDA;
+  tsvm_status st;
+  if (ways == 2)
+    st = KP == 128 ? launch_syrk_tc<2, 128>(ctx, map, (int)T, G, part, err)
+                   : launch_syrk_tc<2, 256>(ctx, map, (int)T, G, part, err);
+  else
+    st = KP == 128 ? launch_syrk_tc<3, 128>(ctx, map, (int)T, G, part, err)
+                   : launch_syrk_tc<3, 256>(ctx, map, (int)T, G, part, err);
+  if (st != TSVM_OK) return st;
+  syrk_reduce<<<(unsigned)ceil_div((int64_t)k * k, 256), 256, 0, ctx->stream>>>(part, G, KP, k,
+                                                                                  G64, err, M);
+  TSVM_LAUNCHED(ctx);
+  return TSVM_OK;
+}
+
+}  // namespace tsvm

@@ -24,6 +24,7 @@ __global__ void __launch_bounds__(256)
 gram_partial_kernel(const float *__restrict__ A, int64_t lda, const float *__restrict__ B,
                     int64_t ldb, int64_t n, int ka, int kb, int tiles_b, int symmetric,
                     int64_t rows_per_split, const double *__restrict__ rowscale,
+                    const int64_t *__restrict__ rowidx, const int *__restrict__ count,
                     double *__restrict__ part) {
   __shared__ double As[kGRows][kGT];
   __shared__ double Bs[kGRows][kGT];
@@ -37,6 +38,11 @@ gram_partial_kernel(const float *__restrict__ A, int64_t lda, const float *__res
     tb = t % tiles_b;
   }
   const int a0 = ta * kGT, b0 = tb * kGT;
+  if (count) {  // row count on the device: split it evenly over gridDim.y
+    n = *count;
+    rows_per_split = (n + gridDim.y - 1) / gridDim.y;
+    rows_per_split = (rows_per_split + kGRows - 1) / kGRows * kGRows;
+  }
   const int64_t r0 = (int64_t)blockIdx.y * rows_per_split;
   const int64_t r1 = min(n, r0 + rows_per_split);
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -51,9 +57,10 @@ gram_partial_kernel(const float *__restrict__ A, int64_t lda, const float *__res
       const int rr = e / kGT, c = e % kGT;
       const int64_t gr = r + rr;
       const bool in = gr < r1;
-      const double sc = in ? (rowscale ? rowscale[gr] : 1.0) : 0.0;
-      As[rr][c] = (in && a0 + c < ka) ? (double)A[gr * lda + a0 + c] * sc : 0.0;
-      Bs[rr][c] = (in && b0 + c < kb) ? (double)B[gr * ldb + b0 + c] : 0.0;
+      const int64_t row = in ? (rowidx ? rowidx[gr] : gr) : 0;
+      const double sc = in ? (rowscale ? rowscale[row] : 1.0) : 0.0;
+      As[rr][c] = (in && a0 + c < ka) ? (double)A[row * lda + a0 + c] * sc : 0.0;
+      Bs[rr][c] = (in && b0 + c < kb) ? (double)B[row * ldb + b0 + c] : 0.0;
     }
     __syncthreads();
 #pragma unroll 8
@@ -189,11 +196,32 @@ tsvm_status gram_fp64(tsvm_context *ctx, const float *A, int64_t lda, const floa
   double *part = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_PART, (size_t)nsplit * ka * kb, &part));
   gram_partial_kernel<<<dim3(ntiles, nsplit), 256, 0, ctx->stream>>>(
-      A, lda, B, ldb, n, ka, kb, tiles_b, symmetric ? 1 : 0, rows_per_split, rowscale, part);
+      A, lda, B, ldb, n, ka, kb, tiles_b, symmetric ? 1 : 0, rows_per_split, rowscale, nullptr,
+      nullptr, part);
   TSVM_LAUNCHED(ctx);
   const int64_t tot = (int64_t)ka * kb;
   gram_reduce_kernel<<<(unsigned)ceil_div(tot, 256), 256, 0, ctx->stream>>>(
       part, nsplit, ka, kb, symmetric ? 1 : 0, G);
+  TSVM_LAUNCHED(ctx);
+  return TSVM_OK;
+}
+
+tsvm_status gram_fp64_rows(tsvm_context *ctx, const float *A, int64_t lda, int64_t n_max, int k,
+                           const int64_t *rowidx, const int *count_dev, const double *rowscale,
+                           double *G) {
+  const int tiles = (int)ceil_div(k, kGT);
+  const int ntiles = tiles * (tiles + 1) / 2;
+  int nsplit = (int)ceil_div(ctx->num_sms * 4, ntiles);
+  const int64_t max_split = ceil_div(n_max, kGRows);
+  if (nsplit > max_split) nsplit = (int)max_split;
+  if (nsplit < 1) nsplit = 1;
+  double *part = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_PART, (size_t)nsplit * k * k, &part));
+  gram_partial_kernel<<<dim3(ntiles, nsplit), 256, 0, ctx->stream>>>(
+      A, lda, A, lda, n_max, k, k, tiles, 1, 0, rowscale, rowidx, count_dev, part);
+  TSVM_LAUNCHED(ctx);
+  gram_reduce_kernel<<<(unsigned)ceil_div((int64_t)k * k, 256), 256, 0, ctx->stream>>>(
+      part, nsplit, k, k, 1, G);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;
 }

@@ -80,4 +80,24 @@ tsvm_status tsvm_test_gram(tsvm_context *ctx, const float *A, int64_t lda, const
   return TSVM_OK;
 }
 
+tsvm_status tsvm_test_syrk_mixed(tsvm_context *ctx, const float *Z, int32_t ldz, int64_t n,
+                                 int32_t k, const double *dinv, double tau, int32_t ways,
+                                 double *M, int32_t *exact_rows) {
+  if (!ctx || !Z || !dinv || !M || n < 1 || k < 1 || ldz < k) return TSVM_ERR_INVALID_ARGUMENT;
+  int64_t *idx = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_IPM_IDX, (size_t)n + 8, &idx));
+  int *cnt = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_MISC, 16, &cnt));
+  double *G64 = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_SMALL3, (size_t)k * k, &G64));
+  TSVM_TRY(big_rows(ctx, dinv, n, tau, idx, cnt));
+  TSVM_TRY(gram_fp64_rows(ctx, Z, ldz, n, k, idx, cnt, dinv, G64));
+  TSVM_TRY(syrk_capacitance_tc(ctx, Z, ldz, n, k, dinv, tau, ways, G64, M));
+  int h = 0;
+  TSVM_CUDA(cudaMemcpyAsync(&h, cnt, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (exact_rows) *exact_rows = h;
+  return TSVM_OK;
+}
+
 }  // extern "C"

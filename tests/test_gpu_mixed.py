@@ -1,0 +1,90 @@
+"""Mixed-precision capacitance matrix M = I + Z^T D^-1 Z: the tensor-core SYRK of the BF16 split
+(rows with small weight) plus the exact FP64 sum of the others, against numpy FP64; and the IPM
+that uses it (with refinement of every solve) against the FP64 IPM on the same Z."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import jaccard
+from oracle import oracle as orc
+from tensorsvm_b200 import _lib, api, synth
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def syrk_mixed(ctx, Z, k, dinv, tau, ways):
+    n, ldz = Z.shape
+    Zd, dd = dev(Z), dev(dinv)
+    M = torch.empty((k, k), dtype=torch.float64, device="cuda")
+    cnt = ctypes.c_int32()
+    _lib.check(ctx.lib.tsvm_test_syrk_mixed(ctx.handle, Zd.data_ptr(), ldz, n, k, dd.data_ptr(),
+                                            float(tau), ways, M.data_ptr(), ctypes.byref(cnt)),
+               "syrk_mixed")
+    return M.cpu().numpy(), cnt.value
+
+
+# n not a multiple of the 64-row chunk, k both below and at the 128/256 strip sizes, ldz > k
+@pytest.mark.parametrize("n,k,ways", [(70001, 256, 2), (70001, 256, 3), (5000, 100, 2),
+                                      (4096, 32, 3), (130, 256, 2), (64, 200, 2)])
+@pytest.mark.parametrize("tau", [100.0, float("inf"), 0.0])
+def test_syrk_mixed_accuracy(ctx, n, k, ways, tau):
+    rng = np.random.default_rng(n + k + ways)
+    ldz = (k + 3) // 4 * 4 + 4
+    Z = rng.standard_normal((n, ldz)).astype(np.float32)
+    dinv = np.exp(rng.uniform(np.log(1e-4), np.log(1e4), n))
+    M, cnt = syrk_mixed(ctx, Z, k, dinv, tau, ways)
+    Zk = Z[:, :k].astype(np.float64)
+    ref = np.eye(k) + (Zk * dinv[:, None]).T @ Zk
+    assert cnt == int(np.sum(dinv > tau))
+    assert np.array_equal(M, M.T)
+    scale = np.sqrt(np.outer(np.diag(ref), np.diag(ref)))
+    err = np.max(np.abs(M - ref) / scale)
+    # BF16 hi+lo keeps ~16 significant bits (lo*lo dropped), hi+mid+lo ~24, both summed in
+    # FP32 by the tensor cores; rows above tau are exact
+    tol = 1e-12 if tau == 0.0 else (1e-4 if ways == 2 else 2e-5)
+    assert err < tol, err
+
+
+@pytest.fixture(scope="module")
+def prob(ctx):
+    X, y = synth.two_gaussians(20000, 18, seed=2, noise=0.1)
+    Z, _ = api.factor(ctx, dev(X), dev(y), 0.05, 128, "fp32")
+    return X, y, Z
+
+
+@pytest.mark.parametrize("sweeps", [1, 2])
+def test_ipm_mixed_matches_fp64(ctx, prob, sweeps):
+    X, y, Z = prob
+    n, k, C = len(y), 128, 32.0
+    yd = dev(y)
+    a64, _, _, s64 = api.ipm(ctx, Z, yd, k, C, precision=_lib.PREC_FP32)
+    am, _, _, sm = api.ipm(ctx, Z, yd, k, C, precision=_lib.PREC_BF16, refine_sweeps=sweeps)
+    assert s64["mixed_syrk"] == 0 and sm["mixed_syrk"] == 1
+    assert sm["status_code"] == _lib.OK, sm
+    assert abs(sm["iters"] - s64["iters"]) <= 2, (sm["iters"], s64["iters"])
+    assert abs(sm["pobj"] - s64["pobj"]) / abs(s64["pobj"]) < 1e-7
+    assert abs(sm["dobj"] - s64["dobj"]) / abs(s64["dobj"]) < 1e-7
+    assert sm["exact_rows_mean"] < 0.1 * n
+    assert sm["refine_res_max"] < 1e-2
+    a64, am = a64.cpu().numpy(), am.cpu().numpy()
+    Zh = Z.cpu().numpy()[:, :k].astype(np.float64)
+    f64 = Zh @ (Zh.T @ (a64 * y))
+    fm = Zh @ (Zh.T @ (am * y))
+    assert np.max(np.abs(fm - f64)) < 1e-4 * max(1.0, np.max(np.abs(f64)))
+    sv64, _ = orc.sv_sets(a64, C)
+    svm, _ = orc.sv_sets(am, C)
+    assert jaccard(sv64, svm) >= 0.999
+
+
+def test_ipm_mixed_rel_gap_stop(ctx, prob):
+    X, y, Z = prob
+    k, C = 128, 32.0
+    _, _, _, sm = api.ipm(ctx, Z, dev(y), k, C, precision=_lib.PREC_BF16, rel_gap_tol=1e-6)
+    assert sm["status_code"] == _lib.OK
+    assert sm["rel_gap"] <= 1e-6 and sm["t_rel_gap_1e6_ms"] > 0
