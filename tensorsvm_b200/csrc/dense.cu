@@ -16,167 +16,282 @@ namespace tsvm {
 namespace {
 
 constexpr int kNB = 32;
+constexpr int kDP = kNB + 1;   // padded shared-memory row of a 32 x 32 block
+constexpr int kMaxDense = 864; // largest n: the Cholesky panel (32 x n doubles) in shared memory
 
-// Left-looking blocked Cholesky in one CTA of 1024 threads.  For each 32-column block:
-// (1) update the panel with the already factored columns (lanes = panel columns, one warp
-// per row), (2) factor the diagonal block with one warp, (3) triangular solve of the panel
-// rows below, one thread per row.
+// Inverse of the lower-triangular nb x nb block Dg into Di (both shared, stride kDP, Di lower
+// with zeros above); rdiag[r] = 1 / Dg[r][r].  Column c by warp c % nwarps: Di[c][c] =
+// rdiag[c] and, for r > c, Di[r][c] = -(sum_{m=c}^{r-1} Dg[r][m] Di[m][c]) rdiag[r] (the lanes
+// split the sum).
+__device__ void tri_inverse_block(const double *Dg, double *Di, int nb, const double *rdiag) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+    const int r = e / kNB, c = e % kNB;
+    if (c > r || r >= nb) Di[r * kDP + c] = 0.0;
+  }
+  __syncthreads();
+  for (int c = warp; c < nb; c += nwarps) {
+    if (lane == 0) Di[c * kDP + c] = rdiag[c];
+    __syncwarp();
+    for (int r = c + 1; r < nb; ++r) {
+      const int m = c + lane;
+      double v = m < r ? Dg[r * kDP + m] * Di[m * kDP + c] : 0.0;
+      v = warp_sum(v);
+      if (lane == 0) Di[r * kDP + c] = -v * rdiag[r];
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+}
+
+// Right-looking blocked Cholesky in one CTA of 1024 threads, 32-column panels:
+//  (a) the diagonal block is factored in shared memory with one thread per element (thread 0
+//      takes each pivot's square root and reciprocal once); (b) its inverse Di is formed and
+//      stored in Dinv (block jb/32, 32 x 32 row-major) for the triangular solves; (c) the panel
+//      below becomes A_below Di^T (one warp per row, the row broadcast by shuffles), kept
+//      transposed in shared memory; (d) the trailing lower triangle is updated with the panel
+//      (4 x 4 register tiles per thread).
 __global__ void __launch_bounds__(1024) chol_kernel(double *__restrict__ A, int n, int lda,
+                                                    double *__restrict__ Dinv,
                                                     int *__restrict__ info) {
-  extern __shared__ double sh[];
+  extern __shared__ double PT[];  // [kNB][ldp] panel, transposed: PT[c][i] = L[r0 + i][jb + c]
+  __shared__ double Dg[kNB * kDP], Di[kNB * kDP];
+  __shared__ double piv[2], rdiag[kNB];
   __shared__ int fail;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ldp = n > kNB ? n - kNB : 1;
   if (tid == 0) fail = 0;
   __syncthreads();
   for (int jb = 0; jb < n; jb += kNB) {
-    const int nb = min(kNB, n - jb);
-    const int ldp = jb + 1;  // padded row stride of the staged panel rows
-    double *Lp = sh;         // [nb][jb] rows jb..jb+nb of L, columns 0..jb
-    for (int e = tid; e < nb * jb; e += blockDim.x) {
-      const int r = e / jb, c = e % jb;
-      Lp[r * ldp + c] = A[(int64_t)(jb + r) * lda + c];
+    const int nb = min(kNB, n - jb), m = n - jb - nb, r0 = jb + nb;
+    {
+      const int r = tid >> 5, c = tid & 31;
+      Dg[r * kDP + c] = (r < nb && c <= r) ? A[(int64_t)(jb + r) * lda + jb + c] : 0.0;
     }
     __syncthreads();
-    // (1) A[i][jb+lane] -= sum_m L[i][m] L[jb+lane][m]  for i >= jb
-    for (int i = jb + warp; i < n; i += nwarps) {
-      if (lane < nb && jb + lane <= i) {
-        const double *Li = A + (int64_t)i * lda;
-        double s = 0.0;
-        for (int m = 0; m < jb; ++m) s = fma(Li[m], Lp[lane * ldp + m], s);
-        A[(int64_t)i * lda + jb + lane] -= s;
-      }
-    }
-    __syncthreads();
-    // (2) diagonal block, one warp, in shared memory
-    double *Dg = sh;  // reuse: [nb][kNB + 1]
-    for (int e = tid; e < nb * nb; e += blockDim.x) {
-      const int r = e / nb, c = e % nb;
-      Dg[r * (kNB + 1) + c] = (c <= r) ? A[(int64_t)(jb + r) * lda + jb + c] : 0.0;
-    }
-    __syncthreads();
-    if (warp == 0) {
+    // (a) thread (r, s) owns Dg[r][s]
+    {
+      const int r = tid >> 5, sidx = tid & 31;
       for (int c = 0; c < nb; ++c) {
-        const double dcc = Dg[c * (kNB + 1) + c];
-        if (!(dcc > 0.0)) {
-          if (lane == 0 && !fail) fail = jb + c + 1;
-          break;
+        if (tid == 0) {
+          const double dcc = Dg[c * kDP + c];
+          if (!(dcc > 0.0)) {
+            fail = jb + c + 1;
+          } else {
+            const double sq = sqrt(dcc);
+            piv[0] = sq;
+            piv[1] = 1.0 / sq;
+            rdiag[c] = piv[1];
+          }
         }
-        const double dc = sqrt(dcc);
-        __syncwarp();
-        if (lane == c) Dg[c * (kNB + 1) + c] = dc;
-        if (lane > c && lane < nb) Dg[lane * (kNB + 1) + c] /= dc;
-        __syncwarp();
-        if (lane > c && lane < nb) {
-          const double lrc = Dg[lane * (kNB + 1) + c];
-          for (int s2 = c + 1; s2 <= lane; ++s2)
-            Dg[lane * (kNB + 1) + s2] -= lrc * Dg[s2 * (kNB + 1) + c];
+        __syncthreads();
+        if (fail) break;
+        const double sq = piv[0], inv = piv[1];
+        const double lrc = Dg[r * kDP + c] * inv, lsc = Dg[sidx * kDP + c] * inv;
+        __syncthreads();
+        if (r < nb) {
+          if (sidx == c && r >= c) Dg[r * kDP + c] = r == c ? sq : lrc;
+          else if (sidx > c && sidx <= r) Dg[r * kDP + sidx] -= lrc * lsc;
         }
-        __syncwarp();
+        __syncthreads();
       }
     }
     __syncthreads();
     if (fail) break;
-    for (int e = tid; e < nb * nb; e += blockDim.x) {
-      const int r = e / nb, c = e % nb;
-      if (c <= r) A[(int64_t)(jb + r) * lda + jb + c] = Dg[r * (kNB + 1) + c];
+    // (b)
+    tri_inverse_block(Dg, Di, nb, rdiag);
+    {
+      double *Dblk = Dinv + (int64_t)(jb / kNB) * kNB * kNB;
+      const int r = tid >> 5, c = tid & 31;
+      Dblk[tid] = Di[r * kDP + c];
+      if (r < nb && c <= r) A[(int64_t)(jb + r) * lda + jb + c] = Dg[r * kDP + c];
     }
-    // (3) rows below: x L_d^T = a  ->  forward substitution per row
-    for (int i = jb + nb + tid; i < n; i += blockDim.x) {
-      double x[kNB];
-      double *Ai = A + (int64_t)i * lda + jb;
+    // (c) L[r0 + i][jb + c] = sum_{q <= c} A[r0 + i][jb + q] Di[c][q]
+    for (int i = warp; i < m; i += (int)(blockDim.x >> 5)) {
+      const double a = lane < nb ? A[(int64_t)(r0 + i) * lda + jb + lane] : 0.0;
+      double v = 0.0;
+#pragma unroll 8
+      for (int q = 0; q < kNB; ++q) {
+        const double aq = __shfl_sync(0xffffffffu, a, q);
+        if (q <= lane) v = fma(aq, Di[lane * kDP + q], v);
+      }
+      if (lane < nb) {
+        PT[lane * ldp + i] = v;
+        A[(int64_t)(r0 + i) * lda + jb + lane] = v;
+      }
+    }
+    __syncthreads();
+    // (d) A[r0 + i][r0 + j] -= sum_c L[r0 + i][jb + c] L[r0 + j][jb + c], j <= i
+    const int nt = (m + 3) / 4;
+    const int ntiles = nt * (nt + 1) / 2;
+    for (int t = tid; t < ntiles; t += blockDim.x) {
+      int ti = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+      while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
+      while (ti * (ti + 1) / 2 > t) --ti;
+      const int tj = t - ti * (ti + 1) / 2;
+      double acc[4][4];
 #pragma unroll
-      for (int c = 0; c < kNB; ++c) x[c] = c < nb ? Ai[c] : 0.0;
+      for (int x = 0; x < 4; ++x)
 #pragma unroll
-      for (int c = 0; c < kNB; ++c) {
-        if (c < nb) {
-          double v = x[c];
-          for (int m = 0; m < c; ++m) v -= x[m] * Dg[c * (kNB + 1) + m];
-          x[c] = v / Dg[c * (kNB + 1) + c];
+        for (int z = 0; z < 4; ++z) acc[x][z] = 0.0;
+      int ia[4], ja[4];
+#pragma unroll
+      for (int x = 0; x < 4; ++x) {
+        ia[x] = min(4 * ti + x, m - 1);   // clamped: rows past m are computed but not stored
+        ja[x] = min(4 * tj + x, m - 1);
+      }
+      for (int c = 0; c < nb; ++c) {
+        const double *pc = PT + c * ldp;
+        double av[4], bv[4];
+#pragma unroll
+        for (int x = 0; x < 4; ++x) {
+          av[x] = pc[ia[x]];
+          bv[x] = pc[ja[x]];
         }
+#pragma unroll
+        for (int x = 0; x < 4; ++x)
+#pragma unroll
+          for (int z = 0; z < 4; ++z) acc[x][z] = fma(av[x], bv[z], acc[x][z]);
       }
 #pragma unroll
-      for (int c = 0; c < kNB; ++c)
-        if (c < nb) Ai[c] = x[c];
+      for (int x = 0; x < 4; ++x)
+#pragma unroll
+        for (int z = 0; z < 4; ++z) {
+          const int i = 4 * ti + x, j = 4 * tj + z;
+          if (i < m && j <= i) A[(int64_t)(r0 + i) * lda + r0 + j] -= acc[x][z];
+        }
     }
     __syncthreads();
   }
   if (tid == 0) *info = fail;
 }
 
-// Solve L L^T X = B for nrhs (<= 4) right-hand sides stored as rows of B.  One CTA.
-__global__ void __launch_bounds__(512) potrs_kernel(const double *__restrict__ L, int n, int lda,
+// Dinv blocks of an existing lower factor L: one CTA per 32 x 32 diagonal block.
+__global__ void __launch_bounds__(1024) diag_inverse_kernel(const double *__restrict__ L, int n,
+                                                            int lda, double *__restrict__ Dinv) {
+  __shared__ double Dg[kNB * kDP], Di[kNB * kDP], rdiag[kNB];
+  const int jb = blockIdx.x * kNB, nb = min(kNB, n - jb);
+  for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+    const int r = e / kNB, c = e % kNB;
+    Dg[r * kDP + c] = (r < nb && c <= r) ? L[(int64_t)(jb + r) * lda + jb + c] : 0.0;
+  }
+  __syncthreads();
+  if (threadIdx.x < nb) rdiag[threadIdx.x] = 1.0 / Dg[threadIdx.x * kDP + threadIdx.x];
+  __syncthreads();
+  tri_inverse_block(Dg, Di, nb, rdiag);
+  for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x)
+    Dinv[(int64_t)blockIdx.x * kNB * kNB + e] = Di[(e / kNB) * kDP + e % kNB];
+}
+
+// Solve L L^T X = B for nrhs (<= 4) right-hand sides (rows of B) with the blocked forward and
+// backward substitutions; the diagonal blocks are applied through their inverses (Dinv, staged
+// in shared memory per block), so every step is a set of independent dot products.  One CTA of
+// 1024 threads.
+__global__ void __launch_bounds__(1024) potrs_kernel(const double *__restrict__ L, int n, int lda,
+                                                    const double *__restrict__ Dinv,
                                                     double *__restrict__ B, int nrhs, int ldb) {
-  __shared__ double Dg[kNB][kNB + 1];
-  __shared__ double yb[4][kNB];
-  const int tid = threadIdx.x;
+  extern __shared__ double y[];      // [nrhs][n], then the backward partials [32][4][kNB]
+  double *part = y + (size_t)nrhs * n;
+  __shared__ double t[4][kNB];
+  __shared__ double Ds[kNB * kDP];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int e = tid; e < nrhs * n; e += blockDim.x) y[e] = B[(int64_t)(e / n) * ldb + e % n];
+  __syncthreads();
   // forward: L y = b
   for (int jb = 0; jb < n; jb += kNB) {
     const int nb = min(kNB, n - jb);
-    for (int e = tid; e < nb * nb; e += blockDim.x) {
-      const int r = e / nb, c = e % nb;
-      Dg[r][c] = c <= r ? L[(int64_t)(jb + r) * lda + jb + c] : 0.0;
-    }
-    __syncthreads();
-    if (tid < nrhs) {
-      double *b = B + (int64_t)tid * ldb + jb;
-      for (int c = 0; c < nb; ++c) {
-        double v = b[c];
-        for (int m = 0; m < c; ++m) v -= Dg[c][m] * yb[tid][m];
-        yb[tid][c] = v / Dg[c][c];
-        b[c] = yb[tid][c];
+    Ds[(tid >> 5) * kDP + (tid & 31)] = Dinv[(int64_t)(jb / kNB) * kNB * kNB + tid];
+    if (warp < nb) {
+      const double *Lr = L + (int64_t)(jb + warp) * lda;
+      double s[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
+      for (int m = lane; m < jb; m += 32) {
+        const double l = __ldcg(Lr + m);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (q < nrhs) s[q] = fma(l, y[q * n + m], s[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double v = warp_sum(s[q]);
+        if (lane == 0 && q < nrhs) t[q][warp] = y[q * n + jb + warp] - v;
       }
     }
     __syncthreads();
-    for (int e = tid; e < (n - jb - nb) * nrhs; e += blockDim.x) {
-      const int i = jb + nb + e / nrhs, r = e % nrhs;
-      const double *Li = L + (int64_t)i * lda + jb;
-      double s = 0.0;
-      for (int c = 0; c < nb; ++c) s = fma(Li[c], yb[r][c], s);
-      B[(int64_t)r * ldb + i] -= s;
+    if (tid < nrhs * nb) {
+      const int q = tid / nb, r = tid % nb;
+      double v = 0.0;
+      for (int c = 0; c <= r; ++c) v = fma(Ds[r * kDP + c], t[q][c], v);
+      y[q * n + jb + r] = v;
     }
     __syncthreads();
   }
   // backward: L^T x = y
-  const int last = ((n - 1) / kNB) * kNB;
-  for (int jb = last; jb >= 0; jb -= kNB) {
+  for (int jb = ((n - 1) / kNB) * kNB; jb >= 0; jb -= kNB) {
     const int nb = min(kNB, n - jb);
-    for (int e = tid; e < nb * nb; e += blockDim.x) {
-      const int r = e / nb, c = e % nb;
-      Dg[r][c] = c <= r ? L[(int64_t)(jb + r) * lda + jb + c] : 0.0;
-    }
-    __syncthreads();
-    if (tid < nrhs) {
-      double *b = B + (int64_t)tid * ldb + jb;
-      for (int c = nb - 1; c >= 0; --c) {
-        double v = b[c];
-        for (int m = c + 1; m < nb; ++m) v -= Dg[m][c] * yb[tid][m];
-        yb[tid][c] = v / Dg[c][c];
-        b[c] = yb[tid][c];
+    Ds[(tid >> 5) * kDP + (tid & 31)] = Dinv[(int64_t)(jb / kNB) * kNB * kNB + tid];
+    {
+      double s[4] = {0.0, 0.0, 0.0, 0.0};
+      if (lane < nb) {
+#pragma unroll 4
+        for (int m = jb + nb + warp; m < n; m += 32) {
+          const double l = __ldcg(L + (int64_t)m * lda + jb + lane);
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (q < nrhs) s[q] = fma(l, y[q * n + m], s[q]);
+        }
       }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) part[(warp * 4 + q) * kNB + lane] = s[q];
     }
     __syncthreads();
-    for (int e = tid; e < jb * nrhs; e += blockDim.x) {
-      const int i = e / nrhs, r = e % nrhs;
-      double s = 0.0;
-      for (int m = 0; m < nb; ++m) s = fma(L[(int64_t)(jb + m) * lda + i], yb[r][m], s);
-      B[(int64_t)r * ldb + i] -= s;
+    if (tid < nrhs * nb) {
+      const int q = tid / nb, r = tid % nb;
+      double v = 0.0;
+      for (int w = 0; w < 32; ++w) v += part[(w * 4 + q) * kNB + r];
+      t[q][r] = y[q * n + jb + r] - v;
+    }
+    __syncthreads();
+    if (tid < nrhs * nb) {
+      const int q = tid / nb, r = tid % nb;
+      double v = 0.0;
+      for (int c = r; c < nb; ++c) v = fma(Ds[c * kDP + r], t[q][c], v);
+      y[q * n + jb + r] = v;
     }
     __syncthreads();
   }
+  for (int e = tid; e < nrhs * n; e += blockDim.x) B[(int64_t)(e / n) * ldb + e % n] = y[e];
 }
 
-// Column-parallel lower-triangular inverse: thread j produces column j of L^-1.
-__global__ void trinv_kernel(const double *__restrict__ L, int n, int lda,
-                             double *__restrict__ Linv) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  for (int i = 0; i < j; ++i) Linv[(int64_t)i * lda + j] = 0.0;
-  Linv[(int64_t)j * lda + j] = 1.0 / L[(int64_t)j * lda + j];
-  for (int i = j + 1; i < n; ++i) {
-    const double *Li = L + (int64_t)i * lda;
-    double s = 0.0;
-    for (int m = j; m < i; ++m) s = fma(Li[m], Linv[(int64_t)m * lda + j], s);
-    Linv[(int64_t)i * lda + j] = -s / Li[i];
+// L^-1 by 32-column blocks, one CTA per block column j: X_jj = Dinv_jj and, going down,
+// X_ij = -Dinv_ii sum_{m=j}^{i-1} L_im X_mj.  X is written (and re-read) in global memory.
+__global__ void __launch_bounds__(1024) trinv_kernel(const double *__restrict__ L, int n, int lda,
+                                                    const double *__restrict__ Dinv,
+                                                    double *__restrict__ X) {
+  __shared__ double T[kNB][kDP];
+  const int jb = blockIdx.x * kNB, nbj = min(kNB, n - jb);
+  const int tid = threadIdx.x, r = tid / kNB, c = tid % kNB;
+  for (int e = tid; e < jb * nbj; e += blockDim.x)
+    X[(int64_t)(e / nbj) * lda + jb + e % nbj] = 0.0;
+  if (r < nbj && c < nbj)
+    X[(int64_t)(jb + r) * lda + jb + c] = Dinv[(int64_t)blockIdx.x * kNB * kNB + r * kNB + c];
+  __syncthreads();
+  for (int ib = jb + kNB; ib < n; ib += kNB) {
+    const int nbi = min(kNB, n - ib);
+    if (r < nbi && c < nbj) {
+      const double *Lr = L + (int64_t)(ib + r) * lda;
+      double v = 0.0;
+      for (int m = jb; m < ib; ++m) v = fma(Lr[m], X[(int64_t)m * lda + jb + c], v);
+      T[r][c] = v;
+    }
+    __syncthreads();
+    if (r < nbi && c < nbj) {
+      const double *Di = Dinv + (int64_t)(ib / kNB) * kNB * kNB + r * kNB;
+      double v = 0.0;
+      for (int q = 0; q <= r; ++q) v = fma(Di[q], T[q][c], v);
+      X[(int64_t)(ib + r) * lda + jb + c] = -v;
+    }
+    __syncthreads();
   }
 }
 
@@ -315,26 +430,38 @@ __global__ void eig_pack_out(const double *__restrict__ A0, const double *__rest
 
 }  // namespace
 
-tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_dev) {
-  if (n < 1 || n > 864) return TSVM_ERR_UNSUPPORTED;  // staged panel must fit shared memory
-  const size_t smem = sizeof(double) * (size_t)kNB * (size_t)(n + 1 > kNB + 1 ? n + 1 : kNB + 1);
+tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_dev, double *Dinv) {
+  if (n < 1 || n > kMaxDense) return TSVM_ERR_UNSUPPORTED;  // panel must fit shared memory
+  const size_t smem = sizeof(double) * (size_t)kNB * (size_t)(n > kNB ? n - kNB : 1);
   TSVM_CUDA(cudaFuncSetAttribute(chol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
-  chol_kernel<<<1, 1024, smem, ctx->stream>>>(A, n, lda, info_dev);
+  chol_kernel<<<1, 1024, smem, ctx->stream>>>(A, n, lda, Dinv, info_dev);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;
 }
 
-tsvm_status potrs_fp64(tsvm_context *ctx, const double *L, int n, int lda, double *B, int nrhs,
-                       int ldb) {
-  if (nrhs < 1 || nrhs > 4) return TSVM_ERR_UNSUPPORTED;
-  potrs_kernel<<<1, 512, 0, ctx->stream>>>(L, n, lda, B, nrhs, ldb);
+tsvm_status tri_diag_inverse(tsvm_context *ctx, const double *L, int n, int lda, double *Dinv) {
+  if (n < 1) return TSVM_ERR_INVALID_ARGUMENT;
+  diag_inverse_kernel<<<(unsigned)ceil_div(n, kNB), 1024, 0, ctx->stream>>>(L, n, lda, Dinv);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;
 }
 
-tsvm_status trinv_lower_fp64(tsvm_context *ctx, const double *L, int n, int lda, double *Linv) {
-  trinv_kernel<<<(unsigned)ceil_div(n, 64), 64, 0, ctx->stream>>>(L, n, lda, Linv);
+tsvm_status potrs_fp64(tsvm_context *ctx, const double *L, int n, int lda, const double *Dinv,
+                       double *B, int nrhs, int ldb) {
+  if (nrhs < 1 || nrhs > 4 || n < 1 || n > kMaxDense) return TSVM_ERR_UNSUPPORTED;
+  const size_t smem = sizeof(double) * ((size_t)nrhs * n + 32 * 4 * kNB);
+  TSVM_CUDA(cudaFuncSetAttribute(potrs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  potrs_kernel<<<1, 1024, smem, ctx->stream>>>(L, n, lda, Dinv, B, nrhs, ldb);
+  TSVM_LAUNCHED(ctx);
+  return TSVM_OK;
+}
+
+tsvm_status trinv_lower_fp64(tsvm_context *ctx, const double *L, int n, int lda,
+                             const double *Dinv, double *Linv) {
+  if (n < 1) return TSVM_ERR_INVALID_ARGUMENT;
+  trinv_kernel<<<(unsigned)ceil_div(n, kNB), 1024, 0, ctx->stream>>>(L, n, lda, Dinv, Linv);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;
 }

@@ -85,7 +85,8 @@ static tsvm_status orthonormalise(tsvm_context *ctx, float *W, int64_t n, int k,
   float *R32 = nullptr;
   int *info = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_SMALL, (size_t)k * k + 8, &G));
-  TSVM_TRY(scratch_t(ctx, SLOT_SMALL2, (size_t)k * k, &Linv));
+  TSVM_TRY(scratch_t(ctx, SLOT_SMALL2, (size_t)k * k + (size_t)ceil_div(k, 32) * 1024, &Linv));
+  double *Dinv = Linv + (size_t)k * k;
   TSVM_TRY(scratch_t(ctx, SLOT_IPM_M, (size_t)kp * kp, &R32));
   info = reinterpret_cast<int *>(G + (size_t)k * k);
   const double u = ldexp(1.0, -53);
@@ -97,7 +98,7 @@ static tsvm_status orthonormalise(tsvm_context *ctx, float *W, int64_t n, int k,
         shift_by_trace<<<1, 256, 0, ctx->stream>>>(G, k, factor);
         TSVM_LAUNCHED(ctx);
       }
-      TSVM_TRY(chol_fp64(ctx, G, k, k, info));
+      TSVM_TRY(chol_fp64(ctx, G, k, k, info, Dinv));
       int hinfo = 0;
       TSVM_CUDA(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
       TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -105,7 +106,7 @@ static tsvm_status orthonormalise(tsvm_context *ctx, float *W, int64_t n, int k,
       if (attempt == 3) return TSVM_ERR_NOT_SPD;
       factor = factor > 0 ? factor * 100.0 : 11.0 * ((double)n * k + (double)k * (k + 1)) * u;
     }
-    TSVM_TRY(trinv_lower_fp64(ctx, G, k, k, Linv));
+    TSVM_TRY(trinv_lower_fp64(ctx, G, k, k, Dinv, Linv));
     rinv_to_fp32<<<(unsigned)ceil_div((int64_t)kp * kp, 256), 256, 0, ctx->stream>>>(Linv, k, kp,
                                                                                       R32);
     TSVM_LAUNCHED(ctx);

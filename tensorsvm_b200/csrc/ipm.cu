@@ -4,9 +4,10 @@
 // in FP64 with about 16 GEMV passes over Z per iteration.  Here:
 //   * Z (n x k) stays resident in HBM in FP32; all vectors (x = alpha, s, xi, D^-1, residuals,
 //     directions) are FP64 on the device; reductions are FP64 with a fixed order.
-//   * Every pass over Z is a fused streaming kernel: `zt_kernel` accumulates Z^T [v1 v2] with a
-//     per-row functor producing v (and side reductions); `zw_kernel` forms Z w per row and runs
-//     a per-row epilogue (residuals, SMW back-substitution, dot products).
+//   * Every pass over Z is one persistent streaming kernel (`stream_kernel`, chunks of Z rows
+//     brought into shared memory by bulk copies): Z^T v with a per-row functor producing v
+//     (and side reductions), Z w per row followed by a per-row epilogue (residuals, SMW
+//     back-substitution, dot products), or Z^T D^-1 Z g for the refinement of the SMW solves.
 //   * The reference's three SMW solves per NewtonStep become two: by linearity
 //     dx = dy (D+Q)^-1 a - (D+Q)^-1 r5, and (D+Q)^-1 a is shared by predictor and corrector.
 //     Per iteration: 5 streaming passes over Z plus one Z^T D^-1 Z pass (vs ~16 + DSYRK).
@@ -17,11 +18,13 @@
 #include <stdio.h>
 
 #include <chrono>
+#include <unordered_map>
 #include <vector>
 
 #include "common.cuh"
 #include "context.h"
 #include "kernels.h"
+#include "tc_common.cuh"
 
 namespace tsvm {
 namespace {
@@ -303,162 +306,6 @@ __device__ __forceinline__ void block_partials(double *sums, double *mins, doubl
   }
 }
 
-template <class Op, int LPR, int CPL>
-__global__ void __launch_bounds__(kThreads)
-zt_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, Op op,
-          const double *__restrict__ scal, double *__restrict__ part_vec, int kz,
-          double *__restrict__ part_s) {
-  constexpr int R = Op::R, NS = Op::NS, NM = Op::NM;
-  constexpr int RPW = 32 / LPR;
-  constexpr int NC = CPL * 4;
-  extern __shared__ double zsh[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int slot = lane / LPR, sl = lane % LPR;
-  op.load(scal);
-  double acc[NC][R];
-#pragma unroll
-  for (int c = 0; c < NC; ++c)
-#pragma unroll
-    for (int r = 0; r < R; ++r) acc[c][r] = 0.0;
-  double sums[NS > 0 ? NS : 1], mins[NM > 0 ? NM : 1];
-#pragma unroll
-  for (int j = 0; j < (NS > 0 ? NS : 1); ++j) sums[j] = 0.0;
-#pragma unroll
-  for (int j = 0; j < (NM > 0 ? NM : 1); ++j) mins[j] = INFINITY;
-  const int64_t gw = (int64_t)blockIdx.x * kWarps + warp;
-  const int64_t stride = (int64_t)gridDim.x * kWarps * 32;
-  for (int64_t base = gw * 32; base < n; base += stride) {
-    double v[R];
-    const int64_t my = base + lane;
-    if (my < n) op.rhs(my, v, sums, mins);
-    else {
-#pragma unroll
-      for (int r = 0; r < R; ++r) v[r] = 0.0;
-    }
-#pragma unroll 4
-    for (int step = 0; step < 32 / RPW; ++step) {
-      const int src = step * RPW + slot;
-      const int64_t row = base + src;
-      double vr[R];
-#pragma unroll
-      for (int r = 0; r < R; ++r) vr[r] = __shfl_sync(0xffffffffu, v[r], src);
-      if (row < n) {
-        const float4 *zr = reinterpret_cast<const float4 *>(Z + row * ldz);
-#pragma unroll
-        for (int c = 0; c < CPL; ++c) {
-          const int g = sl + c * LPR;
-          if (4 * g < k) {
-            float4 z = __ldg(zr + g);
-            if (4 * g + 3 >= k) {
-              if (4 * g + 1 >= k) z.y = 0.f;
-              if (4 * g + 2 >= k) z.z = 0.f;
-              z.w = 0.f;
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-              acc[4 * c + 0][r] = fma((double)z.x, vr[r], acc[4 * c + 0][r]);
-              acc[4 * c + 1][r] = fma((double)z.y, vr[r], acc[4 * c + 1][r]);
-              acc[4 * c + 2][r] = fma((double)z.z, vr[r], acc[4 * c + 2][r]);
-              acc[4 * c + 3][r] = fma((double)z.w, vr[r], acc[4 * c + 3][r]);
-            }
-          }
-        }
-      }
-    }
-  }
-  // reduce the (warp, slot) partial column sums through shared memory
-  const int ncol = LPR * NC;                      // columns covered by one segment
-  double *red = zsh;                              // [kWarps*RPW][R][ncol]
-#pragma unroll
-  for (int c = 0; c < CPL; ++c)
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-#pragma unroll
-      for (int r = 0; r < R; ++r)
-        red[((warp * RPW + slot) * R + r) * ncol + 4 * (sl + c * LPR) + q] = acc[4 * c + q][r];
-  __syncthreads();
-  for (int e = threadIdx.x; e < R * kz; e += kThreads) {
-    const int r = e / kz, col = e % kz;
-    double s = 0.0;
-    if (col < ncol)
-      for (int ws = 0; ws < kWarps * RPW; ++ws) s += red[(ws * R + r) * ncol + col];
-    part_vec[(int64_t)blockIdx.x * R * kz + e] = s;
-  }
-  if (NS + NM > 0) {
-    __syncthreads();
-    block_partials<NS, NM>(sums, mins, part_s, zsh);
-  }
-}
-
-template <class Op, int LPR, int CPL>
-__global__ void __launch_bounds__(kThreads)
-zw_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, Op op,
-          const double *__restrict__ scal, const double *__restrict__ w, int kz,
-          double *__restrict__ part_s) {
-  constexpr int R = Op::R, NS = Op::NS, NM = Op::NM;
-  constexpr int RPW = 32 / LPR;
-  constexpr int NC = CPL * 4;
-  __shared__ double zsh[(NS + NM > 0 ? NS + NM : 1) * kWarps];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int slot = lane / LPR, sl = lane % LPR;
-  op.load(scal);
-  double wr[NC][R];
-#pragma unroll
-  for (int c = 0; c < CPL; ++c)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int col = 4 * (sl + c * LPR) + q;
-#pragma unroll
-      for (int r = 0; r < R; ++r) wr[4 * c + q][r] = col < k ? w[r * kz + col] : 0.0;
-    }
-  double sums[NS > 0 ? NS : 1], mins[NM > 0 ? NM : 1];
-#pragma unroll
-  for (int j = 0; j < (NS > 0 ? NS : 1); ++j) sums[j] = 0.0;
-#pragma unroll
-  for (int j = 0; j < (NM > 0 ? NM : 1); ++j) mins[j] = INFINITY;
-  const int64_t gw = (int64_t)blockIdx.x * kWarps + warp;
-  const int64_t stride = (int64_t)gridDim.x * kWarps * 32;
-  for (int64_t base = gw * 32; base < n; base += stride) {
-    double mine[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) mine[r] = 0.0;
-#pragma unroll 4
-    for (int step = 0; step < 32 / RPW; ++step) {
-      const int64_t row = base + step * RPW + slot;
-      double d[R];
-#pragma unroll
-      for (int r = 0; r < R; ++r) d[r] = 0.0;
-      if (row < n) {
-        const float4 *zr = reinterpret_cast<const float4 *>(Z + row * ldz);
-#pragma unroll
-        for (int c = 0; c < CPL; ++c) {
-          const int g = sl + c * LPR;
-          if (4 * g < k) {
-            const float4 z = __ldg(zr + g);
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-              d[r] = fma((double)z.x, wr[4 * c + 0][r], d[r]);
-              d[r] = fma((double)z.y, wr[4 * c + 1][r], d[r]);
-              d[r] = fma((double)z.z, wr[4 * c + 2][r], d[r]);
-              d[r] = fma((double)z.w, wr[4 * c + 3][r], d[r]);
-            }
-          }
-        }
-      }
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-#pragma unroll
-        for (int o = LPR / 2; o > 0; o >>= 1) d[r] += __shfl_xor_sync(0xffffffffu, d[r], o);
-        const double got = __shfl_sync(0xffffffffu, d[r], (lane % RPW) * LPR);
-        if (lane / RPW == step) mine[r] = got;
-      }
-    }
-    const int64_t my = base + lane;
-    if (my < n) op.row(my, mine, sums, mins);
-  }
-  if (NS + NM > 0) block_partials<NS, NM>(sums, mins, part_s, zsh);
-}
-
 template <class Op>
 __global__ void __launch_bounds__(kThreads)
 vec_kernel(int64_t n, Op op, const double *__restrict__ scal, double *__restrict__ part_s) {
@@ -476,20 +323,69 @@ vec_kernel(int64_t n, Op op, const double *__restrict__ scal, double *__restrict
   if (NS + NM > 0) block_partials<NS, NM>(sums, mins, part_s, vsh);
 }
 
-// Refinement pass: w_r = Z^T D^-1 (Z g_r) for R vectors g_r (kz apart) in one read of Z.  Per
-// row the dot products z . g_r are reduced over the LPR lanes that hold the row, scaled by
-// dinv, and accumulated into the lanes' column sums (FP64, block partials as in zt_kernel).
-template <int R, int LPR, int CPL>
-__global__ void __launch_bounds__(kThreads)
-zgz_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n,
-           const double *__restrict__ dinv, const double *__restrict__ g, int kz,
-           double *__restrict__ part_vec) {
-  constexpr int RPW = 32 / LPR;
+// ---------------------------------------------------------------------------------------
+// Streaming passes over Z, fed by bulk (TMA) copies.  Persistent: one CTA per SM walks its
+// CR-row chunks c, c + G, ...; a producer warp keeps up to `stages` chunks in flight (one
+// contiguous cp.async.bulk per chunk, completion on an mbarrier) and the 8 consumer warps take
+// whole chunks in turn (the j-th chunk of the CTA goes to warp j % 8), so each warp runs the
+// per-row functor for CR rows at once (lane = row, one round trip to the vectors) and then
+// streams the CR rows out of shared memory while the other warps wait on theirs:
+//   MODE_ZT : v = op.rhs(row), acc += z_row v             (Z^T v, row functor)
+//   MODE_ZW : d = z_row . w, then op.row(row, d)            (Z w, row epilogue)
+//   MODE_ZGZ: d = z_row . g, acc += z_row (dinv_row d)      (Z^T D^-1 Z g)
+// Column sums are reduced over the warps in shared memory into one FP64 partial per CTA (fixed
+// order); side sums / minima likewise.  Waits are bounded; a CTA that gives up sets *err.
+// ---------------------------------------------------------------------------------------
+enum StreamMode : int { MODE_ZT = 0, MODE_ZW = 1, MODE_ZGZ = 2 };
+constexpr int kSConsumers = 8;
+constexpr int kSThreads = (kSConsumers + 1) * 32;
+
+struct GramVecOp {  // no per-row functor (MODE_ZGZ)
+  static constexpr int NS = 0, NM = 0;
+  __device__ void load(const double *) {}
+};
+
+template <int MODE, class Op, int R, int CR, int LPR, int CPL>
+__global__ void __launch_bounds__(kSThreads, 1)
+stream_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, Op op,
+              const double *__restrict__ scal, const double *__restrict__ w,
+              const double *__restrict__ dinv, int kz, int stages,
+              double *__restrict__ part_vec, double *__restrict__ part_s, int *__restrict__ err) {
+  constexpr int NS = Op::NS, NM = Op::NM;
+  constexpr int RPW = 32 / LPR;          // rows per warp step
+  constexpr int RW = CR;                 // rows per chunk, all taken by one warp
+  constexpr int STEPS = RW / RPW;
+  static_assert(RW % RPW == 0 && RW <= 32, "chunk rows must be a multiple of rows per step");
   constexpr int NC = CPL * 4;
-  extern __shared__ double zsh[];
+  constexpr bool ACC = MODE != MODE_ZW;
+  constexpr bool DOT = MODE != MODE_ZT;
+  extern __shared__ __align__(128) uint8_t ssm[];
+  const uint32_t chunk_bytes = (uint32_t)(CR * ldz * 4);
+  float *stage0 = reinterpret_cast<float *>(ssm);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(ssm + (size_t)stages * chunk_bytes);
+  const uint32_t b_full = tc::su32(bars), b_empty = b_full + 8 * stages;
+  volatile int *abort = reinterpret_cast<volatile int *>(bars + 2 * stages);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int slot = lane / LPR, sl = lane % LPR;
-  double gr[NC][R], acc[NC][R];
+  const int64_t nchunks = (n + CR - 1) / CR;
+  const int G = gridDim.x;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < stages; ++s) {
+      tc::mbar_init(b_full + 8 * s, 1);
+      tc::mbar_init(b_empty + 8 * s, 1);
+    }
+    *abort = 0;
+    tc::fence_barrier_init();
+  }
+  __syncthreads();
+  op.load(scal);
+  double sums[NS > 0 ? NS : 1], mins[NM > 0 ? NM : 1];
+#pragma unroll
+  for (int j = 0; j < (NS > 0 ? NS : 1); ++j) sums[j] = 0.0;
+#pragma unroll
+  for (int j = 0; j < (NM > 0 ? NM : 1); ++j) mins[j] = INFINITY;
+  double acc[ACC ? NC : 1][R];
+  double wr[DOT ? NC : 1][R];
 #pragma unroll
   for (int c = 0; c < CPL; ++c)
 #pragma unroll
@@ -497,70 +393,163 @@ zgz_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n,
       const int col = 4 * (sl + c * LPR) + q;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        gr[4 * c + q][r] = col < k ? g[r * kz + col] : 0.0;
-        acc[4 * c + q][r] = 0.0;
+        if constexpr (ACC) acc[4 * c + q][r] = 0.0;
+        if constexpr (DOT) wr[4 * c + q][r] = col < k ? w[r * kz + col] : 0.0;
       }
     }
-  const int64_t gw = (int64_t)blockIdx.x * kWarps + warp;
-  const int64_t stride = (int64_t)gridDim.x * kWarps * 32;
-  for (int64_t base = gw * 32; base < n; base += stride) {
-#pragma unroll 2
-    for (int step = 0; step < 32 / RPW; ++step) {
-      const int64_t row = base + step * RPW + slot;
-      if (row < n) {
-        const float4 *zr = reinterpret_cast<const float4 *>(Z + row * ldz);
-        float4 z[CPL];
-        double d[R];
+
+  if (warp == kSConsumers) {
+    if (lane == 0) {
+      int st = 0;
+      uint32_t ph = 0;
+      for (int64_t q = blockIdx.x; q < nchunks; q += G) {
+        if (!tc::mbar_wait(b_empty + 8 * st, ph ^ 1, abort)) break;
+        const int64_t r0 = q * CR;
+        const uint32_t bytes = (uint32_t)((n - r0 < CR ? n - r0 : CR) * ldz * 4);
+        tc::mbar_expect_tx(b_full + 8 * st, bytes);
+        tc::bulk_load(tc::su32(stage0) + st * chunk_bytes, Z + r0 * ldz, bytes, b_full + 8 * st);
+        if (++st == stages) { st = 0; ph ^= 1; }
+      }
+    }
+  } else {
+    int64_t j = warp;   // index of the chunk among this CTA's chunks
+    for (int64_t q = blockIdx.x + (int64_t)warp * G; q < nchunks;
+         q += (int64_t)kSConsumers * G, j += kSConsumers) {
+      const int st = (int)(j % stages);
+      const uint32_t ph = (uint32_t)((j / stages) & 1);
+      if (!tc::mbar_wait(b_full + 8 * st, ph, abort)) break;
+      const float *S = stage0 + (size_t)st * CR * ldz;
+      const int64_t r0 = q * CR;   // first row of the chunk
+      double v[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) d[r] = 0.0;
+      for (int r = 0; r < R; ++r) v[r] = 0.0;
+      if constexpr (MODE == MODE_ZT) {
+        if (lane < RW && r0 + lane < n) op.rhs(r0 + lane, v, sums, mins);
+      }
+      double mine[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) mine[r] = 0.0;
+      constexpr int UNR = CPL >= 4 ? 1 : 4;   // wide rows: keep the register footprint bounded
+#pragma unroll UNR
+      for (int step = 0; step < STEPS; ++step) {
+        const int rw = step * RPW + slot;
+        const int64_t row = r0 + rw;
+        const bool in = row < n;
+        const float4 *zr = reinterpret_cast<const float4 *>(S + (size_t)rw * ldz);
+        float4 z[CPL];
 #pragma unroll
         for (int c = 0; c < CPL; ++c) {
-          const int gq = sl + c * LPR;
-          z[c] = 4 * gq < k ? __ldg(zr + gq) : make_float4(0.f, 0.f, 0.f, 0.f);
+          const int g = sl + c * LPR;
+          float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (in && 4 * g < k) {
+            t = zr[g];
+            if (4 * g + 3 >= k) {
+              if (4 * g + 1 >= k) t.y = 0.f;
+              if (4 * g + 2 >= k) t.z = 0.f;
+              t.w = 0.f;
+            }
+          }
+          z[c] = t;
+        }
+        double vr[R];
+        if constexpr (DOT) {
+          double d[R];
+#pragma unroll
+          for (int r = 0; r < R; ++r) d[r] = 0.0;
+#pragma unroll
+          for (int c = 0; c < CPL; ++c)
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              d[r] = fma((double)z[c].x, wr[4 * c + 0][r], d[r]);
+              d[r] = fma((double)z[c].y, wr[4 * c + 1][r], d[r]);
+              d[r] = fma((double)z[c].z, wr[4 * c + 2][r], d[r]);
+              d[r] = fma((double)z[c].w, wr[4 * c + 3][r], d[r]);
+            }
 #pragma unroll
           for (int r = 0; r < R; ++r) {
-            d[r] = fma((double)z[c].x, gr[4 * c + 0][r], d[r]);
-            d[r] = fma((double)z[c].y, gr[4 * c + 1][r], d[r]);
-            d[r] = fma((double)z[c].z, gr[4 * c + 2][r], d[r]);
-            d[r] = fma((double)z[c].w, gr[4 * c + 3][r], d[r]);
+#pragma unroll
+            for (int o = LPR / 2; o > 0; o >>= 1) d[r] += __shfl_xor_sync(0xffffffffu, d[r], o);
           }
-        }
-        const double di = dinv[row];
+          if constexpr (MODE == MODE_ZW) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
+            for (int s2 = 0; s2 < RPW; ++s2)
 #pragma unroll
-          for (int o = LPR / 2; o > 0; o >>= 1) d[r] += __shfl_xor_sync(0xffffffffu, d[r], o);
-          d[r] *= di;
-        }
+              for (int r = 0; r < R; ++r) {
+                const double got = __shfl_sync(0xffffffffu, d[r], s2 * LPR);
+                if (lane == step * RPW + s2) mine[r] = got;
+              }
+          } else {
+            const double di = in ? dinv[row] : 0.0;
 #pragma unroll
-        for (int c = 0; c < CPL; ++c)
-#pragma unroll
-          for (int r = 0; r < R; ++r) {
-            acc[4 * c + 0][r] = fma((double)z[c].x, d[r], acc[4 * c + 0][r]);
-            acc[4 * c + 1][r] = fma((double)z[c].y, d[r], acc[4 * c + 1][r]);
-            acc[4 * c + 2][r] = fma((double)z[c].z, d[r], acc[4 * c + 2][r]);
-            acc[4 * c + 3][r] = fma((double)z[c].w, d[r], acc[4 * c + 3][r]);
+            for (int r = 0; r < R; ++r) vr[r] = d[r] * di;
           }
+        } else {
+#pragma unroll
+          for (int r = 0; r < R; ++r) vr[r] = __shfl_sync(0xffffffffu, v[r], rw);
+        }
+        if constexpr (ACC) {
+#pragma unroll
+          for (int c = 0; c < CPL; ++c)
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              acc[4 * c + 0][r] = fma((double)z[c].x, vr[r], acc[4 * c + 0][r]);
+              acc[4 * c + 1][r] = fma((double)z[c].y, vr[r], acc[4 * c + 1][r]);
+              acc[4 * c + 2][r] = fma((double)z[c].z, vr[r], acc[4 * c + 2][r]);
+              acc[4 * c + 3][r] = fma((double)z[c].w, vr[r], acc[4 * c + 3][r]);
+            }
+        }
+      }
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(b_empty + 8 * st);
+      if constexpr (MODE == MODE_ZW) {
+        if (lane < RW && r0 + lane < n) op.row(r0 + lane, mine, sums, mins);
       }
     }
   }
-  const int ncol = LPR * NC;
-  double *red = zsh;  // [kWarps*RPW][R][ncol]
+  __syncthreads();  // every chunk consumed: the stage memory is free for the reductions
+  double *red = reinterpret_cast<double *>(ssm);
+  if constexpr (ACC) {
+    constexpr int ncol = LPR * NC;
+    if (warp < kSConsumers) {
 #pragma unroll
-  for (int c = 0; c < CPL; ++c)
+      for (int c = 0; c < CPL; ++c)
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+        for (int qq = 0; qq < 4; ++qq)
 #pragma unroll
-      for (int r = 0; r < R; ++r)
-        red[((warp * RPW + slot) * R + r) * ncol + 4 * (sl + c * LPR) + q] = acc[4 * c + q][r];
-  __syncthreads();
-  for (int e = threadIdx.x; e < R * kz; e += kThreads) {
-    const int r = e / kz, col = e % kz;
-    double sum = 0.0;
-    if (col < ncol)
-      for (int ws = 0; ws < kWarps * RPW; ++ws) sum += red[(ws * R + r) * ncol + col];
-    part_vec[(int64_t)blockIdx.x * R * kz + e] = sum;
+          for (int r = 0; r < R; ++r)
+            red[((warp * RPW + slot) * R + r) * ncol + 4 * (sl + c * LPR) + qq] = acc[4 * c + qq][r];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < R * kz; e += blockDim.x) {
+      const int r = e / kz, col = e % kz;
+      double sum = 0.0;
+      if (col < ncol)
+        for (int ws = 0; ws < kSConsumers * RPW; ++ws) sum += red[(ws * R + r) * ncol + col];
+      part_vec[(int64_t)blockIdx.x * R * kz + e] = sum;
+    }
   }
+  if constexpr (NS + NM > 0) {
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < NS; ++j) {
+      const double t = warp_sum(sums[j]);
+      if (lane == 0) red[j * 9 + warp] = t;
+    }
+#pragma unroll
+    for (int j = 0; j < NM; ++j) {
+      const double t = warp_min(mins[j]);
+      if (lane == 0) red[(NS + j) * 9 + warp] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < NS + NM) {
+      const int j = threadIdx.x;
+      double t = j < NS ? 0.0 : INFINITY;
+      for (int ww = 0; ww < kSConsumers + 1; ++ww)
+        t = j < NS ? t + red[j * 9 + ww] : fmin(t, red[j * 9 + ww]);
+      part_s[(int64_t)blockIdx.x * (NS + NM) + j] = t;
+    }
+  }
+  if (threadIdx.x == 0 && *abort) atomicExch(err, 1);
 }
 
 // c = h0 - (g + w) (the residual h0 - M g of the capacitance solve, M g = g + Z^T D^-1 Z g);
@@ -620,19 +609,29 @@ __global__ void finalize_kernel(const double *__restrict__ part_vec, int nblk, i
                                 double *__restrict__ out_vec, const double *__restrict__ part_s,
                                 int ns, int nm, double *__restrict__ sc, int stage,
                                 const int *__restrict__ info) {
-  const int vb = (nvec + 127) / 128;
+  // vector blocks: 32 entries each, the partials split over 8 warps (strided), then summed in
+  // warp order -- a fixed order, independent of timing
+  const int vb = (nvec + 31) / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if ((int)blockIdx.x < vb) {
-    const int e = blockIdx.x * 128 + threadIdx.x;
+    __shared__ double vsum[8][32];
+    const int e = blockIdx.x * 32 + lane;
+    double s = 0.0;
     if (e < nvec) {
-      double s = 0.0;
-      for (int b = 0; b < nblk; ++b) s += part_vec[(int64_t)b * nvec + e];
-      out_vec[e] = s;
+#pragma unroll 4
+      for (int b = warp; b < nblk; b += 8) s += part_vec[(int64_t)b * nvec + e];
+    }
+    vsum[warp][lane] = s;
+    __syncthreads();
+    if (warp == 0 && e < nvec) {
+      double t = 0.0;
+      for (int w = 0; w < 8; ++w) t += vsum[w][lane];
+      out_vec[e] = t;
     }
     return;
   }
   __shared__ double red[16];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int j = warp; j < ns + nm; j += 4) {
+  for (int j = warp; j < ns + nm; j += 8) {
     double r = j < ns ? 0.0 : INFINITY;
     for (int b = lane; b < nblk; b += 32) {
       const double v = part_s[(int64_t)b * (ns + nm) + j];
@@ -733,85 +732,66 @@ struct Runner {
   int *info;
   const double *dinv;
 
-  template <class Op, int LPR, int CPL>
-  tsvm_status zt_launch(const Op &op, double *out_vec, int stage) {
-    constexpr int R = Op::R;
+  int *err;   // set by a streaming pass that timed out
+
+  // One streaming pass (stream_kernel) with this solve's geometry: one CTA per SM, as many
+  // chunk stages as fit in ~192 KB of shared memory (at least 2, at most 16, and room for the
+  // reduction).
+  template <int MODE, class Op, int R, int CR, int LPR, int CPL>
+  tsvm_status pass_launch(const Op &op, const double *w, double *out_vec, int stage) {
     constexpr int RPW = 32 / LPR;
-    const size_t smem_red = sizeof(double) * (size_t)kWarps * RPW * R * LPR * CPL * 4;
-    const size_t smem = smem_red > sizeof(double) * 64 ? smem_red : sizeof(double) * 64;
-    auto kern = zt_kernel<Op, LPR, CPL>;
-    if (smem > 48 * 1024)
-      TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<nblk, kThreads, smem, ctx->stream>>>(Z, ldz, k, n, op, scal, part_vec, geo.kz, part_s);
+    const size_t chunk = (size_t)CR * ldz * 4;
+    size_t stages = std::min<size_t>(16, std::max<size_t>(2, (192 * 1024) / chunk));
+    const size_t red = sizeof(double) * std::max<size_t>(
+        MODE != MODE_ZW ? (size_t)kSConsumers * RPW * R * LPR * CPL * 4 : 0, 16 * 9);
+    while (stages * chunk < red) ++stages;
+    const size_t smem = stages * chunk + 8 * (2 * stages + 2);
+    auto kern = stream_kernel<MODE, Op, R, CR, LPR, CPL>;
+    TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int grid = (int)std::min<int64_t>(std::min(nblk, ctx->num_sms), ceil_div(n, CR));
+    kern<<<grid, kSThreads, smem, ctx->stream>>>(Z, ldz, k, n, op, scal, w, dinv, geo.kz,
+                                                 (int)stages, part_vec, part_s, err);
     TSVM_LAUNCHED(ctx);
-    return finalize(R * geo.kz, out_vec, Op::NS, Op::NM, stage);
+    return finalize(grid, MODE != MODE_ZW ? R * geo.kz : 0, out_vec, Op::NS, Op::NM, stage);
   }
+  template <int MODE, class Op, int R>
+  tsvm_status pass(const Op &op, const double *w, double *out_vec, int stage) {
+    switch (geo.lpr * 10 + geo.cpl) {
+      case 81: return pass_launch<MODE, Op, R, 32, 8, 1>(op, w, out_vec, stage);
+      case 161: return pass_launch<MODE, Op, R, 32, 16, 1>(op, w, out_vec, stage);
+      case 321: return pass_launch<MODE, Op, R, 32, 32, 1>(op, w, out_vec, stage);
+      case 322: return pass_launch<MODE, Op, R, 16, 32, 2>(op, w, out_vec, stage);
+      case 324: return pass_launch<MODE, Op, R, 8, 32, 4>(op, w, out_vec, stage);
+      case 328: return pass_launch<MODE, Op, R, 8, 32, 8>(op, w, out_vec, stage);
+    }
+    return TSVM_ERR_UNSUPPORTED;
+  }
+  // Z^T v with v from the per-row functor (plus its side reductions)
   template <class Op>
   tsvm_status zt(const Op &op, double *out_vec, int stage) {
-    switch (geo.lpr * 10 + geo.cpl) {
-      case 81: return zt_launch<Op, 8, 1>(op, out_vec, stage);
-      case 161: return zt_launch<Op, 16, 1>(op, out_vec, stage);
-      case 321: return zt_launch<Op, 32, 1>(op, out_vec, stage);
-      case 322: return zt_launch<Op, 32, 2>(op, out_vec, stage);
-      case 324: return zt_launch<Op, 32, 4>(op, out_vec, stage);
-      case 328: return zt_launch<Op, 32, 8>(op, out_vec, stage);
-    }
-    return TSVM_ERR_UNSUPPORTED;
+    return pass<MODE_ZT, Op, Op::R>(op, nullptr, out_vec, stage);
   }
-  template <class Op, int LPR, int CPL>
-  tsvm_status zw_launch(const Op &op, const double *w, int stage) {
-    zw_kernel<Op, LPR, CPL><<<nblk, kThreads, 0, ctx->stream>>>(Z, ldz, k, n, op, scal, w, geo.kz,
-                                                                 part_s);
-    TSVM_LAUNCHED(ctx);
-    return finalize(0, nullptr, Op::NS, Op::NM, stage);
-  }
+  // Z w per row, then the per-row functor
   template <class Op>
   tsvm_status zw(const Op &op, const double *w, int stage) {
-    switch (geo.lpr * 10 + geo.cpl) {
-      case 81: return zw_launch<Op, 8, 1>(op, w, stage);
-      case 161: return zw_launch<Op, 16, 1>(op, w, stage);
-      case 321: return zw_launch<Op, 32, 1>(op, w, stage);
-      case 322: return zw_launch<Op, 32, 2>(op, w, stage);
-      case 324: return zw_launch<Op, 32, 4>(op, w, stage);
-      case 328: return zw_launch<Op, 32, 8>(op, w, stage);
-    }
-    return TSVM_ERR_UNSUPPORTED;
+    return pass<MODE_ZW, Op, Op::R>(op, w, nullptr, stage);
   }
-  template <int R, int LPR, int CPL>
-  tsvm_status zgz_launch(const double *g, double *w) {
-    constexpr int RPW = 32 / LPR;
-    const size_t smem_red = sizeof(double) * (size_t)kWarps * RPW * R * LPR * CPL * 4;
-    auto kern = zgz_kernel<R, LPR, CPL>;
-    if (smem_red > 48 * 1024)
-      TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem_red));
-    kern<<<nblk, kThreads, smem_red, ctx->stream>>>(Z, ldz, k, n, dinv, g, geo.kz, part_vec);
-    TSVM_LAUNCHED(ctx);
-    return finalize(R * geo.kz, w, 0, 0, ST_NONE);
-  }
+  // Z^T D^-1 Z g for R vectors g
   template <int R>
   tsvm_status zgz(const double *g, double *w) {
-    switch (geo.lpr * 10 + geo.cpl) {
-      case 81: return zgz_launch<R, 8, 1>(g, w);
-      case 161: return zgz_launch<R, 16, 1>(g, w);
-      case 321: return zgz_launch<R, 32, 1>(g, w);
-      case 322: return zgz_launch<R, 32, 2>(g, w);
-      case 324: return zgz_launch<R, 32, 4>(g, w);
-      case 328: return zgz_launch<R, 32, 8>(g, w);
-    }
-    return TSVM_ERR_UNSUPPORTED;
+    return pass<MODE_ZGZ, GramVecOp, R>(GramVecOp{}, g, w, ST_NONE);
   }
   // Iterative refinement of the capacitance solve M g = h0 against the exact M (M~ factored in
   // M_fac): per sweep one pass over Z for w = Z^T D^-1 Z g, then g += M~^-1 (h0 - g - w).
   template <int R>
-  tsvm_status refine(const double *M_fac, const double *h0, double *g, double *w, double *c,
-                     int sweeps) {
+  tsvm_status refine(const double *M_fac, const double *M_dinv, const double *h0, double *g,
+                     double *w, double *c, int sweeps) {
     for (int sweep = 0; sweep < sweeps; ++sweep) {
       TSVM_TRY(zgz<R>(g, w));
       refine_resid_kernel<<<1, 256, 0, ctx->stream>>>(h0, g, w, c, R, geo.kz, k, scal, info,
                                                         sweep == 0 ? 1 : 0);
       TSVM_LAUNCHED(ctx);
-      TSVM_TRY(potrs_fp64(ctx, M_fac, k, k, c, R, geo.kz));
+      TSVM_TRY(potrs_fp64(ctx, M_fac, k, k, M_dinv, c, R, geo.kz));
       kvec_add<<<(unsigned)ceil_div(R * geo.kz, 256), 256, 0, ctx->stream>>>(g, c, R * geo.kz);
       TSVM_LAUNCHED(ctx);
     }
@@ -819,15 +799,34 @@ struct Runner {
   }
   template <class Op>
   tsvm_status vec(const Op &op, int stage) {
-    vec_kernel<Op><<<nblk, kThreads, 0, ctx->stream>>>(n, op, scal, part_s);
+    auto kern = vec_kernel<Op>;
+    const int grid = grid_for(reinterpret_cast<const void *>(kern), 0);
+    kern<<<grid, kThreads, 0, ctx->stream>>>(n, op, scal, part_s);
     TSVM_LAUNCHED(ctx);
     if (Op::NS + Op::NM == 0 && stage == ST_NONE) return TSVM_OK;
-    return finalize(0, nullptr, Op::NS, Op::NM, stage);
+    return finalize(grid, 0, nullptr, Op::NS, Op::NM, stage);
   }
-  tsvm_status finalize(int nvec, double *out_vec, int ns, int nm, int stage) {
-    const int vb = (nvec + 127) / 128;
-    finalize_kernel<<<vb + 1, 128, 0, ctx->stream>>>(part_vec, nblk, nvec, out_vec, part_s, ns, nm,
-                                                      scal, stage, info);
+  // Grid of an elementwise launch: all blocks resident at once (the kernels stride over the
+  // rows), at most nblk (the capacity of the partial-sum buffers).
+  std::unordered_map<const void *, int> occ_cache;
+  int grid_for(const void *kern, size_t smem) {
+    auto it = occ_cache.find(kern);
+    int occ;
+    if (it != occ_cache.end()) {
+      occ = it->second;
+    } else {
+      occ = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, smem) != cudaSuccess)
+        occ = 1;
+      occ = std::max(1, occ);
+      occ_cache[kern] = occ;
+    }
+    return std::max(1, std::min(nblk, occ * ctx->num_sms));
+  }
+  tsvm_status finalize(int nparts, int nvec, double *out_vec, int ns, int nm, int stage) {
+    const int vb = (nvec + 31) / 32;
+    finalize_kernel<<<vb + 1, 256, 0, ctx->stream>>>(part_vec, nparts, nvec, out_vec, part_s, ns,
+                                                      nm, scal, stage, info);
     TSVM_LAUNCHED(ctx);
     return TSVM_OK;
   }
@@ -854,7 +853,8 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
   double *vecbuf = nullptr, *sbuf = nullptr, *M = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_IPM_VEC, (size_t)11 * n, &vecbuf));
   TSVM_TRY(scratch_t(ctx, SLOT_IPM_SCAL, (size_t)kNScal + 10 * (size_t)kz + 64, &sbuf));
-  TSVM_TRY(scratch_t(ctx, SLOT_IPM_M, (size_t)k * k, &M));
+  TSVM_TRY(scratch_t(ctx, SLOT_IPM_M, (size_t)k * k + (size_t)ceil_div(k, 32) * 1024, &M));
+  double *Mdinv = M + (size_t)k * k;   // inverses of the 32 x 32 diagonal blocks of chol(M)
   double *part = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_IPM_PART, (size_t)run.nblk * (2 * kz + 16), &part));
   run.part_vec = part;
@@ -866,7 +866,8 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
   double *wv = h0 + 2 * kz;            // 2 x kz  Z^T D^-1 Z g
   double *cv = wv + 2 * kz;            // 2 x kz  residual / correction
   run.info = reinterpret_cast<int *>(cv + 2 * kz);   // [0] Cholesky/refinement status,
-  int *big_count = run.info + 1;                     // [1] rows summed exactly in FP64
+  int *big_count = run.info + 1;                     // [1] rows summed exactly in FP64,
+  run.err = run.info + 2;                            // [2] streaming-pass timeout
 
   Vecs V;
   V.x = vecbuf;
@@ -895,7 +896,7 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
     TSVM_TRY(scratch_t(ctx, SLOT_IPM_IDX, (size_t)n + 8, &big_idx));
     TSVM_TRY(scratch_t(ctx, SLOT_SMALL3, (size_t)k * k, &G64));
   }
-  int host_info[2] = {0, 0};
+  int host_info[3] = {0, 0, 0};
   int64_t exact_rows_sum = 0;
   int exact_rows_max = 0, syrk_retries = 0, mixed_iters = 0;
   double res_max = 0.0;
@@ -904,7 +905,7 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
   hsc[I_C] = C;
   hsc[I_N] = (double)n;
   TSVM_CUDA(cudaMemcpyAsync(run.scal, hsc, sizeof(hsc), cudaMemcpyHostToDevice, ctx->stream));
-  TSVM_CUDA(cudaMemsetAsync(run.info, 0, sizeof(int), ctx->stream));
+  TSVM_CUDA(cudaMemsetAsync(run.info, 0, 3 * sizeof(int), ctx->stream));
 
   // ---- initial point (tensorsvm-train.cu:1535-1579) ----
   double ox;
@@ -953,17 +954,16 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
     TSVM_TRY(run.zw(ResidOp{V, 0.0}, q, ST_RESID));
     TSVM_CUDA(cudaMemcpyAsync(ctx->host_scalars, run.scal, sizeof(double) * kNScal,
                               cudaMemcpyDeviceToHost, ctx->stream));
-    if (mixed)
-      TSVM_CUDA(cudaMemcpyAsync(host_info, run.info, sizeof(host_info), cudaMemcpyDeviceToHost,
-                                ctx->stream));
+    TSVM_CUDA(cudaMemcpyAsync(host_info, run.info, sizeof(host_info), cudaMemcpyDeviceToHost,
+                              ctx->stream));
     TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
     memcpy(sc, ctx->host_scalars, sizeof(sc));
+    if (host_info[2]) return TSVM_ERR_TIMEOUT;
     if (pending_events) {
       ms_syrk += event_ms(ev_syrk0, ev_syrk1);
       ms_factor += event_ms(ev_syrk1, ev_chol1);
       pending_events = false;
     }
-    bool retry = false;
     if (mixed && iter > 0) {  // bookkeeping of the previous iteration's mixed SYRK
       exact_rows_sum += host_info[1];
       exact_rows_max = std::max(exact_rows_max, host_info[1]);
@@ -975,7 +975,6 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
         // the step was not taken: redo the iteration with more rows summed exactly
         ++syrk_retries;
         tau = tau > 1e-6 ? tau / 64.0 : 0.0;
-        retry = true;
         if (opt.verbose) printf("mixed SYRK: retry with tau=%.3e\n", tau);
       } else {
         if (opt.verbose)
@@ -989,7 +988,6 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
       if (r > 1e-4) tau /= 8.0;
       else if (r < 1e-6 && tau < 1e30) tau *= 2.0;
     }
-    (void)retry;
     const double mu = sc[I_MU], nrd = sc[I_NORMRD], nrp = fabs(sc[I_RP]), cond = sc[I_COND];
     if (t_gap < 0 && sc[I_RELGAP] <= 1e-6) {
       const double scale = 1.0 + sqrt((double)n);
@@ -1036,7 +1034,7 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
       TSVM_TRY(small_add_diag(ctx, M, k, k, 1.0));
     }
     TSVM_CUDA(cudaEventRecord(ev_syrk1, ctx->stream));
-    TSVM_TRY(chol_fp64(ctx, M, k, k, run.info));
+    TSVM_TRY(chol_fp64(ctx, M, k, k, run.info, Mdinv));
     TSVM_CUDA(cudaEventRecord(ev_chol1, ctx->stream));
     pending_events = true;
     // predictor: r7 = SMW(r5), b = SMW(a) in one pair of passes
@@ -1044,8 +1042,8 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
     if (sweeps)
       TSVM_CUDA(cudaMemcpyAsync(h0, h, sizeof(double) * 2 * kz, cudaMemcpyDeviceToDevice,
                                 ctx->stream));
-    TSVM_TRY(potrs_fp64(ctx, M, k, k, h, 2, kz));
-    if (sweeps) TSVM_TRY(run.refine<2>(M, h0, h, wv, cv, sweeps));
+    TSVM_TRY(potrs_fp64(ctx, M, k, k, Mdinv, h, 2, kz));
+    if (sweeps) TSVM_TRY(run.refine<2>(M, Mdinv, h0, h, wv, cv, sweeps));
     TSVM_TRY(run.zw(SmwBack2Op{V}, h, ST_DYA));
     TSVM_TRY(run.vec(AffineOp{V, C, 0.0}, ST_ALPHA_AFF));
     TSVM_TRY(run.vec(MuAffOp{V, C, 0.0}, ST_SIGMA));
@@ -1054,8 +1052,8 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
     if (sweeps)
       TSVM_CUDA(cudaMemcpyAsync(h0, h, sizeof(double) * kz, cudaMemcpyDeviceToDevice,
                                 ctx->stream));
-    TSVM_TRY(potrs_fp64(ctx, M, k, k, h, 1, kz));
-    if (sweeps) TSVM_TRY(run.refine<1>(M, h0, h, wv, cv, sweeps));
+    TSVM_TRY(potrs_fp64(ctx, M, k, k, Mdinv, h, 1, kz));
+    if (sweeps) TSVM_TRY(run.refine<1>(M, Mdinv, h0, h, wv, cv, sweeps));
     TSVM_TRY(run.zw(CorrBackOp{V}, h, ST_DYC));
     TSVM_TRY(run.vec(CombineOp{V, C, 0.0, 0.0}, ST_ALPHA));
     TSVM_TRY(run.vec(UpdateOp{V, 0.0, true}, ST_NONE));
@@ -1195,6 +1193,8 @@ tsvm_status bias_rbf(tsvm_context *ctx, const float *Z, int ldz, const float *y,
   int *idx = reinterpret_cast<int *>(out + 4);
   int *cnt = idx + 64;
   run.info = cnt + 1;
+  run.err = cnt + 2;
+  TSVM_CUDA(cudaMemsetAsync(run.err, 0, sizeof(int), ctx->stream));
   TSVM_TRY(run.vec(BiasCountOp{alpha, C}, ST_INIT));  // counts into I_E2SUM / I_E2SQ slots
   TSVM_TRY(run.zt(BiasRhsOp{alpha}, v, ST_NONE));
   first_free_kernel<<<1, 1024, 0, ctx->stream>>>(alpha, n, C, 50, idx, cnt);
@@ -1202,9 +1202,12 @@ tsvm_status bias_rbf(tsvm_context *ctx, const float *Z, int ldz, const float *y,
   bias_terms_kernel<<<1, 256, 0, ctx->stream>>>(Z, ldz, k, y, v, idx, cnt, out);
   TSVM_LAUNCHED(ctx);
   double hs[2], hb[2];
+  int herr = 0;
   TSVM_CUDA(cudaMemcpyAsync(hs, run.scal + I_E2SUM, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
   TSVM_CUDA(cudaMemcpyAsync(hb, out, sizeof(hb), cudaMemcpyDeviceToHost, ctx->stream));
+  TSVM_CUDA(cudaMemcpyAsync(&herr, run.err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (herr) return TSVM_ERR_TIMEOUT;
   if (nsv) *nsv = (int32_t)hs[0];
   if (nfree) *nfree = (int32_t)hs[1];
   if (b) *b = hb[0];

@@ -57,14 +57,19 @@ tsvm_status apply_right_fp32(tsvm_context *ctx, const float *A, int64_t n, int k
                              const float *R, float *Out);
 
 // ---- dense.cu (small k x k FP64, single device) ----------------------------------------
-// In-place lower Cholesky of the n x n row-major matrix A (lda); *info_dev receives 0 or the
-// 1-based failing column. Upper triangle is left untouched.
-tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_dev);
-// Solve (L L^T) X = B for nrhs right-hand sides stored as rows of B (nrhs x ldb).
-tsvm_status potrs_fp64(tsvm_context *ctx, const double *L, int n, int lda, double *B, int nrhs,
-                       int ldb);
+// In-place lower Cholesky of the n x n row-major matrix A (lda, n <= 864); *info_dev receives 0
+// or the 1-based failing column.  Dinv (ceil(n/32) blocks of 32 x 32 doubles) receives the
+// inverses of the diagonal 32 x 32 blocks of L, used by potrs_fp64 and trinv_lower_fp64.
+// The upper triangle is left untouched.
+tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_dev, double *Dinv);
+// Dinv of an existing lower factor L (as chol_fp64 writes it).
+tsvm_status tri_diag_inverse(tsvm_context *ctx, const double *L, int n, int lda, double *Dinv);
+// Solve (L L^T) X = B for nrhs (<= 4) right-hand sides stored as rows of B (nrhs x ldb).
+tsvm_status potrs_fp64(tsvm_context *ctx, const double *L, int n, int lda, const double *Dinv,
+                       double *B, int nrhs, int ldb);
 // Lower-triangular inverse: Linv = L^-1 (both n x n row-major, lda).
-tsvm_status trinv_lower_fp64(tsvm_context *ctx, const double *L, int n, int lda, double *Linv);
+tsvm_status trinv_lower_fp64(tsvm_context *ctx, const double *L, int n, int lda,
+                             const double *Dinv, double *Linv);
 // Symmetric eigen-decomposition by cyclic Jacobi: A (n x n, lda) is overwritten; w (n) gets
 // the eigenvalues, V (n x n row-major) the eigenvectors as COLUMNS.
 tsvm_status eig_jacobi_fp64(tsvm_context *ctx, double *A, int n, int lda, double *w, double *V,

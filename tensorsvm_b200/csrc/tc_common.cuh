@@ -66,6 +66,16 @@ __device__ __forceinline__ void tma_load_2d(const CUtensorMap *map, uint32_t bar
       "l"(map), "r"(bar), "r"(x), "r"(y)
       : "memory");
 }
+// One contiguous global -> shared copy (dst, src and bytes multiples of 16), completion counted
+// on the mbarrier `bar` (no multicast).
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes,
+                                          uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
 __device__ __forceinline__ void fence_barrier_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }

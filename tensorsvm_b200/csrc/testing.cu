@@ -46,7 +46,9 @@ tsvm_status tsvm_test_chol(tsvm_context *ctx, double *A, int32_t n, int32_t *inf
   if (!ctx || !A || n < 1) return TSVM_ERR_INVALID_ARGUMENT;
   int *info = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_MISC, 16, &info));
-  TSVM_TRY(chol_fp64(ctx, A, n, n, info));
+  double *Dinv = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_SMALL2, (size_t)ceil_div(n, 32) * 1024, &Dinv));
+  TSVM_TRY(chol_fp64(ctx, A, n, n, info, Dinv));
   int h = 0;
   TSVM_CUDA(cudaMemcpyAsync(&h, info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -57,7 +59,10 @@ tsvm_status tsvm_test_chol(tsvm_context *ctx, double *A, int32_t n, int32_t *inf
 tsvm_status tsvm_test_potrs(tsvm_context *ctx, const double *L, int32_t n, double *B,
                             int32_t nrhs, int32_t ldb) {
   if (!ctx || !L || !B || n < 1 || ldb < n) return TSVM_ERR_INVALID_ARGUMENT;
-  TSVM_TRY(potrs_fp64(ctx, L, n, n, B, nrhs, ldb));
+  double *Dinv = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_SMALL2, (size_t)ceil_div(n, 32) * 1024, &Dinv));
+  TSVM_TRY(tri_diag_inverse(ctx, L, n, n, Dinv));
+  TSVM_TRY(potrs_fp64(ctx, L, n, n, Dinv, B, nrhs, ldb));
   TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
   return TSVM_OK;
 }
