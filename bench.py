@@ -132,6 +132,17 @@ def barrier(world):
 # our arm
 # ------------------------------------------------------------------------------------------
 
+# DRAM bytes (read + write) per 128 x 64 tile of the tensor-core kernel-block product at k = 256,
+# from one ncu capture at n = 262144 (2.389 GB read + 0.258 GB written, 2048 x 4096 tiles): the
+# J-side operands are re-read once per round of 148 row blocks, so traffic grows with the tiles.
+TC_BYTES_PER_TILE = (2.389420e9 + 0.258439e9) / (2048 * 4096)
+
+
+def tc_traffic(n: int) -> float:
+    tiles = -(-n // 128) * -(-n // 64)
+    return round(TC_BYTES_PER_TILE * tiles, -6)
+
+
 def run_ours(args, world, rank, local):
     import torch
     from tensorsvm_b200 import _lib, api, synth
@@ -240,7 +251,11 @@ def run_ours(args, world, rank, local):
         "roofline": {"bound": "tensor" if tensor else "fp32-simt", "kernel": "kermatmul (fused kernel-block product)",
                      "achieved": round(achieved, 2), "peak": round(peak, 1), "unit": unit,
                      "frac": round(achieved / peak, 4), "peak_source": f"{pk_kind} {pname}",
-                     "traffic": None, "flops_per_launch": km_flops, "ms_per_launch": round(km_ms, 3)},
+                     "traffic": tc_traffic(n) if tensor else None,
+                     "traffic_source": ("dram__bytes_read.sum + dram__bytes_write.sum of one launch "
+                                        "at n=262144 (2.648 GB over 2048x4096 tiles), scaled by "
+                                        "the tile count" if tensor else None),
+                     "flops_per_launch": km_flops, "ms_per_launch": round(km_ms, 3)},
         "e2e": {"value": round(e2e_s, 4), "unit": "s",
                 "h2d_bytes_per_step": int(X.nbytes + y.nbytes), "d2h_bytes_per_step": int(8 * n + 8)},
         "gpu_launches": int(launches),
