@@ -106,6 +106,25 @@ typedef struct tsvm_ipm_stats {
   double exact_rows_mean, refine_res_max;
 } tsvm_ipm_stats;
 
+/* One problem of a batched interior-point solve (all problems share k and ldz). */
+typedef struct tsvm_ipm_problem {
+  const float *Z;      /* device, n x ldz row-major factor (columns k..ldz-1 ignored) */
+  const float *y;      /* device, n labels in {+1, -1} */
+  int64_t n;
+  double C;
+  double *alpha_out;   /* device, n */
+  double *xi_out;      /* device, n, or NULL */
+} tsvm_ipm_problem;
+
+/* How a batched solve ran. */
+typedef struct tsvm_batch_info {
+  int32_t units;       /* work units of the streaming passes (a unit is a row range of one problem) */
+  int32_t unit_rows;   /* rows per unit chosen by the autotuner */
+  int32_t graph_used;  /* 1 if the iterations were replayed from a captured CUDA graph */
+  int32_t iters_max;   /* iterations of the slowest problem */
+  double ms_total, ms_autotune;
+} tsvm_batch_info;
+
 /* Human-readable status. */
 const char *tsvm_status_string(tsvm_status s);
 
@@ -153,6 +172,20 @@ tsvm_status tsvm_linear_factor(tsvm_context *ctx, const float *X, const float *y
 tsvm_status tsvm_ipm(tsvm_context *ctx, const float *Z, int32_t ldz, const float *y, int64_t n,
                      int32_t k, double C, const tsvm_ipm_options *opt, double *alpha_out,
                      double *xi_out, double *ymult_out, tsvm_ipm_stats *stats);
+
+/* Batched interior-point solve (replaces running mpc, T:1507-1840, once per problem): `count`
+ * independent SVM duals of uneven n -- one-vs-rest classes, a (C, gamma) grid, folds -- solved
+ * together.  Every streaming pass is one launch over work units (row ranges of one problem)
+ * of all unconverged problems, the k x k Cholesky and solves are one launch with a CTA per
+ * problem, the host synchronises once per iteration for all stopping rules, and from the second
+ * iteration on the iteration's launches are replayed from a captured CUDA graph.  The unit
+ * size is autotuned on the first pass.  The capacitance matrices are summed in FP64 (the
+ * reference's DSYRK numerics); opt->precision is not used.  stats[count] receives each
+ * problem's statistics (status in stats[i].status); the call returns TSVM_OK when every
+ * problem ended with a usable alpha (OK, WARN_*), else the first failing status. */
+tsvm_status tsvm_ipm_batched(tsvm_context *ctx, const tsvm_ipm_problem *problems, int32_t count,
+                             int32_t k, int32_t ldz, const tsvm_ipm_options *opt,
+                             tsvm_ipm_stats *stats, tsvm_batch_info *info);
 
 /* Bias of the RBF model (replaces tensorsvm-train.cu:355-376): the mean over the first <= 50
  * free SVs j (1e-6 < alpha_j < C - 1e-6, in index order) of y_j - sum_{i in SV} alpha_i y_j

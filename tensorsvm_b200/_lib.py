@@ -39,12 +39,24 @@ EXPORTS = [
     "tsvm_status_string", "tsvm_create", "tsvm_destroy", "tsvm_set_stream",
     "tsvm_ipm_default_options",
     "tsvm_factor", "tsvm_linear_factor", "tsvm_ipm", "tsvm_bias", "tsvm_bias_noalloc",
-    "tsvm_train", "tsvm_kernel_launches",
+    "tsvm_train", "tsvm_kernel_launches", "tsvm_ipm_batched",
 ]
 TEST_EXPORTS = [
     "tsvm_test_rand_stream", "tsvm_test_sketch", "tsvm_test_kermatmul", "tsvm_test_chol",
     "tsvm_test_potrs", "tsvm_test_eig", "tsvm_test_gram", "tsvm_test_syrk_mixed",
 ]
+
+
+class IpmProblem(ctypes.Structure):
+    _fields_ = [("Z", ctypes.c_void_p), ("y", ctypes.c_void_p), ("n", ctypes.c_int64),
+                ("C", ctypes.c_double), ("alpha_out", ctypes.c_void_p),
+                ("xi_out", ctypes.c_void_p)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("units", ctypes.c_int32), ("unit_rows", ctypes.c_int32),
+                ("graph_used", ctypes.c_int32), ("iters_max", ctypes.c_int32),
+                ("ms_total", ctypes.c_double), ("ms_autotune", ctypes.c_double)]
 
 
 class FactorInfo(ctypes.Structure):
@@ -117,6 +129,10 @@ def load() -> ctypes.CDLL:
     lib.tsvm_train.argtypes = [P, P, P, I64, I32, I32, D, D, I32, I32, ctypes.POINTER(IpmOptions),
                                P, ctypes.POINTER(D), ctypes.POINTER(FactorInfo),
                                ctypes.POINTER(IpmStats)]
+    lib.tsvm_ipm_batched.restype = ctypes.c_int
+    lib.tsvm_ipm_batched.argtypes = [P, ctypes.POINTER(IpmProblem), I32, I32, I32,
+                                     ctypes.POINTER(IpmOptions), ctypes.POINTER(IpmStats),
+                                     ctypes.POINTER(BatchInfo)]
     lib.tsvm_kernel_launches.restype = ctypes.c_int64
     lib.tsvm_kernel_launches.argtypes = [P]
     # test hooks (include/tensorsvm_testing.h)

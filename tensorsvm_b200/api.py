@@ -61,6 +61,28 @@ def ipm(ctx, Z, y, k: int, C: float, kernel: int = _lib.KERNEL_RBF, want_xi: boo
     return alpha, xi, ym.value, s
 
 
+def ipm_batched(ctx, Zs, ys, k: int, Cs, kernel: int = _lib.KERNEL_RBF, **opts):
+    """Solve len(Zs) duals together (tsvm_ipm_batched).  Zs: CUDA float32 tensors n_i x ldz (one
+    ldz for all), ys: CUDA float32 labels, Cs: penalties.  Returns (alphas, stats list, info)."""
+    import torch
+    count = len(Zs)
+    ldz = Zs[0].shape[1]
+    if any(Z.shape[1] != ldz for Z in Zs):
+        raise ValueError("all problems need the same ldz")
+    alphas = [torch.empty(Z.shape[0], dtype=torch.float64, device=Z.device) for Z in Zs]
+    probs = (_lib.IpmProblem * count)()
+    for i, (Z, y, C, a) in enumerate(zip(Zs, ys, Cs, alphas)):
+        probs[i].Z, probs[i].y, probs[i].n = _ptr(Z), _ptr(y), Z.shape[0]
+        probs[i].C, probs[i].alpha_out, probs[i].xi_out = float(C), _ptr(a), None
+    o = _lib.default_options(kernel=kernel, **opts)
+    stats = (_lib.IpmStats * count)()
+    info = _lib.BatchInfo()
+    st = ctx.lib.tsvm_ipm_batched(ctx.handle, probs, count, k, ldz, ctypes.byref(o), stats,
+                                  ctypes.byref(info))
+    _lib.check(st, "tsvm_ipm_batched", allow=(_lib.ERR_NOT_SPD,))
+    return alphas, [_fields(s) for s in stats], _fields(info)
+
+
 def bias(ctx, Z, y, alpha, k: int, C: float):
     n, ldz = Z.shape
     b, bs = ctypes.c_double(), ctypes.c_double()

@@ -186,6 +186,25 @@ tsvm_status tsvm_ipm(tsvm_context *ctx, const float *Z, int32_t ldz, const float
   return ipm_solve(ctx, Z, ldz, y, n, k, C, o, alpha_out, xi_out, ymult_out, stats);
 }
 
+tsvm_status tsvm_ipm_batched(tsvm_context *ctx, const tsvm_ipm_problem *problems, int32_t count,
+                             int32_t k, int32_t ldz, const tsvm_ipm_options *opt,
+                             tsvm_ipm_stats *stats, tsvm_batch_info *info) {
+  if (!ctx || !problems || count < 1 || k < 1 || ldz < k || (ldz % 4) != 0)
+    return TSVM_ERR_INVALID_ARGUMENT;
+  for (int32_t p = 0; p < count; ++p) {
+    const tsvm_ipm_problem &q = problems[p];
+    if (!q.Z || !q.y || !q.alpha_out || q.n < 2 || !(q.C > 0) ||
+        (reinterpret_cast<uintptr_t>(q.Z) & 15) != 0)
+      return TSVM_ERR_INVALID_ARGUMENT;
+  }
+  tsvm_ipm_options o;
+  tsvm_ipm_default_options(&o);
+  if (opt) o = *opt;
+  if (o.max_iter < 0 || !(o.tol > 0)) return TSVM_ERR_INVALID_ARGUMENT;
+  TSVM_CUDA(cudaSetDevice(ctx->device));
+  return ipm_solve_batched(ctx, problems, count, k, ldz, o, stats, info);
+}
+
 tsvm_status tsvm_bias(tsvm_context *ctx, const float *Z, int32_t ldz, const float *y,
                       const double *alpha, int64_t n, int32_t k, double C, double *b_out,
                       double *b_std_out, int32_t *n_sv, int32_t *n_free) {

@@ -36,6 +36,12 @@ enum Slot : int {
   SLOT_IPM_PART,      // IPM / bias streaming partial sums (kept apart from SLOT_PART, which the
                       // Z^T D^-1 Z accumulation may regrow inside the iteration)
   SLOT_MISC,
+  SLOT_B_VEC,         // batched IPM: concatenated fp64 vectors and labels of all problems
+  SLOT_B_TABLE,       // batched IPM: work units, unit offsets, Z pointers, flags
+  SLOT_B_SCAL,        // batched IPM: per-problem scalars and k-vectors
+  SLOT_B_M,           // batched IPM: per-problem capacitance matrices and factors
+  SLOT_B_GPART,       // batched IPM: per-unit partial Gram matrices
+  SLOT_B_PART,        // batched IPM: per-unit streaming partial sums
   SLOT_DEV_IN,        // tsvm_train: device copies of host inputs
   SLOT_DEV_Z,         // tsvm_train: factor Z
   SLOT_DEV_OUT,       // tsvm_train: device alpha

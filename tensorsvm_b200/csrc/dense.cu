@@ -53,7 +53,14 @@ __device__ void tri_inverse_block(const double *Dg, double *Di, int nb, const do
 //      (4 x 4 register tiles per thread).
 __global__ void __launch_bounds__(1024) chol_kernel(double *__restrict__ A, int n, int lda,
                                                     double *__restrict__ Dinv,
-                                                    int *__restrict__ info) {
+                                                    int *__restrict__ info, int64_t strideA,
+                                                    int64_t strideD,
+                                                    const int *__restrict__ active) {
+  // batched launches: problem blockIdx.x
+  if (active && !active[blockIdx.x]) return;
+  A += blockIdx.x * strideA;
+  Dinv += blockIdx.x * strideD;
+  info += blockIdx.x;
   extern __shared__ double PT[];  // [kNB][ldp] panel, transposed: PT[c][i] = L[r0 + i][jb + c]
   __shared__ double Dg[kNB * kDP], Di[kNB * kDP];
   __shared__ double piv[2], rdiag[kNB];
@@ -189,7 +196,15 @@ __global__ void __launch_bounds__(1024) diag_inverse_kernel(const double *__rest
 // 1024 threads.
 __global__ void __launch_bounds__(1024) potrs_kernel(const double *__restrict__ L, int n, int lda,
                                                     const double *__restrict__ Dinv,
-                                                    double *__restrict__ B, int nrhs, int ldb) {
+                                                    double *__restrict__ B, int nrhs, int ldb,
+                                                    int64_t strideA, int64_t strideD,
+                                                    int64_t strideB,
+                                                    const int *__restrict__ active) {
+  // batched launches: problem blockIdx.x
+  if (active && !active[blockIdx.x]) return;
+  L += blockIdx.x * strideA;
+  Dinv += blockIdx.x * strideD;
+  B += blockIdx.x * strideB;
   extern __shared__ double y[];      // [nrhs][n], then the backward partials [32][4][kNB]
   double *part = y + (size_t)nrhs * n;
   __shared__ double t[4][kNB];
@@ -435,7 +450,20 @@ tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_de
   const size_t smem = sizeof(double) * (size_t)kNB * (size_t)(n > kNB ? n - kNB : 1);
   TSVM_CUDA(cudaFuncSetAttribute(chol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
-  chol_kernel<<<1, 1024, smem, ctx->stream>>>(A, n, lda, Dinv, info_dev);
+  chol_kernel<<<1, 1024, smem, ctx->stream>>>(A, n, lda, Dinv, info_dev, 0, 0, nullptr);
+  TSVM_LAUNCHED(ctx);
+  return TSVM_OK;
+}
+
+tsvm_status chol_fp64_batched(tsvm_context *ctx, double *A, int n, int lda, int64_t strideA,
+                              int *info_dev, double *Dinv, int64_t strideD, int count,
+                              const int *active) {
+  if (n < 1 || n > kMaxDense || count < 1) return TSVM_ERR_UNSUPPORTED;
+  const size_t smem = sizeof(double) * (size_t)kNB * (size_t)(n > kNB ? n - kNB : 1);
+  TSVM_CUDA(cudaFuncSetAttribute(chol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  chol_kernel<<<count, 1024, smem, ctx->stream>>>(A, n, lda, Dinv, info_dev, strideA, strideD,
+                                                  active);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;
 }
@@ -453,7 +481,20 @@ tsvm_status potrs_fp64(tsvm_context *ctx, const double *L, int n, int lda, const
   const size_t smem = sizeof(double) * ((size_t)nrhs * n + 32 * 4 * kNB);
   TSVM_CUDA(cudaFuncSetAttribute(potrs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
-  potrs_kernel<<<1, 1024, smem, ctx->stream>>>(L, n, lda, Dinv, B, nrhs, ldb);
+  potrs_kernel<<<1, 1024, smem, ctx->stream>>>(L, n, lda, Dinv, B, nrhs, ldb, 0, 0, 0, nullptr);
+  TSVM_LAUNCHED(ctx);
+  return TSVM_OK;
+}
+
+tsvm_status potrs_fp64_batched(tsvm_context *ctx, const double *L, int n, int lda,
+                               int64_t strideA, const double *Dinv, int64_t strideD, double *B,
+                               int nrhs, int ldb, int64_t strideB, int count, const int *active) {
+  if (nrhs < 1 || nrhs > 4 || n < 1 || n > kMaxDense || count < 1) return TSVM_ERR_UNSUPPORTED;
+  const size_t smem = sizeof(double) * ((size_t)nrhs * n + 32 * 4 * kNB);
+  TSVM_CUDA(cudaFuncSetAttribute(potrs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  potrs_kernel<<<count, 1024, smem, ctx->stream>>>(L, n, lda, Dinv, B, nrhs, ldb, strideA,
+                                                   strideD, strideB, active);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;
 }

@@ -17,6 +17,9 @@
 #include <math.h>
 #include <stdio.h>
 
+#include <string.h>
+
+#include <algorithm>
 #include <chrono>
 #include <unordered_map>
 #include <vector>
@@ -308,18 +311,26 @@ __device__ __forceinline__ void block_partials(double *sums, double *mins, doubl
 
 template <class Op>
 __global__ void __launch_bounds__(kThreads)
-vec_kernel(int64_t n, Op op, const double *__restrict__ scal, double *__restrict__ part_s) {
+vec_kernel(int64_t n, Op op, const double *__restrict__ scal, double *__restrict__ part_s,
+           const WorkUnit *__restrict__ units, const int *__restrict__ active) {
   constexpr int NS = Op::NS, NM = Op::NM;
   __shared__ double vsh[(NS + NM > 0 ? NS + NM : 1) * kWarps];
+  int64_t i0 = (int64_t)blockIdx.x * kThreads, i1 = n, istep = (int64_t)gridDim.x * kThreads;
+  if (units) {  // batched: the rows of one work unit, that problem's scalars
+    const WorkUnit u = units[blockIdx.x];
+    if (active && !active[u.p]) return;
+    scal += (size_t)u.p * kNScal;
+    i0 = u.goff;
+    i1 = u.goff + u.rows;
+    istep = kThreads;
+  }
   op.load(scal);
   double sums[NS > 0 ? NS : 1], mins[NM > 0 ? NM : 1];
 #pragma unroll
   for (int j = 0; j < (NS > 0 ? NS : 1); ++j) sums[j] = 0.0;
 #pragma unroll
   for (int j = 0; j < (NM > 0 ? NM : 1); ++j) mins[j] = INFINITY;
-  for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * kThreads)
-    op.row(i, sums, mins);
+  for (int64_t i = i0 + threadIdx.x; i < i1; i += istep) op.row(i, sums, mins);
   if (NS + NM > 0) block_partials<NS, NM>(sums, mins, part_s, vsh);
 }
 
@@ -350,7 +361,9 @@ __global__ void __launch_bounds__(kSThreads, 1)
 stream_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, Op op,
               const double *__restrict__ scal, const double *__restrict__ w,
               const double *__restrict__ dinv, int kz, int stages,
-              double *__restrict__ part_vec, double *__restrict__ part_s, int *__restrict__ err) {
+              double *__restrict__ part_vec, double *__restrict__ part_s, int *__restrict__ err,
+              const WorkUnit *__restrict__ units, const float *const *__restrict__ Zs,
+              const int *__restrict__ active) {
   constexpr int NS = Op::NS, NM = Op::NM;
   constexpr int RPW = 32 / LPR;          // rows per warp step
   constexpr int RW = CR;                 // rows per chunk, all taken by one warp
@@ -367,8 +380,21 @@ stream_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, Op op,
   volatile int *abort = reinterpret_cast<volatile int *>(bars + 2 * stages);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int slot = lane / LPR, sl = lane % LPR;
+  // this CTA's rows: the persistent slice of Z (chunks blockIdx.x, + gridDim.x, ...) or, in a
+  // batched pass, all chunks of one work unit of one problem
+  int64_t goff = 0, q0 = blockIdx.x, qs = gridDim.x;
+  if (units) {
+    const WorkUnit u = units[blockIdx.x];
+    if (active && !active[u.p]) return;
+    Z = Zs[u.p] + u.row0 * ldz;
+    n = u.rows;
+    goff = u.goff;
+    scal += (size_t)u.p * kNScal;
+    if (DOT) w += (size_t)u.p * R * kz;
+    q0 = 0;
+    qs = 1;
+  }
   const int64_t nchunks = (n + CR - 1) / CR;
-  const int G = gridDim.x;
   if (threadIdx.x == 0) {
     for (int s = 0; s < stages; ++s) {
       tc::mbar_init(b_full + 8 * s, 1);
@@ -402,7 +428,7 @@ stream_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, Op op,
     if (lane == 0) {
       int st = 0;
       uint32_t ph = 0;
-      for (int64_t q = blockIdx.x; q < nchunks; q += G) {
+      for (int64_t q = q0; q < nchunks; q += qs) {
         if (!tc::mbar_wait(b_empty + 8 * st, ph ^ 1, abort)) break;
         const int64_t r0 = q * CR;
         const uint32_t bytes = (uint32_t)((n - r0 < CR ? n - r0 : CR) * ldz * 4);
@@ -413,8 +439,8 @@ stream_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, Op op,
     }
   } else {
     int64_t j = warp;   // index of the chunk among this CTA's chunks
-    for (int64_t q = blockIdx.x + (int64_t)warp * G; q < nchunks;
-         q += (int64_t)kSConsumers * G, j += kSConsumers) {
+    for (int64_t q = q0 + (int64_t)warp * qs; q < nchunks;
+         q += (int64_t)kSConsumers * qs, j += kSConsumers) {
       const int st = (int)(j % stages);
       const uint32_t ph = (uint32_t)((j / stages) & 1);
       if (!tc::mbar_wait(b_full + 8 * st, ph, abort)) break;
@@ -424,7 +450,7 @@ stream_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, Op op,
 #pragma unroll
       for (int r = 0; r < R; ++r) v[r] = 0.0;
       if constexpr (MODE == MODE_ZT) {
-        if (lane < RW && r0 + lane < n) op.rhs(r0 + lane, v, sums, mins);
+        if (lane < RW && r0 + lane < n) op.rhs(goff + r0 + lane, v, sums, mins);
       }
       double mine[R];
 #pragma unroll
@@ -479,7 +505,7 @@ stream_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, Op op,
                 if (lane == step * RPW + s2) mine[r] = got;
               }
           } else {
-            const double di = in ? dinv[row] : 0.0;
+            const double di = in ? dinv[goff + row] : 0.0;
 #pragma unroll
             for (int r = 0; r < R; ++r) vr[r] = d[r] * di;
           }
@@ -502,7 +528,7 @@ stream_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, Op op,
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(b_empty + 8 * st);
       if constexpr (MODE == MODE_ZW) {
-        if (lane < RW && r0 + lane < n) op.row(r0 + lane, mine, sums, mins);
+        if (lane < RW && r0 + lane < n) op.row(goff + r0 + lane, mine, sums, mins);
       }
     }
   }
@@ -603,45 +629,9 @@ __global__ void kvec_add(double *__restrict__ g, const double *__restrict__ c, i
   if (e < count) g[e] += c[e];
 }
 
-// Sum block partials in fixed order; the last block also reduces the scalars and runs the
-// scalar stage of the iteration.
-__global__ void finalize_kernel(const double *__restrict__ part_vec, int nblk, int nvec,
-                                double *__restrict__ out_vec, const double *__restrict__ part_s,
-                                int ns, int nm, double *__restrict__ sc, int stage,
-                                const int *__restrict__ info) {
-  // vector blocks: 32 entries each, the partials split over 8 warps (strided), then summed in
-  // warp order -- a fixed order, independent of timing
-  const int vb = (nvec + 31) / 32;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if ((int)blockIdx.x < vb) {
-    __shared__ double vsum[8][32];
-    const int e = blockIdx.x * 32 + lane;
-    double s = 0.0;
-    if (e < nvec) {
-#pragma unroll 4
-      for (int b = warp; b < nblk; b += 8) s += part_vec[(int64_t)b * nvec + e];
-    }
-    vsum[warp][lane] = s;
-    __syncthreads();
-    if (warp == 0 && e < nvec) {
-      double t = 0.0;
-      for (int w = 0; w < 8; ++w) t += vsum[w][lane];
-      out_vec[e] = t;
-    }
-    return;
-  }
-  __shared__ double red[16];
-  for (int j = warp; j < ns + nm; j += 8) {
-    double r = j < ns ? 0.0 : INFINITY;
-    for (int b = lane; b < nblk; b += 32) {
-      const double v = part_s[(int64_t)b * (ns + nm) + j];
-      r = j < ns ? r + v : fmin(r, v);
-    }
-    r = j < ns ? warp_sum(r) : warp_min(r);
-    if (lane == 0) red[j] = r;
-  }
-  __syncthreads();
-  if (threadIdx.x != 0) return;
+// The scalar algebra of one iteration stage on the reduced sums / minima `red`.
+__device__ void scalar_stage(double *__restrict__ sc, const double *red, int stage,
+                             const int *__restrict__ info) {
   const double n = sc[I_N], C = sc[I_C];
   switch (stage) {
     case ST_INIT:
@@ -700,6 +690,48 @@ __global__ void finalize_kernel(const double *__restrict__ part_vec, int nblk, i
   }
 }
 
+// Sum block partials in fixed order; the last block also reduces the scalars and runs the
+// scalar stage of the iteration.
+__global__ void finalize_kernel(const double *__restrict__ part_vec, int nblk, int nvec,
+                                double *__restrict__ out_vec, const double *__restrict__ part_s,
+                                int ns, int nm, double *__restrict__ sc, int stage,
+                                const int *__restrict__ info) {
+  // vector blocks: 32 entries each, the partials split over 8 warps (strided), then summed in
+  // warp order -- a fixed order, independent of timing
+  const int vb = (nvec + 31) / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if ((int)blockIdx.x < vb) {
+    __shared__ double vsum[8][32];
+    const int e = blockIdx.x * 32 + lane;
+    double s = 0.0;
+    if (e < nvec) {
+#pragma unroll 4
+      for (int b = warp; b < nblk; b += 8) s += part_vec[(int64_t)b * nvec + e];
+    }
+    vsum[warp][lane] = s;
+    __syncthreads();
+    if (warp == 0 && e < nvec) {
+      double t = 0.0;
+      for (int w = 0; w < 8; ++w) t += vsum[w][lane];
+      out_vec[e] = t;
+    }
+    return;
+  }
+  __shared__ double red[16];
+  for (int j = warp; j < ns + nm; j += 8) {
+    double r = j < ns ? 0.0 : INFINITY;
+    for (int b = lane; b < nblk; b += 32) {
+      const double v = part_s[(int64_t)b * (ns + nm) + j];
+      r = j < ns ? r + v : fmin(r, v);
+    }
+    r = j < ns ? warp_sum(r) : warp_min(r);
+    if (lane == 0) red[j] = r;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  scalar_stage(sc, red, stage, info);
+}
+
 // ---------------------------------------------------------------------------------------
 // Host-side driver
 // ---------------------------------------------------------------------------------------
@@ -750,7 +782,8 @@ struct Runner {
     TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int grid = (int)std::min<int64_t>(std::min(nblk, ctx->num_sms), ceil_div(n, CR));
     kern<<<grid, kSThreads, smem, ctx->stream>>>(Z, ldz, k, n, op, scal, w, dinv, geo.kz,
-                                                 (int)stages, part_vec, part_s, err);
+                                                 (int)stages, part_vec, part_s, err, nullptr,
+                                                 nullptr, nullptr);
     TSVM_LAUNCHED(ctx);
     return finalize(grid, MODE != MODE_ZW ? R * geo.kz : 0, out_vec, Op::NS, Op::NM, stage);
   }
@@ -801,7 +834,7 @@ struct Runner {
   tsvm_status vec(const Op &op, int stage) {
     auto kern = vec_kernel<Op>;
     const int grid = grid_for(reinterpret_cast<const void *>(kern), 0);
-    kern<<<grid, kThreads, 0, ctx->stream>>>(n, op, scal, part_s);
+    kern<<<grid, kThreads, 0, ctx->stream>>>(n, op, scal, part_s, nullptr, nullptr);
     TSVM_LAUNCHED(ctx);
     if (Op::NS + Op::NM == 0 && stage == ST_NONE) return TSVM_OK;
     return finalize(grid, 0, nullptr, Op::NS, Op::NM, stage);
@@ -1213,6 +1246,480 @@ tsvm_status bias_rbf(tsvm_context *ctx, const float *Z, int ldz, const float *y,
   if (b) *b = hb[0];
   if (bstd) *bstd = hb[1];
   return TSVM_OK;
+}
+
+
+// ---------------------------------------------------------------------------------------
+// Batched interior-point solve: every pass is one launch over the work units (row ranges of
+// one problem) of all unconverged problems; k x k work is one launch with a CTA per problem.
+// ---------------------------------------------------------------------------------------
+namespace {
+
+// Per-problem reduction of the unit partials (units of problem p are ubeg[p] .. ubeg[p+1]-1,
+// summed in that order) and the scalar stage of each active problem.  One block per problem.
+__global__ void finalize_batched_kernel(const double *__restrict__ part_vec,
+                                        const double *__restrict__ part_s,
+                                        const int *__restrict__ ubeg, int nvec,
+                                        double *__restrict__ out_vec, int ns, int nm,
+                                        double *__restrict__ sc, int stage,
+                                        const int *__restrict__ info,
+                                        const int *__restrict__ active) {
+  const int p = blockIdx.x;
+  if (active && !active[p]) return;
+  const int u0 = ubeg[p], u1 = ubeg[p + 1];
+  for (int e = threadIdx.x; e < nvec; e += blockDim.x) {
+    double s = 0.0;
+    for (int u = u0; u < u1; ++u) s += part_vec[(int64_t)u * nvec + e];
+    out_vec[(int64_t)p * nvec + e] = s;
+  }
+  __shared__ double red[16];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int j = warp; j < ns + nm; j += nw) {
+    double r = j < ns ? 0.0 : INFINITY;
+    for (int u = u0 + lane; u < u1; u += 32) {
+      const double v = part_s[(int64_t)u * (ns + nm) + j];
+      r = j < ns ? r + v : fmin(r, v);
+    }
+    r = j < ns ? warp_sum(r) : warp_min(r);
+    if (lane == 0) red[j] = r;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) scalar_stage(sc + (size_t)p * kNScal, red, stage, info + p);
+}
+
+// M_p = I + sum over the units of p of their partial Gram matrices (lower tiles), mirrored.
+__global__ void gram_units_reduce(const double *__restrict__ part, const int *__restrict__ ubeg,
+                                  int k, const int *__restrict__ active, double *__restrict__ M,
+                                  int64_t strideM) {
+  const int p = blockIdx.y;
+  if (active && !active[p]) return;
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)k * k) return;
+  const int r = (int)(e / k), c = (int)(e % k);
+  if (c > r) return;
+  double s = r == c ? 1.0 : 0.0;
+  for (int u = ubeg[p]; u < ubeg[p + 1]; ++u) s += part[(int64_t)u * k * k + (int64_t)r * k + c];
+  double *Mp = M + p * strideM;
+  Mp[(int64_t)r * k + c] = s;
+  Mp[(int64_t)c * k + r] = s;
+}
+
+// Stages and shared memory of one streaming pass (see Runner::pass_launch).
+template <int MODE, int R, int CR, int LPR, int CPL>
+void stream_config(int64_t ldz, size_t *stages_out, size_t *smem_out) {
+  constexpr int RPW = 32 / LPR;
+  const size_t chunk = (size_t)CR * ldz * 4;
+  size_t stages = std::min<size_t>(16, std::max<size_t>(2, (192 * 1024) / chunk));
+  const size_t red = sizeof(double) * std::max<size_t>(
+      MODE != MODE_ZW ? (size_t)kSConsumers * RPW * R * LPR * CPL * 4 : 0, 16 * 9);
+  while (stages * chunk < red) ++stages;
+  *stages_out = stages;
+  *smem_out = stages * chunk + 8 * (2 * stages + 2);
+}
+
+struct BRunner {
+  tsvm_context *ctx;
+  const float *const *Zs;   // device table of the problems' Z
+  int64_t ldz;
+  int k, P, nunits;
+  Geometry geo;
+  const WorkUnit *units;
+  const int *ubeg, *active;
+  double *scal, *part_vec, *part_s;
+  int *info, *err;
+  const double *dinv;
+
+  template <int MODE, class Op, int R, int CR, int LPR, int CPL>
+  tsvm_status pass_launch(const Op &op, const double *w, double *out_vec, int stage) {
+    size_t stages, smem;
+    stream_config<MODE, R, CR, LPR, CPL>(ldz, &stages, &smem);
+    auto kern = stream_kernel<MODE, Op, R, CR, LPR, CPL>;
+    TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<nunits, kSThreads, smem, ctx->stream>>>(nullptr, ldz, k, 0, op, scal, w, dinv, geo.kz,
+                                                   (int)stages, part_vec, part_s, err, units, Zs,
+                                                   active);
+    TSVM_LAUNCHED(ctx);
+    return finalize(MODE != MODE_ZW ? R * geo.kz : 0, out_vec, Op::NS, Op::NM, stage);
+  }
+  template <int MODE, class Op, int R>
+  tsvm_status pass(const Op &op, const double *w, double *out_vec, int stage) {
+    switch (geo.lpr * 10 + geo.cpl) {
+      case 81: return pass_launch<MODE, Op, R, 32, 8, 1>(op, w, out_vec, stage);
+      case 161: return pass_launch<MODE, Op, R, 32, 16, 1>(op, w, out_vec, stage);
+      case 321: return pass_launch<MODE, Op, R, 32, 32, 1>(op, w, out_vec, stage);
+      case 322: return pass_launch<MODE, Op, R, 16, 32, 2>(op, w, out_vec, stage);
+      case 324: return pass_launch<MODE, Op, R, 8, 32, 4>(op, w, out_vec, stage);
+      case 328: return pass_launch<MODE, Op, R, 8, 32, 8>(op, w, out_vec, stage);
+    }
+    return TSVM_ERR_UNSUPPORTED;
+  }
+  template <class Op>
+  tsvm_status zt(const Op &op, double *out_vec, int stage) {
+    return pass<MODE_ZT, Op, Op::R>(op, nullptr, out_vec, stage);
+  }
+  template <class Op>
+  tsvm_status zw(const Op &op, const double *w, int stage) {
+    return pass<MODE_ZW, Op, Op::R>(op, w, nullptr, stage);
+  }
+  template <class Op>
+  tsvm_status vec(const Op &op, int stage) {
+    vec_kernel<Op><<<nunits, kThreads, 0, ctx->stream>>>(0, op, scal, part_s, units, active);
+    TSVM_LAUNCHED(ctx);
+    if (Op::NS + Op::NM == 0 && stage == ST_NONE) return TSVM_OK;
+    return finalize(0, nullptr, Op::NS, Op::NM, stage);
+  }
+  tsvm_status finalize(int nvec, double *out_vec, int ns, int nm, int stage) {
+    finalize_batched_kernel<<<P, 256, 0, ctx->stream>>>(part_vec, part_s, ubeg, nvec, out_vec, ns,
+                                                         nm, scal, stage, info, active);
+    TSVM_LAUNCHED(ctx);
+    return TSVM_OK;
+  }
+};
+
+// Work units of at most `rows` rows (a multiple of 32), each within one problem.
+void build_units(const std::vector<int64_t> &off, int rows, std::vector<WorkUnit> &units,
+                 std::vector<int> &ubeg) {
+  units.clear();
+  ubeg.assign(off.size(), 0);
+  const int P = (int)off.size() - 1;
+  for (int p = 0; p < P; ++p) {
+    ubeg[p] = (int)units.size();
+    const int64_t n = off[p + 1] - off[p];
+    for (int64_t r = 0; r < n; r += rows) {
+      WorkUnit u;
+      u.p = p;
+      u.row0 = r;
+      u.rows = (int32_t)std::min<int64_t>(rows, n - r);
+      u.goff = off[p] + r;
+      units.push_back(u);
+    }
+  }
+  ubeg[P] = (int)units.size();
+}
+
+}  // namespace
+
+tsvm_status ipm_solve_batched(tsvm_context *ctx, const tsvm_ipm_problem *pr, int P, int k,
+                              int ldz, const tsvm_ipm_options &opt, tsvm_ipm_stats *stats,
+                              tsvm_batch_info *binfo) {
+  const auto t_start = std::chrono::steady_clock::now();
+  const Geometry geo = geometry(k);
+  if (geo.kz > 1024 || k > ldz) return TSVM_ERR_UNSUPPORTED;
+  const int kz = geo.kz;
+  std::vector<int64_t> off(P + 1, 0);
+  for (int p = 0; p < P; ++p) off[p + 1] = off[p] + pr[p].n;
+  const int64_t N = off[P];
+
+  // autotuner candidates for the rows per unit; tables sized for the smallest
+  const int cand[] = {4096, 8192, 16384, 32768};
+  std::vector<WorkUnit> units;
+  std::vector<int> ubeg;
+  build_units(off, cand[0], units, ubeg);
+  const int max_units = (int)units.size();
+  if (max_units > 65535) return TSVM_ERR_UNSUPPORTED;
+
+  // device tables: units | ubeg | Z pointers | active | info (P) + err
+  const size_t tb_units = sizeof(WorkUnit) * max_units;
+  const size_t tb_ubeg = sizeof(int) * (P + 1);
+  const size_t tb_z = sizeof(float *) * P;
+  const size_t tb_act = sizeof(int) * P;
+  const size_t tb_info = sizeof(int) * (P + 1);
+  auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  uint8_t *tab = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_B_TABLE,
+                     al(tb_units) + al(tb_ubeg) + al(tb_z) + al(tb_act) + al(tb_info), &tab));
+  WorkUnit *d_units = reinterpret_cast<WorkUnit *>(tab);
+  int *d_ubeg = reinterpret_cast<int *>(tab + al(tb_units));
+  const float **d_z = reinterpret_cast<const float **>(tab + al(tb_units) + al(tb_ubeg));
+  int *d_active = reinterpret_cast<int *>(tab + al(tb_units) + al(tb_ubeg) + al(tb_z));
+  int *d_info =
+      reinterpret_cast<int *>(tab + al(tb_units) + al(tb_ubeg) + al(tb_z) + al(tb_act));
+
+  double *vec = nullptr, *sbuf = nullptr, *Mall = nullptr, *gpart = nullptr, *part = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_B_VEC, (size_t)11 * N + (size_t)N / 2 + 8, &vec));
+  TSVM_TRY(scratch_t(ctx, SLOT_B_SCAL, (size_t)P * (kNScal + 3 * kz), &sbuf));
+  const int64_t strideD = (int64_t)ceil_div(k, 32) * 1024;
+  const int64_t strideM = (int64_t)k * k + strideD;
+  TSVM_TRY(scratch_t(ctx, SLOT_B_M, (size_t)P * strideM, &Mall));
+  TSVM_TRY(scratch_t(ctx, SLOT_B_GPART, (size_t)max_units * k * k, &gpart));
+  TSVM_TRY(scratch_t(ctx, SLOT_B_PART, (size_t)max_units * (2 * kz + 16), &part));
+  float *labels = reinterpret_cast<float *>(vec + (size_t)11 * N);
+  double *scal = sbuf, *q = sbuf + (size_t)P * kNScal, *h = q + (size_t)P * kz;
+
+  Vecs V;
+  V.x = vec;
+  V.s = V.x + N;
+  V.xi = V.s + N;
+  V.dinv = V.xi + N;
+  V.t1 = V.dinv + N;
+  V.t2 = V.t1 + N;
+  V.r7 = V.t2 + N;
+  V.b = V.r7 + N;
+  V.dx = V.b + N;
+  V.ds = V.dx + N;
+  V.dxi = V.ds + N;
+  V.a = labels;
+
+  std::vector<const float *> hz(P);
+  std::vector<int> hact(P, 1);
+  std::vector<double> hsc((size_t)P * kNScal, 0.0);
+  for (int p = 0; p < P; ++p) {
+    hz[p] = pr[p].Z;
+    hsc[(size_t)p * kNScal + I_C] = pr[p].C;
+    hsc[(size_t)p * kNScal + I_N] = (double)pr[p].n;
+    TSVM_CUDA(cudaMemcpyAsync(labels + off[p], pr[p].y, sizeof(float) * pr[p].n,
+                              cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  TSVM_CUDA(cudaMemcpyAsync(d_units, units.data(), sizeof(WorkUnit) * units.size(),
+                            cudaMemcpyHostToDevice, ctx->stream));
+  TSVM_CUDA(cudaMemcpyAsync(d_ubeg, ubeg.data(), tb_ubeg, cudaMemcpyHostToDevice, ctx->stream));
+  TSVM_CUDA(cudaMemcpyAsync(d_z, hz.data(), tb_z, cudaMemcpyHostToDevice, ctx->stream));
+  TSVM_CUDA(cudaMemcpyAsync(d_active, hact.data(), tb_act, cudaMemcpyHostToDevice, ctx->stream));
+  TSVM_CUDA(cudaMemsetAsync(d_info, 0, tb_info, ctx->stream));
+  TSVM_CUDA(cudaMemcpyAsync(scal, hsc.data(), sizeof(double) * hsc.size(), cudaMemcpyHostToDevice,
+                            ctx->stream));
+
+  BRunner br;
+  br.ctx = ctx;
+  br.Zs = d_z;
+  br.ldz = ldz;
+  br.k = k;
+  br.P = P;
+  br.nunits = (int)units.size();
+  br.geo = geo;
+  br.units = d_units;
+  br.ubeg = d_ubeg;
+  br.active = d_active;
+  br.scal = scal;
+  br.part_vec = part;
+  br.part_s = part + (size_t)max_units * 2 * kz;
+  br.info = d_info;
+  br.err = d_info + P;
+  br.dinv = V.dinv;
+
+  auto pull = [&]() -> tsvm_status {  // scalars + info of every problem to the host
+    TSVM_CUDA(cudaMemcpyAsync(hsc.data(), scal, sizeof(double) * hsc.size(),
+                              cudaMemcpyDeviceToHost, ctx->stream));
+    return TSVM_OK;
+  };
+  std::vector<int> hinfo(P + 1, 0);
+
+  // ---- initial points (tensorsvm-train.cu:1535-1579), per problem ----
+  if (opt.kernel == TSVM_KERNEL_RBF) {
+    TSVM_TRY(br.zt(InitRhsOp{V}, q, ST_NONE));
+    TSVM_TRY(br.zw(InitRbfRowOp{V}, q, ST_INIT));
+  }
+  TSVM_TRY(pull());
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int p = 0; p < P; ++p) {
+    double *sp = &hsc[(size_t)p * kNScal];
+    const double C = pr[p].C;
+    double ox = opt.kernel == TSVM_KERNEL_RBF ? sp[I_E2SUM] / sp[I_E2SQ] : 1.0;
+    if (!(ox < 0.99 * C && ox > 0.01 * C)) ox = ox > 0.99 * C ? 0.99 * C : 0.01 * C;
+    sp[I_Y] = ox;
+  }
+  TSVM_CUDA(cudaMemcpyAsync(scal, hsc.data(), sizeof(double) * hsc.size(), cudaMemcpyHostToDevice,
+                            ctx->stream));
+  TSVM_TRY(br.vec(FillOp{V}, ST_NONE));
+  for (int p = 0; p < P; ++p) hsc[(size_t)p * kNScal + I_Y] = 0.0;
+  TSVM_CUDA(cudaMemcpyAsync(scal, hsc.data(), sizeof(double) * hsc.size(), cudaMemcpyHostToDevice,
+                            ctx->stream));
+  if (opt.kernel != TSVM_KERNEL_RBF) {
+    TSVM_TRY(br.zt(XRhsOp{V}, q, ST_NONE));
+    TSVM_TRY(br.zw(InitLinearRowOp{V}, q, ST_NONE));
+  }
+
+  // ---- autotune the rows per unit on the first pass of the iteration (idempotent) ----
+  const auto t_tune0 = std::chrono::steady_clock::now();
+  int best_rows = cand[0];
+  {
+    float best_ms = 1e30f;
+    cudaEvent_t e0 = ctx->ev[4], e1 = ctx->ev[5];
+    std::vector<WorkUnit> cu;
+    std::vector<int> cb;
+    for (int rows : cand) {
+      build_units(off, rows, cu, cb);
+      TSVM_CUDA(cudaMemcpyAsync(d_units, cu.data(), sizeof(WorkUnit) * cu.size(),
+                                cudaMemcpyHostToDevice, ctx->stream));
+      TSVM_CUDA(cudaMemcpyAsync(d_ubeg, cb.data(), tb_ubeg, cudaMemcpyHostToDevice, ctx->stream));
+      br.nunits = (int)cu.size();
+      float ms = 1e30f;
+      for (int rep = 0; rep < 2; ++rep) {
+        TSVM_CUDA(cudaEventRecord(e0, ctx->stream));
+        TSVM_TRY(br.zt(BeginOp{V, 0.0}, q, ST_BEGIN));
+        TSVM_CUDA(cudaEventRecord(e1, ctx->stream));
+        ms = std::min(ms, event_ms(e0, e1));
+      }
+      if (ms < best_ms) {
+        best_ms = ms;
+        best_rows = rows;
+      }
+    }
+    build_units(off, best_rows, units, ubeg);
+    TSVM_CUDA(cudaMemcpyAsync(d_units, units.data(), sizeof(WorkUnit) * units.size(),
+                              cudaMemcpyHostToDevice, ctx->stream));
+    TSVM_CUDA(cudaMemcpyAsync(d_ubeg, ubeg.data(), tb_ubeg, cudaMemcpyHostToDevice, ctx->stream));
+    br.nunits = (int)units.size();
+  }
+  const double ms_tune =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_tune0).count();
+
+  // one iteration after the host's stopping decisions, ending with the next iteration's
+  // Begin/Resid passes (captured once, then replayed)
+  double *M = Mall;
+  double *Mdinv_base = Mall + (size_t)k * k;
+  auto body = [&]() -> tsvm_status {
+    TSVM_TRY(gram_fp64_units(ctx, d_z, ldz, k, d_units, br.nunits, d_active, V.dinv, gpart));
+    gram_units_reduce<<<dim3((unsigned)ceil_div((int64_t)k * k, 256), P), 256, 0, ctx->stream>>>(
+        gpart, d_ubeg, k, d_active, M, strideM);
+    TSVM_LAUNCHED(ctx);
+    TSVM_TRY(chol_fp64_batched(ctx, M, k, k, strideM, d_info, Mdinv_base, strideM, P, d_active));
+    TSVM_TRY(br.zt(SmwRhs2Op{V}, h, ST_NONE));
+    TSVM_TRY(potrs_fp64_batched(ctx, M, k, k, strideM, Mdinv_base, strideM, h, 2, kz,
+                                (int64_t)2 * kz, P, d_active));
+    TSVM_TRY(br.zw(SmwBack2Op{V}, h, ST_DYA));
+    TSVM_TRY(br.vec(AffineOp{V, 0.0, 0.0}, ST_ALPHA_AFF));
+    TSVM_TRY(br.vec(MuAffOp{V, 0.0, 0.0}, ST_SIGMA));
+    TSVM_TRY(br.zt(CorrRhsOp{V, 0.0, 0.0}, h, ST_NONE));
+    TSVM_TRY(potrs_fp64_batched(ctx, M, k, k, strideM, Mdinv_base, strideM, h, 1, kz, kz, P,
+                                d_active));
+    TSVM_TRY(br.zw(CorrBackOp{V}, h, ST_DYC));
+    TSVM_TRY(br.vec(CombineOp{V, 0.0, 0.0, 0.0}, ST_ALPHA));
+    TSVM_TRY(br.vec(UpdateOp{V, 0.0, true}, ST_NONE));
+    TSVM_TRY(br.zt(BeginOp{V, 0.0}, q, ST_BEGIN));
+    TSVM_TRY(br.zw(ResidOp{V, 0.0}, q, ST_RESID));
+    return TSVM_OK;
+  };
+
+  TSVM_TRY(br.zt(BeginOp{V, 0.0}, q, ST_BEGIN));
+  TSVM_TRY(br.zw(ResidOp{V, 0.0}, q, ST_RESID));
+
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  bool graph_failed = false;
+  int64_t graph_launches = 0;
+  std::vector<int> done_iter(P, -1), status(P, TSVM_WARN_MAX_ITER);
+  std::vector<double> t_gap(P, -1.0), last(P * kNScal, 0.0);
+  int iter = 0, iters_max = 0;
+  tsvm_status result = TSVM_OK;
+  for (iter = 0;; ++iter) {
+    TSVM_TRY(pull());
+    TSVM_CUDA(cudaMemcpyAsync(hinfo.data(), d_info, sizeof(int) * (P + 1), cudaMemcpyDeviceToHost,
+                              ctx->stream));
+    TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (hinfo[P]) {
+      result = TSVM_ERR_TIMEOUT;
+      break;
+    }
+    const double tnow =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+    bool changed = false;
+    int nactive = 0;
+    for (int p = 0; p < P; ++p) {
+      if (!hact[p]) continue;
+      const double *sp = &hsc[(size_t)p * kNScal];
+      const double scale = 1.0 + sqrt((double)pr[p].n);
+      const double nrd = sp[I_NORMRD], nrp = fabs(sp[I_RP]);
+      int st = -1;
+      if (iter > 0 && sp[I_INFO] != 0.0) st = TSVM_ERR_NOT_SPD;
+      if (st < 0 && t_gap[p] < 0 && sp[I_RELGAP] <= 1e-6 && nrd / scale <= 1e-6 &&
+          nrp / scale <= 1e-6)
+        t_gap[p] = tnow;
+      if (st < 0 && sp[I_MU] < opt.tol && nrd < opt.tol && nrp < opt.tol) st = TSVM_OK;
+      if (st < 0 && opt.rel_gap_tol > 0 && sp[I_RELGAP] <= opt.rel_gap_tol &&
+          nrd / scale <= opt.rel_gap_tol && nrp / scale <= opt.rel_gap_tol)
+        st = TSVM_OK;
+      if (st < 0 && sp[I_COND] > 1e18) st = TSVM_WARN_ILL_CONDITIONED;
+      if (st < 0 && iter >= opt.max_iter) st = TSVM_WARN_MAX_ITER;
+      if (st >= 0) {
+        status[p] = st;
+        done_iter[p] = iter;
+        hact[p] = 0;
+        changed = true;
+        std::copy(sp, sp + kNScal, last.begin() + (size_t)p * kNScal);
+      } else {
+        ++nactive;
+      }
+    }
+    if (nactive == 0) break;
+    if (changed)
+      TSVM_CUDA(cudaMemcpyAsync(d_active, hact.data(), tb_act, cudaMemcpyHostToDevice,
+                                ctx->stream));
+    if (gexec) {
+      TSVM_CUDA(cudaGraphLaunch(gexec, ctx->stream));
+      ctx->launches += graph_launches;
+      continue;
+    }
+    if (iter >= 1 && !graph_failed) {
+      // capture this iteration's launches (all scratch exists after the first iteration)
+      const int64_t l0 = ctx->launches;
+      if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        const tsvm_status cst = body();
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+        if (cst == TSVM_OK && ce == cudaSuccess && g &&
+            cudaGraphInstantiate(&gexec, g, 0) == cudaSuccess) {
+          graph = g;
+          graph_launches = ctx->launches - l0;
+          ctx->launches = l0;
+          TSVM_CUDA(cudaGraphLaunch(gexec, ctx->stream));
+          ctx->launches += graph_launches;
+          continue;
+        }
+        if (g) cudaGraphDestroy(g);
+        gexec = nullptr;
+        ctx->launches = l0;
+        cudaGetLastError();
+      }
+      graph_failed = true;
+    }
+    TSVM_TRY(body());
+  }
+  iters_max = iter;
+  if (gexec) cudaGraphExecDestroy(gexec);
+  if (graph) cudaGraphDestroy(graph);
+  if (result != TSVM_OK) return result;
+  for (int p = 0; p < P; ++p) {
+    if (pr[p].alpha_out)
+      TSVM_CUDA(cudaMemcpyAsync(pr[p].alpha_out, V.x + off[p], sizeof(double) * pr[p].n,
+                                cudaMemcpyDeviceToDevice, ctx->stream));
+    if (pr[p].xi_out)
+      TSVM_CUDA(cudaMemcpyAsync(pr[p].xi_out, V.xi + off[p], sizeof(double) * pr[p].n,
+                                cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  const double ms_total =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+  for (int p = 0; p < P; ++p) {
+    const double *sp = &last[(size_t)p * kNScal];
+    if (stats) {
+      tsvm_ipm_stats &st = stats[p];
+      memset(&st, 0, sizeof(st));
+      st.iters = done_iter[p];
+      st.status = status[p];
+      st.mu = sp[I_MU];
+      st.norm_rd = sp[I_NORMRD];
+      st.norm_rp = fabs(sp[I_RP]);
+      st.cond_d = sp[I_COND];
+      st.pobj = sp[I_POBJ];
+      st.dobj = sp[I_DOBJ];
+      st.rel_gap = sp[I_RELGAP];
+      st.ms_total = ms_total;
+      st.t_rel_gap_1e6_ms = t_gap[p];
+    }
+    if (result == TSVM_OK && status[p] != TSVM_OK && status[p] != TSVM_WARN_MAX_ITER &&
+        status[p] != TSVM_WARN_ILL_CONDITIONED)
+      result = (tsvm_status)status[p];
+  }
+  if (binfo) {
+    binfo->units = br.nunits;
+    binfo->unit_rows = best_rows;
+    binfo->graph_used = gexec || graph ? 1 : 0;
+    binfo->iters_max = iters_max;
+    binfo->ms_total = ms_total;
+    binfo->ms_autotune = ms_tune;
+  }
+  return result;
 }
 
 }  // namespace tsvm

@@ -40,6 +40,13 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
                          int64_t n, int d, double gamma, const float *A, int kp, float *W,
                          int precision, float *kernel_ms);
 
+// A unit of batched work: rows [row0, row0 + rows) of problem p; goff is the index of the
+// unit's first row in the problems' concatenated per-row vectors.
+struct WorkUnit {
+  int32_t p, rows;
+  int64_t row0, goff;
+};
+
 // ---- tallskinny.cu ---------------------------------------------------------------------
 // G (ka x kb, row-major fp64, ldg = kb) = A^T B over n rows; A n x lda fp32, B n x ldb fp32.
 // If symmetric (A == B, ka == kb) only the lower triangle is accumulated and G is mirrored.
@@ -52,6 +59,12 @@ tsvm_status gram_fp64(tsvm_context *ctx, const float *A, int64_t lda, const floa
 tsvm_status gram_fp64_rows(tsvm_context *ctx, const float *A, int64_t lda, int64_t n_max, int k,
                            const int64_t *rowidx, const int *count_dev, const double *rowscale,
                            double *G);
+// Per-unit partial Gram matrices of a batch: part[u] (k x k, lower 64 x 64 tiles filled) =
+// sum over the unit's rows j of rowscale[goff + j] z_j z_j^T with z_j rows of Zs[p] (lda);
+// units of problems with active[p] == 0 are skipped.
+tsvm_status gram_fp64_units(tsvm_context *ctx, const float *const *Zs, int64_t lda, int k,
+                            const WorkUnit *units, int nunits, const int *active,
+                            const double *rowscale, double *part);
 // Out (n x kp) = A (n x kp) * R (kp x kp, fp32 row-major). Out may alias A.
 tsvm_status apply_right_fp32(tsvm_context *ctx, const float *A, int64_t n, int kp,
                              const float *R, float *Out);
@@ -67,6 +80,14 @@ tsvm_status tri_diag_inverse(tsvm_context *ctx, const double *L, int n, int lda,
 // Solve (L L^T) X = B for nrhs (<= 4) right-hand sides stored as rows of B (nrhs x ldb).
 tsvm_status potrs_fp64(tsvm_context *ctx, const double *L, int n, int lda, const double *Dinv,
                        double *B, int nrhs, int ldb);
+// Batched forms: `count` independent n x n problems at A + b * strideA (Dinv + b * strideD,
+// info_dev[b], B + b * strideB), problems with active[b] == 0 skipped; one CTA per problem.
+tsvm_status chol_fp64_batched(tsvm_context *ctx, double *A, int n, int lda, int64_t strideA,
+                              int *info_dev, double *Dinv, int64_t strideD, int count,
+                              const int *active);
+tsvm_status potrs_fp64_batched(tsvm_context *ctx, const double *L, int n, int lda,
+                               int64_t strideA, const double *Dinv, int64_t strideD, double *B,
+                               int nrhs, int ldb, int64_t strideB, int count, const int *active);
 // Lower-triangular inverse: Linv = L^-1 (both n x n row-major, lda).
 tsvm_status trinv_lower_fp64(tsvm_context *ctx, const double *L, int n, int lda,
                              const double *Dinv, double *Linv);
@@ -94,6 +115,9 @@ tsvm_status syrk_capacitance_tc(tsvm_context *ctx, const float *Z, int ldz, int6
 tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y, int64_t n,
                       int k, double C, const tsvm_ipm_options &opt, double *alpha_out,
                       double *xi_out, double *ymult_out, tsvm_ipm_stats *stats);
+tsvm_status ipm_solve_batched(tsvm_context *ctx, const tsvm_ipm_problem *problems, int count,
+                              int k, int ldz, const tsvm_ipm_options &opt, tsvm_ipm_stats *stats,
+                              tsvm_batch_info *info);
 tsvm_status bias_rbf(tsvm_context *ctx, const float *Z, int ldz, const float *y,
                      const double *alpha, int64_t n, int k, double C, double *b, double *bstd,
                      int32_t *nsv, int32_t *nfree);

@@ -25,7 +25,8 @@ gram_partial_kernel(const float *__restrict__ A, int64_t lda, const float *__res
                     int64_t ldb, int64_t n, int ka, int kb, int tiles_b, int symmetric,
                     int64_t rows_per_split, const double *__restrict__ rowscale,
                     const int64_t *__restrict__ rowidx, const int *__restrict__ count,
-                    double *__restrict__ part) {
+                    const WorkUnit *__restrict__ units, const float *const *__restrict__ Zs,
+                    const int *__restrict__ active, double *__restrict__ part) {
   __shared__ double As[kGRows][kGT];
   __shared__ double Bs[kGRows][kGT];
   int t = blockIdx.x, ta, tb;
@@ -38,12 +39,21 @@ gram_partial_kernel(const float *__restrict__ A, int64_t lda, const float *__res
     tb = t % tiles_b;
   }
   const int a0 = ta * kGT, b0 = tb * kGT;
+  if (units) {  // batched: this block sums the rows of one work unit (symmetric, A = B)
+    const WorkUnit u = units[blockIdx.y];
+    if (active && !active[u.p]) return;
+    A = Zs[u.p] + u.row0 * lda;
+    B = A;
+    n = u.rows;
+    rows_per_split = u.rows;
+    rowscale += u.goff;
+  }
   if (count) {  // row count on the device: split it evenly over gridDim.y
     n = *count;
     rows_per_split = (n + gridDim.y - 1) / gridDim.y;
     rows_per_split = (rows_per_split + kGRows - 1) / kGRows * kGRows;
   }
-  const int64_t r0 = (int64_t)blockIdx.y * rows_per_split;
+  const int64_t r0 = units ? 0 : (int64_t)blockIdx.y * rows_per_split;
   const int64_t r1 = min(n, r0 + rows_per_split);
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   double acc[4][4];
@@ -197,7 +207,7 @@ tsvm_status gram_fp64(tsvm_context *ctx, const float *A, int64_t lda, const floa
   TSVM_TRY(scratch_t(ctx, SLOT_PART, (size_t)nsplit * ka * kb, &part));
   gram_partial_kernel<<<dim3(ntiles, nsplit), 256, 0, ctx->stream>>>(
       A, lda, B, ldb, n, ka, kb, tiles_b, symmetric ? 1 : 0, rows_per_split, rowscale, nullptr,
-      nullptr, part);
+      nullptr, nullptr, nullptr, nullptr, part);
   TSVM_LAUNCHED(ctx);
   const int64_t tot = (int64_t)ka * kb;
   gram_reduce_kernel<<<(unsigned)ceil_div(tot, 256), 256, 0, ctx->stream>>>(
@@ -218,10 +228,24 @@ tsvm_status gram_fp64_rows(tsvm_context *ctx, const float *A, int64_t lda, int64
   double *part = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_PART, (size_t)nsplit * k * k, &part));
   gram_partial_kernel<<<dim3(ntiles, nsplit), 256, 0, ctx->stream>>>(
-      A, lda, A, lda, n_max, k, k, tiles, 1, 0, rowscale, rowidx, count_dev, part);
+      A, lda, A, lda, n_max, k, k, tiles, 1, 0, rowscale, rowidx, count_dev, nullptr, nullptr,
+      nullptr, part);
   TSVM_LAUNCHED(ctx);
   gram_reduce_kernel<<<(unsigned)ceil_div((int64_t)k * k, 256), 256, 0, ctx->stream>>>(
       part, nsplit, k, k, 1, G);
+  TSVM_LAUNCHED(ctx);
+  return TSVM_OK;
+}
+
+tsvm_status gram_fp64_units(tsvm_context *ctx, const float *const *Zs, int64_t lda, int k,
+                            const WorkUnit *units, int nunits, const int *active,
+                            const double *rowscale, double *part) {
+  if (nunits < 1 || nunits > 65535) return TSVM_ERR_UNSUPPORTED;
+  const int tiles = (int)ceil_div(k, kGT);
+  const int ntiles = tiles * (tiles + 1) / 2;
+  gram_partial_kernel<<<dim3(ntiles, nunits), 256, 0, ctx->stream>>>(
+      nullptr, lda, nullptr, lda, 0, k, k, tiles, 1, 0, rowscale, nullptr, nullptr, units, Zs,
+      active, part);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;
 }

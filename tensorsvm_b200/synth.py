@@ -71,6 +71,20 @@ def batch_sizes(count: int = 64, lo: int = 2000, hi: int = 200000, seed: int = 4
     return np.exp(rng.uniform(np.log(lo), np.log(hi), count)).astype(np.int64)
 
 
+def grid_problems(count: int = 64, lo: int = 2000, hi: int = 200000, seed: int = 44, d: int = 28):
+    """The batched workload: `count` tanh-teacher problems of log-uniform sizes on the 8 x 8
+    grid C in 2^{-2, 0, ..., 12}, gamma in 2^{-9, ..., -2} (row-major over (C, gamma)).
+    Returns a list of (X, y, gamma, C)."""
+    sizes = batch_sizes(count, lo, hi, seed)
+    Cs = [2.0 ** e for e in range(-2, 13, 2)]
+    gammas = [2.0 ** e for e in range(-9, -1)]
+    out = []
+    for i in range(count):
+        X, y = tanh_teacher(int(sizes[i]), d=d, seed=1000 + i)
+        out.append((X, y, gammas[i % 8], Cs[(i // 8) % 8]))
+    return out
+
+
 def write_libsvm(path: str, X: np.ndarray, y: np.ndarray) -> None:
     """LIBSVM text, values as %.9g so float32 round-trips exactly; zero features omitted."""
     with open(path, "w") as f:

@@ -1,0 +1,64 @@
+"""Batched interior-point solve (tsvm_ipm_batched) against the single-problem solver on the same
+factors: every problem of a small (C, gamma) grid of uneven sizes must end with the same status,
+iteration count, objective and decision values as its own tsvm_ipm run."""
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+from tensorsvm_b200 import _lib, api, synth
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.fixture(scope="module")
+def grid(ctx):
+    # 8 problems, 600..9000 rows, k = 64 (two of them below one 4096-row work unit)
+    probs = synth.grid_problems(count=8, lo=600, hi=9000, seed=7)
+    k = 64
+    Zs, ys, Cs = [], [], []
+    for X, y, gamma, C in probs:
+        Z, _ = api.factor(ctx, dev(X), dev(y), gamma, k, "fp32")
+        Zs.append(Z)
+        ys.append(dev(y))
+        Cs.append(C)
+    return Zs, ys, Cs, k
+
+
+def decision(Z, k, a, y):
+    Zh = Z.cpu().numpy()[:, :k].astype(np.float64)
+    return Zh @ (Zh.T @ (a * y))
+
+
+@pytest.mark.parametrize("rel_gap_tol", [0.0, 1e-6])
+def test_batched_matches_single(ctx, grid, rel_gap_tol):
+    Zs, ys, Cs, k = grid
+    alphas, stats, info = api.ipm_batched(ctx, Zs, ys, k, Cs, rel_gap_tol=rel_gap_tol)
+    assert info["units"] >= len(Zs) and info["unit_rows"] in (4096, 8192, 16384, 32768)
+    assert info["graph_used"] == 1
+    assert info["iters_max"] == max(s["iters"] for s in stats)
+    for Z, y, C, a, s in zip(Zs, ys, Cs, alphas, stats):
+        a1, _, _, s1 = api.ipm(ctx, Z, y, k, C, rel_gap_tol=rel_gap_tol)
+        assert s["status"] == s1["status_code"]
+        assert abs(s["iters"] - s1["iters"]) <= 1, (s["iters"], s1["iters"])
+        assert abs(s["pobj"] - s1["pobj"]) <= 1e-8 * max(1.0, abs(s1["pobj"]))
+        yh = y.cpu().numpy().astype(np.float64)
+        f = decision(Z, k, a.cpu().numpy(), yh)
+        f1 = decision(Z, k, a1.cpu().numpy(), yh)
+        assert np.max(np.abs(f - f1)) <= 1e-5 * max(1.0, np.max(np.abs(f1)))
+        sv, _ = orc.sv_sets(a.cpu().numpy(), C)
+        sv1, _ = orc.sv_sets(a1.cpu().numpy(), C)
+        assert len(set(sv.tolist()) ^ set(sv1.tolist())) <= max(1, len(sv1) // 1000)
+
+
+def test_batched_single_problem_and_launch_count(ctx, grid):
+    Zs, ys, Cs, k = grid
+    l0 = ctx.launches
+    alphas, stats, info = api.ipm_batched(ctx, Zs[:1], ys[:1], k, Cs[:1])
+    assert stats[0]["status"] == _lib.OK
+    # every iteration is one replay of the captured graph: launches grow with iterations
+    assert ctx.launches - l0 > 10 * stats[0]["iters"]
