@@ -164,6 +164,8 @@ tsvm_status tsvm_linear_factor(tsvm_context *ctx, const float *X, const float *y
  *   y          device, n labels in {+1, -1}
  *   alpha_out  device, n doubles (the dual variables "X" of the reference)
  *   xi_out     device, n doubles or NULL
+ *   s_out      device, n doubles or NULL: the multipliers of alpha >= 0 at the final iterate
+ *              (with xi, ymult and alpha what tsvm_hypergrad needs)
  *   ymult_out  host, the equality multiplier (the reference's local "y"), or NULL
  *   opt        host, NULL for defaults;  stats host, may be NULL
  * Returns TSVM_OK on convergence, TSVM_WARN_ILL_CONDITIONED / TSVM_WARN_MAX_ITER when the
@@ -171,7 +173,8 @@ tsvm_status tsvm_linear_factor(tsvm_context *ctx, const float *X, const float *y
  * Cholesky (outputs hold the last iterate, as the reference leaves X). */
 tsvm_status tsvm_ipm(tsvm_context *ctx, const float *Z, int32_t ldz, const float *y, int64_t n,
                      int32_t k, double C, const tsvm_ipm_options *opt, double *alpha_out,
-                     double *xi_out, double *ymult_out, tsvm_ipm_stats *stats);
+                     double *xi_out, double *s_out, double *ymult_out,
+                     tsvm_ipm_stats *stats);
 
 /* Batched interior-point solve (replaces running mpc, T:1507-1840, once per problem): `count`
  * independent SVM duals of uneven n -- one-vs-rest classes, a (C, gamma) grid, folds -- solved
@@ -186,6 +189,30 @@ tsvm_status tsvm_ipm(tsvm_context *ctx, const float *Z, int32_t ldz, const float
 tsvm_status tsvm_ipm_batched(tsvm_context *ctx, const tsvm_ipm_problem *problems, int32_t count,
                              int32_t k, int32_t ldz, const tsvm_ipm_options *opt,
                              tsvm_ipm_stats *stats, tsvm_batch_info *info);
+
+/* Result of tsvm_hypergrad. */
+typedef struct tsvm_hypergrad_result {
+  double loss;               /* (1/m) sum_v max(0, 1 - y_v f(x_v))^2 on the validation set */
+  double dloss_dlog_gamma;   /* through the dual solution, the bias and the validation kernel */
+  double dloss_dlog_C;
+  int32_t n_free_bias;       /* free SVs the bias was averaged over (<= 50) */
+  double ms;
+} tsvm_hypergrad_result;
+
+/* Hypergradient of the validation squared-hinge loss of a trained RBF SVM (no counterpart in
+ * the reference; extends LRA T:1941-2374, mpc T:1507-1840 and the bias T:355-376).  Given the
+ * training set (X n x d, labels y), gamma, C, k and the factor precision used for training,
+ * the solution of tsvm_ipm (alpha, xi, s, the equality multiplier ymult) and the bias b of
+ * tsvm_bias, the model is f(x) = sum_i alpha_i y_i exp(-gamma ||x_i - x||^2) + b.  The factor
+ * is recomputed (same sketch, same Z as training), the KKT system of the dual is differentiated
+ * implicitly with one adjoint solve through I + Z^T D^-1 Z (SMW, as the IPM's Newton step),
+ * and the gamma derivative goes through the range finder with the sketch held fixed.  dXv
+ * (device, nv x d, may be NULL) receives dL/dXv.  All arrays are device pointers; d <= 64. */
+tsvm_status tsvm_hypergrad(tsvm_context *ctx, const float *X, const float *y, int64_t n, int32_t d,
+                           const float *Xv, const float *yv, int64_t nv, double gamma, double C,
+                           int32_t k, int32_t precision, const double *alpha, const double *xi,
+                           const double *s, double ymult, double b,
+                           tsvm_hypergrad_result *result, float *dXv);
 
 /* Bias of the RBF model (replaces tensorsvm-train.cu:355-376): the mean over the first <= 50
  * free SVs j (1e-6 < alpha_j < C - 1e-6, in index order) of y_j - sum_{i in SV} alpha_i y_j

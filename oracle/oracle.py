@@ -492,3 +492,64 @@ def train_linear(X, labels, C, **mpc_kw):
     r = mpc(Z, labels, C, kernel="linear", **mpc_kw)
     w, b = linear_w_b(X, labels, r.x, C)
     return r, w, b
+
+
+# ----------------------------------------------------------------------------------------
+# Hypergradient (no reference counterpart): the FP64 restatement of tsvm_hypergrad's formulas
+# ----------------------------------------------------------------------------------------
+
+def hypergrad(X, y, Xv, yv, gamma, C, k, alpha, xi, s, b, Q=None):
+    """Validation squared-hinge loss L and dL/dlog(gamma), dL/dlog(C), dL/dXv, in FP64 with
+    exact kernels and a dense KKT solve.  The model is f(x) = sum_i alpha_i y_i K(x_i, x) + b
+    with b = mean of y_j - y_j sum_i alpha_i Z_i.Z_j over the first <= 50 free SVs; the dual
+    was solved on Q = Z Z^T = P Ky P from the range finder (B = Ky Omega, W R = B,
+    P = W W^T), and the gamma derivative differentiates it with the sketch Omega fixed:
+    dQ = dP Ky P + P dKy P + P Ky dP, dP x = (I-P) dB B+ x + B+^T dB^T (I-P) x, dB = dKy Omega.
+    s, xi: the multipliers of the final iterate of the solver (D = s/alpha + xi/(C - alpha)).
+    Returns (L, dL/dlog gamma, dL/dlog C, dL/dXv)."""
+    X = np.asarray(X, np.float64); Xv = np.asarray(Xv, np.float64)
+    y = np.asarray(y, np.float64); yv = np.asarray(yv, np.float64)
+    alpha = np.asarray(alpha, np.float64); xi = np.asarray(xi, np.float64)
+    n, m = len(y), len(yv)
+    Om = polar_sketch(n, k) if Q is None else np.asarray(Q, np.float64)
+    d2 = ((X[:, None, :] - X[None, :, :]) ** 2).sum(-1)
+    Ky = y[:, None] * np.exp(-gamma * d2) * y[None, :]
+    W, R = np.linalg.qr(Ky @ Om)
+    Cm = W.T @ Ky @ W
+    w, V = np.linalg.eigh(0.5 * (Cm + Cm.T))
+    Z = W @ (V * np.sqrt(np.maximum(w, 0.0)))
+    d2tv = ((X[:, None, :] - Xv[None, :, :]) ** 2).sum(-1)
+    Ktv = np.exp(-gamma * d2tv)
+    beta = alpha * y
+    f = Ktv.T @ beta + b
+    h = np.maximum(0.0, 1.0 - yv * f)
+    L = float(np.sum(h * h) / m)
+    g = -2.0 * yv * h / m
+    Gb = float(g.sum())
+    F = [i for i in range(n) if 1e-6 < alpha[i] < C - 1e-6][:50]
+    zF = (y[F][:, None] * Z[F]).sum(0) if F else np.zeros(Z.shape[1])
+    c = y * (Ktv @ g) - (Gb / len(F) if F else 0.0) * (Z @ zF)
+    D = np.asarray(s, np.float64) / alpha + xi / (C - alpha)
+    A = np.zeros((n + 1, n + 1))
+    A[:n, :n] = Z @ Z.T + np.diag(D)
+    A[:n, n] = y
+    A[n, :n] = y
+    lam = np.linalg.solve(A, np.concatenate([c, [0.0]]))[:n]
+    dKy = y[:, None] * (-d2 * np.exp(-gamma * d2)) * y[None, :]
+    P = lambda v: W @ (W.T @ v)
+    Bp = lambda v: np.linalg.solve(R, W.T @ v)
+    BpT = lambda v: W @ np.linalg.solve(R.T, v)
+    u = P(alpha)
+    E1 = Ky @ u
+    D1 = dKy @ (Om @ Bp(E1)); D2 = dKy @ (E1 - P(E1)); D3 = dKy @ u
+    D4 = dKy @ (Om @ Bp(alpha)); D5 = dKy @ (alpha - P(alpha))
+    s2 = (D4 - P(D4)) + BpT(Om.T @ D5)
+    r = (D1 - P(D1)) + BpT(Om.T @ D2) + P(D3) + P(Ky @ s2)
+    dlogC = float(lam @ (C * xi / (C - alpha)))
+    tv = (-d2tv * Ktv).T @ beta
+    dlogg = -gamma * float(lam @ r) - (Gb * gamma * float(np.mean(y[F] * r[F])) if F else 0.0) \
+        + gamma * float(g @ tv)
+    S0 = Ktv.T @ beta
+    S1 = Ktv.T @ (beta[:, None] * X)
+    dXv = -2.0 * gamma * g[:, None] * (Xv * S0[:, None] - S1)
+    return L, dlogg, dlogC, dXv

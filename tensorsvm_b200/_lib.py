@@ -39,7 +39,7 @@ EXPORTS = [
     "tsvm_status_string", "tsvm_create", "tsvm_destroy", "tsvm_set_stream",
     "tsvm_ipm_default_options",
     "tsvm_factor", "tsvm_linear_factor", "tsvm_ipm", "tsvm_bias", "tsvm_bias_noalloc",
-    "tsvm_train", "tsvm_kernel_launches", "tsvm_ipm_batched",
+    "tsvm_train", "tsvm_kernel_launches", "tsvm_ipm_batched", "tsvm_hypergrad",
 ]
 TEST_EXPORTS = [
     "tsvm_test_rand_stream", "tsvm_test_sketch", "tsvm_test_kermatmul", "tsvm_test_chol",
@@ -57,6 +57,12 @@ class BatchInfo(ctypes.Structure):
     _fields_ = [("units", ctypes.c_int32), ("unit_rows", ctypes.c_int32),
                 ("graph_used", ctypes.c_int32), ("iters_max", ctypes.c_int32),
                 ("ms_total", ctypes.c_double), ("ms_autotune", ctypes.c_double)]
+
+
+class HypergradResult(ctypes.Structure):
+    _fields_ = [("loss", ctypes.c_double), ("dloss_dlog_gamma", ctypes.c_double),
+                ("dloss_dlog_C", ctypes.c_double), ("n_free_bias", ctypes.c_int32),
+                ("ms", ctypes.c_double)]
 
 
 class FactorInfo(ctypes.Structure):
@@ -118,7 +124,7 @@ def load() -> ctypes.CDLL:
     lib.tsvm_linear_factor.restype = ctypes.c_int
     lib.tsvm_linear_factor.argtypes = [P, P, P, I64, I32, P, I32]
     lib.tsvm_ipm.restype = ctypes.c_int
-    lib.tsvm_ipm.argtypes = [P, P, I32, P, I64, I32, D, ctypes.POINTER(IpmOptions), P, P,
+    lib.tsvm_ipm.argtypes = [P, P, I32, P, I64, I32, D, ctypes.POINTER(IpmOptions), P, P, P,
                              ctypes.POINTER(D), ctypes.POINTER(IpmStats)]
     lib.tsvm_bias.restype = ctypes.c_int
     lib.tsvm_bias.argtypes = [P, P, I32, P, P, I64, I32, D, ctypes.POINTER(D), ctypes.POINTER(D),
@@ -133,6 +139,9 @@ def load() -> ctypes.CDLL:
     lib.tsvm_ipm_batched.argtypes = [P, ctypes.POINTER(IpmProblem), I32, I32, I32,
                                      ctypes.POINTER(IpmOptions), ctypes.POINTER(IpmStats),
                                      ctypes.POINTER(BatchInfo)]
+    lib.tsvm_hypergrad.restype = ctypes.c_int
+    lib.tsvm_hypergrad.argtypes = [P, P, P, I64, I32, P, P, I64, D, D, I32, I32, P, P, P, D, D,
+                                   ctypes.POINTER(HypergradResult), P]
     lib.tsvm_kernel_launches.restype = ctypes.c_int64
     lib.tsvm_kernel_launches.argtypes = [P]
     # test hooks (include/tensorsvm_testing.h)

@@ -44,20 +44,24 @@ def factor(ctx, X, y, gamma: float, k: int, precision: str = "fp32", Q=None, ldz
 
 
 def ipm(ctx, Z, y, k: int, C: float, kernel: int = _lib.KERNEL_RBF, want_xi: bool = False, **opts):
-    """Solve the dual with Q = Z Z^T; returns (alpha f64 CUDA tensor, xi or None, y_mult, stats)."""
+    """Solve the dual with Q = Z Z^T; returns (alpha f64 CUDA tensor, xi or None, y_mult, stats).
+    With want_xi the multipliers s of alpha >= 0 are returned as stats["s"] as well."""
     import torch
     n, ldz = Z.shape
     alpha = torch.empty(n, dtype=torch.float64, device=Z.device)
     xi = torch.empty(n, dtype=torch.float64, device=Z.device) if want_xi else None
+    sv = torch.empty(n, dtype=torch.float64, device=Z.device) if want_xi else None
     o = _lib.default_options(kernel=kernel, **opts)
     ym = ctypes.c_double()
     stats = _lib.IpmStats()
     st = ctx.lib.tsvm_ipm(ctx.handle, _ptr(Z), ldz, _ptr(y), n, k, float(C), ctypes.byref(o),
-                          _ptr(alpha), _ptr(xi), ctypes.byref(ym), ctypes.byref(stats))
+                          _ptr(alpha), _ptr(xi), _ptr(sv), ctypes.byref(ym), ctypes.byref(stats))
     _lib.check(st, "tsvm_ipm", allow=(_lib.WARN_ILL_CONDITIONED, _lib.WARN_MAX_ITER,
                                        _lib.ERR_NOT_SPD))
     s = _fields(stats)
     s["status_code"] = st
+    if want_xi:
+        s["s"] = sv
     return alpha, xi, ym.value, s
 
 
@@ -81,6 +85,23 @@ def ipm_batched(ctx, Zs, ys, k: int, Cs, kernel: int = _lib.KERNEL_RBF, **opts):
                                   ctypes.byref(info))
     _lib.check(st, "tsvm_ipm_batched", allow=(_lib.ERR_NOT_SPD,))
     return alphas, [_fields(s) for s in stats], _fields(info)
+
+
+def hypergrad(ctx, X, y, Xv, yv, gamma: float, C: float, k: int, alpha, xi, s, ymult: float,
+              b: float, precision: str = "fp32", want_dxv: bool = False):
+    """tsvm_hypergrad on CUDA tensors (the factor is recomputed with `precision`): returns
+    (result dict, dL/dXv tensor or None)."""
+    import torch
+    n, d = X.shape
+    nv = Xv.shape[0]
+    dxv = torch.empty((nv, d), dtype=torch.float32, device=X.device) if want_dxv else None
+    r = _lib.HypergradResult()
+    st = ctx.lib.tsvm_hypergrad(ctx.handle, _ptr(X), _ptr(y), n, d, _ptr(Xv), _ptr(yv), nv,
+                                float(gamma), float(C), k, PRECISIONS[precision], _ptr(alpha),
+                                _ptr(xi), _ptr(s), float(ymult), float(b), ctypes.byref(r),
+                                _ptr(dxv))
+    _lib.check(st, "tsvm_hypergrad")
+    return _fields(r), dxv
 
 
 def bias(ctx, Z, y, alpha, k: int, C: float):

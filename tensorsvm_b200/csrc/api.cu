@@ -174,7 +174,8 @@ tsvm_status tsvm_linear_factor(tsvm_context *ctx, const float *X, const float *y
 
 tsvm_status tsvm_ipm(tsvm_context *ctx, const float *Z, int32_t ldz, const float *y, int64_t n,
                      int32_t k, double C, const tsvm_ipm_options *opt, double *alpha_out,
-                     double *xi_out, double *ymult_out, tsvm_ipm_stats *stats) {
+                     double *xi_out, double *s_out, double *ymult_out,
+                     tsvm_ipm_stats *stats) {
   if (!ctx || !Z || !y || !alpha_out || n < 2 || k < 1 || ldz < k || !(C > 0))
     return TSVM_ERR_INVALID_ARGUMENT;
   if ((ldz % 4) != 0 || (reinterpret_cast<uintptr_t>(Z) & 15) != 0) return TSVM_ERR_INVALID_ARGUMENT;
@@ -183,7 +184,7 @@ tsvm_status tsvm_ipm(tsvm_context *ctx, const float *Z, int32_t ldz, const float
   if (opt) o = *opt;
   if (o.max_iter < 0 || !(o.tol > 0)) return TSVM_ERR_INVALID_ARGUMENT;
   TSVM_CUDA(cudaSetDevice(ctx->device));
-  return ipm_solve(ctx, Z, ldz, y, n, k, C, o, alpha_out, xi_out, ymult_out, stats);
+  return ipm_solve(ctx, Z, ldz, y, n, k, C, o, alpha_out, xi_out, s_out, ymult_out, stats);
 }
 
 tsvm_status tsvm_ipm_batched(tsvm_context *ctx, const tsvm_ipm_problem *problems, int32_t count,
@@ -237,7 +238,7 @@ tsvm_status tsvm_train(tsvm_context *ctx, const float *X, const float *y, int64_
     TSVM_TRY(scratch_t(ctx, SLOT_DEV_Z, (size_t)n * kp, &dZ));
     TSVM_TRY(factor_rbf(ctx, dX, dy, n, d, gamma, k, precision, TSVM_SKETCH_GLIBC, nullptr, dZ, kp,
                         finfo));
-    st = ipm_solve(ctx, dZ, kp, dy, n, k, C, o, dalpha, nullptr, nullptr, istats);
+    st = ipm_solve(ctx, dZ, kp, dy, n, k, C, o, dalpha, nullptr, nullptr, nullptr, istats);
     if (st != TSVM_OK && st != TSVM_WARN_ILL_CONDITIONED && st != TSVM_WARN_MAX_ITER &&
         st != TSVM_ERR_NOT_SPD)
       return st;
@@ -251,7 +252,7 @@ tsvm_status tsvm_train(tsvm_context *ctx, const float *X, const float *y, int64_
     const int ldz = (int)round_up(d, 4);
     TSVM_TRY(scratch_t(ctx, SLOT_DEV_Z, (size_t)n * ldz, &dZ));
     TSVM_TRY(label_rows(ctx, dX, dy, n, d, dZ, ldz));
-    st = ipm_solve(ctx, dZ, ldz, dy, n, d, C, o, dalpha, nullptr, nullptr, istats);
+    st = ipm_solve(ctx, dZ, ldz, dy, n, d, C, o, dalpha, nullptr, nullptr, nullptr, istats);
     if (st != TSVM_OK && st != TSVM_WARN_ILL_CONDITIONED && st != TSVM_WARN_MAX_ITER &&
         st != TSVM_ERR_NOT_SPD)
       return st;

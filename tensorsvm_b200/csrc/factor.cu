@@ -64,6 +64,23 @@ __global__ void eigfactor_to_fp32(const double *__restrict__ V, const double *__
   X32[e] = v;
 }
 
+// Rout = L^T Rin for L lower (k x k, only its lower triangle read) and Rin upper: the combined
+// CholeskyQR factor after one more step (W_new = W L^-T, so B = W_new (L^T R)).
+__global__ void accumulate_r(const double *__restrict__ L, int k, const double *__restrict__ Rin,
+                             double *__restrict__ Rout) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)k * k) return;
+  const int i = (int)(e / k), j = (int)(e % k);
+  double s = 0.0;
+  for (int m = i; m <= j; ++m) s += L[(int64_t)m * k + i] * Rin[(int64_t)m * k + j];
+  Rout[e] = s;
+}
+
+__global__ void set_identity(double *R, int k) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < (int64_t)k * k) R[e] = (e / k == e % k) ? 1.0 : 0.0;
+}
+
 struct Phase {
   tsvm_context *ctx;
   cudaEvent_t a, b;
@@ -80,7 +97,9 @@ static tsvm_status kermatmul(tsvm_context *ctx, const float *Xc, const float *no
   return kermatmul_tc(ctx, Xc, norms, y, n, d, gamma, A, kp, W, precision, kernel_ms);
 }
 
-static tsvm_status orthonormalise(tsvm_context *ctx, float *W, int64_t n, int k, int kp) {
+// Rkeep (2 k x k doubles, may be null): the combined factor R with (input W) = (output W) R.
+static tsvm_status orthonormalise(tsvm_context *ctx, float *W, int64_t n, int k, int kp,
+                                  double *Rkeep) {
   double *G = nullptr, *Linv = nullptr;
   float *R32 = nullptr;
   int *info = nullptr;
@@ -90,6 +109,11 @@ static tsvm_status orthonormalise(tsvm_context *ctx, float *W, int64_t n, int k,
   TSVM_TRY(scratch_t(ctx, SLOT_IPM_M, (size_t)kp * kp, &R32));
   info = reinterpret_cast<int *>(G + (size_t)k * k);
   const double u = ldexp(1.0, -53);
+  const unsigned gk = (unsigned)ceil_div((int64_t)k * k, 256);
+  if (Rkeep) {
+    set_identity<<<gk, 256, 0, ctx->stream>>>(Rkeep, k);
+    TSVM_LAUNCHED(ctx);
+  }
   for (int step = 0; step < 3; ++step) {
     double factor = step == 0 ? 11.0 * ((double)n * k + (double)k * (k + 1)) * u : 0.0;
     for (int attempt = 0; attempt < 4; ++attempt) {
@@ -106,6 +130,13 @@ static tsvm_status orthonormalise(tsvm_context *ctx, float *W, int64_t n, int k,
       if (attempt == 3) return TSVM_ERR_NOT_SPD;
       factor = factor > 0 ? factor * 100.0 : 11.0 * ((double)n * k + (double)k * (k + 1)) * u;
     }
+    if (Rkeep) {
+      double *Rtmp = Rkeep + (size_t)k * k;
+      accumulate_r<<<gk, 256, 0, ctx->stream>>>(G, k, Rkeep, Rtmp);
+      TSVM_LAUNCHED(ctx);
+      TSVM_CUDA(cudaMemcpyAsync(Rkeep, Rtmp, sizeof(double) * k * k, cudaMemcpyDeviceToDevice,
+                                ctx->stream));
+    }
     TSVM_TRY(trinv_lower_fp64(ctx, G, k, k, Dinv, Linv));
     rinv_to_fp32<<<(unsigned)ceil_div((int64_t)kp * kp, 256), 256, 0, ctx->stream>>>(Linv, k, kp,
                                                                                       R32);
@@ -117,7 +148,7 @@ static tsvm_status orthonormalise(tsvm_context *ctx, float *W, int64_t n, int k,
 
 tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_t n, int d,
                        double gamma, int k, int precision, int sketch, const float *Q_user,
-                       float *Z, int ldz, tsvm_factor_info *info) {
+                       float *Z, int ldz, tsvm_factor_info *info, FactorKeep *keep) {
   if (n < 2 || d < 1 || k < 1 || k > 1000 || ldz < k || !(gamma > 0)) return TSVM_ERR_INVALID_ARGUMENT;
   if (k > n) return TSVM_ERR_INVALID_ARGUMENT;
   const int kp = (int)round_up(k, 64);
@@ -138,11 +169,15 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
   } else {
     return TSVM_ERR_INVALID_ARGUMENT;
   }
+  if (keep)
+    TSVM_CUDA(cudaMemcpyAsync(keep->omega, Q, sizeof(float) * n * kp, cudaMemcpyDeviceToDevice,
+                              ctx->stream));
   TSVM_CUDA(cudaEventRecord(ev[1], ctx->stream));
   float km1 = 0.f, km2 = 0.f;
   TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, Q, kp, W, precision, &km1));
   TSVM_CUDA(cudaEventRecord(ev[2], ctx->stream));
-  TSVM_TRY(orthonormalise(ctx, W, n, k, kp));
+  TSVM_TRY(orthonormalise(ctx, W, n, k, kp, keep ? keep->R : nullptr));
+  if (keep) keep->W = W;
   TSVM_CUDA(cudaEventRecord(ev[3], ctx->stream));
   TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, W, kp, Q, precision, &km2));
   TSVM_CUDA(cudaEventRecord(ev[4], ctx->stream));

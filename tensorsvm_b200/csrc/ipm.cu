@@ -41,7 +41,8 @@ enum ScalarIdx : int {
 constexpr int kNScal = 32;
 
 enum Stage : int {
-  ST_NONE = 0, ST_BEGIN, ST_RESID, ST_DYA, ST_ALPHA_AFF, ST_SIGMA, ST_DYC, ST_ALPHA, ST_INIT
+  ST_NONE = 0, ST_BEGIN, ST_RESID, ST_DYA, ST_ALPHA_AFF, ST_SIGMA, ST_DYC, ST_ALPHA, ST_INIT,
+  ST_ADJ
 };
 
 constexpr int kThreads = 256;
@@ -279,6 +280,68 @@ struct BiasRhsOp {
     const double a = alpha[i];
     v[0] = a > 1e-6 ? a : 0.0;
   }
+};
+
+// ---- KKT adjoint of the converged dual (tsvm_hypergrad) ----
+struct VecRhsOp {  // v = src (Z^T src)
+  static constexpr int R = 1, NS = 0, NM = 0;
+  const double *src;
+  __device__ void load(const double *) {}
+  __device__ void rhs(int64_t i, double *v, double *, double *) const { v[0] = src[i]; }
+};
+struct StoreRowOp {  // dst = Z g
+  static constexpr int R = 1, NS = 0, NM = 0;
+  double *dst;
+  __device__ void load(const double *) {}
+  __device__ void row(int64_t i, const double *dot, double *, double *) const { dst[i] = dot[0]; }
+};
+// At the solution: D = s/x + xi/(C - x) of the final iterate, D^-1, and the SMW right-hand
+// sides c/D and a/D.
+struct AdjRowOp {
+  static constexpr int R = 0, NS = 0, NM = 0;
+  Vecs V;
+  const double *c;
+  double C;
+  __device__ void load(const double *sc) { C = sc[I_C]; }
+  __device__ void row(int64_t i, double *, double *) const {
+    const double x = V.x[i], xi = V.xi[i], a = (double)V.a[i];
+    const double D = V.s[i] / x + xi / (C - x);
+    V.dinv[i] = 1.0 / D;
+    V.t1[i] = c[i] / D;
+    V.t2[i] = a / D;
+  }
+};
+// Refinement of the adjoint against the exact operator: rho = c - D lambda - Z Z^T lambda - a nu
+// (dot = (Z Z^T lambda)_i), t1 = rho / D, and a^T lambda for the equality row.
+struct AdjResidOp {
+  static constexpr int R = 1, NS = 1, NM = 0;
+  Vecs V;
+  const double *c, *lam;
+  double nu;
+  __device__ void load(const double *sc) { nu = sc[I_Y]; }
+  __device__ void row(int64_t i, const double *dot, double *sums, double *) const {
+    const double a = (double)V.a[i], di = V.dinv[i];
+    const double rho = c[i] - lam[i] / di - dot[0] - a * nu;
+    V.t1[i] = rho * di;
+    sums[0] += a * lam[i];
+  }
+};
+// lambda += t - dnu u with dnu = (a^T t + a^T lambda) / a^T u (t = S^-1 rho in r7, u in b)
+struct AdjUpdateOp {
+  static constexpr int R = 0, NS = 0, NM = 0;
+  Vecs V;
+  double *lam;
+  double dnu;
+  __device__ void load(const double *sc) { dnu = sc[I_DYC] + sc[I_RP] / sc[I_ATB]; }
+  __device__ void row(int64_t i, double *, double *) const { lam[i] += V.r7[i] - dnu * V.b[i]; }
+};
+struct AdjLambdaOp {  // lambda = (D+Q)^-1 c - nu (D+Q)^-1 a, nu = a^T(D+Q)^-1 c / a^T(D+Q)^-1 a
+  static constexpr int R = 0, NS = 0, NM = 0;
+  Vecs V;
+  double *lam;
+  double nu;
+  __device__ void load(const double *sc) { nu = sc[I_DYA]; }
+  __device__ void row(int64_t i, double *, double *) const { lam[i] = V.r7[i] - nu * V.b[i]; }
 };
 
 // ---------------------------------------------------------------------------------------
@@ -685,6 +748,9 @@ __device__ void scalar_stage(double *__restrict__ sc, const double *red, int sta
       if (sc[I_INFO] == 0.0) sc[I_Y] += al * (sc[I_DYA] + sc[I_DYC]);
       break;
     }
+    case ST_ADJ:  // a^T lambda of the adjoint's current iterate
+      sc[I_RP] = red[0];
+      break;
     default:
       break;
   }
@@ -869,7 +935,7 @@ struct Runner {
 
 tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y, int64_t n,
                       int k, double C, const tsvm_ipm_options &opt, double *alpha_out,
-                      double *xi_out, double *ymult_out, tsvm_ipm_stats *stats) {
+                      double *xi_out, double *s_out, double *ymult_out, tsvm_ipm_stats *stats) {
   const auto t_start = std::chrono::steady_clock::now();
   Runner run;
   run.ctx = ctx;
@@ -1094,6 +1160,9 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
   if (iter >= opt.max_iter) result = TSVM_WARN_MAX_ITER;
   TSVM_CUDA(cudaMemcpyAsync(alpha_out, V.x, sizeof(double) * n, cudaMemcpyDeviceToDevice,
                             ctx->stream));
+  if (s_out)
+    TSVM_CUDA(cudaMemcpyAsync(s_out, V.s, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                              ctx->stream));
   if (xi_out)
     TSVM_CUDA(cudaMemcpyAsync(xi_out, V.xi, sizeof(double) * n, cudaMemcpyDeviceToDevice,
                               ctx->stream));
@@ -1248,6 +1317,164 @@ tsvm_status bias_rbf(tsvm_context *ctx, const float *Z, int ldz, const float *y,
   return TSVM_OK;
 }
 
+
+// ---------------------------------------------------------------------------------------
+// Linear algebra of the KKT adjoint (tsvm_hypergrad)
+// ---------------------------------------------------------------------------------------
+namespace {
+
+// nu of the adjoint: after the first solve nu = I_DYA; each refinement adds dnu.
+__global__ void adj_nu_kernel(double *sc, int first) {
+  if (threadIdx.x != 0) return;
+  if (first) sc[I_Y] = sc[I_DYA];
+  else sc[I_Y] += sc[I_DYC] + sc[I_RP] / sc[I_ATB];
+}
+
+__global__ void add_relative_diag(double *A, int k, double rel) {
+  __shared__ double tr;
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < k; ++i) t += A[(int64_t)i * k + i];
+    tr = t;
+  }
+  __syncthreads();
+  const double shift = rel * tr / k + 1e-300;
+  for (int i = threadIdx.x; i < k; i += blockDim.x) A[(int64_t)i * k + i] += shift;
+}
+
+// A Runner over Z with its own scratch (the adjoint's vectors live in SLOT_IPM_VEC like the
+// solver's: call it after tsvm_ipm, not during).
+tsvm_status make_runner(tsvm_context *ctx, const float *Z, int ldz, int64_t n, int k, Runner &run,
+                        double **sbuf) {
+  run.ctx = ctx;
+  run.Z = Z;
+  run.ldz = ldz;
+  run.n = n;
+  run.k = k;
+  run.geo = geometry(k);
+  if (run.geo.kz > 1024) return TSVM_ERR_UNSUPPORTED;
+  run.nblk = (int)std::min<int64_t>((int64_t)ctx->num_sms * 4, ceil_div(n, kWarps * 32));
+  if (run.nblk < 1) run.nblk = 1;
+  const int kz = run.geo.kz;
+  TSVM_TRY(scratch_t(ctx, SLOT_IPM_SCAL, (size_t)kNScal + 10 * (size_t)kz + 64, sbuf));
+  double *part = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_IPM_PART, (size_t)run.nblk * (2 * kz + 16), &part));
+  run.part_vec = part;
+  run.part_s = part + (size_t)run.nblk * 2 * kz;
+  run.scal = *sbuf;
+  run.info = reinterpret_cast<int *>(*sbuf + kNScal + 9 * kz);
+  run.err = run.info + 2;
+  TSVM_CUDA(cudaMemsetAsync(run.info, 0, 3 * sizeof(int), ctx->stream));
+  return TSVM_OK;
+}
+
+tsvm_status check_runner(tsvm_context *ctx, Runner &run) {
+  int h[3] = {0, 0, 0};
+  TSVM_CUDA(cudaMemcpyAsync(h, run.info, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (h[2]) return TSVM_ERR_TIMEOUT;
+  if (h[0]) return TSVM_ERR_NOT_SPD;
+  return TSVM_OK;
+}
+
+}  // namespace
+
+tsvm_status zt_vec(tsvm_context *ctx, const float *Z, int ldz, int64_t n, int k, const double *v,
+                   double *out) {
+  Runner run;
+  double *sbuf = nullptr;
+  TSVM_TRY(make_runner(ctx, Z, ldz, n, k, run, &sbuf));
+  run.dinv = nullptr;
+  TSVM_TRY(run.zt(VecRhsOp{v}, out, ST_NONE));
+  return check_runner(ctx, run);
+}
+
+tsvm_status zw_vec(tsvm_context *ctx, const float *Z, int ldz, int64_t n, int k, const double *g,
+                   double *out) {
+  Runner run;
+  double *sbuf = nullptr;
+  TSVM_TRY(make_runner(ctx, Z, ldz, n, k, run, &sbuf));
+  run.dinv = nullptr;
+  TSVM_TRY(run.zw(StoreRowOp{out}, g, ST_NONE));
+  return check_runner(ctx, run);
+}
+
+tsvm_status kkt_adjoint(tsvm_context *ctx, const float *Z, int ldz, const float *y, int64_t n,
+                        int k, double C, const double *alpha, const double *xi, const double *s,
+                        const double *c, double *lambda) {
+  Runner run;
+  double *sbuf = nullptr;
+  TSVM_TRY(make_runner(ctx, Z, ldz, n, k, run, &sbuf));
+  const int kz = run.geo.kz;
+  double *vecbuf = nullptr, *M = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_IPM_VEC, (size_t)11 * n, &vecbuf));
+  TSVM_TRY(scratch_t(ctx, SLOT_IPM_M, (size_t)k * k + (size_t)ceil_div(k, 32) * 1024, &M));
+  double *Mdinv = M + (size_t)k * k;
+  Vecs V;
+  V.x = const_cast<double *>(alpha);
+  V.xi = const_cast<double *>(xi);
+  V.s = const_cast<double *>(s);
+  V.dinv = vecbuf + n;
+  V.t1 = V.dinv + n;
+  V.t2 = V.t1 + n;
+  V.r7 = V.t2 + n;
+  V.b = V.r7 + n;
+  V.dx = V.b + n;
+  V.ds = V.dx + n;
+  V.dxi = V.ds + n;
+  V.a = y;
+  run.dinv = V.dinv;
+  double hsc[kNScal] = {0};
+  hsc[I_C] = C;
+  hsc[I_N] = (double)n;
+  hsc[I_RP] = 0.0;
+  TSVM_CUDA(cudaMemcpyAsync(run.scal, hsc, sizeof(hsc), cudaMemcpyHostToDevice, ctx->stream));
+  double *h = sbuf + kNScal + kz;
+  TSVM_TRY(run.vec(AdjRowOp{V, c, 0.0}, ST_NONE));         // D, c/D, a/D
+  TSVM_TRY(gram_fp64(ctx, Z, ldz, Z, ldz, n, k, k, true, M, V.dinv));
+  TSVM_TRY(small_add_diag(ctx, M, k, k, 1.0));
+  TSVM_TRY(chol_fp64(ctx, M, k, k, run.info, Mdinv));
+  TSVM_TRY(run.zt(SmwRhs2Op{V}, h, ST_NONE));
+  TSVM_TRY(potrs_fp64(ctx, M, k, k, Mdinv, h, 2, kz));
+  TSVM_TRY(run.zw(SmwBack2Op{V}, h, ST_DYA));
+  TSVM_TRY(run.vec(AdjLambdaOp{V, lambda, 0.0}, ST_NONE));
+  adj_nu_kernel<<<1, 32, 0, ctx->stream>>>(run.scal, 1);
+  TSVM_LAUNCHED(ctx);
+  // The SMW back-substitution loses accuracy where D is tiny (free support vectors at the end
+  // of the solve: D^-1 ~ 1/mu); refine in n-space against the exact operator D + Z Z^T.
+  for (int sweep = 0; sweep < 3; ++sweep) {
+    TSVM_TRY(run.zt(VecRhsOp{lambda}, h, ST_NONE));                  // Z^T lambda
+    TSVM_TRY(run.zw(AdjResidOp{V, c, lambda, 0.0}, h, ST_ADJ));      // rho / D, a^T lambda
+    TSVM_TRY(run.zt(VecRhsOp{V.t1}, h, ST_NONE));
+    TSVM_TRY(potrs_fp64(ctx, M, k, k, Mdinv, h, 1, kz));
+    TSVM_TRY(run.zw(CorrBackOp{V}, h, ST_DYC));                       // t = S^-1 rho
+    TSVM_TRY(run.vec(AdjUpdateOp{V, lambda, 0.0}, ST_NONE));
+    adj_nu_kernel<<<1, 32, 0, ctx->stream>>>(run.scal, 0);
+    TSVM_LAUNCHED(ctx);
+  }
+  return check_runner(ctx, run);
+}
+
+tsvm_status project_range(tsvm_context *ctx, const float *Z, int ldz, int64_t n, int k,
+                          const double *v, double *out) {
+  Runner run;
+  double *sbuf = nullptr;
+  TSVM_TRY(make_runner(ctx, Z, ldz, n, k, run, &sbuf));
+  const int kz = run.geo.kz;
+  double *G = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_SMALL3, (size_t)k * k + (size_t)ceil_div(k, 32) * 1024, &G));
+  double *Gdinv = G + (size_t)k * k;
+  run.dinv = nullptr;
+  double *q = sbuf + kNScal;
+  TSVM_TRY(gram_fp64(ctx, Z, ldz, Z, ldz, n, k, k, true, G));
+  add_relative_diag<<<1, 256, 0, ctx->stream>>>(G, k, 1e-12);  // clipped (zero) columns
+  TSVM_LAUNCHED(ctx);
+  TSVM_TRY(chol_fp64(ctx, G, k, k, run.info, Gdinv));
+  TSVM_TRY(run.zt(VecRhsOp{v}, q, ST_NONE));
+  TSVM_TRY(potrs_fp64(ctx, G, k, k, Gdinv, q, 1, kz));
+  TSVM_TRY(run.zw(StoreRowOp{out}, q, ST_NONE));
+  return check_runner(ctx, run);
+}
 
 // ---------------------------------------------------------------------------------------
 // Batched interior-point solve: every pass is one launch over the work units (row ranges of

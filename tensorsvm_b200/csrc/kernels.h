@@ -114,7 +114,20 @@ tsvm_status syrk_capacitance_tc(tsvm_context *ctx, const float *Z, int ldz, int6
 // ---- ipm.cu ----------------------------------------------------------------------------
 tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y, int64_t n,
                       int k, double C, const tsvm_ipm_options &opt, double *alpha_out,
-                      double *xi_out, double *ymult_out, tsvm_ipm_stats *stats);
+                      double *xi_out, double *s_out, double *ymult_out, tsvm_ipm_stats *stats);
+// KKT adjoint at a converged dual solution: lambda solves [Q + D, a; a^T, 0][lambda; nu] =
+// [c; 0] with Q = Z Z^T and D = s/x + xi/(C - x) of the final iterate, through SMW.
+// out (kz doubles) = Z^T v and out (n doubles) = Z g through the streaming passes.
+tsvm_status zt_vec(tsvm_context *ctx, const float *Z, int ldz, int64_t n, int k, const double *v,
+                   double *out);
+tsvm_status zw_vec(tsvm_context *ctx, const float *Z, int ldz, int64_t n, int k, const double *g,
+                   double *out);
+tsvm_status kkt_adjoint(tsvm_context *ctx, const float *Z, int ldz, const float *y, int64_t n,
+                        int k, double C, const double *alpha, const double *xi, const double *s,
+                        const double *c, double *lambda);
+// out = Z (Z^T Z)^-1 Z^T v, the projection onto the range of the factor.
+tsvm_status project_range(tsvm_context *ctx, const float *Z, int ldz, int64_t n, int k,
+                          const double *v, double *out);
 tsvm_status ipm_solve_batched(tsvm_context *ctx, const tsvm_ipm_problem *problems, int count,
                               int k, int ldz, const tsvm_ipm_options &opt, tsvm_ipm_stats *stats,
                               tsvm_batch_info *info);
@@ -123,8 +136,16 @@ tsvm_status bias_rbf(tsvm_context *ctx, const float *Z, int ldz, const float *y,
                      int32_t *nsv, int32_t *nfree);
 
 // ---- factor.cu -------------------------------------------------------------------------
+// What the hypergradient keeps of a factorisation: the sketch Omega (n x kp copy), the combined
+// CholeskyQR factor R (k x k upper, pass-1 output B = W R; the buffer holds 2 k x k doubles) and
+// the orthonormal basis W (points into the context's scratch until the next factorisation).
+struct FactorKeep {
+  float *omega;
+  double *R;
+  const float *W;
+};
 tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_t n, int d,
                        double gamma, int k, int precision, int sketch, const float *Q_user,
-                       float *Z, int ldz, tsvm_factor_info *info);
+                       float *Z, int ldz, tsvm_factor_info *info, FactorKeep *keep = nullptr);
 
 }  // namespace tsvm
