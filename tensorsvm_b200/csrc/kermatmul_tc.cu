@@ -48,32 +48,42 @@ using namespace tc;
 
 constexpr int kBM = 128;          // rows of W per CTA (TMEM lanes)
 constexpr int kBJ = 64;           // J block (K of the second MMA, N of the Gram)
-constexpr int kKG = 64;           // Gram K (split features + norms, zero padded)
-constexpr int kXbStages = 6;      // ring of Gram operands (freed as soon as the Gram completes)
-constexpr int kAtStages = 5;      // ring of kernel-block operands (freed after P AT^T)
 constexpr int kThreadsTC = 384;
 constexpr int kMaxSlab = 256;     // columns of W per launch (MMA N <= 256)
+constexpr int kMaxKG = 192;       // widest Gram K (3 d + 6 <= 192: d <= 62)
 
-constexpr uint32_t kXaBytes = kBM * kKG * 2;       // 16 KB
-constexpr uint32_t kXbBytes = kBJ * kKG * 2;       //  8 KB
+// Gram K (split features + norms, zero padded to 64, 128 or 192) and the ring depths that
+// fit 227 KB of shared memory with it: 16 + 6x8 + 5x32, 32 + 4x16 + 4x32, 48 + 3x24 + 3x32 KB.
+template <int KG>
+struct GramCfg {
+  static constexpr uint32_t kXaBytes = kBM * KG * 2;   // XA tile, KG/64 128-byte-wide chunks
+  static constexpr uint32_t kXbBytes = kBJ * KG * 2;
+  static constexpr int kXbStages = KG == 64 ? 6 : KG == 128 ? 4 : 3;
+  static constexpr int kAtStages = KG == 64 ? 5 : KG == 128 ? 4 : 3;
+};
 
 __host__ __device__ constexpr uint32_t align1k(uint32_t v) { return (v + 1023u) & ~1023u; }
 
 // Shared-memory layout, all operand tiles 1024-byte aligned (128B swizzle atoms):
-// [XA 16 KB][XB ring: 6 x 8 KB][AT ring: 5 x kpw*128 B][barriers].  P lives in TMEM.
-// Offsets are computed arithmetically (no arrays), so they stay in registers.
+// [XA][XB ring][AT ring: kpw*128 B each][barriers].  P lives in TMEM.  Offsets are computed
+// arithmetically (no arrays), so they stay in registers.
+template <int KG>
 struct SmemLayout {
   uint32_t at0, at_bytes, bars, total;
   __host__ __device__ uint32_t xa() const { return 0; }
-  __host__ __device__ uint32_t xb(int s) const { return kXaBytes + (uint32_t)s * kXbBytes; }
+  __host__ __device__ uint32_t xb(int s) const {
+    return GramCfg<KG>::kXaBytes + (uint32_t)s * GramCfg<KG>::kXbBytes;
+  }
   __host__ __device__ uint32_t at(int s) const { return at0 + (uint32_t)s * at_bytes; }
 };
 
-__host__ __device__ inline SmemLayout smem_layout(int kpw) {
-  SmemLayout L{};
-  L.at0 = kXaBytes + kXbStages * kXbBytes;
+template <int KG>
+__host__ __device__ inline SmemLayout<KG> smem_layout(int kpw) {
+  using C = GramCfg<KG>;
+  SmemLayout<KG> L{};
+  L.at0 = C::kXaBytes + C::kXbStages * C::kXbBytes;
   L.at_bytes = align1k((uint32_t)kpw * kBJ * 2);
-  L.bars = L.at0 + kAtStages * L.at_bytes;
+  L.bars = L.at0 + C::kAtStages * L.at_bytes;
   L.total = L.bars + 512;
   return L;
 }
@@ -131,7 +141,7 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
 // ---------------------------------------------------------------------------------------
 constexpr int kSBufs = 4;
 
-template <bool BF16, int NPOLY>
+template <bool BF16, int NPOLY, int KG>
 __global__ void __launch_bounds__(kThreadsTC, 1)
 kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
                     const __grid_constant__ CUtensorMap map_xb,
@@ -142,7 +152,10 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
   const uint32_t raw = su32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   uint8_t *sbase = smem_raw + (base - raw);
-  const SmemLayout L = smem_layout(kpw);
+  using Cfg = GramCfg<KG>;
+  constexpr int kXbStages = Cfg::kXbStages, kAtStages = Cfg::kAtStages;
+  constexpr uint32_t kXaBytes = Cfg::kXaBytes, kXbBytes = Cfg::kXbBytes;
+  const SmemLayout<KG> L = smem_layout<KG>(kpw);
   uint64_t *bars = reinterpret_cast<uint64_t *>(sbase + L.bars);
   // barrier slots (8 bytes each)
   const uint32_t b_xbfull = su32(bars);                  // [kXbStages] Gram operand loaded
@@ -207,11 +220,16 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
       for (int rb = blockIdx.x, r = 0; ok && rb < nrb; rb += G, ++r) {
         if (r > 0 && !mbar_wait(b_xaempty, (r - 1) & 1, abort)) break;
         mbar_expect_tx(b_xafull, kXaBytes);
-        tma_load_2d(&map_xa, b_xafull, base + L.xa(), 0, rb * kBM);
+#pragma unroll
+        for (int kc = 0; kc < KG / 64; ++kc)   // one 128-byte-wide chunk of K per box
+          tma_load_2d(&map_xa, b_xafull, base + L.xa() + kc * (kBM * 128), kc * 64, rb * kBM);
         for (int t = 0; t < ntiles; ++t) {
           if (!mbar_wait(b_xbempty + 8 * st, ph ^ 1, abort)) { ok = false; break; }
           mbar_expect_tx(b_xbfull + 8 * st, kXbBytes);
-          tma_load_2d(&map_xb, b_xbfull + 8 * st, base + L.xb(st), 0, t * kBJ);
+#pragma unroll
+          for (int kc = 0; kc < KG / 64; ++kc)
+            tma_load_2d(&map_xb, b_xbfull + 8 * st, base + L.xb(st) + kc * (kBJ * 128), kc * 64,
+                        t * kBJ);
           if (++st == kXbStages) { st = 0; ph ^= 1; }
         }
       }
@@ -253,8 +271,11 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
           tc_fence_after();
           const uint64_t dxb = dxb0 + (uint64_t)((st * kXbBytes) >> 4);
 #pragma unroll
-          for (int kk = 0; kk < kKG / 16; ++kk)
-            umma(tmem + b * kBJ, dxa + 2 * kk, dxb + 2 * kk, idg, kk > 0 ? 1u : 0u);
+          for (int kk = 0; kk < KG / 16; ++kk) {   // chunk kk/4 of K, 32-byte step kk%4 in it
+            const uint64_t oa = (uint64_t)(((kk >> 2) * (kBM * 128)) >> 4) + 2 * (kk & 3);
+            const uint64_t ob = (uint64_t)(((kk >> 2) * (kBJ * 128)) >> 4) + 2 * (kk & 3);
+            umma(tmem + b * kBJ, dxa + oa, dxb + ob, idg, kk > 0 ? 1u : 0u);
+          }
           umma_commit(b_sfull + 8 * b);
           umma_commit(b_xbempty + 8 * st);
           if (++st == kXbStages) { st = 0; sph ^= 1; }
@@ -365,11 +386,12 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
 // ---------------------------------------------------------------------------------------
 // XA/XB rows (n_pad x 64 FP16) from centred features: see the file comment for the layout.
 __global__ void prep_gram_operands(const float *__restrict__ Xc, int64_t n, int64_t n_pad, int d,
-                                   double scale, __half *__restrict__ XA, __half *__restrict__ XB) {
+                                   int KG, double scale, __half *__restrict__ XA,
+                                   __half *__restrict__ XB) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_pad) return;
-  __half *a = XA + i * kKG, *b = XB + i * kKG;
-  for (int c = 0; c < kKG; ++c) {
+  __half *a = XA + i * KG, *b = XB + i * KG;
+  for (int c = 0; c < KG; ++c) {
     a[c] = __float2half_rn(0.f);
     b[c] = __float2half_rn(0.f);
   }
@@ -478,22 +500,37 @@ int poly_split() {
   return v;
 }
 
-TcKernel select_kernel(bool bf16, int npoly) {
+TcKernel select_kernel(bool bf16, int npoly, int KG) {
+  if (KG == 128) return bf16 ? kermatmul_tc_kernel<true, 0, 128> : kermatmul_tc_kernel<false, 0, 128>;
+  if (KG == 192) return bf16 ? kermatmul_tc_kernel<true, 0, 192> : kermatmul_tc_kernel<false, 0, 192>;
 #define TSVM_SEL(P) \
-  if (npoly == P) return bf16 ? kermatmul_tc_kernel<true, P> : kermatmul_tc_kernel<false, P>;
+  if (npoly == P) \
+    return bf16 ? kermatmul_tc_kernel<true, P, 64> : kermatmul_tc_kernel<false, P, 64>;
   TSVM_SEL(0)
   TSVM_SEL(2)
   TSVM_SEL(4)
   TSVM_SEL(6)
   TSVM_SEL(8)
 #undef TSVM_SEL
-  return bf16 ? kermatmul_tc_kernel<true, 4> : kermatmul_tc_kernel<false, 4>;
+  return bf16 ? kermatmul_tc_kernel<true, 4, 64> : kermatmul_tc_kernel<false, 4, 64>;
+}
+
+// Gram K for d features: 3 d split products + 6 norm terms, rounded up to a 64-wide chunk.
+int gram_k(int d) {
+  const int need = 3 * d + 6;
+  return need <= 64 ? 64 : need <= 128 ? 128 : 192;
+}
+
+size_t tc_smem(int KG, int kpw) {
+  if (KG == 128) return smem_layout<128>(kpw).total + 1024;
+  if (KG == 192) return smem_layout<192>(kpw).total + 1024;
+  return smem_layout<64>(kpw).total + 1024;
 }
 
 }  // namespace
 
 bool kermatmul_tc_supported(int d, int kp) {
-  return d >= 1 && 3 * d + 6 <= kKG && kp >= 64 && kp % 64 == 0 && encode_fn() != nullptr;
+  return d >= 1 && 3 * d + 6 <= kMaxKG && kp >= 64 && kp % 64 == 0 && encode_fn() != nullptr;
 }
 
 tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms, const float *y,
@@ -503,10 +540,11 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
   if (!kermatmul_tc_supported(d, kp)) return TSVM_ERR_UNSUPPORTED;
   const bool bf16 = precision == TSVM_PREC_BF16;
   const int64_t n_pad = round_up(n, kBM);
+  const int KG = gram_k(d);
   // operands
   __half *XA = nullptr;
-  TSVM_TRY(scratch_t(ctx, SLOT_OPX, (size_t)2 * n_pad * kKG, &XA));
-  __half *XB = XA + (size_t)n_pad * kKG;
+  TSVM_TRY(scratch_t(ctx, SLOT_OPX, (size_t)2 * n_pad * KG, &XA));
+  __half *XB = XA + (size_t)n_pad * KG;
   uint16_t *AT = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_OPA, (size_t)kp * n_pad, &AT));
   double *part = nullptr;
@@ -515,8 +553,8 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
   float *scale = reinterpret_cast<float *>(part + nb);
   int *err = reinterpret_cast<int *>(scale + 4);
   const double xscale = sqrt(2.0 * gamma * 1.4426950408889634);
-  prep_gram_operands<<<(unsigned)ceil_div(n_pad, 256), 256, 0, ctx->stream>>>(Xc, n, n_pad, d,
-                                                                              xscale, XA, XB);
+  prep_gram_operands<<<(unsigned)ceil_div(n_pad, 256), 256, 0, ctx->stream>>>(
+      Xc, n, n_pad, d, KG, xscale, XA, XB);
   TSVM_LAUNCHED(ctx);
   sumsq_partial<<<nb, 256, 0, ctx->stream>>>(A, n * (int64_t)kp, part);
   TSVM_LAUNCHED(ctx);
@@ -533,8 +571,8 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
   TSVM_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
 
   CUtensorMap mxa, mxb;
-  if (!make_map(&mxa, XA, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, kKG, n_pad, 64, kBM) ||
-      !make_map(&mxb, XB, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, kKG, n_pad, 64, kBJ))
+  if (!make_map(&mxa, XA, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, KG, n_pad, 64, kBM) ||
+      !make_map(&mxb, XB, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, KG, n_pad, 64, kBJ))
     return TSVM_ERR_CUDA;
   const int ntiles = (int)(n_pad / kBJ);
   const int nrb = (int)(n_pad / kBM);
@@ -547,9 +585,8 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
     if (!make_map(&mat, AT, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
                   kBJ, (uint64_t)ntiles * kp, kBJ, kpw))
       return TSVM_ERR_CUDA;
-    const SmemLayout L = smem_layout(kpw);
-    const size_t smem = L.total + 1024;
-    auto kern = select_kernel(bf16, poly_split());
+    const size_t smem = tc_smem(KG, kpw);
+    auto kern = select_kernel(bf16, poly_split(), KG);
     TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<grid, kThreadsTC, smem, ctx->stream>>>(mxa, mxb, mat, y, scale + 1, n, nrb, ntiles, kp,
                                                   c0, kpw, W, kp, err);

@@ -119,7 +119,9 @@ def test_kermatmul_fp32(ctx, n, d, kp):
 
 
 @pytest.mark.parametrize("prec,tol", [(_lib.PREC_FP16, 2e-3), (_lib.PREC_BF16, 1.5e-2)])
-@pytest.mark.parametrize("n,d,kp", [(3001, 18, 64), (517, 12, 256), (1000, 18, 448), (300, 3, 128)])
+@pytest.mark.parametrize("n,d,kp", [(3001, 18, 64), (517, 12, 256), (1000, 18, 448), (300, 3, 128),
+                                    # Gram K 128 and 192 (d > 19), with column slabs
+                                    (1500, 28, 256), (700, 40, 128), (900, 54, 448), (600, 62, 64)])
 def test_kermatmul_tensor_core(ctx, n, d, kp, prec, tol):
     rng = np.random.default_rng(n + kp)
     X = rng.standard_normal((n, d)).astype(np.float32)

@@ -175,6 +175,19 @@ def test_factor_tensor_core_matches_oracle(ctx, c1, prec):
     assert err < (2e-3 if prec == "fp16" else 2e-2), err
 
 
+@pytest.mark.parametrize("prec", ["fp16", "bf16"])
+def test_factor_tensor_core_wide_features(ctx, prec):
+    # d = 54 (the covtype-shaped config): Gram K = 192 on the tensor cores
+    X, y, g, C, k = synth.make("c3", n=3000)
+    k = 64
+    Z, info = api.factor(ctx, dev(X), dev(y), g, k, prec)
+    Zh = Z.cpu().numpy()[:, :k].astype(np.float64)
+    f = orc.lra(X, y, g, k)
+    G, Gr = Zh @ Zh.T, f.U @ f.U.T
+    err = np.linalg.norm(G - Gr) / np.linalg.norm(Gr)
+    assert err < (2e-3 if prec == "fp16" else 2e-2), err
+
+
 def test_train_tensor_core_against_fp64_oracle(ctx, c1):
     X, y, g, C, k = c1
     m = api.train(ctx, X, y, _lib.KERNEL_RBF, g, C, k, "fp16")
