@@ -155,10 +155,13 @@ def run_ours(args, world, rank, local):
     ctx.set_stream(stream.cuda_stream)
     prec = args.precision
 
+    last = {}
+
     def step(precision):
         Z, finfo = api.factor(ctx, Xd, yd, GAMMA, K, precision)
         alpha, _, _, st = api.ipm(ctx, Z, yd, K, CPEN, rel_gap_tol=1e-6,
                                   precision=_lib.PREC_FP32 if precision == "fp32" else _lib.PREC_BF16)
+        last[precision] = (Z, alpha)
         return finfo, st
 
     with torch.cuda.stream(stream):
@@ -205,6 +208,12 @@ def run_ours(args, world, rank, local):
             f1.record(stream)
             torch.cuda.synchronize()
             fp32_s = f0.elapsed_time(f1) / 1e3
+            # full-size agreement of the two models' decision values (each through its own factor)
+            fm = decision_values(ctx, *last[prec], yd, K, CPEN)
+            f32 = decision_values(ctx, *last["fp32"], yd, K, CPEN)
+            sign_agree = float((torch.sign(fm) == torch.sign(f32)).double().mean())
+            dec_rel = float((fm - f32).abs().max() / f32.abs().max())
+            del last["fp32"]
     sec = total_ms / 1e3 / args.steps
     sec, e2e_s = dist_max([sec, (sum(e2e_ms) / max(1, len(e2e_ms))) / 1e3], world)
     if rank != 0:
@@ -262,11 +271,21 @@ def run_ours(args, world, rank, local):
         "clocks": clk.summary(),
     }
     if fp32_s is not None:
-        line["fp32_form"] = {"value": round(fp32_s, 3), "unit": "s", "speedup_mixed_vs_fp32": round(fp32_s / sec, 2)}
+        line["fp32_form"] = {"value": round(fp32_s, 3), "unit": "s", "speedup_mixed_vs_fp32": round(fp32_s / sec, 2),
+                             "decision_sign_agreement": sign_agree,
+                             "decision_max_rel_diff": dec_rel}
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
     ctx.close()
     return line
+
+
+def decision_values(ctx, Z, alpha, y, k, C):
+    """Training-set decision values f = Z_k Z_k^T (alpha o y) + b of a solved model, in FP64."""
+    from tensorsvm_b200 import api
+    b = api.bias(ctx, Z, y, alpha, k, C)[0]
+    Zk = Z[:, :k].double()
+    return Zk @ (Zk.T @ (alpha * y.double())) + b
 
 
 def cpu_baseline(args):
@@ -286,6 +305,204 @@ def cpu_baseline(args):
             "sample": f"FP64 oracle (numpy/OpenBLAS) on n={ns} rows of the same generator: "
                       f"factor {t1 - t0:.2f}s scaled by (n/ns)^2, IPM {t2 - t1:.2f}s "
                       f"({r.iters} it) scaled by n/ns"}
+
+
+# ------------------------------------------------------------------------------------------
+# the other workloads (--workload): wide features, the batched grid, the hypergradient.  Rank 0
+# only; each prints its own JSON line.  The default line above is the benchmark contract.
+# ------------------------------------------------------------------------------------------
+
+def _timed(stream, fn):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return out, e0.elapsed_time(e1) / 1e3
+
+
+def _base_line(args, metric, value, config):
+    return {"metric": metric, "value": round(value, 4), "unit": "s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "data": "synthetic", "config": config}
+
+
+def run_wide(args, ctx, stream):
+    """n=500,000, d=54 (10 uniform + one-hot groups of 4 and 40), gamma 0.02, C 32, k 400: the
+    fp16 tensor-core factor + IPM against the FP32 form, to rel. gap 1e-6."""
+    import torch
+    from tensorsvm_b200 import _lib, api, synth
+    X, y, gamma, C, k = synth.make("c3", n=args.n if args.n != N_DEFAULT else None)
+    Xd, yd = torch.from_numpy(X).cuda(), torch.from_numpy(y).cuda()
+    n = X.shape[0]
+
+    def solve(prec):
+        Z, fi = api.factor(ctx, Xd, yd, gamma, k, prec)
+        a, _, _, st = api.ipm(ctx, Z, yd, k, C, rel_gap_tol=1e-6,
+                              precision=_lib.PREC_FP32 if prec == "fp32" else _lib.PREC_BF16)
+        return Z, a, fi, st
+
+    for _ in range(args.warmup):
+        solve(args.precision)
+    times, res = [], None
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            res, t = _timed(stream, lambda: solve(args.precision))
+            times.append(t)
+    Z, a, fi, st = res
+    (Z32, a32, fi32, st32), t32 = _timed(stream, lambda: solve("fp32"))
+    fm = decision_values(ctx, Z, a, yd, k, C)
+    f32 = decision_values(ctx, Z32, a32, yd, k, C)
+    sec = statistics.mean(times)
+    line = _base_line(args, "s to rel. gap 1e-6, n=500k d=54 k=400 (fp16 TC vs FP32 form)", sec,
+                      {"workload": "mixed_onehot_rbf", "n": n, "d": X.shape[1], "k": k,
+                       "gamma": gamma, "C": C, "precision": args.precision})
+    line.update({
+        "dtype": f"{args.precision} contractions (fp32 accum), f64 k x k + IPM vectors",
+        "phases_ms": {"factor": round(fi["ms_total"], 1), "kermatmul_per_launch": round(fi["ms_kermatmul_kernel"] / 2, 1),
+                      "ipm": round(st["ms_total"], 1), "ipm_iters": st["iters"],
+                      "ipm_syrk": round(st["ms_syrk"], 1), "mixed_syrk": st["mixed_syrk"]},
+        "tflops_kermatmul": round(fi["flops_kermatmul"] / (fi["ms_kermatmul_kernel"] / 1e3) / 1e12, 1),
+        "solution": {"rel_gap": st["rel_gap"], "pobj": st["pobj"], "iters": st["iters"]},
+        "fp32_form": {"value": round(t32, 3), "unit": "s", "speedup": round(t32 / sec, 2),
+                      "pobj": st32["pobj"], "iters": st32["iters"],
+                      "pobj_rel_diff": abs(st["pobj"] - st32["pobj"]) / abs(st32["pobj"]),
+                      "decision_sign_agreement": float((torch.sign(fm) == torch.sign(f32)).double().mean()),
+                      "decision_max_rel_diff": float((fm - f32).abs().max() / f32.abs().max())},
+        "step_s": [round(t, 3) for t in times], "clocks": clk.summary()})
+    return line
+
+
+def run_grid(args, ctx, stream):
+    """64 tanh-teacher problems (n log-uniform in [2000, 200000], d=28) on the 8 x 8 (C, gamma)
+    grid, k=128: tensor-core factors + one batched IPM, against the same factors solved one by
+    one and against 64 plain FP32 solves (FP32 factor + FP32 IPM)."""
+    import torch
+    from tensorsvm_b200 import _lib, api, synth
+    probs = synth.grid_problems(count=64)
+    k = 128
+    Xs = [torch.from_numpy(X).cuda() for X, _, _, _ in probs]
+    ys = [torch.from_numpy(y).cuda() for _, y, _, _ in probs]
+    gs = [g for _, _, g, _ in probs]
+    Cs = [C for _, _, _, C in probs]
+    rows = sum(X.shape[0] for X in Xs)
+
+    def factors(prec):
+        return [api.factor(ctx, X, y, g, k, prec)[0] for X, y, g in zip(Xs, ys, gs)]
+
+    def batched():
+        Zs = factors(args.precision)
+        _, t_ipm = _timed(stream, lambda: api.ipm_batched(ctx, Zs, ys, k, Cs, rel_gap_tol=1e-6))
+        return Zs, t_ipm
+
+    def sequential(Zs, prec):
+        out = []
+        for Z, y, C in zip(Zs, ys, Cs):
+            out.append(api.ipm(ctx, Z, y, k, C, rel_gap_tol=1e-6, precision=prec)[3])
+        return out
+
+    for _ in range(args.warmup):
+        batched()
+    times, ipm_times = [], []
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            (Zs, t_ipm), t = _timed(stream, batched)
+            times.append(t)
+            ipm_times.append(t_ipm)
+    _, t_fac = _timed(stream, lambda: factors(args.precision))
+    (alphas, bstats, info) = api.ipm_batched(ctx, Zs, ys, k, Cs, rel_gap_tol=1e-6)
+    seq_stats, t_seq_ipm = _timed(stream, lambda: sequential(Zs, _lib.PREC_BF16))
+    del Zs
+    Z32, t_fac32 = _timed(stream, lambda: factors("fp32"))
+    st32, t_ipm32 = _timed(stream, lambda: sequential(Z32, _lib.PREC_FP32))
+    sec = statistics.mean(times)
+    line = _base_line(args, "s for a 64-problem (C, gamma) grid: factors + batched IPM to rel. gap 1e-6",
+                      sec, {"workload": "tanh_teacher_grid", "problems": 64, "rows_total": rows,
+                            "n_min": min(X.shape[0] for X in Xs), "n_max": max(X.shape[0] for X in Xs),
+                            "d": 28, "k": k, "precision": args.precision})
+    line.update({
+        "dtype": f"{args.precision} kernel-block product, f32/f64 IPM",
+        "phases_s": {"factors": round(t_fac, 3), "batched_ipm": round(statistics.mean(ipm_times), 3),
+                     "batched_ms_autotune": round(info["ms_autotune"], 1),
+                     "unit_rows": info["unit_rows"], "units": info["units"],
+                     "graph_used": info["graph_used"], "iters_max": info["iters_max"]},
+        "sequential_same_factors": {"ipm_s": round(t_seq_ipm, 3), "total_s": round(t_fac + t_seq_ipm, 3),
+                                    "speedup_batched_ipm": round(t_seq_ipm / statistics.mean(ipm_times), 2)},
+        "plain_fp32_sequential": {"factors_s": round(t_fac32, 3), "ipm_s": round(t_ipm32, 3),
+                                  "total_s": round(t_fac32 + t_ipm32, 3),
+                                  "speedup": round((t_fac32 + t_ipm32) / sec, 2)},
+        "iters": {"batched": [s["iters"] for s in bstats], "sequential": [s["iters"] for s in seq_stats]},
+        "status_ok": sum(1 for s in bstats if s["status"] == _lib.OK),
+        "step_s": [round(t, 3) for t in times], "clocks": clk.summary()})
+    return line
+
+
+def run_hypergrad(args, ctx, stream):
+    """Validation squared-hinge hypergradient, n=200,000 train + 50,000 validation, d=28,
+    gamma 0.03, C 16, k 256: forward (factor + IPM + bias + loss) and backward (tsvm_hypergrad,
+    factor recomputed) times."""
+    import torch
+    from tensorsvm_b200 import _lib, api, synth
+    X, y, gamma, C, k = synth.make("c5")
+    Xv, yv, _, _, _ = synth.make("c5_val")
+    Xd, yd = torch.from_numpy(X).cuda(), torch.from_numpy(y).cuda()
+    Xvd, yvd = torch.from_numpy(Xv).cuda(), torch.from_numpy(yv).cuda()
+    prec = args.precision
+
+    def forward():
+        Z, _ = api.factor(ctx, Xd, yd, gamma, k, prec)
+        a, xi, ym, st = api.ipm(ctx, Z, yd, k, C, want_xi=True, tol=1e-9,
+                                precision=_lib.PREC_FP32 if prec == "fp32" else _lib.PREC_BF16)
+        b = api.bias(ctx, Z, yd, a, k, C)[0]
+        del Z
+        return a, xi, st["s"], ym, b, st
+
+    def backward(sol):
+        a, xi, s, ym, b, _ = sol
+        return api.hypergrad(ctx, Xd, yd, Xvd, yvd, gamma, C, k, a, xi, s, ym, b, precision=prec,
+                             want_dxv=True)
+
+    for _ in range(args.warmup):
+        backward(forward())
+    fw, bw, res = [], [], None
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            sol, tf = _timed(stream, forward)
+            res, tb = _timed(stream, lambda: backward(sol))
+            fw.append(tf)
+            bw.append(tb)
+    r, dxv = res
+    sec = statistics.mean(fw) + statistics.mean(bw)
+    line = _base_line(args, "s for forward + backward of the validation-loss hypergradient "
+                            "(n=200k + 50k, d=28, k=256)", sec,
+                      {"workload": "tanh_teacher_hypergrad", "n": X.shape[0], "n_val": Xv.shape[0],
+                       "d": X.shape[1], "k": k, "gamma": gamma, "C": C, "precision": prec})
+    line.update({
+        "dtype": f"{prec} kernel-block product, f64 IPM and adjoint",
+        "forward_s": round(statistics.mean(fw), 3), "backward_s": round(statistics.mean(bw), 3),
+        "backward_ms_inside": round(r["ms"], 1), "ipm_iters": sol[5]["iters"],
+        "loss": r["loss"], "dloss_dlog_gamma": r["dloss_dlog_gamma"], "dloss_dlog_C": r["dloss_dlog_C"],
+        "n_free_bias": r["n_free_bias"], "dxv_norm": float(dxv.double().norm()),
+        "clocks": clk.summary()})
+    return line
+
+
+def run_workload(args, world, rank, local):
+    if rank != 0:
+        return None
+    import torch
+    from tensorsvm_b200 import _lib
+    torch.cuda.set_device(local)
+    ctx = _lib.Context(local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    fn = {"wide": run_wide, "grid": run_grid, "hypergrad": run_hypergrad}[args.workload]
+    with torch.cuda.stream(stream):
+        line = fn(args, ctx, stream)
+    line["gpu_launches"] = int(ctx.launches)
+    ctx.close()
+    return line
 
 
 # ------------------------------------------------------------------------------------------
@@ -370,9 +587,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=16384)
     ap.add_argument("--ref-sample", type=int, default=262144)
+    ap.add_argument("--workload", default="two_gaussians", choices=["two_gaussians", "wide", "grid", "hypergrad"],
+                    help="two_gaussians (default): the benchmark line; wide: n=500k d=54 k=400; "
+                         "grid: 64-problem batched (C, gamma) grid; hypergrad: validation-loss "
+                         "hypergradient at n=200k + 50k")
     args = ap.parse_args()
     world, rank, local = dist_setup()
-    if args.impl == "reference":
+    if args.workload != "two_gaussians" and args.impl == "ours":
+        line = run_workload(args, world, rank, local)
+    elif args.impl == "reference":
         line = run_reference(args, world, rank)
     else:
         line = run_ours(args, world, rank, local)

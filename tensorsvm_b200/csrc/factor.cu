@@ -88,13 +88,15 @@ struct Phase {
 
 }  // namespace
 
+// round_back: see kermatmul_tc (ignored by the FP32 form, whose operand is not rounded).
 static tsvm_status kermatmul(tsvm_context *ctx, const float *Xc, const float *norms,
                              const float *y, int64_t n, int d, double gamma, const float *A,
-                             int kp, float *W, int precision, float *kernel_ms) {
+                             int kp, float *W, int precision, float *kernel_ms,
+                             float *round_back = nullptr) {
   if (precision == TSVM_PREC_FP32)
     return kermatmul_fp32(ctx, Xc, norms, y, n, d, gamma, A, kp, W);
   if (!kermatmul_tc_supported(d, kp)) return TSVM_ERR_UNSUPPORTED;
-  return kermatmul_tc(ctx, Xc, norms, y, n, d, gamma, A, kp, W, precision, kernel_ms);
+  return kermatmul_tc(ctx, Xc, norms, y, n, d, gamma, A, kp, W, precision, kernel_ms, round_back);
 }
 
 // Rkeep (2 k x k doubles, may be null): the combined factor R with (input W) = (output W) R.
@@ -179,7 +181,10 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
   TSVM_TRY(orthonormalise(ctx, W, n, k, kp, keep ? keep->R : nullptr));
   if (keep) keep->W = W;
   TSVM_CUDA(cudaEventRecord(ev[3], ctx->stream));
-  TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, W, kp, Q, precision, &km2));
+  // the second pass rounds the orthonormal basis W to the tensor-core operand type in place:
+  // C = W^T (K W) and Z = W V diag(sqrt w) then use the W the tensor cores contracted, so the
+  // weak eigen-directions of C do not pick up the rounding of one side only
+  TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, W, kp, Q, precision, &km2, W));
   TSVM_CUDA(cudaEventRecord(ev[4], ctx->stream));
   double *Cm = nullptr, *V = nullptr, *w = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_SMALL, (size_t)k * k + 8, &Cm));

@@ -146,8 +146,9 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
 kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
                     const __grid_constant__ CUtensorMap map_xb,
                     const __grid_constant__ CUtensorMap map_at, const float *__restrict__ y,
-                    const float *__restrict__ inv_scale, int64_t n, int nrb, int ntiles, int kp,
-                    int c0, int kpw, float *__restrict__ W, int64_t ldw, int *__restrict__ err) {
+                    const float *__restrict__ inv_scale, const float *__restrict__ ccol,
+                    int64_t n, int nrb, int ntiles, int kp, int c0, int kpw,
+                    float *__restrict__ W, int64_t ldw, int *__restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   const uint32_t raw = su32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -323,6 +324,7 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
     const int row = q * 32 + lane;        // row of the 128-row block (TMEM lane)
     const uint32_t lane_off = (uint32_t)(q * 32) << 16;
     const int half = kpw / 2;
+    const float shift = inv_scale[1];   // the kernel's sampled mean, taken off every P entry
     bool ok = true;
     for (int rb = blockIdx.x, r = 0; ok && rb < nrb; rb += G, ++r) {
       const uint32_t T0 = (uint32_t)r * (uint32_t)ntiles;   // flat index of the first J block
@@ -339,12 +341,13 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
         uint32_t pk[32];
 #pragma unroll
         for (int c = 0; c < 16; ++c)
-          pk[c] = pack2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c]), 2 * c),
-                              exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c + 1]), 2 * c + 1));
+          pk[c] = pack2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c]), 2 * c) - shift,
+                              exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c + 1]), 2 * c + 1) - shift);
 #pragma unroll
         for (int c = 0; c < 16; ++c)
-          pk[16 + c] = pack2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c]), 2 * c),
-                                   exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c + 1]), 2 * c + 1));
+          pk[16 + c] =
+              pack2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c]), 2 * c) - shift,
+                          exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c + 1]), 2 * c + 1) - shift);
         tmem_st32(tb, pk);   // P over the first 32 columns of the buffer (S is no longer needed)
         tmem_wait_st();
         tc_fence_before();
@@ -360,12 +363,17 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
         tmem_ld32(t_w + cc + lane_off, v);
         tmem_wait_ld();
         if (gi < n) {
+          // W = (sum_j (P_ij - shift) A_j + shift sum_j A_j) y_i / s
           float4 *dst = reinterpret_cast<float4 *>(W + gi * ldw + c0 + cc);
+          const float4 *cs = reinterpret_cast<const float4 *>(ccol + c0 + cc);
 #pragma unroll
-          for (int j = 0; j < 8; ++j)
-            dst[j] = make_float4(__uint_as_float(v[4 * j]) * sc, __uint_as_float(v[4 * j + 1]) * sc,
-                                 __uint_as_float(v[4 * j + 2]) * sc,
-                                 __uint_as_float(v[4 * j + 3]) * sc);
+          for (int j = 0; j < 8; ++j) {
+            const float4 a = cs[j];
+            dst[j] = make_float4((__uint_as_float(v[4 * j]) + a.x) * sc,
+                                 (__uint_as_float(v[4 * j + 1]) + a.y) * sc,
+                                 (__uint_as_float(v[4 * j + 2]) + a.z) * sc,
+                                 (__uint_as_float(v[4 * j + 3]) + a.w) * sc);
+          }
         }
       }
       tc_fence_before();
@@ -454,40 +462,118 @@ __global__ void choose_scale(const double *__restrict__ part, int nb, int64_t co
 // j < n, and zeros for j in [n, n_pad).  Each J block's kernel-block operand is one contiguous
 // kp x 128-byte slab, so a TMA box touches one or two pages; with the plain [kp][n] layout a box
 // spans kp rows 2n bytes apart (256 pages at n = 1M), which overruns the address-translation
-// caches.  32x32 transpose tiles.
+// caches.  32x32 transpose tiles; block (x, y) takes the row tiles x, x + gridDim.x, ... of
+// column group y and leaves the column sums of the rounded operand over its rows in
+// cpart[x][c] (fixed order: the sums are the same on every run).
+// With `round_back` set (it may alias A) the operand as the tensor cores see it, A rounded to
+// the 16-bit type on the scaled grid (s is a power of two, y = +-1, so the round trip is exact),
+// is written back over A: a caller that forms W^T (K W) afterwards then contracts the same W on
+// both sides, and the projection C = W^T K W stays consistent with the rounded operand.
 template <typename T>
-__global__ void prep_at(const float *__restrict__ A, const float *__restrict__ y, int64_t n,
-                        int64_t n_pad, int kp, const float *__restrict__ scale, T *__restrict__ AT) {
+__device__ __forceinline__ float round16(float v) {
+  if constexpr (std::is_same<T, __half>::value)
+    return __half2float(__float2half_rn(v));
+  else
+    return __bfloat162float(__float2bfloat16_rn(v));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+prep_at(const float *A, const float *__restrict__ y, int64_t n, int64_t n_pad, int kp,
+        const float *__restrict__ scale, T *__restrict__ AT, float *round_back,
+        double *__restrict__ cpart) {
   __shared__ float tile[32][33];
-  const int64_t j0 = (int64_t)blockIdx.x * 32;
+  __shared__ double red[8][33];
   const int c0 = blockIdx.y * 32;
-  const float s = scale[0];
-  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-    const int64_t j = j0 + r;
-    const int c = c0 + threadIdx.x;
-    float v = 0.f;
-    if (j < n && c < kp) v = A[j * kp + c] * y[j] * s;
-    tile[r][threadIdx.x] = v;
-  }
-  __syncthreads();
-  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-    const int c = c0 + r;
-    const int64_t j = j0 + threadIdx.x;
-    if (c < kp && j < n_pad) {
-      const int64_t o = ((j / kBJ) * kp + c) * kBJ + (j % kBJ);
-      if constexpr (sizeof(T) == 2 && std::is_same<T, __half>::value)
-        AT[o] = __float2half_rn(tile[threadIdx.x][r]);
-      else
-        AT[o] = __float2bfloat16_rn(tile[threadIdx.x][r]);
+  const float s = scale[0], inv_s = scale[1];
+  double csum = 0.0;   // column c0 + threadIdx.x over the rows this thread loads
+  for (int64_t j0 = (int64_t)blockIdx.x * 32; j0 < n_pad; j0 += (int64_t)gridDim.x * 32) {
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const int64_t j = j0 + r;
+      const int c = c0 + threadIdx.x;
+      float v = 0.f;
+      if (j < n && c < kp) {
+        const float yj = y[j];
+        v = round16<T>(A[j * kp + c] * yj * s);
+        if (round_back) round_back[j * kp + c] = v * inv_s * yj;
+      }
+      tile[r][threadIdx.x] = v;
+      csum += (double)v;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const int c = c0 + r;
+      const int64_t j = j0 + threadIdx.x;
+      if (c < kp && j < n_pad) {
+        const int64_t o = ((j / kBJ) * kp + c) * kBJ + (j % kBJ);
+        if constexpr (sizeof(T) == 2 && std::is_same<T, __half>::value)
+          AT[o] = __float2half_rn(tile[threadIdx.x][r]);
+        else
+          AT[o] = __float2bfloat16_rn(tile[threadIdx.x][r]);
+      }
     }
   }
+  red[threadIdx.y][threadIdx.x] = csum;
+  __syncthreads();
+  if (threadIdx.y == 0 && c0 + (int)threadIdx.x < kp) {
+    double t = 0.0;
+    for (int r = 0; r < 8; ++r) t += red[r][threadIdx.x];
+    cpart[(int64_t)blockIdx.x * kp + c0 + threadIdx.x] = t;
+  }
+}
+
+// Mean of the RBF kernel over the m x m pairs of m rows spread evenly over the data (rows
+// i n / m): the constant taken off every kernel entry before it is rounded to 16 bits.  For a
+// flat kernel (entries in [0.75, 1], say) the 16-bit rounding error then scales with the
+// entries' spread about the mean rather than with the entries, and the weak eigen-directions
+// of the kernel stay above it.  Block i sums row i; part[i] (fixed order).
+__global__ void __launch_bounds__(256)
+kernel_mean_rows(const float *__restrict__ Xc, int64_t n, int d, int m, float gamma,
+                 double *__restrict__ part) {
+  __shared__ float xi[kMaxKG];
+  __shared__ double sh[8];
+  const int64_t ri = (int64_t)blockIdx.x * n / m;
+  for (int c = threadIdx.x; c < d; c += blockDim.x) xi[c] = Xc[ri * d + c];
+  __syncthreads();
+  double acc = 0.0;
+  for (int j = threadIdx.x; j < m; j += blockDim.x) {
+    const int64_t rj = (int64_t)j * n / m;
+    float d2 = 0.f;
+    for (int c = 0; c < d; ++c) {
+      const float t = xi[c] - Xc[rj * d + c];
+      d2 = fmaf(t, t, d2);
+    }
+    acc += (double)expf(-gamma * d2);
+  }
+  double v[1] = {acc};
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+
+// scale[2] = shift = the mean over the m partial row sums; ccol[c] = shift * sum_x cpart[x][c].
+__global__ void kernel_mean_finish(const double *__restrict__ part, int m, float *scale) {
+  if (threadIdx.x != 0) return;
+  double t = 0.0;
+  for (int i = 0; i < m; ++i) t += part[i];
+  scale[2] = (float)(t / ((double)m * m));
+}
+
+__global__ void column_shift(const double *__restrict__ cpart, int nparts, int kp,
+                             const float *__restrict__ scale, float *__restrict__ ccol) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= kp) return;
+  double t = 0.0;
+  for (int x = 0; x < nparts; ++x) t += cpart[(int64_t)x * kp + c];
+  ccol[c] = (float)((double)scale[2] * t);
 }
 
 // ---------------------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------------------
 using TcKernel = void (*)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const float *,
-                          const float *, int64_t, int, int, int, int, int, float *, int64_t, int *);
+                          const float *, const float *, int64_t, int, int, int, int, int, float *,
+                          int64_t, int *);
 
 // Exps per 8 columns evaluated by the FMA-pipe polynomial (the rest on MUFU); tunable through
 // TSVM_TC_POLY (0, 2, 4, 6 or 8) for the autotuning sweep in the benchmarks.
@@ -535,7 +621,7 @@ bool kermatmul_tc_supported(int d, int kp) {
 
 tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms, const float *y,
                          int64_t n, int d, double gamma, const float *A, int kp, float *W,
-                         int precision, float *kernel_ms) {
+                         int precision, float *kernel_ms, float *round_back) {
   (void)norms;
   if (!kermatmul_tc_supported(d, kp)) return TSVM_ERR_UNSUPPORTED;
   const bool bf16 = precision == TSVM_PREC_BF16;
@@ -547,11 +633,19 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
   __half *XB = XA + (size_t)n_pad * KG;
   uint16_t *AT = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_OPA, (size_t)kp * n_pad, &AT));
-  double *part = nullptr;
+  // SLOT_MISC: sum-of-squares partials [nb] | scale: s, 1/s, shift, - (4 floats) | err |
+  // kernel-mean row sums [m] | column-sum partials [rg][kp] | ccol [kp floats]
   const int nb = ctx->num_sms * 2;
-  TSVM_TRY(scratch_t(ctx, SLOT_MISC, (size_t)nb + 16, &part));
+  const int m = n < 1024 ? (int)n : 1024;
+  const int rg = (int)(n_pad / 32 < (int64_t)nb ? n_pad / 32 : nb);
+  const size_t o_samp = (size_t)nb + 8, o_cpart = o_samp + 1024;
+  const size_t o_ccol = o_cpart + (size_t)rg * kp;
+  double *part = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_MISC, o_ccol + (size_t)kp / 2 + 16, &part));
   float *scale = reinterpret_cast<float *>(part + nb);
   int *err = reinterpret_cast<int *>(scale + 4);
+  double *samp = part + o_samp, *cpart = part + o_cpart;
+  float *ccol = reinterpret_cast<float *>(part + o_ccol);   // o_ccol is even: 16-byte aligned
   const double xscale = sqrt(2.0 * gamma * 1.4426950408889634);
   prep_gram_operands<<<(unsigned)ceil_div(n_pad, 256), 256, 0, ctx->stream>>>(
       Xc, n, n_pad, d, KG, xscale, XA, XB);
@@ -560,13 +654,19 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
   TSVM_LAUNCHED(ctx);
   choose_scale<<<1, 32, 0, ctx->stream>>>(part, nb, n * (int64_t)kp, scale);
   TSVM_LAUNCHED(ctx);
-  const dim3 tgrid((unsigned)(n_pad / 32), (unsigned)ceil_div(kp, 32));
+  kernel_mean_rows<<<m, 256, 0, ctx->stream>>>(Xc, n, d, m, (float)gamma, samp);
+  TSVM_LAUNCHED(ctx);
+  kernel_mean_finish<<<1, 32, 0, ctx->stream>>>(samp, m, scale);
+  TSVM_LAUNCHED(ctx);
+  const dim3 tgrid((unsigned)rg, (unsigned)ceil_div(kp, 32));
   if (bf16)
     prep_at<__nv_bfloat16><<<tgrid, dim3(32, 8), 0, ctx->stream>>>(
-        A, y, n, n_pad, kp, scale, reinterpret_cast<__nv_bfloat16 *>(AT));
+        A, y, n, n_pad, kp, scale, reinterpret_cast<__nv_bfloat16 *>(AT), round_back, cpart);
   else
-    prep_at<__half><<<tgrid, dim3(32, 8), 0, ctx->stream>>>(A, y, n, n_pad, kp, scale,
-                                                           reinterpret_cast<__half *>(AT));
+    prep_at<__half><<<tgrid, dim3(32, 8), 0, ctx->stream>>>(
+        A, y, n, n_pad, kp, scale, reinterpret_cast<__half *>(AT), round_back, cpart);
+  TSVM_LAUNCHED(ctx);
+  column_shift<<<(unsigned)ceil_div(kp, 256), 256, 0, ctx->stream>>>(cpart, rg, kp, scale, ccol);
   TSVM_LAUNCHED(ctx);
   TSVM_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
 
@@ -588,8 +688,8 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
     const size_t smem = tc_smem(KG, kpw);
     auto kern = select_kernel(bf16, poly_split(), KG);
     TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<grid, kThreadsTC, smem, ctx->stream>>>(mxa, mxb, mat, y, scale + 1, n, nrb, ntiles, kp,
-                                                  c0, kpw, W, kp, err);
+    kern<<<grid, kThreadsTC, smem, ctx->stream>>>(mxa, mxb, mat, y, scale + 1, ccol, n, nrb,
+                                                  ntiles, kp, c0, kpw, W, kp, err);
     TSVM_LAUNCHED(ctx);
   }
   TSVM_CUDA(cudaEventRecord(e1, ctx->stream));

@@ -36,9 +36,10 @@ tsvm_status kermatmul_fp32(tsvm_context *ctx, const float *Xc, const float *norm
 // ---- kermatmul_tc.cu -------------------------------------------------------------------
 bool kermatmul_tc_supported(int d, int kp);
 // Tensor-core (tcgen05) version; precision TSVM_PREC_FP16 or TSVM_PREC_BF16 for P and A.
+// round_back (may be A itself, or null) receives A rounded to the 16-bit operand type.
 tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms, const float *y,
                          int64_t n, int d, double gamma, const float *A, int kp, float *W,
-                         int precision, float *kernel_ms);
+                         int precision, float *kernel_ms, float *round_back = nullptr);
 
 // A unit of batched work: rows [row0, row0 + rows) of problem p; goff is the index of the
 // unit's first row in the problems' concatenated per-row vectors.

@@ -201,3 +201,35 @@ def test_train_tensor_core_against_fp64_oracle(ctx, c1):
     # block and the operand moves the weakest ones, and the flat rank-32 dual moves alpha along
     # them: 98.7% sign agreement measured on this split (100% for the FP32 form)
     assert np.mean(np.sign(dv) == np.sign(dv_o)) >= 0.98
+
+
+@pytest.fixture(scope="module")
+def flat_kernel_oracle():
+    # d = 54 one-hot + uniform features at gamma = 0.02: every kernel entry lies in about
+    # [0.75, 1], and C's eigenvalues span 18057 .. 0.052 (ratio 2.9e-6) at n = 20000, k = 400
+    X, y, g, C, _ = synth.make("c3", n=20000)
+    k = 400
+    f, r, b = orc.train_rbf(X, y, g, C, k, rel_gap_tol=1e-6)
+    fv = f.U @ (f.U.T @ (r.x * y)) + b
+    return X, y, g, C, k, f.eigvals, r.log[-1][5], fv
+
+
+@pytest.mark.parametrize("prec,pobj_tol,eig_tol", [("fp16", 3e-4, 0.05), ("bf16", 5e-2, 0.7)])
+def test_flat_kernel_tensor_core_against_fp64_oracle(ctx, flat_kernel_oracle, prec, pobj_tol,
+                                                     eig_tol):
+    # 16-bit rounding of entries near 1 would put noise of ~2 sigma sqrt(n) = 0.04 on the kernel,
+    # the size of its weakest kept eigenvalue (measured before the mean shift: fp16 objective
+    # 5.3e-2 off, smallest eigenvalue -0.001); with the sampled mean taken off every entry before
+    # rounding, measured 6.6e-5 and 0.0509 (fp16), 1.5e-2 (bf16); the FP32 form 3.2e-4
+    X, y, g, C, k, w, pobj_o, fv_o = flat_kernel_oracle
+    Z, info = api.factor(ctx, dev(X), dev(y), g, k, prec)
+    assert abs(info["eig_min"] - w.min()) <= eig_tol * w.min()
+    yd = dev(y)
+    a, _, _, st = api.ipm(ctx, Z, yd, k, C, rel_gap_tol=1e-6, precision=_lib.PREC_BF16)
+    assert abs(st["pobj"] - pobj_o) <= pobj_tol * abs(pobj_o), (st["pobj"], pobj_o)
+    b = api.bias(ctx, Z, yd, a, k, C)[0]
+    Zk = Z[:, :k].double()
+    fv = (Zk @ (Zk.T @ (a * yd.double())) + b).cpu().numpy()
+    assert np.mean(np.sign(fv) == np.sign(fv_o)) >= 0.999
+    if prec == "fp16":
+        assert np.max(np.abs(fv - fv_o)) <= 2e-3 * np.max(np.abs(fv_o))
