@@ -86,8 +86,10 @@ class ClockSampler:
         mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[j] for s in self.samples for j in range(4) if s[3 + j] == "Active"})
+        pw = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "power_w": statistics.median(pw) if pw else None,
                 "samples": len(self.samples)}
 
 

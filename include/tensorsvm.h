@@ -249,6 +249,75 @@ tsvm_status tsvm_train(tsvm_context *ctx, const float *X, const float *y, int64_
                        const tsvm_ipm_options *opt, double *alpha_out, double *b_out,
                        tsvm_factor_info *finfo, tsvm_ipm_stats *istats);
 
+/* A trained binary model as the model file holds it (writemodel, tensorsvm-train.cu:340-349
+ * LIBLINEAR, 384-406 RBF):
+ *   RBF:    f(x) = sum_i coef_i exp(-gamma ||sv_i - x||^2) - rho, coef_i = y_i alpha_i over the
+ *           nsv support vectors (rows of sv, nsv x d row-major), rho = -b;
+ *   LINEAR: f(x) = w . x - rho with w = sv (d floats), coef and gamma unused, rho = -b.
+ * The predicted label is the model's first label (+1 side) when f(x) > 0, else the second. */
+typedef struct tsvm_model_view {
+  int32_t kernel;        /* TSVM_KERNEL_RBF or TSVM_KERNEL_LINEAR */
+  int32_t d;             /* features */
+  int64_t nsv;           /* support vectors (RBF) */
+  const float *sv;       /* RBF: nsv x d; LINEAR: w, d floats */
+  const double *coef;    /* RBF: nsv coefficients */
+  double rho;
+  double gamma;
+} tsvm_model_view;
+
+/* Decision values f(x_v) of m rows (no counterpart in the reference, which leaves prediction
+ * to ThunderSVM, README.md:27-31; its own predict T:166-270 is never called).  The model's
+ * arrays, X (m x d row-major) and f (m doubles) are device pointers. */
+tsvm_status tsvm_decision_values(tsvm_context *ctx, const tsvm_model_view *model, const float *X,
+                                 int64_t m, double *f);
+
+/* tsvm_decision_values on HOST buffers (the model's arrays, X and f): copies in, computes,
+ * copies f back. */
+tsvm_status tsvm_predict(tsvm_context *ctx, const tsvm_model_view *model, const float *X,
+                         int64_t m, double *f);
+
+/* Frobenius norms ||K~||_F and ||K~ - Z Z^T||_F, K~_ij = y_i y_j exp(-gamma ||x_i - x_j||^2),
+ * in FP64 (replaces rbf_fnorm_res, tensorsvm-train.cu:2388-2467, run by -analysis).
+ * X (n x d), y (n), Z (n x ldz, first k columns used) device; fnorm, fnorm_res host. */
+tsvm_status tsvm_kernel_residual(tsvm_context *ctx, const float *X, const float *y, int64_t n,
+                                 int32_t d, double gamma, const float *Z, int32_t ldz, int32_t k,
+                                 double *fnorm, double *fnorm_res);
+
+/* tsvm_kernel_residual of the last RBF tsvm_train on this context (its device copies of X and
+ * y and its factor), as the reference's -analysis follows its LRA.  TSVM_ERR_INVALID_ARGUMENT
+ * when the context has not trained an RBF model, or a later call reused that memory. */
+tsvm_status tsvm_train_residual(tsvm_context *ctx, double *fnorm, double *fnorm_res);
+
+/* ---- Host I/O (no device work, no context) ------------------------------------------------ */
+
+/* LIBSVM text reader (replaces libsvmread, tensorsvm-train.cu:1162-1278), parsed by `threads`
+ * host threads (0: one per core).  *labels (n floats) and *X (n x d row-major, dense) are
+ * allocated here: release them with tsvm_free.  Indices are shifted by the smallest index seen
+ * (1 for 1-based files); d is the largest index (+1 for a 0-based file).  scale256 divides every
+ * value by 256 (-scale256).  A malformed or empty line returns TSVM_ERR_IO with *bad_line set to
+ * its 1-based number (the reference prints a message and keeps what it read). */
+tsvm_status tsvm_read_libsvm(const char *path, int32_t scale256, int32_t threads, float **labels,
+                             float **X, int64_t *n, int64_t *d, int64_t *nnz, int64_t *bad_line);
+void tsvm_free(void *p);
+
+/* Model file writer (replaces writemodel, tensorsvm-train.cu:273-417), byte-identical text:
+ * RBF: LIBSVM c_svc header and one "y_j alpha_j idx:val ..." line per SV (alpha_j > 1e-6),
+ * values "%7f", zero features omitted, nr_sv = (free, bounded), rho = -b;  LINEAR: LIBLINEAR
+ * header, w = sum_SV alpha_j y_j x_j (%.16f per line) and b.  X, y (+-1), alpha host; the SV
+ * lines are formatted by `threads` threads (0: one per core).  n_sv, n_free may be NULL. */
+tsvm_status tsvm_write_model(const char *path, int32_t kernel, const float *X, const float *y,
+                             const double *alpha, int64_t n, int32_t d, double C, double gamma,
+                             double b, int32_t pos, int32_t neg, int32_t threads, int64_t *n_sv,
+                             int64_t *n_free);
+
+/* Model file reader (either format above; LIBSVM RBF files written by other tools too): fills
+ * *model with host arrays allocated here (release with tsvm_free_model) and the two labels
+ * (f > 0 predicts label_pos).  For RBF models d is the largest feature index in the SV
+ * section; pad rows and SVs to a common d before predicting. */
+tsvm_status tsvm_read_model(const char *path, tsvm_model_view *model, int32_t *label_pos,
+                            int32_t *label_neg);
+void tsvm_free_model(tsvm_model_view *model);
+
 /* Number of tensorsvm kernels this library launched since the context was created. */
 int64_t tsvm_kernel_launches(const tsvm_context *ctx);
 

@@ -40,6 +40,8 @@ EXPORTS = [
     "tsvm_ipm_default_options",
     "tsvm_factor", "tsvm_linear_factor", "tsvm_ipm", "tsvm_bias", "tsvm_bias_noalloc",
     "tsvm_train", "tsvm_kernel_launches", "tsvm_ipm_batched", "tsvm_hypergrad",
+    "tsvm_decision_values", "tsvm_predict", "tsvm_kernel_residual", "tsvm_train_residual",
+    "tsvm_read_libsvm", "tsvm_free", "tsvm_write_model", "tsvm_read_model", "tsvm_free_model",
 ]
 TEST_EXPORTS = [
     "tsvm_test_rand_stream", "tsvm_test_sketch", "tsvm_test_kermatmul", "tsvm_test_chol",
@@ -63,6 +65,12 @@ class HypergradResult(ctypes.Structure):
     _fields_ = [("loss", ctypes.c_double), ("dloss_dlog_gamma", ctypes.c_double),
                 ("dloss_dlog_C", ctypes.c_double), ("n_free_bias", ctypes.c_int32),
                 ("ms", ctypes.c_double)]
+
+
+class ModelView(ctypes.Structure):
+    _fields_ = [("kernel", ctypes.c_int32), ("d", ctypes.c_int32), ("nsv", ctypes.c_int64),
+                ("sv", ctypes.c_void_p), ("coef", ctypes.c_void_p), ("rho", ctypes.c_double),
+                ("gamma", ctypes.c_double)]
 
 
 class FactorInfo(ctypes.Structure):
@@ -142,6 +150,27 @@ def load() -> ctypes.CDLL:
     lib.tsvm_hypergrad.restype = ctypes.c_int
     lib.tsvm_hypergrad.argtypes = [P, P, P, I64, I32, P, P, I64, D, D, I32, I32, P, P, P, D, D,
                                    ctypes.POINTER(HypergradResult), P]
+    MV = ctypes.POINTER(ModelView)
+    PD = ctypes.POINTER(D)
+    PP = ctypes.POINTER(P)
+    PI64 = ctypes.POINTER(I64)
+    for name, res, args in [
+        ("tsvm_decision_values", ctypes.c_int, [P, MV, P, I64, P]),
+        ("tsvm_predict", ctypes.c_int, [P, MV, P, I64, P]),
+        ("tsvm_kernel_residual", ctypes.c_int, [P, P, P, I64, I32, D, P, I32, I32, PD, PD]),
+        ("tsvm_train_residual", ctypes.c_int, [P, PD, PD]),
+        ("tsvm_read_libsvm", ctypes.c_int, [ctypes.c_char_p, I32, I32, PP, PP, PI64, PI64, PI64,
+                                            PI64]),
+        ("tsvm_free", None, [P]),
+        ("tsvm_write_model", ctypes.c_int, [ctypes.c_char_p, I32, P, P, P, I64, I32, D, D, D, I32,
+                                            I32, I32, PI64, PI64]),
+        ("tsvm_read_model", ctypes.c_int, [ctypes.c_char_p, MV, ctypes.POINTER(I32),
+                                           ctypes.POINTER(I32)]),
+        ("tsvm_free_model", None, [MV]),
+    ]:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
     lib.tsvm_kernel_launches.restype = ctypes.c_int64
     lib.tsvm_kernel_launches.argtypes = [P]
     # test hooks (include/tensorsvm_testing.h)

@@ -147,51 +147,119 @@ def train(ctx, X: np.ndarray, y: np.ndarray, kernel: int = _lib.KERNEL_RBF, gamm
                  factor_info=_fields(finfo), ipm_stats=_fields(istats))
 
 
-def write_model(path: str, model: Model, X: np.ndarray, labels: np.ndarray, pos: int, neg: int):
-    """The reference's model text: LIBSVM rbf (T:384-406) or LIBLINEAR (T:340-349)."""
-    alpha, C = model.alpha, model.C
-    sv = np.nonzero(alpha > 1e-6)[0]
-    free = sv[alpha[sv] < C - 1e-6]
-    with open(path, "w") as f:
-        if model.kernel == _lib.KERNEL_RBF:
-            f.write("svm_type c_svc\nkernel_type rbf\n")
-            f.write("gamma %.7f\n" % model.gamma)
-            f.write("nr_class 2\ntotal_sv %d\n" % len(sv))
-            f.write("rho %f\n" % (-model.b))
-            f.write("label %d %d\n" % (pos, neg))
-            f.write("nr_sv %d %d\nSV\n" % (len(free), len(sv) - len(free)))
-            for j in sv:
-                parts = ["%7f " % (float(labels[j]) * float(alpha[j]))]
-                for c in np.nonzero(X[j])[0]:
-                    parts.append("%d:%7f " % (c + 1, float(X[j, c])))
-                f.write("".join(parts) + "\n")
-        else:
-            d = X.shape[1]
-            w = (alpha[sv] * labels[sv].astype(np.float64)) @ X[sv].astype(np.float64)
-            f.write("solver_type L2R_L1LOSS_SVC_DUAL\nnr_class 2\n")
-            f.write("label %d %d\nnr_feature %d\nbias %d\nw\n" % (pos, neg, d, 1))
-            for v in w:
-                f.write("%.16f \n" % v)
-            f.write("%.16f\n" % model.b)
+def write_model(path: str, model: Model, X: np.ndarray, labels: np.ndarray, pos: int, neg: int,
+                threads: int = 0):
+    """The reference's model text through tsvm_write_model: LIBSVM rbf (T:384-406) or LIBLINEAR
+    (T:340-349).  Returns (number of SVs, number of free SVs)."""
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    labels = np.ascontiguousarray(labels, dtype=np.float32)
+    alpha = np.ascontiguousarray(model.alpha, dtype=np.float64)
+    n, d = X.shape
+    nsv, nfree = ctypes.c_int64(), ctypes.c_int64()
+    st = _lib.load().tsvm_write_model(path.encode(), model.kernel, X.ctypes.data, labels.ctypes.data,
+                                      alpha.ctypes.data, n, d, float(model.C), float(model.gamma),
+                                      float(model.b), pos, neg, threads, ctypes.byref(nsv),
+                                      ctypes.byref(nfree))
+    _lib.check(st, "tsvm_write_model")
+    return nsv.value, nfree.value
 
 
-def read_libsvm(path: str):
-    """Dense float32 instances and labels, 1-based indices (tensorsvm-train.cu:1162-1278)."""
-    labels, rows, max_index, min_index = [], [], 0, 1
-    with open(path) as f:
-        for line in f:
-            toks = line.split()
-            if not toks:
-                continue
-            labels.append(float(toks[0]))
-            feats = [(int(t.split(":")[0]), float(t.split(":")[1])) for t in toks[1:]]
-            for i, _ in feats:
-                min_index = min(min_index, i)
-                max_index = max(max_index, i)
-            rows.append(feats)
-    nf = max_index - min_index + 1 if min_index == 0 else max_index
-    X = np.zeros((len(rows), nf), dtype=np.float32)
-    for r, feats in enumerate(rows):
-        for i, v in feats:
-            X[r, i - min_index] = v
-    return np.asarray(labels, dtype=np.float32), X
+def read_libsvm(path: str, scale256: bool = False, threads: int = 0):
+    """(labels float32, X float32 n x d dense) through tsvm_read_libsvm (tensorsvm-train.cu:
+    1162-1278 semantics, parallel parse).  A malformed line raises TsvmError with .line set."""
+    lib = _lib.load()
+    L, M = ctypes.c_void_p(), ctypes.c_void_p()
+    n, d, nnz, bad = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+    st = lib.tsvm_read_libsvm(path.encode(), int(scale256), threads, ctypes.byref(L),
+                              ctypes.byref(M), ctypes.byref(n), ctypes.byref(d), ctypes.byref(nnz),
+                              ctypes.byref(bad))
+    if st != _lib.OK:
+        err = _lib.TsvmError(st, f"tsvm_read_libsvm({path}) line {bad.value}")
+        err.line = bad.value
+        raise err
+    try:
+        labels = np.ctypeslib.as_array(ctypes.cast(L, ctypes.POINTER(ctypes.c_float)),
+                                       shape=(n.value,)).copy() if n.value else np.zeros(0, np.float32)
+        X = np.ctypeslib.as_array(ctypes.cast(M, ctypes.POINTER(ctypes.c_float)),
+                                  shape=(n.value, d.value)).copy() if n.value * d.value \
+            else np.zeros((n.value, d.value), np.float32)
+    finally:
+        lib.tsvm_free(L)
+        lib.tsvm_free(M)
+    return labels, X
+
+
+@dataclass
+class ModelFile:
+    kernel: int
+    pos: int
+    neg: int
+    rho: float
+    gamma: float
+    sv: np.ndarray          # RBF: nsv x d; LINEAR: w (d)
+    coef: np.ndarray        # RBF: nsv
+
+
+def read_model(path: str) -> ModelFile:
+    """A model file (either format tsvm_write_model writes) through tsvm_read_model."""
+    lib = _lib.load()
+    mv = _lib.ModelView()
+    pos, neg = ctypes.c_int32(), ctypes.c_int32()
+    _lib.check(lib.tsvm_read_model(path.encode(), ctypes.byref(mv), ctypes.byref(pos),
+                                   ctypes.byref(neg)), "tsvm_read_model")
+    try:
+        rows = mv.nsv if mv.kernel == _lib.KERNEL_RBF else 1
+        sv = np.ctypeslib.as_array(ctypes.cast(mv.sv, ctypes.POINTER(ctypes.c_float)),
+                                   shape=(rows, mv.d)).copy()
+        coef = (np.ctypeslib.as_array(ctypes.cast(mv.coef, ctypes.POINTER(ctypes.c_double)),
+                                      shape=(mv.nsv,)).copy()
+                if mv.kernel == _lib.KERNEL_RBF and mv.nsv else np.zeros(0))
+    finally:
+        lib.tsvm_free_model(ctypes.byref(mv))
+    return ModelFile(kernel=mv.kernel, pos=pos.value, neg=neg.value, rho=mv.rho, gamma=mv.gamma,
+                     sv=sv if mv.kernel == _lib.KERNEL_RBF else sv[0], coef=coef)
+
+
+def predict(ctx, model: ModelFile, X: np.ndarray) -> np.ndarray:
+    """Decision values (float64) of host rows X through tsvm_predict; rows and SVs are padded to
+    a common width."""
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    m, dx = X.shape
+    sv = np.atleast_2d(model.sv)
+    d = max(dx, sv.shape[1])
+    if dx < d:
+        X = np.ascontiguousarray(np.pad(X, ((0, 0), (0, d - dx))))
+    if sv.shape[1] < d:
+        sv = np.pad(sv, ((0, 0), (0, d - sv.shape[1])))
+    sv = np.ascontiguousarray(sv, dtype=np.float32)
+    coef = np.ascontiguousarray(model.coef, dtype=np.float64)
+    mv = _lib.ModelView(kernel=model.kernel, d=d, nsv=sv.shape[0] if model.kernel == _lib.KERNEL_RBF else 0,
+                        sv=sv.ctypes.data, coef=coef.ctypes.data if coef.size else None,
+                        rho=model.rho, gamma=model.gamma)
+    f = np.empty(m, dtype=np.float64)
+    _lib.check(ctx.lib.tsvm_predict(ctx.handle, ctypes.byref(mv), X.ctypes.data, m, f.ctypes.data),
+               "tsvm_predict")
+    return f
+
+
+def decision_values(ctx, kernel: int, sv, coef, rho: float, gamma: float, X):
+    """tsvm_decision_values on CUDA tensors (sv nsv x d or w, coef float64, X m x d)."""
+    import torch
+    m, d = X.shape
+    f = torch.empty(m, dtype=torch.float64, device=X.device)
+    mv = _lib.ModelView(kernel=kernel, d=d, nsv=sv.shape[0] if kernel == _lib.KERNEL_RBF else 0,
+                        sv=_ptr(sv), coef=_ptr(coef) if coef is not None else None, rho=float(rho),
+                        gamma=float(gamma))
+    _lib.check(ctx.lib.tsvm_decision_values(ctx.handle, ctypes.byref(mv), _ptr(X), m, _ptr(f)),
+               "tsvm_decision_values")
+    return f
+
+
+def kernel_residual(ctx, X, y, gamma: float, Z, k: int):
+    """(||K~||_F, ||K~ - Z Z^T||_F) in FP64 through tsvm_kernel_residual (CUDA tensors)."""
+    n, d = X.shape
+    a, b = ctypes.c_double(), ctypes.c_double()
+    _lib.check(ctx.lib.tsvm_kernel_residual(ctx.handle, _ptr(X), _ptr(y), n, d, float(gamma),
+                                            _ptr(Z), Z.shape[1], k, ctypes.byref(a),
+                                            ctypes.byref(b)), "tsvm_kernel_residual")
+    return a.value, b.value

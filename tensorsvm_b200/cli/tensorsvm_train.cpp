@@ -16,6 +16,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <chrono>
 #include <string>
 #include <vector>
@@ -51,7 +52,8 @@ void help_msg() {
          "-prec fp32|bf16|fp16 : contraction precision (overrides -tensorcore)\n"
          "-rel_gap tol : also stop at relative duality gap <= tol\n"
          "-scale256 : divide feature values by 256\n"
-         "-analysis : report ||K - Z Z'||_F / ||K||_F (not available in this build)\n"
+         "-analysis : report ||K||_F and ||K - Z Z'||_F (RBF, FP64 on the GPU)\n"
+         "-test file : accuracy of the trained model on a LIBSVM test file\n"
          "-q : quiet\n");
 }
 
@@ -102,140 +104,81 @@ bool parse(int argc, char **argv, Args &a) {
   return a.train != nullptr;
 }
 
-// Two-pass LIBSVM reader with the reference's index rules: dense row-major float, indices
-// shifted by the smallest index seen (1 for 1-based files), strictly increasing indices.
+// LIBSVM reader of the library (tsvm_read_libsvm: parallel parse, the reference's index rules)
+// with the reference's messages (tensorsvm-train.cu:1210-1211, 1236, 1245).
 bool libsvm_read(const char *path, bool scale256, std::vector<float> &labels,
                  std::vector<float> &inst, long &n, long &nf) {
-  FILE *f = fopen(path, "r");
-  if (!f) {
-    fprintf(stderr, "Can't open %s\n", path);
+  float *L = nullptr, *M = nullptr;
+  int64_t n64 = 0, d64 = 0, nnz = 0, bad = 0;
+  const tsvm_status st = tsvm_read_libsvm(path, scale256 ? 1 : 0, 0, &L, &M, &n64, &d64, &nnz,
+                                          &bad);
+  if (st != TSVM_OK) {
+    if (bad > 0) printf("Wrong input format at line %ld\n", (long)bad);
+    else fprintf(stderr, "Can't open %s\n", path);
     return false;
   }
-  std::vector<char> buf(1 << 20);
-  std::vector<std::vector<std::pair<int, float>>> rows;
-  long max_index = 0, min_index = 1, elements = 0, l = 0;
-  std::string line;
-  auto read_line = [&](std::string &out) -> bool {
-    out.clear();
-    while (fgets(buf.data(), (int)buf.size(), f)) {
-      out.append(buf.data());
-      if (!out.empty() && out.back() == '\n') return true;
-    }
-    return !out.empty();
-  };
-  while (read_line(line)) {
-    ++l;
-    char *s = &line[0];
-    char *save = nullptr;
-    char *label = strtok_r(s, " \t\n\r", &save);
-    if (!label) {
-      printf("Empty line at line %ld\n", l);
-      fclose(f);
-      return false;
-    }
-    char *end = nullptr;
-    const double lab = strtod(label, &end);
-    if (end == label || *end != '\0') {
-      printf("Wrong input format at line %ld\n", l);
-      fclose(f);
-      return false;
-    }
-    std::vector<std::pair<int, float>> feats;
-    int prev = -1;
-    while (true) {
-      char *idx = strtok_r(nullptr, ":", &save);
-      char *val = strtok_r(nullptr, " \t\n\r", &save);
-      if (!val) break;
-      errno = 0;
-      const long index = strtol(idx, &end, 10);
-      if (end == idx || errno != 0 || *end != '\0' || index <= prev) {
-        printf("Wrong input format at line %ld\n", l);
-        fclose(f);
-        return false;
-      }
-      prev = (int)index;
-      errno = 0;
-      float v = (float)strtod(val, &end);
-      if (end == val || errno != 0 || (*end != '\0' && !isspace((unsigned char)*end))) {
-        printf("Wrong input format at line %ld\n", l);
-        fclose(f);
-        return false;
-      }
-      if (scale256) v /= 256;
-      feats.emplace_back((int)index, v);
-      if (index < min_index) min_index = index;
-      if (index > max_index) max_index = index;
-      ++elements;
-    }
-    labels.push_back((float)lab);
-    rows.push_back(std::move(feats));
-  }
-  fclose(f);
-  n = (long)rows.size();
-  nf = min_index == 0 ? max_index + 1 : max_index;
-  inst.assign((size_t)n * nf, 0.f);
-  for (long i = 0; i < n; ++i)
-    for (auto &p : rows[i]) inst[(size_t)i * nf + (p.first - min_index)] = p.second;
-  printf("Dataset size %ld #features %ld nnz=%ld sparsity=%3f%%\n", n, nf, elements,
-         n && nf ? 100.0 * elements / ((double)n * nf) : 0.0);
+  n = (long)n64;
+  nf = (long)d64;
+  labels.assign(L, L + n);
+  inst.assign(M, M + (size_t)n * nf);
+  tsvm_free(L);
+  tsvm_free(M);
+  printf("Dataset size %ld #features %ld nnz=%ld sparsity=%3f%%\n", n, nf, (long)nnz,
+         n && nf ? 100.0 * nnz / ((double)n * nf) : 0.0);
   return true;
 }
 
-bool write_model(const char *path, const Args &a, double gamma, const std::vector<float> &X,
-                 const std::vector<float> &y, const std::vector<double> &alpha, long n, long d,
-                 double b, int pos, int neg) {
-  std::vector<long> sv, freesv;
-  for (long i = 0; i < n; ++i)
-    if (alpha[i] > 1e-6) {
-      sv.push_back(i);
-      if (alpha[i] < a.C - 1e-6) freesv.push_back(i);
-    }
-  printf("#BSV %zu, #SV %zu\n", freesv.size(), sv.size());
-  FILE *f = fopen(path, "w");
-  if (!f) {
-    fprintf(stderr, "Can't open %s\n", path);
+// Decision values of the in-memory model on a test file, the accuracy line of the reference's
+// (disabled) predict (tensorsvm-train.cu:223, 267).
+bool run_test(tsvm_context *ctx, const Args &a, double gamma, const std::vector<float> &X,
+              const std::vector<float> &y, const std::vector<double> &alpha, long n, long d,
+              double b, int pos, int neg) {
+  std::vector<float> tl, tx;
+  long tn = 0, td = 0;
+  printf("testfilepath=%s\n", a.test);
+  if (!libsvm_read(a.test, a.scale256, tl, tx, tn, td)) return false;
+  if (td != d) printf("training #feature(%ld) != testing feature (%ld)\n", d, td);
+  const long dd = std::max(d, td);
+  std::vector<float> T((size_t)tn * dd, 0.f);
+  for (long i = 0; i < tn; ++i)
+    for (long c = 0; c < td; ++c) T[(size_t)i * dd + c] = tx[(size_t)i * td + c];
+  std::vector<float> sv;
+  std::vector<double> coef;
+  tsvm_model_view m{};
+  m.d = (int32_t)dd;
+  m.rho = -b;
+  if (a.T == 0) {
+    sv.assign(dd, 0.f);
+    std::vector<double> w(d, 0.0);
+    for (long j = 0; j < n; ++j)
+      if (alpha[j] > 1e-6)
+        for (long c = 0; c < d; ++c) w[c] += alpha[j] * y[j] * X[(size_t)j * d + c];
+    for (long c = 0; c < d; ++c) sv[c] = (float)w[c];
+    m.kernel = TSVM_KERNEL_LINEAR;
+  } else {
+    for (long j = 0; j < n; ++j)
+      if (alpha[j] > 1e-6) {
+        coef.push_back(y[j] * alpha[j]);
+        for (long c = 0; c < dd; ++c) sv.push_back(c < d ? X[(size_t)j * d + c] : 0.f);
+      }
+    m.kernel = TSVM_KERNEL_RBF;
+    m.nsv = (int64_t)coef.size();
+    m.coef = coef.data();
+    m.gamma = gamma;
+  }
+  m.sv = sv.data();
+  std::vector<double> f(tn);
+  const tsvm_status st = tsvm_predict(ctx, &m, T.data(), tn, f.data());
+  if (st != TSVM_OK) {
+    fprintf(stderr, "tensorsvm: %s\n", tsvm_status_string(st));
     return false;
   }
-  if (a.T == 0) {
-    std::vector<double> w(d, 0.0);
-    for (long j : sv)
-      for (long c = 0; c < d; ++c) w[c] += alpha[j] * y[j] * X[(size_t)j * d + c];
-    fprintf(f, "solver_type L2R_L1LOSS_SVC_DUAL\n");
-    fprintf(f, "nr_class 2\n");
-    fprintf(f, "label %d %d\n", pos, neg);
-    fprintf(f, "nr_feature %ld\n", d);
-    fprintf(f, "bias %d\n", 1);
-    fprintf(f, "w\n");
-    for (long c = 0; c < d; ++c) fprintf(f, "%.16f \n", w[c]);
-    fprintf(f, "%.16f\n", b);
-  } else {
-    fprintf(f, "svm_type c_svc\n");
-    fprintf(f, "kernel_type rbf\n");
-    fprintf(f, "gamma %.7f\n", gamma);
-    fprintf(f, "nr_class 2\n");
-    fprintf(f, "total_sv %zu\n", sv.size());
-    fprintf(f, "rho %f\n", -b);
-    fprintf(f, "label %d %d\n", pos, neg);
-    fprintf(f, "nr_sv %zu %zu\n", freesv.size(), sv.size() - freesv.size());
-    fprintf(f, "SV\n");
-    std::string line;
-    char tmp[64];
-    for (long j : sv) {
-      line.clear();
-      snprintf(tmp, sizeof tmp, "%7f ", y[j] * alpha[j]);
-      line += tmp;
-      for (long c = 0; c < d; ++c) {
-        const float v = X[(size_t)j * d + c];
-        if (v > 0 || v < 0) {
-          snprintf(tmp, sizeof tmp, "%ld:%7f ", c + 1, v);
-          line += tmp;
-        }
-      }
-      line += '\n';
-      fputs(line.c_str(), f);
-    }
+  long yes = 0;
+  for (long i = 0; i < tn; ++i) {
+    const double t = (int)tl[i] == pos ? 1.0 : (int)tl[i] == neg ? -1.0 : 0.0;
+    if (f[i] * t > 0) ++yes;
   }
-  fclose(f);
+  printf("prediction accuracy %.3f (%ld/%ld)\n", tn ? 1.0 * yes / tn : 0.0, yes, tn);
   return true;
 }
 
@@ -286,8 +229,6 @@ int main(int argc, char **argv) {
     printf("unimplemented pgd\n");
     return 1;
   }
-  if (a.analysis) printf("-analysis is not available in this build; ignored\n");
-  if (a.test) printf("-test not implemented\n");
   double gamma = a.g;
   if (a.T == 2 && !(gamma > 0)) gamma = 1.0 / (double)d;
   int precision = a.precision >= 0 ? a.precision : (a.tensorcore ? TSVM_PREC_FP16 : TSVM_PREC_FP32);
@@ -331,9 +272,33 @@ int main(int argc, char **argv) {
   printf("\033[95mMPC elapsed time = %.4f seconds\033[39m (%d iterations, %s)\n",
          istats.ms_total / 1e3, istats.iters, tsvm_status_string(st));
   printf("train elapsed time = %.4f seconds\n", secs);
+  if (a.analysis && a.T == 2) {
+    // ||K~||_F and ||K~ - Z Z^T||_F of this factor (the reference's -analysis, T:2328-2360)
+    const auto ta = std::chrono::steady_clock::now();
+    double kn = 0, kr = 0;
+    st = tsvm_train_residual(ctx, &kn, &kr);
+    if (st != TSVM_OK) {
+      fprintf(stderr, "tensorsvm: %s\n", tsvm_status_string(st));
+      tsvm_destroy(ctx);
+      return 1;
+    }
+    printf("fnorm(K)=%.3e fnorm(K-U*U=%.3e')\n", kn, kr);
+    printf("rbf_fnorm_res elapsed time = %.4f seconds\n",
+           std::chrono::duration<double>(std::chrono::steady_clock::now() - ta).count());
+  }
   printf("Writemodel ");
-  const bool ok = write_model(model.c_str(), a, gamma, X, labels, alpha, n, d, b, pos, neg);
+  const auto tw = std::chrono::steady_clock::now();
+  int64_t nsv = 0, nfree = 0;
+  st = tsvm_write_model(model.c_str(), a.T == 0 ? TSVM_KERNEL_LINEAR : TSVM_KERNEL_RBF, X.data(),
+                        labels.data(), alpha.data(), n, (int32_t)d, a.C, gamma, b, pos, neg, 0,
+                        &nsv, &nfree);
+  printf("#BSV %lld, #SV %lld\n", (long long)nfree, (long long)nsv);
+  if (st != TSVM_OK) fprintf(stderr, "Can't write %s\n", model.c_str());
+  printf("elapsed time = %.4f seconds\n",
+         std::chrono::duration<double>(std::chrono::steady_clock::now() - tw).count());
   printf("approx mean b=%.6e\n", b);
+  bool ok = st == TSVM_OK;
+  if (ok && a.test) ok = run_test(ctx, a, gamma, X, labels, alpha, n, d, b, pos, neg);
   tsvm_destroy(ctx);
   return ok ? 0 : 1;
 }

@@ -227,6 +227,7 @@ tsvm_status tsvm_train(tsvm_context *ctx, const float *X, const float *y, int64_
   o.kernel = kernel;
   float *dX = nullptr, *dZ = nullptr;
   double *dalpha = nullptr;
+  ctx->last_train.valid = false;
   TSVM_TRY(scratch_t(ctx, SLOT_DEV_IN, (size_t)n * d + (size_t)n + 64, &dX));
   float *dy = dX + (size_t)n * d;
   TSVM_CUDA(cudaMemcpyAsync(dX, X, sizeof(float) * n * d, cudaMemcpyHostToDevice, ctx->stream));
@@ -244,6 +245,12 @@ tsvm_status tsvm_train(tsvm_context *ctx, const float *X, const float *y, int64_
       return st;
     double b = 0.0;
     TSVM_TRY(bias_rbf(ctx, dZ, kp, dy, dalpha, n, k, C, &b, nullptr, nullptr, nullptr));
+    ctx->last_train.valid = true;
+    ctx->last_train.n = n;
+    ctx->last_train.d = d;
+    ctx->last_train.k = k;
+    ctx->last_train.ldz = kp;
+    ctx->last_train.gamma = gamma;
     if (b_out) *b_out = b;
     TSVM_CUDA(cudaMemcpyAsync(alpha_out, dalpha, sizeof(double) * n, cudaMemcpyDeviceToHost,
                               ctx->stream));
@@ -262,6 +269,85 @@ tsvm_status tsvm_train(tsvm_context *ctx, const float *X, const float *y, int64_
     if (b_out) linear_bias_host(X, y, alpha_out, n, d, C, b_out);
   }
   return st;
+}
+
+tsvm_status tsvm_decision_values(tsvm_context *ctx, const tsvm_model_view *model, const float *X,
+                                 int64_t m, double *f) {
+  if (!ctx || !model || !X || !f || m < 0 || model->d < 1 || !model->sv)
+    return TSVM_ERR_INVALID_ARGUMENT;
+  if (model->kernel != TSVM_KERNEL_RBF && model->kernel != TSVM_KERNEL_LINEAR)
+    return TSVM_ERR_UNSUPPORTED;
+  if (model->kernel == TSVM_KERNEL_RBF && (model->nsv < 0 || (model->nsv > 0 && !model->coef)))
+    return TSVM_ERR_INVALID_ARGUMENT;
+  if (m == 0) return TSVM_OK;
+  TSVM_CUDA(cudaSetDevice(ctx->device));
+  TSVM_TRY(decision_values(ctx, model, X, m, f));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSVM_OK;
+}
+
+tsvm_status tsvm_predict(tsvm_context *ctx, const tsvm_model_view *model, const float *X,
+                         int64_t m, double *f) {
+  if (!ctx || !model || !X || !f || m < 0 || model->d < 1 || !model->sv)
+    return TSVM_ERR_INVALID_ARGUMENT;
+  if (model->kernel != TSVM_KERNEL_RBF && model->kernel != TSVM_KERNEL_LINEAR)
+    return TSVM_ERR_UNSUPPORTED;
+  const bool rbf = model->kernel == TSVM_KERNEL_RBF;
+  if (rbf && (model->nsv < 0 || (model->nsv > 0 && !model->coef))) return TSVM_ERR_INVALID_ARGUMENT;
+  if (m == 0) return TSVM_OK;
+  TSVM_CUDA(cudaSetDevice(ctx->device));
+  const int64_t d = model->d;
+  const int64_t nsv = rbf ? model->nsv : 0;
+  const size_t sv_floats = rbf ? (size_t)(nsv * d) : (size_t)d;
+  // layout: coef (nsv doubles) | sv floats | X floats, each 256-byte aligned
+  const size_t o_sv = round_up((int64_t)nsv * 8, 256);
+  const size_t o_x = o_sv + round_up((int64_t)sv_floats * 4, 256);
+  const size_t bytes = o_x + (size_t)m * d * 4 + 256;
+  uint8_t *buf = nullptr;
+  double *df = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_PRED_IN, bytes, &buf));
+  TSVM_TRY(scratch_t(ctx, SLOT_PRED_OUT, (size_t)m, &df));
+  double *dcoef = reinterpret_cast<double *>(buf);
+  float *dsv = reinterpret_cast<float *>(buf + o_sv);
+  float *dX = reinterpret_cast<float *>(buf + o_x);
+  if (nsv > 0)
+    TSVM_CUDA(cudaMemcpyAsync(dcoef, model->coef, sizeof(double) * nsv, cudaMemcpyHostToDevice,
+                              ctx->stream));
+  if (sv_floats > 0)
+    TSVM_CUDA(cudaMemcpyAsync(dsv, model->sv, sizeof(float) * sv_floats, cudaMemcpyHostToDevice,
+                              ctx->stream));
+  TSVM_CUDA(cudaMemcpyAsync(dX, X, sizeof(float) * m * d, cudaMemcpyHostToDevice, ctx->stream));
+  tsvm_model_view dv = *model;
+  dv.sv = dsv;
+  dv.coef = rbf ? dcoef : nullptr;
+  dv.nsv = nsv;
+  TSVM_TRY(decision_values(ctx, &dv, dX, m, df));
+  TSVM_CUDA(cudaMemcpyAsync(f, df, sizeof(double) * m, cudaMemcpyDeviceToHost, ctx->stream));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSVM_OK;
+}
+
+tsvm_status tsvm_kernel_residual(tsvm_context *ctx, const float *X, const float *y, int64_t n,
+                                 int32_t d, double gamma, const float *Z, int32_t ldz, int32_t k,
+                                 double *fnorm, double *fnorm_res) {
+  if (!ctx || !X || !y || !Z || n < 1 || d < 1 || k < 1 || ldz < k || !(gamma > 0))
+    return TSVM_ERR_INVALID_ARGUMENT;
+  TSVM_CUDA(cudaSetDevice(ctx->device));
+  double out[2];
+  TSVM_TRY(kernel_residual(ctx, X, y, n, d, gamma, Z, ldz, k, out));
+  if (fnorm) *fnorm = out[0];
+  if (fnorm_res) *fnorm_res = out[1];
+  return TSVM_OK;
+}
+
+tsvm_status tsvm_train_residual(tsvm_context *ctx, double *fnorm, double *fnorm_res) {
+  if (!ctx || !ctx->last_train.valid) return TSVM_ERR_INVALID_ARGUMENT;
+  const auto &t = ctx->last_train;
+  const float *dX = static_cast<const float *>(ctx->buf[SLOT_DEV_IN]);
+  const float *dZ = static_cast<const float *>(ctx->buf[SLOT_DEV_Z]);
+  if (!dX || !dZ) return TSVM_ERR_INVALID_ARGUMENT;
+  return tsvm_kernel_residual(ctx, dX, dX + (size_t)t.n * t.d, t.n, t.d, t.gamma, dZ, t.ldz, t.k,
+                              fnorm, fnorm_res);
 }
 
 }  // extern "C"

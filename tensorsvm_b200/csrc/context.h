@@ -47,6 +47,8 @@ enum Slot : int {
   SLOT_DEV_IN,        // tsvm_train: device copies of host inputs
   SLOT_DEV_Z,         // tsvm_train: factor Z
   SLOT_DEV_OUT,       // tsvm_train: device alpha
+  SLOT_PRED_IN,       // tsvm_predict: device copies of the model and the rows
+  SLOT_PRED_OUT,      // tsvm_predict: decision values
   SLOT_COUNT_
 };
 
@@ -65,6 +67,13 @@ struct tsvm_context {
   int jump_levels = 0;
   // pinned host staging for small device->host reads
   double *host_scalars = nullptr;
+  // the last RBF tsvm_train (its X, y in SLOT_DEV_IN and Z in SLOT_DEV_Z), for -analysis
+  struct {
+    bool valid = false;
+    int64_t n = 0;
+    int d = 0, k = 0, ldz = 0;
+    double gamma = 0.0;
+  } last_train;
 };
 
 namespace tsvm {

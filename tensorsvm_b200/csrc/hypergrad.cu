@@ -287,6 +287,7 @@ extern "C" tsvm_status tsvm_hypergrad(tsvm_context *ctx, const float *X, const f
   const int kp = (int)round_up(k, 64);
   // recompute the factorisation, keeping Omega, R and W
   float *Zf = nullptr, *Om = nullptr;
+  ctx->last_train.valid = false;   // the factor below overwrites tsvm_train's Z
   TSVM_TRY(scratch_t(ctx, SLOT_DEV_Z, (size_t)n * kp, &Zf));
   TSVM_TRY(scratch_t(ctx, SLOT_HG_OMEGA, (size_t)n * kp, &Om));
   double *Rbuf = nullptr;

@@ -141,7 +141,7 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
 // ---------------------------------------------------------------------------------------
 constexpr int kSBufs = 4;
 
-template <bool BF16, int NPOLY, int KG>
+template <bool BF16, int NPOLY, int KG, bool SHIFT>
 __global__ void __launch_bounds__(kThreadsTC, 1)
 kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
                     const __grid_constant__ CUtensorMap map_xb,
@@ -324,7 +324,10 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
     const int row = q * 32 + lane;        // row of the 128-row block (TMEM lane)
     const uint32_t lane_off = (uint32_t)(q * 32) << 16;
     const int half = kpw / 2;
-    const float shift = inv_scale[1];   // the kernel's sampled mean, taken off every P entry
+    // SHIFT: the kernel's sampled mean, taken off every P entry.  A separate instantiation: the
+    // subtraction alone, even of zero, made the pass at n = 1M, d = 18 run at 0.95 GHz instead
+    // of 1.33 GHz under the power cap (the same cycles per tile, more energy per cycle).
+    const float shift = SHIFT ? inv_scale[1] : 0.f;
     bool ok = true;
     for (int rb = blockIdx.x, r = 0; ok && rb < nrb; rb += G, ++r) {
       const uint32_t T0 = (uint32_t)r * (uint32_t)ntiles;   // flat index of the first J block
@@ -339,15 +342,26 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
         tmem_ld32(tb + 32, s1);
         tmem_wait_ld();
         uint32_t pk[32];
+        if constexpr (SHIFT) {
 #pragma unroll
-        for (int c = 0; c < 16; ++c)
-          pk[c] = pack2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c]), 2 * c) - shift,
-                              exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c + 1]), 2 * c + 1) - shift);
+          for (int c = 0; c < 16; ++c)
+            pk[c] = pack2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c]), 2 * c) - shift,
+                                exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c + 1]), 2 * c + 1) - shift);
 #pragma unroll
-        for (int c = 0; c < 16; ++c)
-          pk[16 + c] =
-              pack2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c]), 2 * c) - shift,
-                          exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c + 1]), 2 * c + 1) - shift);
+          for (int c = 0; c < 16; ++c)
+            pk[16 + c] =
+                pack2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c]), 2 * c) - shift,
+                            exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c + 1]), 2 * c + 1) - shift);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 16; ++c)
+            pk[c] = pack2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c]), 2 * c),
+                                exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c + 1]), 2 * c + 1));
+#pragma unroll
+          for (int c = 0; c < 16; ++c)
+            pk[16 + c] = pack2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c]), 2 * c),
+                                     exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c + 1]), 2 * c + 1));
+        }
         tmem_st32(tb, pk);   // P over the first 32 columns of the buffer (S is no longer needed)
         tmem_wait_st();
         tc_fence_before();
@@ -368,7 +382,7 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
           const float4 *cs = reinterpret_cast<const float4 *>(ccol + c0 + cc);
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
-            const float4 a = cs[j];
+            const float4 a = SHIFT ? cs[j] : make_float4(0.f, 0.f, 0.f, 0.f);
             dst[j] = make_float4((__uint_as_float(v[4 * j]) + a.x) * sc,
                                  (__uint_as_float(v[4 * j + 1]) + a.y) * sc,
                                  (__uint_as_float(v[4 * j + 2]) + a.z) * sc,
@@ -523,20 +537,21 @@ prep_at(const float *A, const float *__restrict__ y, int64_t n, int64_t n_pad, i
   }
 }
 
-// Mean of the RBF kernel over the m x m pairs of m rows spread evenly over the data (rows
-// i n / m): the constant taken off every kernel entry before it is rounded to 16 bits.  For a
-// flat kernel (entries in [0.75, 1], say) the 16-bit rounding error then scales with the
-// entries' spread about the mean rather than with the entries, and the weak eigen-directions
-// of the kernel stay above it.  Block i sums row i; part[i] (fixed order).
+// Mean and second moment of the RBF kernel over the m x m pairs of m rows spread evenly over the
+// data (rows i n / m), for the constant taken off every kernel entry before it is rounded to
+// 16 bits.  For a flat kernel (entries in [0.75, 1], say) the rounding error then scales with
+// the entries' spread about the mean rather than with the entries, and the weak
+// eigen-directions of the kernel stay above it.  Block i sums row i: part[2 i], part[2 i + 1]
+// (fixed order).
 __global__ void __launch_bounds__(256)
 kernel_mean_rows(const float *__restrict__ Xc, int64_t n, int d, int m, float gamma,
                  double *__restrict__ part) {
   __shared__ float xi[kMaxKG];
-  __shared__ double sh[8];
+  __shared__ double sh[16];
   const int64_t ri = (int64_t)blockIdx.x * n / m;
   for (int c = threadIdx.x; c < d; c += blockDim.x) xi[c] = Xc[ri * d + c];
   __syncthreads();
-  double acc = 0.0;
+  double acc = 0.0, acc2 = 0.0;
   for (int j = threadIdx.x; j < m; j += blockDim.x) {
     const int64_t rj = (int64_t)j * n / m;
     float d2 = 0.f;
@@ -544,19 +559,39 @@ kernel_mean_rows(const float *__restrict__ Xc, int64_t n, int d, int m, float ga
       const float t = xi[c] - Xc[rj * d + c];
       d2 = fmaf(t, t, d2);
     }
-    acc += (double)expf(-gamma * d2);
+    const double e = (double)expf(-gamma * d2);
+    acc += e;
+    acc2 += e * e;
   }
-  double v[1] = {acc};
-  block_sum<1>(v, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+  double v[2] = {acc, acc2};
+  block_sum<2>(v, sh);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = v[0];
+    part[2 * blockIdx.x + 1] = v[1];
+  }
 }
 
-// scale[2] = shift = the mean over the m partial row sums; ccol[c] = shift * sum_x cpart[x][c].
+// Shift only where it pays: the rounding error's scale drops from rms(P) to std(P), a factor
+// sqrt(E[P^2] / var P).  Below 4 (a variance ratio of 16; the two-Gaussian and tanh-teacher
+// kernels at gamma 0.03-0.05 sit at 4-6.5) the gain is small, and the subtraction in the exp
+// warps costs about a quarter of the pass when the Gram product is short (K = 64: the pass at
+// n = 1M, d = 18 ran at 0.95 GHz instead of 1.33 GHz under the power cap, in the same cycles).
+// Flat kernels (d = 54 one-hot at gamma 0.02: ratio ~1900; gamma <= 2^-7 at d = 28: >= 76) take
+// it; there the K = 192 Gram product hides it.
+constexpr double kShiftMinRatio = 16.0;
+
+// scale[2] = shift (the sampled mean, or 0 when the kernel is not flat enough to need it).
 __global__ void kernel_mean_finish(const double *__restrict__ part, int m, float *scale) {
   if (threadIdx.x != 0) return;
-  double t = 0.0;
-  for (int i = 0; i < m; ++i) t += part[i];
-  scale[2] = (float)(t / ((double)m * m));
+  double t = 0.0, t2 = 0.0;
+  for (int i = 0; i < m; ++i) {
+    t += part[2 * i];
+    t2 += part[2 * i + 1];
+  }
+  const double mm = (double)m * m;
+  const double mean = t / mm, second = t2 / mm;
+  const double var = second - mean * mean;
+  scale[2] = second >= kShiftMinRatio * var ? (float)mean : 0.f;
 }
 
 __global__ void column_shift(const double *__restrict__ cpart, int nparts, int kp,
@@ -586,19 +621,24 @@ int poly_split() {
   return v;
 }
 
-TcKernel select_kernel(bool bf16, int npoly, int KG) {
-  if (KG == 128) return bf16 ? kermatmul_tc_kernel<true, 0, 128> : kermatmul_tc_kernel<false, 0, 128>;
-  if (KG == 192) return bf16 ? kermatmul_tc_kernel<true, 0, 192> : kermatmul_tc_kernel<false, 0, 192>;
+TcKernel select_kernel(bool bf16, int npoly, int KG, bool shift) {
+  if (shift) {   // flat kernels: MUFU exps only
+    if (KG == 128) return bf16 ? kermatmul_tc_kernel<true, 0, 128, true> : kermatmul_tc_kernel<false, 0, 128, true>;
+    if (KG == 192) return bf16 ? kermatmul_tc_kernel<true, 0, 192, true> : kermatmul_tc_kernel<false, 0, 192, true>;
+    return bf16 ? kermatmul_tc_kernel<true, 0, 64, true> : kermatmul_tc_kernel<false, 0, 64, true>;
+  }
+  if (KG == 128) return bf16 ? kermatmul_tc_kernel<true, 0, 128, false> : kermatmul_tc_kernel<false, 0, 128, false>;
+  if (KG == 192) return bf16 ? kermatmul_tc_kernel<true, 0, 192, false> : kermatmul_tc_kernel<false, 0, 192, false>;
 #define TSVM_SEL(P) \
   if (npoly == P) \
-    return bf16 ? kermatmul_tc_kernel<true, P, 64> : kermatmul_tc_kernel<false, P, 64>;
+    return bf16 ? kermatmul_tc_kernel<true, P, 64, false> : kermatmul_tc_kernel<false, P, 64, false>;
   TSVM_SEL(0)
   TSVM_SEL(2)
   TSVM_SEL(4)
   TSVM_SEL(6)
   TSVM_SEL(8)
 #undef TSVM_SEL
-  return bf16 ? kermatmul_tc_kernel<true, 4, 64> : kermatmul_tc_kernel<false, 4, 64>;
+  return bf16 ? kermatmul_tc_kernel<true, 4, 64, false> : kermatmul_tc_kernel<false, 4, 64, false>;
 }
 
 // Gram K for d features: 3 d split products + 6 norm terms, rounded up to a 64-wide chunk.
@@ -634,11 +674,11 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
   uint16_t *AT = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_OPA, (size_t)kp * n_pad, &AT));
   // SLOT_MISC: sum-of-squares partials [nb] | scale: s, 1/s, shift, - (4 floats) | err |
-  // kernel-mean row sums [m] | column-sum partials [rg][kp] | ccol [kp floats]
+  // kernel-moment row sums [2 m] | column-sum partials [rg][kp] | ccol [kp floats]
   const int nb = ctx->num_sms * 2;
   const int m = n < 1024 ? (int)n : 1024;
   const int rg = (int)(n_pad / 32 < (int64_t)nb ? n_pad / 32 : nb);
-  const size_t o_samp = (size_t)nb + 8, o_cpart = o_samp + 1024;
+  const size_t o_samp = (size_t)nb + 8, o_cpart = o_samp + 2048;
   const size_t o_ccol = o_cpart + (size_t)rg * kp;
   double *part = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_MISC, o_ccol + (size_t)kp / 2 + 16, &part));
@@ -658,6 +698,10 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
   TSVM_LAUNCHED(ctx);
   kernel_mean_finish<<<1, 32, 0, ctx->stream>>>(samp, m, scale);
   TSVM_LAUNCHED(ctx);
+  float hshift = 0.f;   // picks the kernel instantiation
+  TSVM_CUDA(cudaMemcpyAsync(&hshift, scale + 2, sizeof(float), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
   const dim3 tgrid((unsigned)rg, (unsigned)ceil_div(kp, 32));
   if (bf16)
     prep_at<__nv_bfloat16><<<tgrid, dim3(32, 8), 0, ctx->stream>>>(
@@ -686,7 +730,7 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
                   kBJ, (uint64_t)ntiles * kp, kBJ, kpw))
       return TSVM_ERR_CUDA;
     const size_t smem = tc_smem(KG, kpw);
-    auto kern = select_kernel(bf16, poly_split(), KG);
+    auto kern = select_kernel(bf16, poly_split(), KG, hshift != 0.f);
     TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<grid, kThreadsTC, smem, ctx->stream>>>(mxa, mxb, mat, y, scale + 1, ccol, n, nrb,
                                                   ntiles, kp, c0, kpw, W, kp, err);

@@ -149,4 +149,12 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
                        double gamma, int k, int precision, int sketch, const float *Q_user,
                        float *Z, int ldz, tsvm_factor_info *info, FactorKeep *keep = nullptr);
 
+// ---- predict.cu ---------------------------------------------------------------------------
+// Decision values of m rows under a model (device arrays); asynchronous on ctx->stream.
+tsvm_status decision_values(tsvm_context *ctx, const tsvm_model_view *mv, const float *X,
+                            int64_t m, double *f);
+// out2 (host): ||K~||_F, ||K~ - Z Z^T||_F in FP64; synchronises.
+tsvm_status kernel_residual(tsvm_context *ctx, const float *X, const float *y, int64_t n, int d,
+                            double gamma, const float *Z, int64_t ldz, int k, double *out2);
+
 }  // namespace tsvm

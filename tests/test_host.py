@@ -98,7 +98,10 @@ def test_model_writer_matches_reference_format(tmp_path):
     assert path.read_text() == ref_text
     lin = api.Model(kernel=_lib.KERNEL_LINEAR, alpha=alpha, b=0.5, C=32.0, gamma=0.0, status=0)
     api.write_model(str(path), lin, X, y, 1, -1)
-    w, _ = (alpha[alpha > 1e-6] * y[alpha > 1e-6]) @ X[alpha > 1e-6].astype(np.float64), 0
+    # w summed over the SVs in index order, as writemodel's loop (T:330-335) does
+    w = np.zeros(X.shape[1])
+    for j in np.nonzero(alpha > 1e-6)[0]:
+        w += alpha[j] * float(y[j]) * X[j].astype(np.float64)
     assert path.read_text() == orc.format_model_linear(w, 0.5, X.shape[1], 1, -1)
 
 
