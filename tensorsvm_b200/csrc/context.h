@@ -44,6 +44,8 @@ enum Slot : int {
   SLOT_B_PART,        // batched IPM: per-unit streaming partial sums
   SLOT_HG_OMEGA,      // hypergradient: copy of the factor's sketch
   SLOT_HG_R,          // hypergradient: combined CholeskyQR factor and k-vectors
+  SLOT_HG_KPART,      // hypergradient: per-split partial kernel-vector products
+  SLOT_HG_W,          // hypergradient: the factor's orthonormal basis before rounding
   SLOT_DEV_IN,        // tsvm_train: device copies of host inputs
   SLOT_DEV_Z,         // tsvm_train: factor Z
   SLOT_DEV_OUT,       // tsvm_train: device alpha

@@ -179,7 +179,9 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
   TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, Q, kp, W, precision, &km1));
   TSVM_CUDA(cudaEventRecord(ev[2], ctx->stream));
   TSVM_TRY(orthonormalise(ctx, W, n, k, kp, keep ? keep->R : nullptr));
-  if (keep) keep->W = W;
+  if (keep)
+    TSVM_CUDA(cudaMemcpyAsync(keep->W, W, sizeof(float) * n * kp, cudaMemcpyDeviceToDevice,
+                              ctx->stream));
   TSVM_CUDA(cudaEventRecord(ev[3], ctx->stream));
   // the second pass rounds the orthonormal basis W to the tensor-core operand type in place:
   // C = W^T (K W) and Z = W V diag(sqrt w) then use the W the tensor cores contracted, so the

@@ -36,81 +36,160 @@
 namespace tsvm {
 namespace {
 
-constexpr int kKP = 256;   // threads (= rows of A) per block
-constexpr int kKT = 64;    // columns (rows of B) staged per tile
+constexpr int kKP = 256;   // threads per block
+constexpr int kKT = 64;    // rows of B staged per tile
 constexpr int kKMaxD = 64;
 
 // out[i][c] = sum_j w_ij exp(-gamma ||a_i - b_j||^2) U[j][c], w_ij = 1 or -||a_i - b_j||^2
-// (DERIV), for NU columns of U (FP64, nb x NU) and out (FP64, na x NU).
-template <int NU, bool DERIV>
+// (DERIV), for NU columns of U (FP64, nb x nu_total) and out (FP64, na x nu_total).  Each thread
+// keeps R rows of A in registers (rows blockIdx * 256 R + threadIdx + 256 r); a tile of 64 rows
+// of B (with their squared norms) and of U sits in shared memory and is read as broadcasts, four
+// features per load.  ||a - b||^2 = ||a||^2 + ||b||^2 - 2 a.b in FP32 (clamped at 0: the
+// relative error of the kernel value stays ~1e-7 gamma ||a||^2), each tile's 64 terms summed in
+// FP32, the tiles in FP64.  Block (x, y) sums the B rows [y jc, (y + 1) jc): with
+// gridDim.y > 1 its sums go to out + y * na * nu_total and kprod_reduce adds the splits in order.
+template <int DC, int R, int NU, bool DERIV>
 __global__ void __launch_bounds__(kKP)
 kprod_kernel(const float *__restrict__ A, int64_t na, const float *__restrict__ B, int64_t nb,
              int d, float gl2 /* gamma log2 e */, const double *__restrict__ U, int nu_total,
-             int c0, double *__restrict__ out) {
-  __shared__ float Bs[kKT][kKMaxD + 1];
+             int c0, int64_t jc, double *__restrict__ out) {
+  __shared__ __align__(16) float Bs[kKT][DC];
+  __shared__ float Bn[kKT];
   __shared__ float Us[kKT][NU];
-  const int64_t i = (int64_t)blockIdx.x * kKP + threadIdx.x;
-  float a[kKMaxD];
+  float a[R][DC], an[R];
 #pragma unroll
-  for (int c = 0; c < kKMaxD; ++c) a[c] = (i < na && c < d) ? A[i * d + c] : 0.f;
-  double acc[NU];
+  for (int r = 0; r < R; ++r) {
+    const int64_t i = (int64_t)blockIdx.x * kKP * R + threadIdx.x + kKP * r;
+    an[r] = 0.f;
 #pragma unroll
-  for (int u = 0; u < NU; ++u) acc[u] = 0.0;
-  for (int64_t j0 = 0; j0 < nb; j0 += kKT) {
+    for (int c = 0; c < DC; ++c) {
+      a[r][c] = (i < na && c < d) ? A[i * d + c] : 0.f;
+      an[r] = fmaf(a[r][c], a[r][c], an[r]);
+    }
+  }
+  double acc[R][NU];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int u = 0; u < NU; ++u) acc[r][u] = 0.0;
+  const int64_t jbeg = (int64_t)blockIdx.y * jc;
+  const int64_t jend = jbeg + jc < nb ? jbeg + jc : nb;
+  out += (int64_t)blockIdx.y * na * nu_total;
+  for (int64_t j0 = jbeg; j0 < jend; j0 += kKT) {
     __syncthreads();
-    for (int e = threadIdx.x; e < kKT * kKMaxD; e += kKP) {
-      const int r = e / kKMaxD, c = e % kKMaxD;
+    for (int e = threadIdx.x; e < kKT * DC; e += kKP) {
+      const int r = e / DC, c = e % DC;
       const int64_t j = j0 + r;
-      Bs[r][c] = (j < nb && c < d) ? B[j * d + c] : 0.f;
+      Bs[r][c] = (j < jend && c < d) ? B[j * d + c] : 0.f;
     }
     for (int e = threadIdx.x; e < kKT * NU; e += kKP) {
       const int r = e / NU, u = e % NU;
       const int64_t j = j0 + r;
-      Us[r][u] = (j < nb && c0 + u < nu_total) ? (float)U[j * nu_total + c0 + u] : 0.f;
+      Us[r][u] = (j < jend && c0 + u < nu_total) ? (float)U[j * nu_total + c0 + u] : 0.f;
     }
     __syncthreads();
-    float part[NU];
+    if (threadIdx.x < kKT) {
+      float t = 0.f;
 #pragma unroll
-    for (int u = 0; u < NU; ++u) part[u] = 0.f;
-    const int jn = (int)(nb - j0 < kKT ? nb - j0 : kKT);
-    for (int r = 0; r < jn; ++r) {
-      float dist = 0.f;
+      for (int c = 0; c < DC; ++c) t = fmaf(Bs[threadIdx.x][c], Bs[threadIdx.x][c], t);
+      Bn[threadIdx.x] = t;
+    }
+    __syncthreads();
+    float part[R][NU];
 #pragma unroll
-      for (int c = 0; c < kKMaxD; ++c) {
-        if (c < d) {
-          const float t = a[c] - Bs[r][c];
-          dist = fmaf(t, t, dist);
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int u = 0; u < NU; ++u) part[r][u] = 0.f;
+    const int jn = (int)(jend - j0 < kKT ? jend - j0 : kKT);
+    for (int jj = 0; jj < jn; ++jj) {
+      float dot[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) dot[r] = 0.f;
+      const float4 *brow = reinterpret_cast<const float4 *>(&Bs[jj][0]);
+#pragma unroll
+      for (int c4 = 0; c4 < DC / 4; ++c4) {
+        const float4 bv = brow[c4];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          dot[r] = fmaf(a[r][4 * c4], bv.x, dot[r]);
+          dot[r] = fmaf(a[r][4 * c4 + 1], bv.y, dot[r]);
+          dot[r] = fmaf(a[r][4 * c4 + 2], bv.z, dot[r]);
+          dot[r] = fmaf(a[r][4 * c4 + 3], bv.w, dot[r]);
         }
       }
-      float e;
-      asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(-gl2 * dist));
-      if (DERIV) e *= -dist;
+      const float bn = Bn[jj];
 #pragma unroll
-      for (int u = 0; u < NU; ++u) part[u] = fmaf(e, Us[r][u], part[u]);
+      for (int r = 0; r < R; ++r) {
+        const float d2 = fmaxf(fmaf(-2.f, dot[r], an[r] + bn), 0.f);
+        float e;
+        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(-gl2 * d2));
+        if (DERIV) e *= -d2;
+#pragma unroll
+        for (int u = 0; u < NU; ++u) part[r][u] = fmaf(e, Us[jj][u], part[r][u]);
+      }
     }
 #pragma unroll
-    for (int u = 0; u < NU; ++u) acc[u] += (double)part[u];
-  }
-  if (i < na) {
+    for (int r = 0; r < R; ++r)
 #pragma unroll
-    for (int u = 0; u < NU; ++u)
-      if (c0 + u < nu_total) out[i * nu_total + c0 + u] = acc[u];
+      for (int u = 0; u < NU; ++u) acc[r][u] += (double)part[r][u];
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int64_t i = (int64_t)blockIdx.x * kKP * R + threadIdx.x + kKP * r;
+    if (i < na) {
+#pragma unroll
+      for (int u = 0; u < NU; ++u)
+        if (c0 + u < nu_total) out[i * nu_total + c0 + u] = acc[r][u];
+    }
   }
 }
 
-template <int NU, bool DERIV>
-tsvm_status kprod(tsvm_context *ctx, const float *A, int64_t na, const float *B, int64_t nb,
-                  int d, double gamma, const double *U, int nu_total, double *out) {
-  const float gl2 = (float)(gamma * 1.4426950408889634);
+__global__ void kprod_reduce(const double *__restrict__ part, int nsplit, int64_t count,
+                             double *__restrict__ out) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= count) return;
+  double t = 0.0;
+  for (int y = 0; y < nsplit; ++y) t += part[(int64_t)y * count + e];
+  out[e] = t;
+}
+
+template <int DC, int R, int NU, bool DERIV>
+tsvm_status kprod_launch(tsvm_context *ctx, const float *A, int64_t na, const float *B, int64_t nb,
+                         int d, float gl2, const double *U, int nu_total, double *out) {
+  // split B over gridDim.y so that the grid covers the SMs about eight times over
+  const int64_t rowblocks = ceil_div(na, (int64_t)kKP * R);
+  int64_t split = ceil_div((int64_t)ctx->num_sms * 8, rowblocks);
+  split = std::max<int64_t>(1, std::min<int64_t>({split, 64, ceil_div(nb, (int64_t)kKT * 4)}));
+  const int64_t jc = round_up(ceil_div(nb, split), kKT);
+  split = ceil_div(nb, jc);
+  double *dst = out;
+  if (split > 1)
+    TSVM_TRY(scratch_t(ctx, SLOT_HG_KPART, (size_t)split * na * nu_total, &dst));
   for (int c0 = 0; c0 < nu_total; c0 += NU) {
-    kprod_kernel<NU, DERIV><<<(unsigned)ceil_div(na, kKP), kKP, 0, ctx->stream>>>(
-        A, na, B, nb, d, gl2, U, nu_total, c0, out);
+    kprod_kernel<DC, R, NU, DERIV><<<dim3((unsigned)rowblocks, (unsigned)split), kKP, 0,
+                                     ctx->stream>>>(A, na, B, nb, d, gl2, U, nu_total, c0, jc, dst);
+    TSVM_LAUNCHED(ctx);
+  }
+  if (split > 1) {
+    const int64_t count = na * nu_total;
+    kprod_reduce<<<(unsigned)ceil_div(count, 256), 256, 0, ctx->stream>>>(dst, (int)split, count,
+                                                                           out);
     TSVM_LAUNCHED(ctx);
   }
   return TSVM_OK;
 }
 
-// elementwise helpers ---------------------------------------------------------------------
+// NU: columns of U handled per launch (1, 8 or 32); d <= kKMaxD.
+template <int NU, bool DERIV>
+tsvm_status kprod(tsvm_context *ctx, const float *A, int64_t na, const float *B, int64_t nb,
+                  int d, double gamma, const double *U, int nu_total, double *out) {
+  const float gl2 = (float)(gamma * 1.4426950408889634);
+  constexpr int R32 = NU == 1 ? 4 : NU == 8 ? 2 : 1;
+  constexpr int R64 = NU == 1 ? 2 : 1;
+  if (d <= 32) return kprod_launch<32, R32, NU, DERIV>(ctx, A, na, B, nb, d, gl2, U, nu_total, out);
+  return kprod_launch<64, R64, NU, DERIV>(ctx, A, na, B, nb, d, gl2, U, nu_total, out);
+}
+
 __global__ void beta_kernel(const double *alpha, const float *y, int64_t n, double *beta) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) beta[i] = alpha[i] * (double)y[i];
@@ -292,7 +371,9 @@ extern "C" tsvm_status tsvm_hypergrad(tsvm_context *ctx, const float *X, const f
   TSVM_TRY(scratch_t(ctx, SLOT_HG_OMEGA, (size_t)n * kp, &Om));
   double *Rbuf = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_HG_R, (size_t)2 * k * k + 2 * (size_t)kp + 64, &Rbuf));
-  FactorKeep keep{Om, Rbuf, nullptr};
+  float *Wk = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_HG_W, (size_t)n * kp, &Wk));
+  FactorKeep keep{Om, Rbuf, Wk};
   TSVM_TRY(factor_rbf(ctx, X, y, n, d, gamma, k, precision, TSVM_SKETCH_GLIBC, nullptr, Zf, kp,
                       nullptr, &keep));
   // scratch: n-vectors beta, c, lam, u, E1, tmp, t2, s2, r + U5/D5 (5 n each); nv-vectors
@@ -415,7 +496,7 @@ extern "C" tsvm_status tsvm_hypergrad(tsvm_context *ctx, const float *X, const f
     S = bx + (size_t)n * (d + 1);
     beta_x_kernel<<<gn, 256, 0, st>>>(beta, X, n, d, bx);
     TSVM_LAUNCHED(ctx);
-    TSVM_TRY((kprod<8, false>(ctx, Xv, nv, X, n, d, gamma, bx, d + 1, S)));
+    TSVM_TRY((kprod<32, false>(ctx, Xv, nv, X, n, d, gamma, bx, d + 1, S)));
     dxv_kernel<<<gv, 256, 0, st>>>(S, Xv, g, nv, d, gamma, dXv);
     TSVM_LAUNCHED(ctx);
   }

@@ -139,11 +139,12 @@ tsvm_status bias_rbf(tsvm_context *ctx, const float *Z, int ldz, const float *y,
 // ---- factor.cu -------------------------------------------------------------------------
 // What the hypergradient keeps of a factorisation: the sketch Omega (n x kp copy), the combined
 // CholeskyQR factor R (k x k upper, pass-1 output B = W R; the buffer holds 2 k x k doubles) and
-// the orthonormal basis W (points into the context's scratch until the next factorisation).
+// a copy of the orthonormal basis W (n x kp) taken before the second pass rounds W in place to
+// the tensor-core operand type (B = W R holds for the copy, not for the rounded W).
 struct FactorKeep {
   float *omega;
   double *R;
-  const float *W;
+  float *W;
 };
 tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_t n, int d,
                        double gamma, int k, int precision, int sketch, const float *Q_user,

@@ -25,9 +25,10 @@ def data():
     return X, y, Xv, yv
 
 
-def train(ctx, X, y, gamma, C):
-    Z, _ = api.factor(ctx, X, y, gamma, K, "fp32")
-    alpha, xi, ym, st = api.ipm(ctx, Z, y, K, C, want_xi=True, tol=1e-9)
+def train(ctx, X, y, gamma, C, prec="fp32"):
+    Z, _ = api.factor(ctx, X, y, gamma, K, prec)
+    alpha, xi, ym, st = api.ipm(ctx, Z, y, K, C, want_xi=True, tol=1e-9,
+                                precision=_lib.PREC_FP32 if prec == "fp32" else _lib.PREC_BF16)
     b, _, _, _ = api.bias(ctx, Z, y, alpha, K, C)
     return Z, alpha, (xi, st["s"]), ym, b
 
@@ -78,6 +79,23 @@ def test_hypergrad_matches_fp64_restatement(ctx, data):
     err = np.linalg.norm(dxv.cpu().numpy() - dxv_o) / np.linalg.norm(dxv_o)
     assert err < 1e-4, err
     assert 0 < res["n_free_bias"] <= 50
+
+
+def test_hypergrad_fp16_factor_matches_fp64_restatement(ctx, data):
+    # the tensor-core factor rounds its second-pass basis to FP16 in place; the range-finder
+    # derivative needs the basis before rounding (B = W R), which R^-1 would otherwise amplify
+    X, y, Xv, yv = data
+    gamma, C = 0.03, 16.0
+    Xd, yd, Xvd, yvd = dev(X), dev(y), dev(Xv), dev(yv)
+    Z, alpha, xi, ym, b = train(ctx, Xd, yd, gamma, C, "fp16")
+    res, _ = api.hypergrad(ctx, Xd, yd, Xvd, yvd, gamma, C, K, alpha, xi[0], xi[1], ym, b,
+                           precision="fp16")
+    L, dg, dc, _ = orc.hypergrad(X, y, Xv, yv, gamma, C, K, alpha.cpu().numpy(),
+                                 xi[0].cpu().numpy(), xi[1].cpu().numpy(), b)
+    assert abs(res["loss"] - L) <= 1e-4 * max(1.0, L)
+    # the oracle differentiates its own FP64 factor: the FP16 factor's rounding shows up here
+    assert abs(res["dloss_dlog_C"] - dc) <= 3e-2 * max(abs(dc), 1e-3 * L), (res, dc)
+    assert abs(res["dloss_dlog_gamma"] - dg) <= 3e-2 * max(abs(dg), 1e-3 * L), (res, dg)
 
 
 def test_hypergrad_autograd_matches_central_differences(ctx, data):
