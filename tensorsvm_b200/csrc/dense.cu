@@ -425,6 +425,140 @@ jacobi_kernel(double *__restrict__ A0, double *__restrict__ A1, double *__restri
   if (blockIdx.x == 0 && threadIdx.x == 0) *sweeps_out = sweep;
 }
 
+// The same cyclic Jacobi in one CTA for ne <= 128 (the grid version pays a grid barrier per
+// round, ~2000 of them at ne = 128): the lower triangle of A packed in shared memory
+// (r (r + 1) / 2 + c) and Vt (row p = eigenvector p) beside it, 196 KB at ne = 128.  A round
+// rotates ne / 2 disjoint pairs; with J_i the rotation of pair i, the 2 x 2 block of rows of
+// pair i and columns of pair j becomes J_i^T A_ij J_j, one block per thread with no conflicts
+// (blocks i > j are the transposes of i < j and are not stored), and rows p, q of Vt are rotated
+// alongside.  Same rotation formulas, ordering, tolerance and sweep limit as jacobi_kernel.
+constexpr int kJacobiSmallNe = 128;
+
+__device__ __forceinline__ int pk(int r, int c, const int *roff) {
+  return r >= c ? roff[r] + c : roff[c] + r;
+}
+
+__global__ void __launch_bounds__(1024, 1)
+jacobi_small_kernel(const double *__restrict__ A, int n, int lda, int ne, int max_sweeps,
+                    double tol, double *__restrict__ w, double *__restrict__ V,
+                    int *__restrict__ sweeps_out) {
+  extern __shared__ double jsh[];
+  const int np = ne / 2;
+  double *P = jsh;                                        // packed lower triangle
+  double *Vt = P + (size_t)ne * (ne + 1) / 2;             // ne x ne
+  double *cs = Vt + (size_t)ne * ne;                      // [np]
+  double *sn = cs + np;                                   // [np]
+  double *red = sn + np;                                  // [64]
+  int *pp = reinterpret_cast<int *>(red + 64);            // [np]
+  int *qq = pp + np;                                      // [np]
+  int *roff = qq + np;                                    // [ne]
+  for (int r = threadIdx.x; r < ne; r += blockDim.x) roff[r] = r * (r + 1) / 2;
+  __syncthreads();
+  for (int r = threadIdx.x; r < ne; r += blockDim.x)
+    for (int c = 0; c <= r; ++c) P[roff[r] + c] = (r < n && c < n) ? A[(int64_t)r * lda + c] : 0.0;
+  for (int e = threadIdx.x; e < ne * ne; e += blockDim.x) Vt[e] = (e / ne == e % ne) ? 1.0 : 0.0;
+  __syncthreads();
+  // this thread's 2 x 2 blocks (i, j), i <= j over the pairs (at most 3 at ne = 128), fixed
+  // for the whole solve: enumerate the upper triangle of pairs row by row
+  constexpr int kMaxB = 3;
+  const int nblk = np * (np + 1) / 2;
+  int bi[kMaxB], bj[kMaxB];
+  int nb = 0;
+  for (int b = threadIdx.x; b < nblk && nb < kMaxB; b += blockDim.x, ++nb) {
+    int i = 0, rem = b;
+    while (rem >= np - i) { rem -= np - i; ++i; }
+    bi[nb] = i;
+    bj[nb] = i + rem;
+  }
+  // this thread's Vt elements: e = tid + 1024 u, pair e / ne, column e % ne
+  const int m0 = threadIdx.x / ne, col0 = threadIdx.x % ne;
+  const int dm = blockDim.x / ne, dc = blockDim.x % ne;
+  int sweep = 0;
+  for (sweep = 0; sweep < max_sweeps; ++sweep) {
+    for (int round = 0; round < ne - 1; ++round) {
+      for (int m = threadIdx.x; m < np; m += blockDim.x) {
+        const int p = circle_player(m, round, ne), q = circle_player(ne - 1 - m, round, ne);
+        const double app = P[pk(p, p, roff)], aqq = P[pk(q, q, roff)], apq = P[pk(p, q, roff)];
+        double c = 1.0, sv = 0.0;
+        if (fabs(apq) > 1e-300) {
+          const double tau = (aqq - app) / (2.0 * apq);
+          double t;
+          if (fabs(tau) > 1e150) t = 0.5 / tau;
+          else t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+          c = 1.0 / sqrt(1.0 + t * t);
+          sv = t * c;
+        }
+        cs[m] = c;
+        sn[m] = sv;
+        pp[m] = p;
+        qq[m] = q;
+      }
+      __syncthreads();
+      for (int u = 0; u < nb; ++u) {
+        const int i = bi[u], j = bj[u];
+        const int pi = pp[i], qi = qq[i], pj = pp[j], qj = qq[j];
+        const double ci = cs[i], si = sn[i], cj = cs[j], sj = sn[j];
+        const int i00 = pk(pi, pj, roff), i01 = pk(pi, qj, roff), i10 = pk(qi, pj, roff),
+                  i11 = pk(qi, qj, roff);
+        const double a00 = P[i00], a01 = P[i01], a10 = P[i10], a11 = P[i11];
+        // columns of pair j: (x_p, x_q) -> (c x_p - s x_q, s x_p + c x_q)
+        const double b00 = cj * a00 - sj * a01, b01 = sj * a00 + cj * a01;
+        const double b10 = cj * a10 - sj * a11, b11 = sj * a10 + cj * a11;
+        // rows of pair i
+        const double n00 = ci * b00 - si * b10, n10 = si * b00 + ci * b10;
+        const double n01 = ci * b01 - si * b11, n11 = si * b01 + ci * b11;
+        if (i == j) {
+          P[i00] = n00;
+          P[i01] = 0.5 * (n01 + n10);
+          P[i11] = n11;
+        } else {
+          P[i00] = n00;
+          P[i01] = n01;
+          P[i10] = n10;
+          P[i11] = n11;
+        }
+      }
+      for (int m = m0, col = col0; m < np;) {
+        const double c = cs[m], sv = sn[m];
+        double *vp = Vt + (size_t)pp[m] * ne, *vq = Vt + (size_t)qq[m] * ne;
+        const double a = vp[col], bq = vq[col];
+        vp[col] = c * a - sv * bq;
+        vq[col] = sv * a + c * bq;
+        m += dm;
+        col += dc;
+        if (col >= ne) { col -= ne; ++m; }
+      }
+      __syncthreads();
+    }
+    // convergence: off-diagonal mass against the diagonal
+    double off = 0.0, dia = 0.0;
+    for (int r = threadIdx.x; r < ne; r += blockDim.x) {
+      for (int c = 0; c < r; ++c) off += 2.0 * P[roff[r] + c] * P[roff[r] + c];
+      dia += P[roff[r] + r] * P[roff[r] + r];
+    }
+    off = warp_sum(off);
+    dia = warp_sum(dia);
+    if ((threadIdx.x & 31) == 0) {
+      red[threadIdx.x >> 5] = off;
+      red[32 + (threadIdx.x >> 5)] = dia;
+    }
+    __syncthreads();
+    double o = 0.0, dsum = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+      o += red[k];
+      dsum += red[32 + k];
+    }
+    __syncthreads();
+    if (o <= tol * tol * (dsum + o)) { ++sweep; break; }
+  }
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int r = e / n, c = e % n;
+    V[e] = Vt[(size_t)c * ne + r];
+    if (c == 0) w[r] = P[roff[r] + r];
+  }
+  if (threadIdx.x == 0) *sweeps_out = sweep;
+}
+
 __global__ void eig_pack_in(const double *__restrict__ A, int n, int lda, int ne,
                             double *__restrict__ A0, double *__restrict__ Vt) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -524,6 +658,24 @@ tsvm_status eig_jacobi_fp64(tsvm_context *ctx, double *A, int n, int lda, double
   if (n < 1 || n > 1024) return TSVM_ERR_UNSUPPORTED;
   int ne = n + (n & 1);
   if (ne < 2) ne = 2;
+  if (ne <= kJacobiSmallNe) {
+    int *sweeps_dev = nullptr;
+    TSVM_TRY(scratch_t(ctx, SLOT_SMALL3, 4, &sweeps_dev));
+    const int np = ne / 2;
+    const size_t smem = sizeof(double) * ((size_t)ne * (ne + 1) / 2 + (size_t)ne * ne + 2 * np + 64) +
+                        sizeof(int) * (2 * np + ne);
+    TSVM_CUDA(cudaFuncSetAttribute(jacobi_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+    jacobi_small_kernel<<<1, 1024, smem, ctx->stream>>>(A, n, lda, ne, 40, 1e-13, w, V,
+                                                         sweeps_dev);
+    TSVM_LAUNCHED(ctx);
+    int sweeps = 0;
+    TSVM_CUDA(cudaMemcpyAsync(&sweeps, sweeps_dev, sizeof(int), cudaMemcpyDeviceToHost,
+                              ctx->stream));
+    TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (sweeps_out) *sweeps_out = sweeps;
+    return TSVM_OK;
+  }
   double *buf = nullptr;
   const size_t need = (size_t)3 * ne * ne + 8 + 4;
   TSVM_TRY(scratch_t(ctx, SLOT_SMALL3, need, &buf));

@@ -622,19 +622,20 @@ stream_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, Op op,
 #pragma unroll
     for (int j = 0; j < NS; ++j) {
       const double t = warp_sum(sums[j]);
-      if (lane == 0) red[j * 9 + warp] = t;
+      if (lane == 0) red[j * (kSConsumers + 1) + warp] = t;
     }
 #pragma unroll
     for (int j = 0; j < NM; ++j) {
       const double t = warp_min(mins[j]);
-      if (lane == 0) red[(NS + j) * 9 + warp] = t;
+      if (lane == 0) red[(NS + j) * (kSConsumers + 1) + warp] = t;
     }
     __syncthreads();
     if (threadIdx.x < NS + NM) {
       const int j = threadIdx.x;
       double t = j < NS ? 0.0 : INFINITY;
       for (int ww = 0; ww < kSConsumers + 1; ++ww)
-        t = j < NS ? t + red[j * 9 + ww] : fmin(t, red[j * 9 + ww]);
+        t = j < NS ? t + red[j * (kSConsumers + 1) + ww]
+                   : fmin(t, red[j * (kSConsumers + 1) + ww]);
       part_s[(int64_t)blockIdx.x * (NS + NM) + j] = t;
     }
   }
@@ -841,7 +842,8 @@ struct Runner {
     const size_t chunk = (size_t)CR * ldz * 4;
     size_t stages = std::min<size_t>(16, std::max<size_t>(2, (192 * 1024) / chunk));
     const size_t red = sizeof(double) * std::max<size_t>(
-        MODE != MODE_ZW ? (size_t)kSConsumers * RPW * R * LPR * CPL * 4 : 0, 16 * 9);
+        MODE != MODE_ZW ? (size_t)kSConsumers * RPW * R * LPR * CPL * 4 : 0,
+        16 * (kSConsumers + 1));
     while (stages * chunk < red) ++stages;
     const size_t smem = stages * chunk + 8 * (2 * stages + 2);
     auto kern = stream_kernel<MODE, Op, R, CR, LPR, CPL>;
@@ -1538,7 +1540,8 @@ void stream_config(int64_t ldz, size_t *stages_out, size_t *smem_out) {
   const size_t chunk = (size_t)CR * ldz * 4;
   size_t stages = std::min<size_t>(16, std::max<size_t>(2, (192 * 1024) / chunk));
   const size_t red = sizeof(double) * std::max<size_t>(
-      MODE != MODE_ZW ? (size_t)kSConsumers * RPW * R * LPR * CPL * 4 : 0, 16 * 9);
+      MODE != MODE_ZW ? (size_t)kSConsumers * RPW * R * LPR * CPL * 4 : 0,
+        16 * (kSConsumers + 1));
   while (stages * chunk < red) ++stages;
   *stages_out = stages;
   *smem_out = stages * chunk + 8 * (2 * stages + 2);

@@ -68,7 +68,8 @@ def test_cholesky_reports_indefinite(ctx):
     assert info.value == 18
 
 
-@pytest.mark.parametrize("k", [2, 7, 32, 128, 256])
+# k <= 128: the one-CTA packed solver; above: the cooperative-grid one
+@pytest.mark.parametrize("k", [2, 7, 32, 127, 128, 130, 256])
 def test_jacobi_eigensolver(ctx, k):
     rng = np.random.default_rng(100 + k)
     A = rng.standard_normal((k, k))
