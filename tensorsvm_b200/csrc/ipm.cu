@@ -518,80 +518,144 @@ stream_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, Op op,
       double mine[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) mine[r] = 0.0;
-      constexpr int UNR = CPL >= 4 ? 1 : 4;   // wide rows: keep the register footprint bounded
-#pragma unroll UNR
-      for (int step = 0; step < STEPS; ++step) {
-        const int rw = step * RPW + slot;
-        const int64_t row = r0 + rw;
-        const bool in = row < n;
-        const float4 *zr = reinterpret_cast<const float4 *>(S + (size_t)rw * ldz);
-        float4 z[CPL];
+      if constexpr (MODE == MODE_ZW && LPR == 32) {
+        // Z w with whole rows per lane group: every lane keeps its partial dot products for all
+        // RW rows of the chunk, then one recursive-halving exchange leaves each row's total in
+        // 32 / RW lanes (about one double shuffle per row instead of a 5-level tree per row).
+        constexpr int B = RW == 32 ? 5 : RW == 16 ? 4 : RW == 8 ? 3 : RW == 4 ? 2 : RW == 2 ? 1 : 0;
+        static_assert((1 << B) == RW, "chunk rows must be a power of two");
+        double pr[RW][R];
 #pragma unroll
-        for (int c = 0; c < CPL; ++c) {
-          const int g = sl + c * LPR;
-          float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (in && 4 * g < k) {
-            t = zr[g];
-            if (4 * g + 3 >= k) {
-              if (4 * g + 1 >= k) t.y = 0.f;
-              if (4 * g + 2 >= k) t.z = 0.f;
-              t.w = 0.f;
-            }
-          }
-          z[c] = t;
-        }
-        double vr[R];
-        if constexpr (DOT) {
-          double d[R];
+        for (int rr = 0; rr < RW; ++rr)
 #pragma unroll
-          for (int r = 0; r < R; ++r) d[r] = 0.0;
+          for (int r = 0; r < R; ++r) pr[rr][r] = 0.0;
 #pragma unroll
-          for (int c = 0; c < CPL; ++c)
+        for (int rr = 0; rr < RW; ++rr) {
+          const bool in = r0 + rr < n;
+          const float4 *zr = reinterpret_cast<const float4 *>(S + (size_t)rr * ldz);
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-              d[r] = fma((double)z[c].x, wr[4 * c + 0][r], d[r]);
-              d[r] = fma((double)z[c].y, wr[4 * c + 1][r], d[r]);
-              d[r] = fma((double)z[c].z, wr[4 * c + 2][r], d[r]);
-              d[r] = fma((double)z[c].w, wr[4 * c + 3][r], d[r]);
-            }
-#pragma unroll
-          for (int r = 0; r < R; ++r) {
-#pragma unroll
-            for (int o = LPR / 2; o > 0; o >>= 1) d[r] += __shfl_xor_sync(0xffffffffu, d[r], o);
-          }
-          if constexpr (MODE == MODE_ZW) {
-#pragma unroll
-            for (int s2 = 0; s2 < RPW; ++s2)
-#pragma unroll
-              for (int r = 0; r < R; ++r) {
-                const double got = __shfl_sync(0xffffffffu, d[r], s2 * LPR);
-                if (lane == step * RPW + s2) mine[r] = got;
+          for (int c = 0; c < CPL; ++c) {
+            const int g = lane + c * 32;
+            float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (in && 4 * g < k) {
+              t = zr[g];
+              if (4 * g + 3 >= k) {
+                if (4 * g + 1 >= k) t.y = 0.f;
+                if (4 * g + 2 >= k) t.z = 0.f;
+                t.w = 0.f;
               }
-          } else {
-            const double di = in ? dinv[goff + row] : 0.0;
-#pragma unroll
-            for (int r = 0; r < R; ++r) vr[r] = d[r] * di;
-          }
-        } else {
-#pragma unroll
-          for (int r = 0; r < R; ++r) vr[r] = __shfl_sync(0xffffffffu, v[r], rw);
-        }
-        if constexpr (ACC) {
-#pragma unroll
-          for (int c = 0; c < CPL; ++c)
+            }
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-              acc[4 * c + 0][r] = fma((double)z[c].x, vr[r], acc[4 * c + 0][r]);
-              acc[4 * c + 1][r] = fma((double)z[c].y, vr[r], acc[4 * c + 1][r]);
-              acc[4 * c + 2][r] = fma((double)z[c].z, vr[r], acc[4 * c + 2][r]);
-              acc[4 * c + 3][r] = fma((double)z[c].w, vr[r], acc[4 * c + 3][r]);
+              pr[rr][r] = fma((double)t.x, wr[4 * c + 0][r], pr[rr][r]);
+              pr[rr][r] = fma((double)t.y, wr[4 * c + 1][r], pr[rr][r]);
+              pr[rr][r] = fma((double)t.z, wr[4 * c + 2][r], pr[rr][r]);
+              pr[rr][r] = fma((double)t.w, wr[4 * c + 3][r], pr[rr][r]);
+            }
+          }
+        }
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(b_empty + 8 * st);   // the chunk is in registers now
+        // step s (lane offset 16 >> s) keeps the upper half of the rows where the lane bit is set
+#pragma unroll
+        for (int sb = 0; sb < B; ++sb) {
+          const int off = 16 >> sb;
+          const int half = RW >> (sb + 1);
+          const bool upper = (lane & off) != 0;
+#pragma unroll
+          for (int i = 0; i < half; ++i)
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const double keep = upper ? pr[half + i][r] : pr[i][r];
+              const double send = upper ? pr[i][r] : pr[half + i][r];
+              pr[i][r] = keep + __shfl_xor_sync(0xffffffffu, send, off);
             }
         }
-      }
-      __syncwarp();
-      if (lane == 0) tc::mbar_arrive(b_empty + 8 * st);
-      if constexpr (MODE == MODE_ZW) {
-        if (lane < RW && r0 + lane < n) op.row(goff + r0 + lane, mine, sums, mins);
+#pragma unroll
+        for (int off = 16 >> B; off > 0; off >>= 1)
+#pragma unroll
+          for (int r = 0; r < R; ++r) pr[0][r] += __shfl_xor_sync(0xffffffffu, pr[0][r], off);
+        const int myrow = (lane >> (5 - B)) & (RW - 1);
+#pragma unroll
+        for (int r = 0; r < R; ++r) mine[r] = pr[0][r];
+        if ((lane & ((32 >> B) - 1)) == 0 && r0 + myrow < n)
+          op.row(goff + r0 + myrow, mine, sums, mins);
+      } else {
+        constexpr int UNR = CPL >= 4 ? 1 : 4;   // wide rows: keep the register footprint bounded
+  #pragma unroll UNR
+        for (int step = 0; step < STEPS; ++step) {
+          const int rw = step * RPW + slot;
+          const int64_t row = r0 + rw;
+          const bool in = row < n;
+          const float4 *zr = reinterpret_cast<const float4 *>(S + (size_t)rw * ldz);
+          float4 z[CPL];
+  #pragma unroll
+          for (int c = 0; c < CPL; ++c) {
+            const int g = sl + c * LPR;
+            float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (in && 4 * g < k) {
+              t = zr[g];
+              if (4 * g + 3 >= k) {
+                if (4 * g + 1 >= k) t.y = 0.f;
+                if (4 * g + 2 >= k) t.z = 0.f;
+                t.w = 0.f;
+              }
+            }
+            z[c] = t;
+          }
+          double vr[R];
+          if constexpr (DOT) {
+            double d[R];
+  #pragma unroll
+            for (int r = 0; r < R; ++r) d[r] = 0.0;
+  #pragma unroll
+            for (int c = 0; c < CPL; ++c)
+  #pragma unroll
+              for (int r = 0; r < R; ++r) {
+                d[r] = fma((double)z[c].x, wr[4 * c + 0][r], d[r]);
+                d[r] = fma((double)z[c].y, wr[4 * c + 1][r], d[r]);
+                d[r] = fma((double)z[c].z, wr[4 * c + 2][r], d[r]);
+                d[r] = fma((double)z[c].w, wr[4 * c + 3][r], d[r]);
+              }
+  #pragma unroll
+            for (int r = 0; r < R; ++r) {
+  #pragma unroll
+              for (int o = LPR / 2; o > 0; o >>= 1) d[r] += __shfl_xor_sync(0xffffffffu, d[r], o);
+            }
+            if constexpr (MODE == MODE_ZW) {
+  #pragma unroll
+              for (int s2 = 0; s2 < RPW; ++s2)
+  #pragma unroll
+                for (int r = 0; r < R; ++r) {
+                  const double got = __shfl_sync(0xffffffffu, d[r], s2 * LPR);
+                  if (lane == step * RPW + s2) mine[r] = got;
+                }
+            } else {
+              const double di = in ? dinv[goff + row] : 0.0;
+  #pragma unroll
+              for (int r = 0; r < R; ++r) vr[r] = d[r] * di;
+            }
+          } else {
+  #pragma unroll
+            for (int r = 0; r < R; ++r) vr[r] = __shfl_sync(0xffffffffu, v[r], rw);
+          }
+          if constexpr (ACC) {
+  #pragma unroll
+            for (int c = 0; c < CPL; ++c)
+  #pragma unroll
+              for (int r = 0; r < R; ++r) {
+                acc[4 * c + 0][r] = fma((double)z[c].x, vr[r], acc[4 * c + 0][r]);
+                acc[4 * c + 1][r] = fma((double)z[c].y, vr[r], acc[4 * c + 1][r]);
+                acc[4 * c + 2][r] = fma((double)z[c].z, vr[r], acc[4 * c + 2][r]);
+                acc[4 * c + 3][r] = fma((double)z[c].w, vr[r], acc[4 * c + 3][r]);
+              }
+          }
+        }
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(b_empty + 8 * st);
+        if constexpr (MODE == MODE_ZW) {
+          if (lane < RW && r0 + lane < n) op.row(goff + r0 + lane, mine, sums, mins);
+        }
       }
     }
   }
