@@ -33,6 +33,7 @@ enum Slot : int {
   SLOT_SYRK_PART,     // IPM: per-CTA FP32 partial Gram matrices of the tensor-core SYRK
   SLOT_SYRK_CNT,      // IPM: per-block counts of the exactly summed (large-weight) rows
   SLOT_IPM_IDX,       // IPM: indices of the exactly summed rows
+  SLOT_SYRK_PLAN,     // IPM: column windows of the tensor-core SYRK for k > 256
   SLOT_IPM_PART,      // IPM / bias streaming partial sums (kept apart from SLOT_PART, which the
                       // Z^T D^-1 Z accumulation may regrow inside the iteration)
   SLOT_MISC,
@@ -69,6 +70,8 @@ struct tsvm_context {
   int jump_levels = 0;
   // pinned host staging for small device->host reads
   double *host_scalars = nullptr;
+  // width k whose column-window table SLOT_SYRK_PLAN holds (-1: none)
+  int syrk_plan_k = -1;
   // the last RBF tsvm_train (its X, y in SLOT_DEV_IN and Z in SLOT_DEV_Z), for -analysis
   struct {
     bool valid = false;

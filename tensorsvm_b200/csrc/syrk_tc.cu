@@ -17,7 +17,16 @@
 // feed 128 x N x 16 MMAs for the lower block strips (rows 0-127 x cols 0-127, rows 128-255 x
 // cols 0-255).  Warp 0 issues TMA, warp 1 owns TMEM and issues MMAs, warps 2-5 drain the
 // FP32 accumulators to per-CTA partials.  All waits are bounded.
+//
+// k > 256 (up to 425): the columns are cut into groups and covered by windows of at most 256
+// columns such that every pair of groups shares a window (3 groups, windows of 2, for k <= 384;
+// 5 groups, windows of 3, for k <= 425: {0,1,2} {0,3,4} {1,3,4} {2,3,4}); each window is one
+// gather + split + tensor-core SYRK of its columns, and each block of M is written by the first
+// window that holds both of its groups.
 #include <cuda_bf16.h>
+
+#include <algorithm>
+#include <vector>
 
 #include "common.cuh"
 #include "context.h"
@@ -30,6 +39,7 @@ namespace {
 using namespace tc;
 
 constexpr int kSJ = 64;              // rows of Z per chunk (MMA K of one chunk, 4 x 16)
+constexpr int kSyrkMaxK = 425;       // widest capacitance matrix the windows cover
 constexpr int kSyrkThreads = 192;
 
 template <int WAYS, int KP>
@@ -45,10 +55,13 @@ struct SyrkCfg {
 
 // parts[w][t][c][jl] (BF16): WAYS-term split of sqrt(dinv_j) Z[j][c], j = 64 t + jl; zero for
 // rows with dinv_j > tau, rows j >= n and columns c >= k.  grid (T, KP / 32), block (32, 8).
+// cols (may be null: the identity) maps the KP columns of the operand to columns of Z; columns
+// c >= k (k = the window's width) are zero.
 template <int WAYS>
 __global__ void __launch_bounds__(256)
 syrk_prep(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, int64_t T, int KP,
-          const double *__restrict__ dinv, double tau, __nv_bfloat16 *__restrict__ parts) {
+          const double *__restrict__ dinv, double tau, const int *__restrict__ cols,
+          __nv_bfloat16 *__restrict__ parts) {
   __shared__ float tile[kSJ][33];
   __shared__ float wrow[kSJ];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
@@ -69,7 +82,7 @@ syrk_prep(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, int64_t T,
     const int c = c0 + tx;
     float v = 0.f;
     const float w = wrow[r];
-    if (w != 0.f && c < k) v = Z[j * ldz + c] * w;
+    if (w != 0.f && c < k) v = Z[j * ldz + (cols ? cols[c] : c)] * w;
     tile[r][tx] = v;
   }
   __syncthreads();
@@ -215,22 +228,29 @@ syrk_tc_kernel(const __grid_constant__ CUtensorMap map, int T, float *__restrict
   }
 }
 
-// M[r][c] = M[c][r] = (r == c) + G64[r][c] + sum_g part[g][r][c] (FP64, CTA order), r >= c.
-// A timed-out tensor-core launch (err set) poisons M with NaN.
-__global__ void syrk_reduce(const float *__restrict__ part, int G, int KP, int k,
+// M[R][C] = M[C][R] = (R == C) + G64[R][C] + sum_g part[g][r][c] (FP64, CTA order) for the
+// window entries r >= c, R = cols[r], C = cols[c] (identity when cols is null), k the full width,
+// wl the window's.  With a window plan only the entries whose group pair this window owns
+// (owner[gid[R] * ng + gid[C]] == win) are written.  A timed-out tensor-core launch (err set)
+// poisons M with NaN.
+__global__ void syrk_reduce(const float *__restrict__ part, int G, int KP, int k, int wl,
+                            const int *__restrict__ cols, const int *__restrict__ gid,
+                            const int *__restrict__ owner, int ng, int win,
                             const double *__restrict__ G64, const int *__restrict__ err,
                             double *__restrict__ M) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (int64_t)k * k) return;
-  const int r = (int)(e / k), c = (int)(e % k);
+  if (e >= (int64_t)wl * wl) return;
+  const int r = (int)(e / wl), c = (int)(e % wl);
   if (c > r) return;
+  const int R = cols ? cols[r] : r, C = cols ? cols[c] : c;
+  if (owner && owner[gid[R] * ng + gid[C]] != win) return;
   double s = 0.0;
   for (int g = 0; g < G; ++g) s += (double)part[((size_t)g * KP + r) * KP + c];
-  if (G64) s += G64[(size_t)r * k + c];
-  if (r == c) s += 1.0;
+  if (G64) s += G64[(size_t)R * k + C];
+  if (R == C) s += 1.0;
   if (*err) s = NAN;
-  M[(size_t)r * k + c] = s;
-  M[(size_t)c * k + r] = s;
+  M[(size_t)R * k + C] = s;
+  M[(size_t)C * k + R] = s;
 }
 
 // Rows with dinv > tau, in index order: per-block counts over contiguous row ranges, then each
@@ -286,6 +306,43 @@ big_rows_index(const double *__restrict__ dinv, int64_t n, double tau,
   }
 }
 
+// Column windows for k > 256 (see the file comment).
+struct SyrkPlan {
+  int ng = 1, nw = 1;
+  int gbeg[6] = {0};                 // group g = columns [gbeg[g], gbeg[g + 1])
+  int wg[4][3] = {{0}};              // groups of each window
+  int wn[4] = {1};                   // groups per window
+};
+
+SyrkPlan syrk_plan(int k) {
+  SyrkPlan p;
+  if (k <= 256) {
+    p.gbeg[1] = k;
+    return p;
+  }
+  if (k <= 384) {
+    p.ng = 3;
+    p.nw = 3;
+    const int w[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+    for (int i = 0; i < 3; ++i) {
+      p.wn[i] = 2;
+      p.wg[i][0] = w[i][0];
+      p.wg[i][1] = w[i][1];
+    }
+  } else {
+    p.ng = 5;
+    p.nw = 4;
+    const int w[4][3] = {{0, 1, 2}, {0, 3, 4}, {1, 3, 4}, {2, 3, 4}};
+    for (int i = 0; i < 4; ++i) {
+      p.wn[i] = 3;
+      for (int j = 0; j < 3; ++j) p.wg[i][j] = w[i][j];
+    }
+  }
+  const int gs = (k + p.ng - 1) / p.ng;
+  for (int g = 0; g <= p.ng; ++g) p.gbeg[g] = std::min(k, g * gs);
+  return p;
+}
+
 template <int WAYS, int KP>
 tsvm_status launch_syrk_tc(tsvm_context *ctx, const CUtensorMap &map, int T, int G, float *part,
                            int *err) {
@@ -300,7 +357,7 @@ tsvm_status launch_syrk_tc(tsvm_context *ctx, const CUtensorMap &map, int T, int
 
 }  // namespace
 
-bool syrk_tc_supported(int k) { return k >= 1 && k <= 256 && tc::encode_fn() != nullptr; }
+bool syrk_tc_supported(int k) { return k >= 1 && k <= kSyrkMaxK && tc::encode_fn() != nullptr; }
 
 tsvm_status big_rows(tsvm_context *ctx, const double *dinv, int64_t n, double tau, int64_t *idx,
                      int *count_dev) {
@@ -318,37 +375,80 @@ tsvm_status syrk_capacitance_tc(tsvm_context *ctx, const float *Z, int ldz, int6
                                 const double *dinv, double tau, int ways, const double *G64,
                                 double *M) {
   if (!syrk_tc_supported(k) || (ways != 2 && ways != 3)) return TSVM_ERR_UNSUPPORTED;
-  const int KP = k <= 128 ? 128 : 256;
+  const SyrkPlan plan = syrk_plan(k);
+  // per window: its columns (device table), width and tensor-core width
+  int *dplan = nullptr;   // [nw][256] columns | gid[k] | owner[ng][ng]
+  const int *dgid = nullptr, *downer = nullptr;
+  std::vector<int> wl(plan.nw), hplan;
+  if (plan.nw > 1) {
+    hplan.assign((size_t)plan.nw * 256 + k + plan.ng * plan.ng, 0);
+    std::vector<int> owner(plan.ng * plan.ng, -1);
+    for (int w = 0; w < plan.nw; ++w) {
+      int c = 0;
+      for (int j = 0; j < plan.wn[w]; ++j) {
+        const int g = plan.wg[w][j];
+        for (int col = plan.gbeg[g]; col < plan.gbeg[g + 1]; ++col) hplan[(size_t)w * 256 + c++] = col;
+        for (int j2 = 0; j2 < plan.wn[w]; ++j2) {
+          const int g2 = plan.wg[w][j2];
+          if (owner[g * plan.ng + g2] < 0) owner[g * plan.ng + g2] = w;
+        }
+      }
+      wl[w] = c;
+    }
+    for (int g = 0; g < plan.ng; ++g)
+      for (int col = plan.gbeg[g]; col < plan.gbeg[g + 1]; ++col) hplan[(size_t)plan.nw * 256 + col] = g;
+    std::copy(owner.begin(), owner.end(), hplan.begin() + (size_t)plan.nw * 256 + k);
+    TSVM_TRY(scratch_t(ctx, SLOT_SYRK_PLAN, hplan.size(), &dplan));
+    if (ctx->syrk_plan_k != k) {   // the table depends on k only: upload once per width
+      TSVM_CUDA(cudaMemcpyAsync(dplan, hplan.data(), sizeof(int) * hplan.size(),
+                                cudaMemcpyHostToDevice, ctx->stream));
+      TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+      ctx->syrk_plan_k = k;
+    }
+    dgid = dplan + (size_t)plan.nw * 256;
+    downer = dgid + k;
+  } else {
+    wl[0] = k;
+  }
+  int wmax = 0;
+  for (int w = 0; w < plan.nw; ++w) wmax = std::max(wmax, wl[w]);
+  const int KPmax = wmax <= 128 ? 128 : 256;
   const int64_t T = ceil_div(n, (int64_t)kSJ);
-  if ((int64_t)ways * T * KP > (int64_t)INT32_MAX) return TSVM_ERR_UNSUPPORTED;
+  if ((int64_t)ways * T * KPmax > (int64_t)INT32_MAX) return TSVM_ERR_UNSUPPORTED;
   __nv_bfloat16 *parts = nullptr;
-  TSVM_TRY(scratch_t(ctx, SLOT_SYRK_OP, (size_t)ways * T * KP * kSJ, &parts));
+  TSVM_TRY(scratch_t(ctx, SLOT_SYRK_OP, (size_t)ways * T * KPmax * kSJ, &parts));
   const int G = (int)std::min<int64_t>(ctx->num_sms, T);
   float *part = nullptr;
-  TSVM_TRY(scratch_t(ctx, SLOT_SYRK_PART, (size_t)G * KP * KP + 64, &part));
-  int *err = reinterpret_cast<int *>(part + (size_t)G * KP * KP);
+  TSVM_TRY(scratch_t(ctx, SLOT_SYRK_PART, (size_t)G * KPmax * KPmax + 64, &part));
+  int *err = reinterpret_cast<int *>(part + (size_t)G * KPmax * KPmax);
   TSVM_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
-  const dim3 pgrid((unsigned)T, (unsigned)(KP / 32));
-  if (ways == 2)
-    syrk_prep<2><<<pgrid, dim3(32, 8), 0, ctx->stream>>>(Z, ldz, k, n, T, KP, dinv, tau, parts);
-  else
-    syrk_prep<3><<<pgrid, dim3(32, 8), 0, ctx->stream>>>(Z, ldz, k, n, T, KP, dinv, tau, parts);
-  TSVM_LAUNCHED(ctx);
-  CUtensorMap map;
-  if (!tc::make_map(&map, parts, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, kSJ, (uint64_t)ways * T * KP,
-                    kSJ, KP))
-    return TSVM_ERR_CUDA;
-  tsvm_status st;
-  if (ways == 2)
-    st = KP == 128 ? launch_syrk_tc<2, 128>(ctx, map, (int)T, G, part, err)
-                   : launch_syrk_tc<2, 256>(ctx, map, (int)T, G, part, err);
-  else
-    st = KP == 128 ? launch_syrk_tc<3, 128>(ctx, map, (int)T, G, part, err)
-                   : launch_syrk_tc<3, 256>(ctx, map, (int)T, G, part, err);
-  if (st != TSVM_OK) return st;
-  syrk_reduce<<<(unsigned)ceil_div((int64_t)k * k, 256), 256, 0, ctx->stream>>>(part, G, KP, k,
-                                                                                  G64, err, M);
-  TSVM_LAUNCHED(ctx);
+  for (int w = 0; w < plan.nw; ++w) {
+    const int KP = wl[w] <= 128 ? 128 : 256;
+    const int *cols = plan.nw > 1 ? dplan + (size_t)w * 256 : nullptr;
+    const dim3 pgrid((unsigned)T, (unsigned)(KP / 32));
+    if (ways == 2)
+      syrk_prep<2><<<pgrid, dim3(32, 8), 0, ctx->stream>>>(Z, ldz, wl[w], n, T, KP, dinv, tau,
+                                                           cols, parts);
+    else
+      syrk_prep<3><<<pgrid, dim3(32, 8), 0, ctx->stream>>>(Z, ldz, wl[w], n, T, KP, dinv, tau,
+                                                           cols, parts);
+    TSVM_LAUNCHED(ctx);
+    CUtensorMap map;
+    if (!tc::make_map(&map, parts, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, kSJ,
+                      (uint64_t)ways * T * KP, kSJ, KP))
+      return TSVM_ERR_CUDA;
+    tsvm_status st;
+    if (ways == 2)
+      st = KP == 128 ? launch_syrk_tc<2, 128>(ctx, map, (int)T, G, part, err)
+                     : launch_syrk_tc<2, 256>(ctx, map, (int)T, G, part, err);
+    else
+      st = KP == 128 ? launch_syrk_tc<3, 128>(ctx, map, (int)T, G, part, err)
+                     : launch_syrk_tc<3, 256>(ctx, map, (int)T, G, part, err);
+    if (st != TSVM_OK) return st;
+    syrk_reduce<<<(unsigned)ceil_div((int64_t)wl[w] * wl[w], 256), 256, 0, ctx->stream>>>(
+        part, G, KP, k, wl[w], cols, dgid, downer, plan.ng, w, G64, err, M);
+    TSVM_LAUNCHED(ctx);
+  }
   return TSVM_OK;
 }
 

@@ -29,9 +29,11 @@ def syrk_mixed(ctx, Z, k, dinv, tau, ways):
     return M.cpu().numpy(), cnt.value
 
 
-# n not a multiple of the 64-row chunk, k both below and at the 128/256 strip sizes, ldz > k
+# n not a multiple of the 64-row chunk, k both below and at the 128/256 strip sizes, ldz > k;
+# k > 256 through column windows (3 groups up to 384, 5 groups up to 425)
 @pytest.mark.parametrize("n,k,ways", [(70001, 256, 2), (70001, 256, 3), (5000, 100, 2),
-                                      (4096, 32, 3), (130, 256, 2), (64, 200, 2)])
+                                      (4096, 32, 3), (130, 256, 2), (64, 200, 2),
+                                      (9001, 300, 2), (20000, 400, 2), (777, 425, 3)])
 @pytest.mark.parametrize("tau", [100.0, float("inf"), 0.0])
 def test_syrk_mixed_accuracy(ctx, n, k, ways, tau):
     rng = np.random.default_rng(n + k + ways)
@@ -56,6 +58,26 @@ def prob(ctx):
     X, y = synth.two_gaussians(20000, 18, seed=2, noise=0.1)
     Z, _ = api.factor(ctx, dev(X), dev(y), 0.05, 128, "fp32")
     return X, y, Z
+
+
+def test_ipm_mixed_wide_k_matches_fp64(ctx):
+    # k = 400 (the d = 54 configuration's rank): the capacitance matrix through four windows.
+    # The benchmark's stopping rule: on this flat kernel the absolute 1e-7 residual rule can end
+    # in max/min(D) > 1e18 (WARN_ILL_CONDITIONED) before the residual rule is met.
+    X, y, g, C, _ = synth.make("c3", n=20000)
+    k = 400
+    Z, _ = api.factor(ctx, dev(X), dev(y), g, k, "fp32")
+    yd = dev(y)
+    a64, _, _, s64 = api.ipm(ctx, Z, yd, k, C, precision=_lib.PREC_FP32, rel_gap_tol=1e-6)
+    am, _, _, sm = api.ipm(ctx, Z, yd, k, C, precision=_lib.PREC_BF16, rel_gap_tol=1e-6)
+    assert s64["mixed_syrk"] == 0 and sm["mixed_syrk"] == 1
+    assert s64["status_code"] == _lib.OK and sm["status_code"] == _lib.OK, (s64, sm)
+    assert abs(sm["iters"] - s64["iters"]) <= 2, (sm["iters"], s64["iters"])
+    assert abs(sm["pobj"] - s64["pobj"]) / abs(s64["pobj"]) < 1e-6
+    Zh = Z.cpu().numpy()[:, :k].astype(np.float64)
+    f64 = Zh @ (Zh.T @ (a64.cpu().numpy() * y))
+    fm = Zh @ (Zh.T @ (am.cpu().numpy() * y))
+    assert np.max(np.abs(fm - f64)) < 1e-4 * max(1.0, np.max(np.abs(f64)))
 
 
 @pytest.mark.parametrize("sweeps", [1, 2])
