@@ -135,9 +135,9 @@ def barrier(world):
 # ------------------------------------------------------------------------------------------
 
 # DRAM bytes (read + write) per 128 x 64 tile of the tensor-core kernel-block product at k = 256,
-# from one ncu capture at n = 262144 (2.389 GB read + 0.258 GB written, 2048 x 4096 tiles): the
+# from one ncu capture at n = 262144 (2.390 GB read + 0.259 GB written, 2048 x 4096 tiles): the
 # J-side operands are re-read once per round of 148 row blocks, so traffic grows with the tiles.
-TC_BYTES_PER_TILE = (2.389420e9 + 0.258439e9) / (2048 * 4096)
+TC_BYTES_PER_TILE = (2.390065e9 + 0.259050e9) / (2048 * 4096)
 
 
 def tc_traffic(n: int) -> float:
@@ -264,7 +264,7 @@ def run_ours(args, world, rank, local):
                      "frac": round(achieved / peak, 4), "peak_source": f"{pk_kind} {pname}",
                      "traffic": tc_traffic(n) if tensor else None,
                      "traffic_source": ("dram__bytes_read.sum + dram__bytes_write.sum of one launch "
-                                        "at n=262144 (2.648 GB over 2048x4096 tiles), scaled by "
+                                        "at n=262144 (2.649 GB over 2048x4096 tiles), scaled by "
                                         "the tile count" if tensor else None),
                      "flops_per_launch": km_flops, "ms_per_launch": round(km_ms, 3)},
         "e2e": {"value": round(e2e_s, 4), "unit": "s",

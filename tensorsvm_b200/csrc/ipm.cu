@@ -515,6 +515,12 @@ stream_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, Op op,
       if constexpr (MODE == MODE_ZT) {
         if (lane < RW && r0 + lane < n) op.rhs(goff + r0 + lane, v, sums, mins);
       }
+      // Z^T D^-1 Z g: the chunk's D^-1 values, loaded once per chunk (lane = row) and passed to
+      // each row's lanes by a shuffle, off the per-row dependency chain
+      double dch = 0.0;
+      if constexpr (MODE == MODE_ZGZ) {
+        if (lane < RW && r0 + lane < n) dch = dinv[goff + r0 + lane];
+      }
       double mine[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) mine[r] = 0.0;
@@ -631,7 +637,7 @@ stream_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, Op op,
                   if (lane == step * RPW + s2) mine[r] = got;
                 }
             } else {
-              const double di = in ? dinv[goff + row] : 0.0;
+              const double di = __shfl_sync(0xffffffffu, dch, rw);
   #pragma unroll
               for (int r = 0; r < R; ++r) vr[r] = d[r] * di;
             }

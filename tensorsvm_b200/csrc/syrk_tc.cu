@@ -54,7 +54,7 @@ struct SyrkCfg {
 };
 
 // parts[w][t][c][jl] (BF16): WAYS-term split of sqrt(dinv_j) Z[j][c], j = 64 t + jl; zero for
-// rows with dinv_j > tau, rows j >= n and columns c >= k.  grid (T, KP / 32), block (32, 8).
+// rows with dinv_j > tau, rows j >= n and columns c >= k.  grid (T, KP / 128), block (32, 8).
 // cols (may be null: the identity) maps the KP columns of the operand to columns of Z; columns
 // c >= k (k = the window's width) are zero.
 template <int WAYS>
@@ -62,11 +62,14 @@ __global__ void __launch_bounds__(256)
 syrk_prep(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, int64_t T, int KP,
           const double *__restrict__ dinv, double tau, const int *__restrict__ cols,
           __nv_bfloat16 *__restrict__ parts) {
-  __shared__ float tile[kSJ][33];
+  // a block takes 64 rows x 128 columns: 32 loads in flight per thread (one 128-byte row
+  // segment per warp and load), written back as WAYS BF16 tiles of 128 columns x 64 rows
+  constexpr int kPC = 128;
+  __shared__ float tile[kSJ][kPC + 1];
   __shared__ float wrow[kSJ];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
   const int64_t t = blockIdx.x;
-  const int c0 = blockIdx.y * 32;
+  const int c0 = blockIdx.y * kPC;
   if (tid < kSJ) {
     const int64_t j = t * kSJ + tid;
     float w = 0.f;
@@ -77,17 +80,21 @@ syrk_prep(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, int64_t T,
     wrow[tid] = w;
   }
   __syncthreads();
+#pragma unroll
   for (int r = ty; r < kSJ; r += 8) {
     const int64_t j = t * kSJ + r;
-    const int c = c0 + tx;
-    float v = 0.f;
     const float w = wrow[r];
-    if (w != 0.f && c < k) v = Z[j * ldz + (cols ? cols[c] : c)] * w;
-    tile[r][tx] = v;
+#pragma unroll
+    for (int g = 0; g < kPC / 32; ++g) {
+      const int c = c0 + 32 * g + tx;
+      float v = 0.f;
+      if (w != 0.f && c < k) v = Z[j * ldz + (cols ? cols[c] : c)] * w;
+      tile[r][32 * g + tx] = v;
+    }
   }
   __syncthreads();
   const size_t part_stride = (size_t)T * KP * kSJ;
-  for (int cc = ty; cc < 32; cc += 8) {
+  for (int cc = ty; cc < kPC && c0 + cc < KP; cc += 8) {
     const int c = c0 + cc;
     float v0 = tile[2 * tx][cc], v1 = tile[2 * tx + 1][cc];
     __nv_bfloat162 *dst =
@@ -425,7 +432,7 @@ tsvm_status syrk_capacitance_tc(tsvm_context *ctx, const float *Z, int ldz, int6
   for (int w = 0; w < plan.nw; ++w) {
     const int KP = wl[w] <= 128 ? 128 : 256;
     const int *cols = plan.nw > 1 ? dplan + (size_t)w * 256 : nullptr;
-    const dim3 pgrid((unsigned)T, (unsigned)(KP / 32));
+    const dim3 pgrid((unsigned)T, (unsigned)(KP / 128));
     if (ways == 2)
       syrk_prep<2><<<pgrid, dim3(32, 8), 0, ctx->stream>>>(Z, ldz, wl[w], n, T, KP, dinv, tau,
                                                            cols, parts);
