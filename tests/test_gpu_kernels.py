@@ -88,16 +88,19 @@ def test_jacobi_eigensolver(ctx, k):
     assert np.linalg.norm(Vh.T @ Vh - np.eye(k)) < 1e-11
 
 
-@pytest.mark.parametrize("sym", [True, False])
-def test_gram_fp64_exact_products(ctx, sym):
-    rng = np.random.default_rng(7)
-    n, ka, kb = 10007, 70, 70 if sym else 33
-    A = rng.standard_normal((n, 72)).astype(np.float32)
-    B = A if sym else rng.standard_normal((n, 36)).astype(np.float32)
+# symmetric and general, narrow and wide (k = 400: seven 64-column tiles), ld > k
+@pytest.mark.parametrize("sym,ka,kb", [(True, 70, 70), (False, 70, 33), (True, 256, 256),
+                                       (False, 256, 256), (True, 400, 400), (False, 130, 200)])
+def test_gram_fp64_exact_products(ctx, sym, ka, kb):
+    rng = np.random.default_rng(7 + ka)
+    n = 10007
+    lda, ldb = ka + 2, kb + 3
+    A = rng.standard_normal((n, lda)).astype(np.float32)
+    B = A if sym else rng.standard_normal((n, ldb)).astype(np.float32)
     s = rng.random(n) + 0.5
     G = torch.empty((ka, kb), dtype=torch.float64, device="cuda")
     Ad, Bd, sd = dev(A), dev(B), dev(s)
-    _lib.check(ctx.lib.tsvm_test_gram(ctx.handle, P(Ad), 72, P(Bd), B.shape[1], n, ka, kb,
+    _lib.check(ctx.lib.tsvm_test_gram(ctx.handle, P(Ad), lda, P(Bd), B.shape[1], n, ka, kb,
                                       int(sym), P(sd), P(G)), "gram")
     ref = (A[:, :ka].astype(np.float64) * s[:, None]).T @ B[:, :kb].astype(np.float64)
     assert np.allclose(G.cpu().numpy(), ref, rtol=1e-12, atol=1e-9)
