@@ -393,8 +393,50 @@ def run_grid(args, ctx, stream):
     def factors(prec):
         return [api.factor(ctx, X, y, g, k, prec)[0] for X, y, g in zip(Xs, ys, gs)]
 
+    # the tensor-core factors on `factor_threads` host threads, one context and stream each
+    # (contexts are per host thread): the problems are independent and most are small, so one
+    # factorisation leaves most SMs idle.  Longest-first assignment by the estimated cost
+    # (n^2 for the kernel-block passes plus a fixed part); the main stream waits for all workers.
+    from concurrent.futures import ThreadPoolExecutor
+    nthreads = max(1, args.factor_threads)
+    workers = []
+    for _ in range(nthreads):
+        wctx, wst = _lib.Context(torch.cuda.current_device()), torch.cuda.Stream()
+        wctx.set_stream(wst.cuda_stream)
+        workers.append((wctx, wst))
+    cost = [float(X.shape[0]) ** 2 + 2.5e9 for X in Xs]
+    load = [0.0] * nthreads
+    assign = [[] for _ in range(nthreads)]
+    for i in sorted(range(len(Xs)), key=lambda i: -cost[i]):
+        w = min(range(nthreads), key=lambda w: load[w])
+        assign[w].append(i)
+        load[w] += cost[i]
+    dev_index = torch.cuda.current_device()
+
+    def factors_parallel(prec):
+        start = torch.cuda.Event()
+        start.record(stream)
+        out = [None] * len(Xs)
+
+        def work(w):
+            torch.cuda.set_device(dev_index)
+            wctx, wst = workers[w]
+            wst.wait_event(start)
+            with torch.cuda.stream(wst):
+                for i in assign[w]:
+                    out[i] = api.factor(wctx, Xs[i], ys[i], gs[i], k, prec)[0]
+            done = torch.cuda.Event()
+            done.record(wst)
+            return done
+
+        with ThreadPoolExecutor(nthreads) as ex:
+            evs = list(ex.map(work, range(nthreads)))
+        for ev in evs:
+            stream.wait_event(ev)
+        return out
+
     def batched():
-        Zs = factors(args.precision)
+        Zs = factors_parallel(args.precision)
         _, t_ipm = _timed(stream, lambda: api.ipm_batched(ctx, Zs, ys, k, Cs, rel_gap_tol=1e-6))
         return Zs, t_ipm
 
@@ -412,7 +454,9 @@ def run_grid(args, ctx, stream):
             (Zs, t_ipm), t = _timed(stream, batched)
             times.append(t)
             ipm_times.append(t_ipm)
-    _, t_fac = _timed(stream, lambda: factors(args.precision))
+    _, t_fac = _timed(stream, lambda: factors_parallel(args.precision))
+    factors(args.precision)   # the main context's scratch, sized before it is timed
+    _, t_fac_seq = _timed(stream, lambda: factors(args.precision))
     (alphas, bstats, info) = api.ipm_batched(ctx, Zs, ys, k, Cs, rel_gap_tol=1e-6)
     seq_stats, t_seq_ipm = _timed(stream, lambda: sequential(Zs, _lib.PREC_BF16))
     del Zs
@@ -422,10 +466,12 @@ def run_grid(args, ctx, stream):
     line = _base_line(args, "s for a 64-problem (C, gamma) grid: factors + batched IPM to rel. gap 1e-6",
                       sec, {"workload": "tanh_teacher_grid", "problems": 64, "rows_total": rows,
                             "n_min": min(X.shape[0] for X in Xs), "n_max": max(X.shape[0] for X in Xs),
-                            "d": 28, "k": k, "precision": args.precision})
+                            "d": 28, "k": k, "precision": args.precision,
+                            "factor_threads": nthreads})
     line.update({
         "dtype": f"{args.precision} kernel-block product, f32/f64 IPM",
-        "phases_s": {"factors": round(t_fac, 3), "batched_ipm": round(statistics.mean(ipm_times), 3),
+        "phases_s": {"factors": round(t_fac, 3), "factors_one_thread": round(t_fac_seq, 3),
+                     "batched_ipm": round(statistics.mean(ipm_times), 3),
                      "batched_ms_autotune": round(info["ms_autotune"], 1),
                      "unit_rows": info["unit_rows"], "units": info["units"],
                      "graph_used": info["graph_used"], "iters_max": info["iters_max"]},
@@ -437,6 +483,8 @@ def run_grid(args, ctx, stream):
         "iters": {"batched": [s["iters"] for s in bstats], "sequential": [s["iters"] for s in seq_stats]},
         "status_ok": sum(1 for s in bstats if s["status"] == _lib.OK),
         "step_s": [round(t, 3) for t in times], "clocks": clk.summary()})
+    for wctx, _ in workers:
+        wctx.close()
     return line
 
 
@@ -589,6 +637,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=16384)
     ap.add_argument("--ref-sample", type=int, default=262144)
+    ap.add_argument("--factor-threads", type=int, default=4,
+                    help="grid workload: host threads (one context each) for the 64 factors")
     ap.add_argument("--workload", default="two_gaussians", choices=["two_gaussians", "wide", "grid", "hypergrad"],
                     help="two_gaussians (default): the benchmark line; wide: n=500k d=54 k=400; "
                          "grid: 64-problem batched (C, gamma) grid; hypergrad: validation-loss "
