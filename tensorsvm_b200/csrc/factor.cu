@@ -76,6 +76,16 @@ __global__ void accumulate_r(const double *__restrict__ L, int k, const double *
   Rout[e] = s;
 }
 
+__global__ void fill_value(double *v, int64_t n, double value) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = value;
+}
+
+__global__ void set_scaled_identity(double *A, int k, double value) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < (int64_t)k * k) A[e] = (e / k == e % k) ? value : 0.0;
+}
+
 __global__ void set_identity(double *R, int k) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e < (int64_t)k * k) R[e] = (e / k == e % k) ? 1.0 : 0.0;
@@ -100,8 +110,12 @@ static tsvm_status kermatmul(tsvm_context *ctx, const float *Xc, const float *no
 }
 
 // Rkeep (2 k x k doubles, may be null): the combined factor R with (input W) = (output W) R.
+// tc_gram: steps 2 and 3 (W already near-orthonormal after the shifted first step) take their
+// Gram matrix from the tensor-core SYRK with a 3-way BF16 split (about FP32 accuracy, the
+// precision W is stored in) instead of the exact FP64 sum; the first, ill-conditioned step
+// always uses the exact FP64 Gram.
 static tsvm_status orthonormalise(tsvm_context *ctx, float *W, int64_t n, int k, int kp,
-                                  double *Rkeep) {
+                                  double *Rkeep, bool tc_gram = false) {
   double *G = nullptr, *Linv = nullptr;
   float *R32 = nullptr;
   int *info = nullptr;
@@ -119,7 +133,19 @@ static tsvm_status orthonormalise(tsvm_context *ctx, float *W, int64_t n, int k,
   for (int step = 0; step < 3; ++step) {
     double factor = step == 0 ? 11.0 * ((double)n * k + (double)k * (k + 1)) * u : 0.0;
     for (int attempt = 0; attempt < 4; ++attempt) {
-      TSVM_TRY(gram_fp64(ctx, W, kp, W, kp, n, k, k, true, G));
+      if (tc_gram && step > 0 && attempt == 0) {
+        // M = I + sum_j 1 * w_j w_j^T (every row on the tensor cores) plus the exact -I
+        double *ones = nullptr, *negI = nullptr;
+        TSVM_TRY(scratch_t(ctx, SLOT_IPM_VEC, (size_t)n, &ones));
+        TSVM_TRY(scratch_t(ctx, SLOT_SMALL3, (size_t)k * k, &negI));
+        fill_value<<<(unsigned)ceil_div(n, 256), 256, 0, ctx->stream>>>(ones, n, 1.0);
+        TSVM_LAUNCHED(ctx);
+        set_scaled_identity<<<gk, 256, 0, ctx->stream>>>(negI, k, -1.0);
+        TSVM_LAUNCHED(ctx);
+        TSVM_TRY(syrk_capacitance_tc(ctx, W, kp, n, k, ones, 2.0, 3, negI, G));
+      } else {
+        TSVM_TRY(gram_fp64(ctx, W, kp, W, kp, n, k, k, true, G));
+      }
       if (factor > 0) {
         shift_by_trace<<<1, 256, 0, ctx->stream>>>(G, k, factor);
         TSVM_LAUNCHED(ctx);
@@ -178,7 +204,9 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
   float km1 = 0.f, km2 = 0.f;
   TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, Q, kp, W, precision, &km1));
   TSVM_CUDA(cudaEventRecord(ev[2], ctx->stream));
-  TSVM_TRY(orthonormalise(ctx, W, n, k, kp, keep ? keep->R : nullptr));
+  const bool tc_gram = precision != TSVM_PREC_FP32 && keep == nullptr && syrk_tc_supported(k) &&
+                       k >= 32;
+  TSVM_TRY(orthonormalise(ctx, W, n, k, kp, keep ? keep->R : nullptr, tc_gram));
   if (keep)
     TSVM_CUDA(cudaMemcpyAsync(keep->W, W, sizeof(float) * n * kp, cudaMemcpyDeviceToDevice,
                               ctx->stream));
