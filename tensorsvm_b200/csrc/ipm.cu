@@ -157,7 +157,7 @@ __device__ __forceinline__ void ratio_update(double &m, double x, double s, doub
 }
 // Affine direction (T:1815-1820 with dx = dy b - r7) and its ratio test (T:1733-1739).
 struct AffineOp {
-  static constexpr int R = 0, NS = 0, NM = 1;
+  static constexpr int NS = 0, NM = 1;
   Vecs V;
   double C, dy;
   __device__ void load(const double *sc) { C = sc[I_C]; dy = sc[I_DYA]; }
@@ -174,7 +174,7 @@ struct AffineOp {
   }
 };
 struct MuAffOp {  // T:1741-1745
-  static constexpr int R = 0, NS = 1, NM = 0;
+  static constexpr int NS = 1, NM = 0;
   Vecs V;
   double C, al;
   __device__ void load(const double *sc) { C = sc[I_C]; al = sc[I_ALPHA_AFF]; }
@@ -212,7 +212,7 @@ struct CorrBackOp {
 };
 // Corrector direction, sum with the affine one (T:1759-1761), ratio test (T:1762-1769).
 struct CombineOp {
-  static constexpr int R = 0, NS = 0, NM = 1;
+  static constexpr int NS = 0, NM = 1;
   Vecs V;
   double C, smu, dyc;
   __device__ void load(const double *sc) {
@@ -235,7 +235,7 @@ struct CombineOp {
   }
 };
 struct UpdateOp {  // T:1772-1776; skipped when the Cholesky failed this iteration
-  static constexpr int R = 0, NS = 0, NM = 0;
+  static constexpr int NS = 0, NM = 0;
   Vecs V;
   double al;
   bool ok;
@@ -248,7 +248,7 @@ struct UpdateOp {  // T:1772-1776; skipped when the Cholesky failed this iterati
   }
 };
 struct FillOp {  // x = ox, s = xi = 1
-  static constexpr int R = 0, NS = 0, NM = 0;
+  static constexpr int NS = 0, NM = 0;
   Vecs V;
   double ox;
   __device__ void load(const double *sc) { ox = sc[I_Y]; }
@@ -260,7 +260,7 @@ struct FillOp {  // x = ox, s = xi = 1
 };
 // Bias (T:355-376): counts of SVs / free SVs; v = alpha on SVs for v = sum alpha_i Z_i.
 struct BiasCountOp {
-  static constexpr int R = 0, NS = 2, NM = 0;
+  static constexpr int NS = 2, NM = 0;
   const double *alpha;
   double C;
   __device__ void load(const double *) {}
@@ -298,7 +298,7 @@ struct StoreRowOp {  // dst = Z g
 // At the solution: D = s/x + xi/(C - x) of the final iterate, D^-1, and the SMW right-hand
 // sides c/D and a/D.
 struct AdjRowOp {
-  static constexpr int R = 0, NS = 0, NM = 0;
+  static constexpr int NS = 0, NM = 0;
   Vecs V;
   const double *c;
   double C;
@@ -328,7 +328,7 @@ struct AdjResidOp {
 };
 // lambda += t - dnu u with dnu = (a^T t + a^T lambda) / a^T u (t = S^-1 rho in r7, u in b)
 struct AdjUpdateOp {
-  static constexpr int R = 0, NS = 0, NM = 0;
+  static constexpr int NS = 0, NM = 0;
   Vecs V;
   double *lam;
   double dnu;
@@ -336,7 +336,7 @@ struct AdjUpdateOp {
   __device__ void row(int64_t i, double *, double *) const { lam[i] += V.r7[i] - dnu * V.b[i]; }
 };
 struct AdjLambdaOp {  // lambda = (D+Q)^-1 c - nu (D+Q)^-1 a, nu = a^T(D+Q)^-1 c / a^T(D+Q)^-1 a
-  static constexpr int R = 0, NS = 0, NM = 0;
+  static constexpr int NS = 0, NM = 0;
   Vecs V;
   double *lam;
   double nu;
@@ -364,11 +364,14 @@ __device__ __forceinline__ void block_partials(double *sums, double *mins, doubl
     if (lane == 0) sh[(NS + j) * kWarps + warp] = v;
   }
   __syncthreads();
-  if (threadIdx.x < NS + NM) {
-    const int j = threadIdx.x;
-    double r = j < NS ? 0.0 : INFINITY;
-    for (int w = 0; w < kWarps; ++w) r = j < NS ? r + sh[j * kWarps + w] : fmin(r, sh[j * kWarps + w]);
-    part_s[(int64_t)blockIdx.x * (NS + NM) + j] = r;
+  if constexpr (NS + NM > 0) {
+    if (threadIdx.x < NS + NM) {
+      const int j = threadIdx.x;
+      double r = j < NS ? 0.0 : INFINITY;
+      for (int w = 0; w < kWarps; ++w)
+        r = j < NS ? r + sh[j * kWarps + w] : fmin(r, sh[j * kWarps + w]);
+      part_s[(int64_t)blockIdx.x * (NS + NM) + j] = r;
+    }
   }
 }
 
