@@ -49,31 +49,6 @@ float event_ms(cudaEvent_t a, cudaEvent_t b) {
 }
 
 // Host-side linear model (w, b) from alpha, as writemodel does (tensorsvm-train.cu:301-332).
-static void linear_bias_host(const float *X, const float *y, const double *alpha, int64_t n,
-                             int d, double C, double *b_out) {
-  std::vector<double> w(d, 0.0);
-  std::vector<int64_t> freeidx;
-  for (int64_t i = 0; i < n; ++i) {
-    if (alpha[i] > 1e-6) {
-      for (int c = 0; c < d; ++c) w[c] += alpha[i] * y[i] * X[i * d + c];
-      if (alpha[i] < C - 1e-6) freeidx.push_back(i);
-    }
-  }
-  const int64_t m = std::min<int64_t>((int64_t)freeidx.size(), 5000);
-  double b = 0.0;
-  if (m > 0) {
-    double s = 0.0;
-    for (int64_t t = 0; t < m; ++t) {
-      const int64_t j = freeidx[t];
-      double v = y[j];
-      for (int c = 0; c < d; ++c) v -= w[c] * X[j * d + c];
-      s += v;
-    }
-    b = s / m;
-  }
-  *b_out = b;
-}
-
 }  // namespace tsvm
 
 using namespace tsvm;
@@ -263,10 +238,10 @@ tsvm_status tsvm_train(tsvm_context *ctx, const float *X, const float *y, int64_
     if (st != TSVM_OK && st != TSVM_WARN_ILL_CONDITIONED && st != TSVM_WARN_MAX_ITER &&
         st != TSVM_ERR_NOT_SPD)
       return st;
+    if (b_out) TSVM_TRY(linear_bias(ctx, dX, dy, dalpha, n, d, C, b_out));
     TSVM_CUDA(cudaMemcpyAsync(alpha_out, dalpha, sizeof(double) * n, cudaMemcpyDeviceToHost,
                               ctx->stream));
     TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (b_out) linear_bias_host(X, y, alpha_out, n, d, C, b_out);
   }
   return st;
 }

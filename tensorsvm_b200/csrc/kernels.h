@@ -23,6 +23,9 @@ tsvm_status centre_features(tsvm_context *ctx, const float *X, int64_t n, int d,
 tsvm_status pad_rows(tsvm_context *ctx, const float *src, int64_t lds, int64_t n, int k,
                      float *dst, int64_t ldd);
 // Z = diag(y) X padded to ldz columns (linear kernel, tensorsvm-train.cu:909-914).
+// Linear model bias (writemodel's rule) from device X (n x d), labels and alpha; b_host host.
+tsvm_status linear_bias(tsvm_context *ctx, const float *X, const float *y, const double *alpha,
+                        int64_t n, int d, double C, double *b_host);
 tsvm_status label_rows(tsvm_context *ctx, const float *X, const float *y, int64_t n, int d,
                        float *Z, int64_t ldz);
 
