@@ -432,32 +432,60 @@ jacobi_kernel(double *__restrict__ A0, double *__restrict__ A1, double *__restri
 // pair i and columns of pair j becomes J_i^T A_ij J_j, one block per thread with no conflicts
 // (blocks i > j are the transposes of i < j and are not stored), and rows p, q of Vt are rotated
 // alongside.  Same rotation formulas, ordering, tolerance and sweep limit as jacobi_kernel.
+// A round is bound by shared-memory wavefronts (at ne = 128: 2 x 2 block updates ~1450,
+// Vt rows 2048); pair indices and packed offsets are computed, not loaded, (c, s) is one
+// broadcast 16-byte load, and the rotations of round r + 1 (two warps, a chain of FP64
+// divisions and square roots) are computed while round r rotates the rows of Vt.
 constexpr int kJacobiSmallNe = 128;
 
-__device__ __forceinline__ int pk(int r, int c, const int *roff) {
-  return r >= c ? roff[r] + c : roff[c] + r;
+__device__ __forceinline__ int pk(int r, int c) {
+  return r >= c ? r * (r + 1) / 2 + c : c * (c + 1) / 2 + r;
+}
+
+// pair m of a round: (circle_player(m), circle_player(ne - 1 - m)); round < ne - 1 and
+// m < ne / 2 keep each sum below 2 (ne - 1), so one conditional subtraction is the modulo
+__device__ __forceinline__ void round_pair(int m, int round, int ne, int &p, int &q) {
+  int a = m - 1 + round;
+  if (a >= ne - 1) a -= ne - 1;
+  p = m == 0 ? 0 : 1 + a;
+  int b = ne - 2 - m + round;
+  if (b >= ne - 1) b -= ne - 1;
+  q = 1 + b;
 }
 
 __global__ void __launch_bounds__(1024, 1)
 jacobi_small_kernel(const double *__restrict__ A, int n, int lda, int ne, int max_sweeps,
                     double tol, double *__restrict__ w, double *__restrict__ V,
                     int *__restrict__ sweeps_out) {
-  extern __shared__ double jsh[];
+  extern __shared__ double2 jsh2[];
   const int np = ne / 2;
-  double *P = jsh;                                        // packed lower triangle
+  double2 *rot = jsh2;                                    // [2][np] (c, s), by round parity
+  double *red = reinterpret_cast<double *>(rot + 2 * np); // [64]
+  double *P = red + 64;                                   // packed lower triangle
   double *Vt = P + (size_t)ne * (ne + 1) / 2;             // ne x ne
-  double *cs = Vt + (size_t)ne * ne;                      // [np]
-  double *sn = cs + np;                                   // [np]
-  double *red = sn + np;                                  // [64]
-  int *pp = reinterpret_cast<int *>(red + 64);            // [np]
-  int *qq = pp + np;                                      // [np]
-  int *roff = qq + np;                                    // [ne]
-  for (int r = threadIdx.x; r < ne; r += blockDim.x) roff[r] = r * (r + 1) / 2;
-  __syncthreads();
   for (int r = threadIdx.x; r < ne; r += blockDim.x)
-    for (int c = 0; c <= r; ++c) P[roff[r] + c] = (r < n && c < n) ? A[(int64_t)r * lda + c] : 0.0;
+    for (int c = 0; c <= r; ++c)
+      P[r * (r + 1) / 2 + c] = (r < n && c < n) ? A[(int64_t)r * lda + c] : 0.0;
   for (int e = threadIdx.x; e < ne * ne; e += blockDim.x) Vt[e] = (e / ne == e % ne) ? 1.0 : 0.0;
   __syncthreads();
+  // rotations of `round` into dst (threads m < np: warps 0 and 1 at ne = 128)
+  auto rotations = [&](int round, double2 *dst) {
+    for (int m = threadIdx.x; m < np; m += blockDim.x) {
+      int p, q;
+      round_pair(m, round, ne, p, q);
+      const double app = P[pk(p, p)], aqq = P[pk(q, q)], apq = P[pk(p, q)];
+      double c = 1.0, sv = 0.0;
+      if (fabs(apq) > 1e-300) {
+        const double tau = (aqq - app) / (2.0 * apq);
+        double t;
+        if (fabs(tau) > 1e150) t = 0.5 / tau;
+        else t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+        c = 1.0 / sqrt(1.0 + t * t);
+        sv = t * c;
+      }
+      dst[m] = make_double2(c, sv);
+    }
+  };
   // this thread's 2 x 2 blocks (i, j), i <= j over the pairs (at most 3 at ne = 128), fixed
   // for the whole solve: enumerate the upper triangle of pairs row by row
   constexpr int kMaxB = 3;
@@ -475,31 +503,18 @@ jacobi_small_kernel(const double *__restrict__ A, int n, int lda, int ne, int ma
   const int dm = blockDim.x / ne, dc = blockDim.x % ne;
   int sweep = 0;
   for (sweep = 0; sweep < max_sweeps; ++sweep) {
+    rotations(0, rot);
+    __syncthreads();
     for (int round = 0; round < ne - 1; ++round) {
-      for (int m = threadIdx.x; m < np; m += blockDim.x) {
-        const int p = circle_player(m, round, ne), q = circle_player(ne - 1 - m, round, ne);
-        const double app = P[pk(p, p, roff)], aqq = P[pk(q, q, roff)], apq = P[pk(p, q, roff)];
-        double c = 1.0, sv = 0.0;
-        if (fabs(apq) > 1e-300) {
-          const double tau = (aqq - app) / (2.0 * apq);
-          double t;
-          if (fabs(tau) > 1e150) t = 0.5 / tau;
-          else t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-          c = 1.0 / sqrt(1.0 + t * t);
-          sv = t * c;
-        }
-        cs[m] = c;
-        sn[m] = sv;
-        pp[m] = p;
-        qq[m] = q;
-      }
-      __syncthreads();
+      const double2 *cur = rot + (round & 1) * np;
       for (int u = 0; u < nb; ++u) {
         const int i = bi[u], j = bj[u];
-        const int pi = pp[i], qi = qq[i], pj = pp[j], qj = qq[j];
-        const double ci = cs[i], si = sn[i], cj = cs[j], sj = sn[j];
-        const int i00 = pk(pi, pj, roff), i01 = pk(pi, qj, roff), i10 = pk(qi, pj, roff),
-                  i11 = pk(qi, qj, roff);
+        int pi, qi, pj, qj;
+        round_pair(i, round, ne, pi, qi);
+        round_pair(j, round, ne, pj, qj);
+        const double2 ri = cur[i], rj = cur[j];
+        const double ci = ri.x, si = ri.y, cj = rj.x, sj = rj.y;
+        const int i00 = pk(pi, pj), i01 = pk(pi, qj), i10 = pk(qi, pj), i11 = pk(qi, qj);
         const double a00 = P[i00], a01 = P[i01], a10 = P[i10], a11 = P[i11];
         // columns of pair j: (x_p, x_q) -> (c x_p - s x_q, s x_p + c x_q)
         const double b00 = cj * a00 - sj * a01, b01 = sj * a00 + cj * a01;
@@ -518,12 +533,18 @@ jacobi_small_kernel(const double *__restrict__ A, int n, int lda, int ne, int ma
           P[i11] = n11;
         }
       }
+      __syncthreads();
+      // the next round's rotations read the updated P and write the other parity slot, which
+      // nothing reads until the barrier below; Vt only needs this round's rotations
+      if (round + 1 < ne - 1) rotations(round + 1, rot + ((round + 1) & 1) * np);
       for (int m = m0, col = col0; m < np;) {
-        const double c = cs[m], sv = sn[m];
-        double *vp = Vt + (size_t)pp[m] * ne, *vq = Vt + (size_t)qq[m] * ne;
+        const double2 r = cur[m];
+        int p, q;
+        round_pair(m, round, ne, p, q);
+        double *vp = Vt + (size_t)p * ne, *vq = Vt + (size_t)q * ne;
         const double a = vp[col], bq = vq[col];
-        vp[col] = c * a - sv * bq;
-        vq[col] = sv * a + c * bq;
+        vp[col] = r.x * a - r.y * bq;
+        vq[col] = r.y * a + r.x * bq;
         m += dm;
         col += dc;
         if (col >= ne) { col -= ne; ++m; }
@@ -533,8 +554,9 @@ jacobi_small_kernel(const double *__restrict__ A, int n, int lda, int ne, int ma
     // convergence: off-diagonal mass against the diagonal
     double off = 0.0, dia = 0.0;
     for (int r = threadIdx.x; r < ne; r += blockDim.x) {
-      for (int c = 0; c < r; ++c) off += 2.0 * P[roff[r] + c] * P[roff[r] + c];
-      dia += P[roff[r] + r] * P[roff[r] + r];
+      const double *row = P + r * (r + 1) / 2;
+      for (int c = 0; c < r; ++c) off += 2.0 * row[c] * row[c];
+      dia += row[r] * row[r];
     }
     off = warp_sum(off);
     dia = warp_sum(dia);
@@ -554,7 +576,7 @@ jacobi_small_kernel(const double *__restrict__ A, int n, int lda, int ne, int ma
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     const int r = e / n, c = e % n;
     V[e] = Vt[(size_t)c * ne + r];
-    if (c == 0) w[r] = P[roff[r] + r];
+    if (c == 0) w[r] = P[r * (r + 1) / 2 + r];
   }
   if (threadIdx.x == 0) *sweeps_out = sweep;
 }
@@ -662,8 +684,8 @@ tsvm_status eig_jacobi_fp64(tsvm_context *ctx, double *A, int n, int lda, double
     int *sweeps_dev = nullptr;
     TSVM_TRY(scratch_t(ctx, SLOT_SMALL3, 4, &sweeps_dev));
     const int np = ne / 2;
-    const size_t smem = sizeof(double) * ((size_t)ne * (ne + 1) / 2 + (size_t)ne * ne + 2 * np + 64) +
-                        sizeof(int) * (2 * np + ne);
+    const size_t smem = sizeof(double2) * 2 * np +
+                        sizeof(double) * (64 + (size_t)ne * (ne + 1) / 2 + (size_t)ne * ne);
     TSVM_CUDA(cudaFuncSetAttribute(jacobi_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
     jacobi_small_kernel<<<1, 1024, smem, ctx->stream>>>(A, n, lda, ne, 40, 1e-13, w, V,

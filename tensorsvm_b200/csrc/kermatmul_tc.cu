@@ -458,11 +458,20 @@ __global__ void sumsq_partial(const float *__restrict__ A, int64_t count, double
 }
 
 // s = 2^round(-log2(rms)): puts the operand's RMS near 1 in FP16/BF16.
+// The partials are staged in shared memory by the whole block, then summed by one thread in
+// index order (the same sum on every run; a serial chain of global loads took ~20-60 us).
+constexpr int kStageMax = 2048;
+
 __global__ void choose_scale(const double *__restrict__ part, int nb, int64_t count,
                              float *__restrict__ scale) {
+  __shared__ double sp[kStageMax];
+  const int staged = nb < kStageMax ? nb : kStageMax;
+  for (int b = threadIdx.x; b < staged; b += blockDim.x) sp[b] = part[b];
+  __syncthreads();
   if (threadIdx.x != 0) return;
   double s = 0.0;
-  for (int b = 0; b < nb; ++b) s += part[b];
+  for (int b = 0; b < staged; ++b) s += sp[b];
+  for (int b = staged; b < nb; ++b) s += part[b];
   const double rms = sqrt(s / (double)(count > 0 ? count : 1));
   int e = 0;
   if (rms > 0.0 && isfinite(rms)) e = (int)lrint(-log2(rms));
@@ -581,12 +590,16 @@ kernel_mean_rows(const float *__restrict__ Xc, int64_t n, int d, int m, float ga
 constexpr double kShiftMinRatio = 16.0;
 
 // scale[2] = shift (the sampled mean, or 0 when the kernel is not flat enough to need it).
+// m <= kStageMax / 2 (the host caps the sample at 1024 rows).
 __global__ void kernel_mean_finish(const double *__restrict__ part, int m, float *scale) {
+  __shared__ double sp[kStageMax];
+  for (int i = threadIdx.x; i < 2 * m; i += blockDim.x) sp[i] = part[i];
+  __syncthreads();
   if (threadIdx.x != 0) return;
   double t = 0.0, t2 = 0.0;
   for (int i = 0; i < m; ++i) {
-    t += part[2 * i];
-    t2 += part[2 * i + 1];
+    t += sp[2 * i];
+    t2 += sp[2 * i + 1];
   }
   const double mm = (double)m * m;
   const double mean = t / mm, second = t2 / mm;
@@ -676,7 +689,7 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
   // SLOT_MISC: sum-of-squares partials [nb] | scale: s, 1/s, shift, - (4 floats) | err |
   // kernel-moment row sums [2 m] | column-sum partials [rg][kp] | ccol [kp floats]
   const int nb = ctx->num_sms * 2;
-  const int m = n < 1024 ? (int)n : 1024;
+  const int m = n < kStageMax / 2 ? (int)n : kStageMax / 2;
   const int rg = (int)(n_pad / 32 < (int64_t)nb ? n_pad / 32 : nb);
   const size_t o_samp = (size_t)nb + 8, o_cpart = o_samp + 2048;
   const size_t o_ccol = o_cpart + (size_t)rg * kp;
@@ -692,11 +705,11 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
   TSVM_LAUNCHED(ctx);
   sumsq_partial<<<nb, 256, 0, ctx->stream>>>(A, n * (int64_t)kp, part);
   TSVM_LAUNCHED(ctx);
-  choose_scale<<<1, 32, 0, ctx->stream>>>(part, nb, n * (int64_t)kp, scale);
+  choose_scale<<<1, 256, 0, ctx->stream>>>(part, nb, n * (int64_t)kp, scale);
   TSVM_LAUNCHED(ctx);
   kernel_mean_rows<<<m, 256, 0, ctx->stream>>>(Xc, n, d, m, (float)gamma, samp);
   TSVM_LAUNCHED(ctx);
-  kernel_mean_finish<<<1, 32, 0, ctx->stream>>>(samp, m, scale);
+  kernel_mean_finish<<<1, 256, 0, ctx->stream>>>(samp, m, scale);
   TSVM_LAUNCHED(ctx);
   float hshift = 0.f;   // picks the kernel instantiation
   TSVM_CUDA(cudaMemcpyAsync(&hshift, scale + 2, sizeof(float), cudaMemcpyDeviceToHost,
