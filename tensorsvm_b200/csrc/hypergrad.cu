@@ -44,28 +44,36 @@ constexpr int kKMaxD = 64;
 // (DERIV), for NU columns of U (FP64, nb x nu_total) and out (FP64, na x nu_total).  Each thread
 // keeps R rows of A in registers (rows blockIdx * 256 R + threadIdx + 256 r); a tile of 64 rows
 // of B (with their squared norms) and of U sits in shared memory and is read as broadcasts, four
-// features per load.  ||a - b||^2 = ||a||^2 + ||b||^2 - 2 a.b in FP32 (clamped at 0: the
-// relative error of the kernel value stays ~1e-7 gamma ||a||^2), each tile's 64 terms summed in
-// FP32, the tiles in FP64.  Block (x, y) sums the B rows [y jc, (y + 1) jc): with
-// gridDim.y > 1 its sums go to out + y * na * nu_total and kprod_reduce adds the splits in order.
+// features per load.  DC is d rounded up to a multiple of 4 (16 ... 32, or 64), so no FMA is
+// spent on padding at d = 18 or 28.  The exponent -gamma log2(e) ||a - b||^2 is one FMA chain:
+// it starts at -g (||a||^2 + ||b||^2) (g = gamma log2 e) and adds (2 g a) . b, the A rows being
+// scaled by 2 g once; it is clamped at 0 (the relative error of the kernel value stays ~1e-7
+// gamma ||a||^2).  DERIV weights by the exponent t = -g ||a - b||^2 and divides by g at the
+// end (t / g = -||a - b||^2).  Each tile's 64 terms are summed in FP32, the tiles in FP64.  Block (x, y) sums the B
+// rows [y jc, (y + 1) jc): with gridDim.y > 1 its sums go to out + y * na * nu_total and
+// kprod_reduce adds the splits in order.
 template <int DC, int R, int NU, bool DERIV>
 __global__ void __launch_bounds__(kKP)
 kprod_kernel(const float *__restrict__ A, int64_t na, const float *__restrict__ B, int64_t nb,
              int d, float gl2 /* gamma log2 e */, const double *__restrict__ U, int nu_total,
              int c0, int64_t jc, double *__restrict__ out) {
+  static_assert(DC % 4 == 0, "B rows are read as float4");
   __shared__ __align__(16) float Bs[kKT][DC];
   __shared__ float Bn[kKT];
   __shared__ float Us[kKT][NU];
   float a[R][DC], an[R];
+  const float g2 = 2.f * gl2;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int64_t i = (int64_t)blockIdx.x * kKP * R + threadIdx.x + kKP * r;
-    an[r] = 0.f;
+    float t = 0.f;
 #pragma unroll
     for (int c = 0; c < DC; ++c) {
-      a[r][c] = (i < na && c < d) ? A[i * d + c] : 0.f;
-      an[r] = fmaf(a[r][c], a[r][c], an[r]);
+      const float v = (i < na && c < d) ? A[i * d + c] : 0.f;
+      t = fmaf(v, v, t);
+      a[r][c] = g2 * v;
     }
+    an[r] = -gl2 * t;
   }
   double acc[R][NU];
 #pragma unroll
@@ -92,7 +100,7 @@ kprod_kernel(const float *__restrict__ A, int64_t na, const float *__restrict__ 
       float t = 0.f;
 #pragma unroll
       for (int c = 0; c < DC; ++c) t = fmaf(Bs[threadIdx.x][c], Bs[threadIdx.x][c], t);
-      Bn[threadIdx.x] = t;
+      Bn[threadIdx.x] = -gl2 * t;
     }
     __syncthreads();
     float part[R][NU];
@@ -102,28 +110,28 @@ kprod_kernel(const float *__restrict__ A, int64_t na, const float *__restrict__ 
       for (int u = 0; u < NU; ++u) part[r][u] = 0.f;
     const int jn = (int)(jend - j0 < kKT ? jend - j0 : kKT);
     for (int jj = 0; jj < jn; ++jj) {
-      float dot[R];
+      const float bn = Bn[jj];
+      float ex[R];
 #pragma unroll
-      for (int r = 0; r < R; ++r) dot[r] = 0.f;
+      for (int r = 0; r < R; ++r) ex[r] = an[r] + bn;
       const float4 *brow = reinterpret_cast<const float4 *>(&Bs[jj][0]);
 #pragma unroll
       for (int c4 = 0; c4 < DC / 4; ++c4) {
         const float4 bv = brow[c4];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          dot[r] = fmaf(a[r][4 * c4], bv.x, dot[r]);
-          dot[r] = fmaf(a[r][4 * c4 + 1], bv.y, dot[r]);
-          dot[r] = fmaf(a[r][4 * c4 + 2], bv.z, dot[r]);
-          dot[r] = fmaf(a[r][4 * c4 + 3], bv.w, dot[r]);
+          ex[r] = fmaf(a[r][4 * c4], bv.x, ex[r]);
+          ex[r] = fmaf(a[r][4 * c4 + 1], bv.y, ex[r]);
+          ex[r] = fmaf(a[r][4 * c4 + 2], bv.z, ex[r]);
+          ex[r] = fmaf(a[r][4 * c4 + 3], bv.w, ex[r]);
         }
       }
-      const float bn = Bn[jj];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const float d2 = fmaxf(fmaf(-2.f, dot[r], an[r] + bn), 0.f);
+        const float t = fminf(ex[r], 0.f);
         float e;
-        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(-gl2 * d2));
-        if (DERIV) e *= -d2;
+        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(t));
+        if (DERIV) e *= t;
 #pragma unroll
         for (int u = 0; u < NU; ++u) part[r][u] = fmaf(e, Us[jj][u], part[r][u]);
       }
@@ -133,13 +141,14 @@ kprod_kernel(const float *__restrict__ A, int64_t na, const float *__restrict__ 
 #pragma unroll
       for (int u = 0; u < NU; ++u) acc[r][u] += (double)part[r][u];
   }
+  const double w = DERIV ? 1.0 / (double)gl2 : 1.0;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int64_t i = (int64_t)blockIdx.x * kKP * R + threadIdx.x + kKP * r;
     if (i < na) {
 #pragma unroll
       for (int u = 0; u < NU; ++u)
-        if (c0 + u < nu_total) out[i * nu_total + c0 + u] = acc[r][u];
+        if (c0 + u < nu_total) out[i * nu_total + c0 + u] = DERIV ? w * acc[r][u] : acc[r][u];
     }
   }
 }
@@ -186,6 +195,10 @@ tsvm_status kprod(tsvm_context *ctx, const float *A, int64_t na, const float *B,
   const float gl2 = (float)(gamma * 1.4426950408889634);
   constexpr int R32 = NU == 1 ? 4 : NU == 8 ? 2 : 1;
   constexpr int R64 = NU == 1 ? 2 : 1;
+  if (d <= 16) return kprod_launch<16, R32, NU, DERIV>(ctx, A, na, B, nb, d, gl2, U, nu_total, out);
+  if (d <= 20) return kprod_launch<20, R32, NU, DERIV>(ctx, A, na, B, nb, d, gl2, U, nu_total, out);
+  if (d <= 24) return kprod_launch<24, R32, NU, DERIV>(ctx, A, na, B, nb, d, gl2, U, nu_total, out);
+  if (d <= 28) return kprod_launch<28, R32, NU, DERIV>(ctx, A, na, B, nb, d, gl2, U, nu_total, out);
   if (d <= 32) return kprod_launch<32, R32, NU, DERIV>(ctx, A, na, B, nb, d, gl2, U, nu_total, out);
   return kprod_launch<64, R64, NU, DERIV>(ctx, A, na, B, nb, d, gl2, U, nu_total, out);
 }
