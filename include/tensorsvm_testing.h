@@ -44,6 +44,13 @@ tsvm_status tsvm_test_syrk_mixed(tsvm_context *ctx, const float *Z, int32_t ldz,
                                  int32_t k, const double *dinv, double tau, int32_t ways,
                                  double *M, int32_t *exact_rows);
 
+/* One cooperative launch of `blocks` blocks (<= the SM count) meeting once at the grid barrier of
+ * the cooperative eigensolver, which expects `arrivals` blocks and polls at most `max_spins`
+ * (<= 2^24) times.  *released_blocks: how many were released.  Returns TSVM_ERR_TIMEOUT when the
+ * wait ran out (arrivals > blocks: an arrival that never comes), the context staying usable. */
+tsvm_status tsvm_test_grid_barrier(tsvm_context *ctx, int32_t blocks, int32_t arrivals,
+                                   int64_t max_spins, int32_t *released_blocks);
+
 #ifdef __cplusplus
 }
 #endif

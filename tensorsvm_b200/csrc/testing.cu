@@ -5,7 +5,23 @@
 #include "kernels.h"
 #include "tensorsvm_testing.h"
 
+#include <vector>
+
 using namespace tsvm;
+
+namespace {
+
+// Every block arrives once at a grid barrier that expects `arrivals` blocks and records whether
+// it was released.  With arrivals > gridDim.x the last arrival never comes: each block gives up
+// after max_spins polls, sets the barrier's error flag and returns (the bounded wait of the
+// cooperative eigensolver, made to run out).
+__global__ void barrier_probe(GridBarrier *gb, unsigned int arrivals, long long max_spins,
+                              int *released) {
+  const bool ok = grid_sync(gb, arrivals, max_spins);
+  if (threadIdx.x == 0) released[blockIdx.x] = ok ? 1 : 0;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -103,6 +119,32 @@ tsvm_status tsvm_test_syrk_mixed(tsvm_context *ctx, const float *Z, int32_t ldz,
   TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
   if (exact_rows) *exact_rows = h;
   return TSVM_OK;
+}
+
+tsvm_status tsvm_test_grid_barrier(tsvm_context *ctx, int32_t blocks, int32_t arrivals,
+                                   int64_t max_spins, int32_t *released_blocks) {
+  if (!ctx || blocks < 1 || blocks > ctx->num_sms || arrivals < 1 || max_spins < 1 ||
+      max_spins > (1ll << 24))
+    return TSVM_ERR_INVALID_ARGUMENT;
+  int *buf = nullptr;   // GridBarrier (4 ints) | released[blocks]
+  TSVM_TRY(scratch_t(ctx, SLOT_MISC, (size_t)blocks + 4, &buf));
+  TSVM_CUDA(cudaMemsetAsync(buf, 0, sizeof(int) * ((size_t)blocks + 4), ctx->stream));
+  GridBarrier *gb = reinterpret_cast<GridBarrier *>(buf);
+  int *released = buf + 4;
+  unsigned int arr = (unsigned int)arrivals;
+  long long spins = max_spins;
+  void *args[] = {&gb, &arr, &spins, &released};
+  TSVM_CUDA(cudaLaunchCooperativeKernel((const void *)barrier_probe, dim3((unsigned)blocks),
+                                        dim3(64), args, 0, ctx->stream));
+  TSVM_LAUNCHED(ctx);
+  std::vector<int> h((size_t)blocks + 4);
+  TSVM_CUDA(cudaMemcpyAsync(h.data(), buf, sizeof(int) * h.size(), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  int n = 0;
+  for (int b = 0; b < blocks; ++b) n += h[4 + b];
+  if (released_blocks) *released_blocks = n;
+  return h[2] ? TSVM_ERR_TIMEOUT : TSVM_OK;   // GridBarrier::error
 }
 
 }  // extern "C"

@@ -88,6 +88,24 @@ def test_jacobi_eigensolver(ctx, k):
     assert np.linalg.norm(Vh.T @ Vh - np.eye(k)) < 1e-11
 
 
+def test_grid_barrier_wait_runs_out_and_context_stays_usable(ctx):
+    # the cooperative eigensolver's grid barrier with an arrival that never comes: every block
+    # gives up after its bounded poll count, the error flag reads back as a status, and the same
+    # context then runs a barrier that completes and a solve
+    released = ctypes.c_int32(-1)
+    st = ctx.lib.tsvm_test_grid_barrier(ctx.handle, 8, 9, 1 << 14, ctypes.byref(released))
+    assert st == _lib.ERR_TIMEOUT and released.value == 0
+    st = ctx.lib.tsvm_test_grid_barrier(ctx.handle, 8, 8, 1 << 14, ctypes.byref(released))
+    assert st == _lib.OK and released.value == 8
+    S = np.diag(np.arange(1.0, 9.0))
+    w = torch.empty(8, dtype=torch.float64, device="cuda")
+    V = torch.empty((8, 8), dtype=torch.float64, device="cuda")
+    sweeps = ctypes.c_int32(0)
+    _lib.check(ctx.lib.tsvm_test_eig(ctx.handle, P(dev(S)), 8, P(w), P(V), ctypes.byref(sweeps)),
+               "eig")
+    assert np.allclose(np.sort(w.cpu().numpy()), np.arange(1.0, 9.0))
+
+
 # symmetric and general, narrow and wide (k = 400: seven 64-column tiles), ld > k
 @pytest.mark.parametrize("sym,ka,kb", [(True, 70, 70), (False, 70, 33), (True, 256, 256),
                                        (False, 256, 256), (True, 400, 400), (False, 130, 200)])

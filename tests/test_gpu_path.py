@@ -133,6 +133,17 @@ def test_rel_gap_stop_and_stats(ctx, c1, c1_factor):
     assert st["rel_gap"] <= 1e-6 and st["t_rel_gap_1e6_ms"] > 0
 
 
+def test_ipm_iteration_cap_returns_its_own_status(ctx, c1, c1_factor):
+    # the reference's 100-iteration cap (T:1603) as a distinct warning, outputs still valid
+    X, y, g, C, k = c1
+    Z, _ = c1_factor
+    alpha, _, _, st = api.ipm(ctx, Z, dev(y), k, C, max_iter=3)
+    assert st["status_code"] == _lib.WARN_MAX_ITER
+    assert st["iters"] == 3
+    a = alpha.cpu().numpy()
+    assert np.all(np.isfinite(a)) and a.min() > 0.0 and a.max() < C
+
+
 def test_ipm_nan_input_reports_not_spd(ctx):
     X, y = synth.two_gaussians(256, 3, seed=2)
     Z = torch.zeros((256, 64), dtype=torch.float32, device="cuda")
