@@ -117,6 +117,35 @@ def test_mpc_two_point_known_answer():
     assert np.allclose(w, [1.0, 0.0], atol=1e-6) and abs(b) < 1e-6
 
 
+def test_mpc_four_point_known_answer():
+    # x = +-1 and +-2 on a line, labels by sign: the hard-margin support vectors are +-1 with
+    # alpha = 2/||x+ - x-||^2 = 0.5, the outer points carry alpha = 0; w = (1, 0), b = 0
+    X = np.array([[1.0, 0.0], [-1.0, 0.0], [2.0, 0.0], [-2.0, 0.0]])
+    y = np.array([1.0, -1.0, 1.0, -1.0])
+    r = orc.mpc(X * y[:, None], y, 10.0, kernel="linear", tol=1e-10)
+    assert r.status in ("converged", "ill_conditioned")
+    assert np.allclose(r.x, [0.5, 0.5, 0.0, 0.0], atol=1e-6)
+    w, b = orc.linear_w_b(X, y, r.x, 10.0)
+    assert np.allclose(w, [1.0, 0.0], atol=1e-6) and abs(b) < 1e-6
+
+
+def test_rbf_full_rank_matches_sklearn_exact_kernel():
+    # k = n: the factor reproduces the labelled kernel, so the dual is the exact-kernel SVM's;
+    # sklearn's SVC (libsvm SMO) is an independent solver of it
+    from sklearn.svm import SVC
+    X, y = synth.two_gaussians(160, 4, seed=11)
+    g, C = 0.3, 2.0
+    f = orc.lra(X, y, g, 160)
+    r = orc.mpc(f.U, y, C, tol=1e-10)
+    K = orc.labelled_kernel(X, y, g)
+    m = SVC(kernel="rbf", gamma=g, C=C, tol=1e-12).fit(X.astype(np.float64), y)
+    a = np.zeros(len(y))
+    a[m.support_] = np.abs(m.dual_coef_.ravel())
+    obj = lambda al: 0.5 * al @ K @ al - al.sum()
+    assert abs(obj(r.x) - obj(a)) / abs(obj(a)) < 1e-7   # measured 3.8e-9
+    assert jaccard(set(np.where(r.x > 1e-6 * C)[0]), set(m.support_)) > 0.98   # measured 0.991
+
+
 def test_mpc_linear_matches_sklearn_objective():
     from sklearn.svm import SVC
     X, y = synth.two_gaussians(400, 5, seed=3)
