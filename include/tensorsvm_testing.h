@@ -44,6 +44,11 @@ tsvm_status tsvm_test_syrk_mixed(tsvm_context *ctx, const float *Z, int32_t ldz,
                                  int32_t k, const double *dinv, double tau, int32_t ways,
                                  double *M, int32_t *exact_rows);
 
+/* Allocation-failure injection: after `after` more device allocations of ctx's scratch (0: the
+ * next one), growing a scratch buffer returns TSVM_ERR_OUT_OF_MEMORY instead of calling
+ * cudaMalloc; -1 switches the hook off.  The context stays usable. */
+tsvm_status tsvm_test_fail_alloc(tsvm_context *ctx, int32_t after);
+
 /* One cooperative launch of `blocks` blocks (<= the SM count) meeting once at the grid barrier of
  * the cooperative eigensolver, which expects `arrivals` blocks and polls at most `max_spins`
  * (<= 2^24) times.  *released_blocks: how many were released.  Returns TSVM_ERR_TIMEOUT when the

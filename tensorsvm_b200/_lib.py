@@ -46,7 +46,7 @@ EXPORTS = [
 TEST_EXPORTS = [
     "tsvm_test_rand_stream", "tsvm_test_sketch", "tsvm_test_kermatmul", "tsvm_test_chol",
     "tsvm_test_potrs", "tsvm_test_eig", "tsvm_test_gram", "tsvm_test_syrk_mixed",
-    "tsvm_test_grid_barrier",
+    "tsvm_test_grid_barrier", "tsvm_test_fail_alloc",
 ]
 
 
@@ -185,6 +185,7 @@ def load() -> ctypes.CDLL:
         "tsvm_test_gram": [P, P, I64, P, I64, I64, I32, I32, I32, P, P],
         "tsvm_test_syrk_mixed": [P, P, I32, I64, I32, P, D, I32, P, ctypes.POINTER(I32)],
         "tsvm_test_grid_barrier": [P, I32, I32, I64, ctypes.POINTER(I32)],
+        "tsvm_test_fail_alloc": [P, I32],
     }.items():
         fn = getattr(lib, name)
         fn.restype = ctypes.c_int

@@ -32,6 +32,8 @@ tsvm_status scratch(tsvm_context *ctx, Slot s, size_t bytes, void **out) {
       ctx->buf[s] = nullptr;
       ctx->bytes[s] = 0;
     }
+    // test hook (tsvm_test_fail_alloc): the allocation after the next `alloc_fail_after` fails
+    if (ctx->alloc_fail_after >= 0 && ctx->alloc_fail_after-- == 0) return TSVM_ERR_OUT_OF_MEMORY;
     void *p = nullptr;
     TSVM_CUDA(cudaMalloc(&p, bytes));
     ctx->buf[s] = p;
@@ -47,8 +49,6 @@ float event_ms(cudaEvent_t a, cudaEvent_t b) {
   cudaEventElapsedTime(&ms, a, b);
   return ms;
 }
-
-// Host-side linear model (w, b) from alpha, as writemodel does (tensorsvm-train.cu:301-332).
 }  // namespace tsvm
 
 using namespace tsvm;

@@ -72,6 +72,9 @@ struct tsvm_context {
   double *host_scalars = nullptr;
   // width k whose column-window table SLOT_SYRK_PLAN holds (-1: none)
   int syrk_plan_k = -1;
+  // test hook: scratch growth fails with TSVM_ERR_OUT_OF_MEMORY after this many more device
+  // allocations (-1: never)
+  int alloc_fail_after = -1;
   // the last RBF tsvm_train (its X, y in SLOT_DEV_IN and Z in SLOT_DEV_Z), for -analysis
   struct {
     bool valid = false;

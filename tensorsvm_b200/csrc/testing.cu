@@ -121,6 +121,12 @@ tsvm_status tsvm_test_syrk_mixed(tsvm_context *ctx, const float *Z, int32_t ldz,
   return TSVM_OK;
 }
 
+tsvm_status tsvm_test_fail_alloc(tsvm_context *ctx, int32_t after) {
+  if (!ctx || after < -1) return TSVM_ERR_INVALID_ARGUMENT;
+  ctx->alloc_fail_after = after;
+  return TSVM_OK;
+}
+
 tsvm_status tsvm_test_grid_barrier(tsvm_context *ctx, int32_t blocks, int32_t arrivals,
                                    int64_t max_spins, int32_t *released_blocks) {
   if (!ctx || blocks < 1 || blocks > ctx->num_sms || arrivals < 1 || max_spins < 1 ||

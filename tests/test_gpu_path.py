@@ -144,6 +144,24 @@ def test_ipm_iteration_cap_returns_its_own_status(ctx, c1, c1_factor):
     assert np.all(np.isfinite(a)) and a.min() > 0.0 and a.max() < C
 
 
+def test_allocation_failure_returns_status_and_context_recovers():
+    # injected on the host, in a fresh context (every scratch buffer still to be allocated):
+    # the failing allocation surfaces as TSVM_ERR_OUT_OF_MEMORY, not a crash, at the first
+    # allocation and in the middle of a factorisation; with the hook off the same context works
+    X, y = synth.two_gaussians(2000, 8, seed=4)
+    with _lib.Context(0) as c:
+        Xd, yd = dev(X), dev(y)
+        for after in (0, 3):
+            _lib.check(c.lib.tsvm_test_fail_alloc(c.handle, after), "fail_alloc")
+            with pytest.raises(_lib.TsvmError) as err:
+                api.factor(c, Xd, yd, 0.1, 32, "fp32")
+            assert err.value.status == _lib.ERR_OUT_OF_MEMORY
+        _lib.check(c.lib.tsvm_test_fail_alloc(c.handle, -1), "fail_alloc")
+        Z, info = api.factor(c, Xd, yd, 0.1, 32, "fp32")
+        alpha, _, _, st = api.ipm(c, Z, yd, 32, 1.0, rel_gap_tol=1e-6)
+        assert st["status_code"] == _lib.OK and bool(torch.isfinite(alpha).all())
+
+
 def test_ipm_nan_input_reports_not_spd(ctx):
     X, y = synth.two_gaussians(256, 3, seed=2)
     Z = torch.zeros((256, 64), dtype=torch.float32, device="cuda")
