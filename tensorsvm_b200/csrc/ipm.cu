@@ -1105,7 +1105,7 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
     double oxv = ox;
     TSVM_CUDA(cudaMemcpyAsync(run.scal + I_Y, &oxv, sizeof(double), cudaMemcpyHostToDevice,
                               ctx->stream));
-    TSVM_TRY(run.vec(FillOp{V}, ST_NONE));
+    TSVM_TRY(run.vec(FillOp{V, 0.0}, ST_NONE));
     double zero = 0.0;
     TSVM_CUDA(cudaMemcpyAsync(run.scal + I_Y, &zero, sizeof(double), cudaMemcpyHostToDevice,
                               ctx->stream));
@@ -1823,7 +1823,7 @@ tsvm_status ipm_solve_batched(tsvm_context *ctx, const tsvm_ipm_problem *pr, int
   }
   TSVM_CUDA(cudaMemcpyAsync(scal, hsc.data(), sizeof(double) * hsc.size(), cudaMemcpyHostToDevice,
                             ctx->stream));
-  TSVM_TRY(br.vec(FillOp{V}, ST_NONE));
+  TSVM_TRY(br.vec(FillOp{V, 0.0}, ST_NONE));
   for (int p = 0; p < P; ++p) hsc[(size_t)p * kNScal + I_Y] = 0.0;
   TSVM_CUDA(cudaMemcpyAsync(scal, hsc.data(), sizeof(double) * hsc.size(), cudaMemcpyHostToDevice,
                             ctx->stream));
