@@ -4,6 +4,7 @@
 #   make oracle     -> oracle/_build/liboracle_sketch.so
 #   make reference  -> oracle/_ref/tensorsvm-train-ref (needs the reference source)
 NVCC      ?= nvcc
+CUDA_HOME ?= /usr/local/cuda
 ARCH      := -gencode arch=compute_100a,code=sm_100a
 NVFLAGS   := -O3 -std=c++17 $(ARCH) -lineinfo -Xcompiler -fPIC -Iinclude -Itensorsvm_b200/csrc \
              --expt-relaxed-constexpr -Xptxas -warn-spills
@@ -23,9 +24,9 @@ $(OBJDIR)/%.o: tensorsvm_b200/csrc/%.cu $(HDRS)
 	@mkdir -p $(OBJDIR)
 	$(NVCC) $(NVFLAGS) -c $< -o $@
 
-$(OBJDIR)/%.host.o: tensorsvm_b200/csrc/%.cpp include/tensorsvm.h
+$(OBJDIR)/%.host.o: tensorsvm_b200/csrc/%.cpp include/tensorsvm.h tensorsvm_b200/csrc/trace.h
 	@mkdir -p $(OBJDIR)
-	g++ -O3 -std=c++17 -fPIC -pthread -Wall -Iinclude -c $< -o $@
+	g++ -O3 -std=c++17 -fPIC -pthread -Wall -Iinclude -I$(CUDA_HOME)/include -c $< -o $@
 
 $(LIB): $(OBJS)
 	@mkdir -p $(dir $@)

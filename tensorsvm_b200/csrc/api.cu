@@ -10,6 +10,7 @@
 #include "common.cuh"
 #include "context.h"
 #include "kernels.h"
+#include "trace.h"
 
 namespace tsvm {
 
@@ -135,6 +136,7 @@ tsvm_status tsvm_factor(tsvm_context *ctx, const float *X, const float *y, int64
   if (!ctx || !X || !y || !Z) return TSVM_ERR_INVALID_ARGUMENT;
   if (precision < TSVM_PREC_FP32 || precision > TSVM_PREC_FP16) return TSVM_ERR_INVALID_ARGUMENT;
   TSVM_CUDA(cudaSetDevice(ctx->device));
+  TraceRange tr("tsvm_factor");
   return factor_rbf(ctx, X, y, n, d, gamma, k, precision, sketch, Q_user, Z, ldz, info);
 }
 
@@ -159,6 +161,7 @@ tsvm_status tsvm_ipm(tsvm_context *ctx, const float *Z, int32_t ldz, const float
   if (opt) o = *opt;
   if (o.max_iter < 0 || !(o.tol > 0)) return TSVM_ERR_INVALID_ARGUMENT;
   TSVM_CUDA(cudaSetDevice(ctx->device));
+  TraceRange tr("tsvm_ipm");
   return ipm_solve(ctx, Z, ldz, y, n, k, C, o, alpha_out, xi_out, s_out, ymult_out, stats);
 }
 
@@ -178,6 +181,7 @@ tsvm_status tsvm_ipm_batched(tsvm_context *ctx, const tsvm_ipm_problem *problems
   if (opt) o = *opt;
   if (o.max_iter < 0 || !(o.tol > 0)) return TSVM_ERR_INVALID_ARGUMENT;
   TSVM_CUDA(cudaSetDevice(ctx->device));
+  TraceRange tr("tsvm_ipm_batched");
   return ipm_solve_batched(ctx, problems, count, k, ldz, o, stats, info);
 }
 
@@ -186,6 +190,7 @@ tsvm_status tsvm_bias(tsvm_context *ctx, const float *Z, int32_t ldz, const floa
                       double *b_std_out, int32_t *n_sv, int32_t *n_free) {
   if (!ctx || !Z || !y || !alpha || n < 1 || k < 1 || ldz < k) return TSVM_ERR_INVALID_ARGUMENT;
   TSVM_CUDA(cudaSetDevice(ctx->device));
+  TraceRange tr("tsvm_bias");
   return bias_rbf(ctx, Z, ldz, y, alpha, n, k, C, b_out, b_std_out, n_sv, n_free);
 }
 
@@ -196,6 +201,7 @@ tsvm_status tsvm_train(tsvm_context *ctx, const float *X, const float *y, int64_
   if (!ctx || !X || !y || !alpha_out || n < 2 || d < 1) return TSVM_ERR_INVALID_ARGUMENT;
   if (kernel != TSVM_KERNEL_LINEAR && kernel != TSVM_KERNEL_RBF) return TSVM_ERR_UNSUPPORTED;
   TSVM_CUDA(cudaSetDevice(ctx->device));
+  TraceRange tr("tsvm_train");
   tsvm_ipm_options o;
   tsvm_ipm_default_options(&o);
   if (opt) o = *opt;
@@ -256,6 +262,7 @@ tsvm_status tsvm_decision_values(tsvm_context *ctx, const tsvm_model_view *model
     return TSVM_ERR_INVALID_ARGUMENT;
   if (m == 0) return TSVM_OK;
   TSVM_CUDA(cudaSetDevice(ctx->device));
+  TraceRange tr("tsvm_decision_values");
   TSVM_TRY(decision_values(ctx, model, X, m, f));
   TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
   return TSVM_OK;

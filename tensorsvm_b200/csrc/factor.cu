@@ -19,6 +19,7 @@
 #include "common.cuh"
 #include "context.h"
 #include "kernels.h"
+#include "trace.h"
 
 namespace tsvm {
 namespace {
@@ -181,6 +182,8 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
   if (k > n) return TSVM_ERR_INVALID_ARGUMENT;
   const int kp = (int)round_up(k, 64);
   cudaEvent_t *ev = ctx->ev;
+  TracePhases phase;
+  phase.next("factor: sketch");
   TSVM_CUDA(cudaEventRecord(ev[0], ctx->stream));
   float *Xc = nullptr, *Q = nullptr, *W = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_XC, (size_t)n * d + (size_t)n + 64, &Xc));
@@ -201,9 +204,11 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
     TSVM_CUDA(cudaMemcpyAsync(keep->omega, Q, sizeof(float) * n * kp, cudaMemcpyDeviceToDevice,
                               ctx->stream));
   TSVM_CUDA(cudaEventRecord(ev[1], ctx->stream));
+  phase.next("factor: kernel-block pass 1");
   float km1 = 0.f, km2 = 0.f;
   TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, Q, kp, W, precision, &km1));
   TSVM_CUDA(cudaEventRecord(ev[2], ctx->stream));
+  phase.next("factor: orthonormalise");
   const bool tc_gram = precision != TSVM_PREC_FP32 && keep == nullptr && syrk_tc_supported(k) &&
                        k >= 32;
   TSVM_TRY(orthonormalise(ctx, W, n, k, kp, keep ? keep->R : nullptr, tc_gram));
@@ -211,11 +216,13 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
     TSVM_CUDA(cudaMemcpyAsync(keep->W, W, sizeof(float) * n * kp, cudaMemcpyDeviceToDevice,
                               ctx->stream));
   TSVM_CUDA(cudaEventRecord(ev[3], ctx->stream));
+  phase.next("factor: kernel-block pass 2");
   // the second pass rounds the orthonormal basis W to the tensor-core operand type in place:
   // C = W^T (K W) and Z = W V diag(sqrt w) then use the W the tensor cores contracted, so the
   // weak eigen-directions of C do not pick up the rounding of one side only
   TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, W, kp, Q, precision, &km2, W));
   TSVM_CUDA(cudaEventRecord(ev[4], ctx->stream));
+  phase.next("factor: projection and eigensolver");
   double *Cm = nullptr, *V = nullptr, *w = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_SMALL, (size_t)k * k + 8, &Cm));
   TSVM_TRY(scratch_t(ctx, SLOT_SMALL2, (size_t)k * k + (size_t)k, &V));

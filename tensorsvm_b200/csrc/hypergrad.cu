@@ -32,6 +32,7 @@
 #include "common.cuh"
 #include "context.h"
 #include "kernels.h"
+#include "trace.h"
 
 namespace tsvm {
 namespace {
@@ -374,6 +375,7 @@ extern "C" tsvm_status tsvm_hypergrad(tsvm_context *ctx, const float *X, const f
     return TSVM_ERR_INVALID_ARGUMENT;
   if (precision < TSVM_PREC_FP32 || precision > TSVM_PREC_FP16) return TSVM_ERR_INVALID_ARGUMENT;
   TSVM_CUDA(cudaSetDevice(ctx->device));
+  TraceRange trace_call("tsvm_hypergrad");
   const auto t0 = std::chrono::steady_clock::now();
   cudaStream_t st = ctx->stream;
   const int kp = (int)round_up(k, 64);

@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "tensorsvm.h"
+#include "trace.h"
 
 namespace {
 
@@ -174,6 +175,7 @@ tsvm_status tsvm_read_libsvm(const char *path, int32_t scale256, int32_t threads
   *labels = nullptr;
   *X = nullptr;
   if (bad_line) *bad_line = 0;
+  tsvm::TraceRange trace_call("tsvm_read_libsvm");
   std::string text;
   if (!read_file(path, text)) return TSVM_ERR_IO;
   const int nt = pick_threads(threads);
@@ -238,6 +240,7 @@ tsvm_status tsvm_write_model(const char *path, int32_t kernel, const float *X, c
                              int64_t *n_free) {
   if (!path || !X || !y || !alpha || n < 0 || d < 1) return TSVM_ERR_INVALID_ARGUMENT;
   if (kernel != TSVM_KERNEL_RBF && kernel != TSVM_KERNEL_LINEAR) return TSVM_ERR_UNSUPPORTED;
+  tsvm::TraceRange trace_call("tsvm_write_model");
   std::vector<int64_t> sv;
   int64_t nfree = 0;
   for (int64_t i = 0; i < n; ++i)

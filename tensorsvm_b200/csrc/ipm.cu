@@ -28,6 +28,7 @@
 #include "context.h"
 #include "kernels.h"
 #include "tc_common.cuh"
+#include "trace.h"
 
 namespace tsvm {
 namespace {
@@ -1124,6 +1125,7 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
   double sc[kNScal];
   double t_gap = -1.0;
   for (iter = 0; iter < opt.max_iter; ++iter) {
+    TraceRange trace_iter("ipm iteration");
     TSVM_TRY(run.zt(BeginOp{V, C}, q, ST_BEGIN));
     TSVM_TRY(run.zw(ResidOp{V, 0.0}, q, ST_RESID));
     TSVM_CUDA(cudaMemcpyAsync(ctx->host_scalars, run.scal, sizeof(double) * kNScal,
@@ -1906,6 +1908,7 @@ tsvm_status ipm_solve_batched(tsvm_context *ctx, const tsvm_ipm_problem *pr, int
   int iter = 0, iters_max = 0;
   tsvm_status result = TSVM_OK;
   for (iter = 0;; ++iter) {
+    TraceRange trace_iter("batched ipm iteration");
     TSVM_TRY(pull());
     TSVM_CUDA(cudaMemcpyAsync(hinfo.data(), d_info, sizeof(int) * (P + 1), cudaMemcpyDeviceToHost,
                               ctx->stream));
