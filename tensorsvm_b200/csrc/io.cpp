@@ -3,9 +3,11 @@
 // The reference reads its training file with two single-threaded strtok/strtod passes
 // (libsvmread, tensorsvm-train.cu:1162-1278) and writes the model with one fprintf per feature
 // (writemodel, tensorsvm-train.cu:273-417); at a million rows both take seconds, longer than
-// the GPU solve.  Here the file is read into memory once, split at line boundaries into one
-// chunk per thread, and each thread parses its chunk (std::from_chars: exact, no locale);
-// the dense matrix is then filled chunk by chunk.  The writer formats the support-vector
+// the GPU solve.  Here the file is mapped, split at line boundaries into one chunk per thread,
+// and each thread parses its chunk in one pass over each token: plain decimal numbers by an
+// exact fast path, anything else by std::from_chars (exact, no locale), so every value is the
+// double strtod would give, then rounded to float as the reference does.  The dense matrix
+// is then filled chunk by chunk.  The writer formats the support-vector
 // lines in parallel chunks (std::to_chars, fixed with 6 digits: the same digits as the
 // reference's "%7f", whose width never pads since every value prints at least 8 characters)
 // and writes the chunks in order, so the file is byte-identical to a sequential writer's.
@@ -22,7 +24,10 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <fcntl.h>
+#include <sys/mman.h>
 #include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <charconv>
@@ -56,19 +61,54 @@ void parallel_for(int nt, F &&fn) {
 
 inline bool is_blank(char c) { return c == ' ' || c == '\t' || c == '\r'; }
 
-bool read_file(const char *path, std::string &out) {
-  FILE *f = fopen(path, "rb");
-  if (!f) return false;
-  struct stat st;
-  if (fstat(fileno(f), &st) != 0) {
-    fclose(f);
-    return false;
+// The training file, mapped read-only (the parsing threads fault its pages in, each in its own
+// chunk); a file that cannot be mapped is read into memory instead.
+class FileView {
+ public:
+  ~FileView() {
+    if (map_) munmap(map_, size_);
   }
-  out.resize((size_t)st.st_size);
-  const size_t got = st.st_size ? fread(&out[0], 1, out.size(), f) : 0;
-  fclose(f);
-  return got == out.size();
-}
+  bool open(const char *path) {
+    const int fd = ::open(path, O_RDONLY);
+    if (fd < 0) return false;
+    struct stat st;
+    if (fstat(fd, &st) != 0) {
+      close(fd);
+      return false;
+    }
+    size_ = (size_t)st.st_size;
+    if (size_ > 0) {
+      void *m = mmap(nullptr, size_, PROT_READ, MAP_PRIVATE, fd, 0);
+      if (m != MAP_FAILED) {
+        map_ = m;
+        data_ = static_cast<const char *>(m);
+      } else {
+        copy_.resize(size_);
+        size_t got = 0;
+        while (got < size_) {
+          const ssize_t r = read(fd, &copy_[got], size_ - got);
+          if (r <= 0) break;
+          got += (size_t)r;
+        }
+        if (got != size_) {
+          close(fd);
+          return false;
+        }
+        data_ = copy_.data();
+      }
+    }
+    close(fd);
+    return true;
+  }
+  const char *data() const { return data_; }
+  size_t size() const { return size_; }
+
+ private:
+  void *map_ = nullptr;
+  const char *data_ = "";
+  size_t size_ = 0;
+  std::string copy_;
+};
 
 // strtod-like number: an optional '+' (from_chars takes only '-'), then from_chars.
 template <class T>
@@ -77,6 +117,105 @@ bool parse_num(const char *b, const char *e, T &v) {
   if (b >= e) return false;
   auto r = std::from_chars(b, e, v);
   return r.ec == std::errc() && r.ptr == e;
+}
+
+// Exact decimal -> double for the common number form [+-]digits[.digits][(e|E)[+-]digits] with
+// at most 19 digits, an integer part below 2^53 and a decimal exponent within +-22: the integer
+// and the power of ten are exact doubles, so one IEEE multiplication or division rounds the
+// value correctly, giving the double std::from_chars (and strtod) give (Clinger's fast path,
+// PLDI 1990).  Scans from p and returns the end of the number, or nullptr when the text there
+// is not of that form (the caller then applies the general token rules).
+constexpr double kPow10[23] = {1e0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7,
+                               1e8,  1e9,  1e10, 1e11, 1e12, 1e13, 1e14, 1e15,
+                               1e16, 1e17, 1e18, 1e19, 1e20, 1e21, 1e22};
+
+inline bool is_digit(char c) { return (unsigned)(c - '0') < 10u; }
+
+const char *scan_decimal(const char *p, const char *e, double &out) {
+  bool neg = false;
+  if (p < e && (*p == '+' || *p == '-')) {
+    neg = *p == '-';
+    ++p;
+  }
+  uint64_t m = 0;
+  int nd = 0, frac = 0;
+  while (p < e && is_digit(*p)) {
+    m = m * 10 + (uint64_t)(*p - '0');
+    ++p;
+    if (++nd > 19) return nullptr;
+  }
+  if (nd == 0) return nullptr;
+  if (p < e && *p == '.') {
+    ++p;
+    if (p == e || !is_digit(*p)) return nullptr;
+    while (p < e && is_digit(*p)) {
+      m = m * 10 + (uint64_t)(*p - '0');
+      ++p;
+      ++frac;
+      if (++nd > 19) return nullptr;
+    }
+  }
+  int ex = 0;
+  if (p < e && (*p == 'e' || *p == 'E')) {
+    ++p;
+    bool eneg = false;
+    if (p < e && (*p == '+' || *p == '-')) {
+      eneg = *p == '-';
+      ++p;
+    }
+    int nde = 0;
+    while (p < e && is_digit(*p)) {
+      ex = ex * 10 + (*p - '0');
+      ++p;
+      if (++nde > 4) return nullptr;
+    }
+    if (nde == 0) return nullptr;
+    if (eneg) ex = -ex;
+  }
+  if (m > (1ull << 53)) return nullptr;
+  const int e10 = ex - frac;
+  if (e10 > 22 || e10 < -22) return nullptr;
+  double v = (double)m;
+  v = e10 >= 0 ? v * kPow10[e10] : v / kPow10[-e10];
+  out = neg ? -v : v;
+  return p;
+}
+
+// A number token [b, first blank or eol): the fast scan when it covers the whole token, else
+// parse_num on the token.  *end receives the token's end.
+inline bool parse_token(const char *b, const char *eol, double &v, const char **end) {
+  const char *r = scan_decimal(b, eol, v);
+  if (r && (r == eol || is_blank(*r))) {
+    *end = r;
+    return true;
+  }
+  const char *t = b;
+  while (t < eol && !is_blank(*t)) ++t;
+  *end = t;
+  return parse_num(b, t, v);
+}
+
+// index:value pair starting at q (not blank): the index as plain digits up to the colon, else
+// the general rule (the token up to the first ':' or blank must parse as an integer).
+inline bool parse_index(const char *q, const char *eol, int64_t &index, const char **colon) {
+  const char *p = q;
+  int64_t v = 0;
+  int nd = 0;
+  while (p < eol && is_digit(*p) && nd < 18) {
+    v = v * 10 + (*p - '0');
+    ++p;
+    ++nd;
+  }
+  if (nd > 0 && p < eol && *p == ':') {
+    index = v;
+    *colon = p;
+    return true;
+  }
+  p = q;
+  while (p < eol && *p != ':' && !is_blank(*p)) ++p;
+  *colon = p;
+  if (p == eol || *p != ':') return false;
+  return parse_num(q, p, index);
 }
 
 struct Chunk {
@@ -102,10 +241,9 @@ void parse_chunk(Chunk &c, bool scale256) {
       c.bad_local = line;
       return;
     }
-    const char *t = q;
-    while (t < eol && !is_blank(*t)) ++t;
     double lab;
-    if (!parse_num(q, t, lab)) {
+    const char *t;
+    if (!parse_token(q, eol, lab, &t)) {
       c.bad_local = line;
       return;
     }
@@ -114,21 +252,15 @@ void parse_chunk(Chunk &c, bool scale256) {
     while (true) {
       while (q < eol && is_blank(*q)) ++q;
       if (q == eol) break;
-      const char *colon = q;
-      while (colon < eol && *colon != ':' && !is_blank(*colon)) ++colon;
-      if (colon == eol || *colon != ':') {
-        c.bad_local = line;
-        return;
-      }
+      const char *colon;
       int64_t index;
-      if (!parse_num(q, colon, index) || index <= prev || index < 0) {
+      if (!parse_index(q, eol, index, &colon) || index <= prev || index < 0) {
         c.bad_local = line;
         return;
       }
-      const char *vb = colon + 1, *ve = vb;
-      while (ve < eol && !is_blank(*ve)) ++ve;
       double v;
-      if (!parse_num(vb, ve, v)) {
+      const char *ve;
+      if (!parse_token(colon + 1, eol, v, &ve)) {
         c.bad_local = line;
         return;
       }
@@ -176,8 +308,8 @@ tsvm_status tsvm_read_libsvm(const char *path, int32_t scale256, int32_t threads
   *X = nullptr;
   if (bad_line) *bad_line = 0;
   tsvm::TraceRange trace_call("tsvm_read_libsvm");
-  std::string text;
-  if (!read_file(path, text)) return TSVM_ERR_IO;
+  FileView text;
+  if (!text.open(path)) return TSVM_ERR_IO;
   const int nt = pick_threads(threads);
   // chunk boundaries at line starts, about text.size() / nt bytes apart
   std::vector<Chunk> ch(nt);
@@ -316,8 +448,8 @@ tsvm_status tsvm_read_model(const char *path, tsvm_model_view *m, int32_t *label
                             int32_t *label_neg) {
   if (!path || !m) return TSVM_ERR_INVALID_ARGUMENT;
   *m = tsvm_model_view{};
-  std::string text;
-  if (!read_file(path, text)) return TSVM_ERR_IO;
+  FileView text;
+  if (!text.open(path)) return TSVM_ERR_IO;
   const char *p = text.data(), *end = p + text.size();
   auto next_line = [&](std::string &line) -> bool {
     if (p >= end) return false;

@@ -26,6 +26,27 @@ def test_reader_matches_oracle_any_thread_count(tmp_path, threads):
     assert np.array_equal(X2, X)
 
 
+def test_reader_values_are_strtod_rounded_to_float(tmp_path):
+    # every value is the correctly rounded double of its decimal text (what strtod gives),
+    # then rounded to float: the fast path for plain decimals and the general path agree
+    rng = np.random.default_rng(12)
+    toks = ["1e22", "1e23", "9007199254740993", "123456789012345678901", "-0", "+5", "4.9e-324",
+            "1.7976931348623157e308", "00012.50", "1.5E+05", "-2.5e-22", "7e-23", "1e0",
+            "0.000000000000000000000001", "3.4028235e38", "1.1754944e-38", "0.1", "-0.3"]
+    for _ in range(3000):
+        x = rng.uniform(-1, 1) * 10.0 ** rng.integers(-40, 40)
+        toks.append(rng.choice(["%.9g", "%.17g", "%.6e", "%.3f", "%.25g"]) % x)
+    lines = ["1 " + " ".join(f"{j + 1}:{t}" for j, t in enumerate(toks[i:i + 7]))
+             for i in range(0, len(toks) - 6, 7)]
+    p = write_lines(tmp_path / "v.train", lines)
+    _, X = api.read_libsvm(p, threads=3)
+    with np.errstate(over="ignore"):   # beyond float range: inf, as the C cast gives
+        want = np.array([[np.float32(float(t)) for t in toks[i:i + 7]]
+                         for i in range(0, len(toks) - 6, 7)], dtype=np.float32)
+    assert X.shape == want.shape
+    assert np.array_equal(X.view(np.uint32), want.view(np.uint32))
+
+
 def test_reader_index_rules_and_scale256(tmp_path):
     # 0-based indices give max index + 1 columns; '+1' labels; tabs and CRLF; scale256
     p = write_lines(tmp_path / "z.train", ["+1 0:1.5\t3:2", "-1 1:-4 2:8e-1\r", "1"])
