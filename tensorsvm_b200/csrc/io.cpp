@@ -8,8 +8,9 @@
 // exact fast path, anything else by std::from_chars (exact, no locale), so every value is the
 // double strtod would give, then rounded to float as the reference does.  The dense matrix
 // is then filled chunk by chunk.  The writer formats the support-vector
-// lines in parallel chunks (std::to_chars, fixed with 6 digits: the same digits as the
-// reference's "%7f", whose width never pads since every value prints at least 8 characters)
+// lines in parallel chunks (6 fixed decimals, exactly the reference's "%7f", whose width never
+// pads since every value prints at least 8 characters: std::to_chars for the coefficients, an
+// exact integer rounding for the float features)
 // and writes the chunks in order, so the file is byte-identical to a sequential writer's.
 //
 // Reader semantics kept from the reference: tokens separated by blanks, a label then
@@ -294,6 +295,30 @@ inline void put_int(std::string &s, int64_t v) {
   s.append(buf, r.ptr);
 }
 
+// "%7f" digits of a float, without the general conversion: x = m 2^e with |m| < 2^24, so
+// x 10^6 = m 15625 2^(e+6) has at most 38 significant bits and is exact in double; rounding it
+// to an integer to nearest, ties to even (as printf rounds the exact value) gives the six
+// decimals.  The sign is x's, so a negative value that rounds to zero prints "-0.000000" as
+// printf does.  Values of 9e9 and above, infinities and NaN take put_fixed6.
+inline void put_fixed6_float(std::string &s, float x) {
+  const double t = (double)x * 1e6;
+  if (!(fabs(t) < 9.0e15)) {
+    put_fixed6(s, (double)x);
+    return;
+  }
+  const uint64_t q = (uint64_t)fabs(nearbyint(t));
+  if (signbit(x)) s += '-';
+  put_int(s, (int64_t)(q / 1000000));
+  char frac[6];
+  uint64_t f = q % 1000000;
+  for (int i = 5; i >= 0; --i) {
+    frac[i] = (char)('0' + f % 10);
+    f /= 10;
+  }
+  s += '.';
+  s.append(frac, 6);
+}
+
 }  // namespace
 
 extern "C" {
@@ -423,7 +448,7 @@ tsvm_status tsvm_write_model(const char *path, int32_t kernel, const float *X, c
           if (v > 0 || v < 0) {
             put_int(s, c + 1);
             s += ':';
-            put_fixed6(s, (double)v);
+            put_fixed6_float(s, v);
             s += ' ';
           }
         }
