@@ -196,6 +196,12 @@ inline bool parse_token(const char *b, const char *eol, double &v, const char **
   return parse_num(b, t, v);
 }
 
+// A number occupying exactly [b, e), by the fast scan or parse_num.
+inline bool parse_value(const char *b, const char *e, double &v) {
+  const char *r = scan_decimal(b, e, v);
+  return r == e || parse_num(b, e, v);
+}
+
 // index:value pair starting at q (not blank): the index as plain digits up to the colon, else
 // the general rule (the token up to the first ':' or blank must parse as an integer).
 inline bool parse_index(const char *q, const char *eol, int64_t &index, const char **colon) {
@@ -317,6 +323,64 @@ inline void put_fixed6_float(std::string &s, float x) {
   }
   s += '.';
   s.append(frac, 6);
+}
+
+// Support-vector lines of a model file ("coef idx:val ..."), parsed per chunk of lines as the
+// training file is: a line is trimmed of trailing '\r' and ' ', empty lines are skipped, the
+// coefficient is the first token, and each later token is "idx:val" with idx >= 1.
+struct SvChunk {
+  const char *begin = nullptr, *end = nullptr;
+  std::vector<double> coef;
+  std::vector<int64_t> row_ptr{0};
+  std::vector<int> idx;
+  std::vector<float> val;
+  int maxi = 0;
+  bool bad = false;
+};
+
+void parse_sv_chunk(SvChunk &c) {
+  const char *p = c.begin;
+  while (p < c.end) {
+    const char *eol = static_cast<const char *>(memchr(p, '\n', (size_t)(c.end - p)));
+    if (!eol) eol = c.end;
+    const char *e = eol;
+    while (e > p && (e[-1] == '\r' || e[-1] == ' ')) --e;
+    const char *q = p;
+    p = eol < c.end ? eol + 1 : c.end;
+    if (q == e) continue;
+    const char *t = q;
+    while (t < e && !is_blank(*t)) ++t;
+    double cv;
+    if (!parse_value(q, t, cv)) {
+      c.bad = true;
+      return;
+    }
+    q = t;
+    while (true) {
+      while (q < e && is_blank(*q)) ++q;
+      if (q >= e) break;
+      const char *colon = q;
+      while (colon < e && *colon != ':') ++colon;
+      if (colon >= e) {
+        c.bad = true;
+        return;
+      }
+      const char *ve = colon + 1;
+      while (ve < e && !is_blank(*ve)) ++ve;
+      int index;
+      double v;
+      if (!parse_num(q, colon, index) || !parse_value(colon + 1, ve, v) || index < 1) {
+        c.bad = true;
+        return;
+      }
+      c.idx.push_back(index);
+      c.val.push_back((float)v);
+      c.maxi = std::max(c.maxi, index);
+      q = ve;
+    }
+    c.coef.push_back(cv);
+    c.row_ptr.push_back((int64_t)c.idx.size());
+  }
 }
 
 }  // namespace
@@ -534,40 +598,34 @@ tsvm_status tsvm_read_model(const char *path, tsvm_model_view *m, int32_t *label
     m->rho = -bias;
     return TSVM_OK;
   }
-  // RBF: one line per SV, "coef idx:val ..." with 1-based indices
-  std::vector<double> coef;
-  std::vector<std::vector<std::pair<int, float>>> rows;
-  int maxi = 0;
-  while (next_line(line)) {
-    if (line.empty()) continue;
-    const char *q = line.c_str(), *e = q + line.size();
-    const char *t = q;
-    while (t < e && !is_blank(*t)) ++t;
-    double cv;
-    if (!parse_num(q, t, cv)) return TSVM_ERR_IO;
-    std::vector<std::pair<int, float>> feats;
-    q = t;
-    while (true) {
-      while (q < e && is_blank(*q)) ++q;
-      if (q >= e) break;
-      const char *colon = q;
-      while (colon < e && *colon != ':') ++colon;
-      const char *ve = colon + 1;
-      while (ve < e && !is_blank(*ve)) ++ve;
-      int idx;
-      double v;
-      if (colon >= e || !parse_num(q, colon, idx) || !parse_num(colon + 1, ve, v) || idx < 1)
-        return TSVM_ERR_IO;
-      feats.emplace_back(idx, (float)v);
-      maxi = std::max(maxi, idx);
-      q = ve;
+  // RBF: one line per SV, "coef idx:val ..." with 1-based indices, parsed in parallel chunks
+  const int nt = pick_threads(0);
+  std::vector<SvChunk> ch(nt);
+  const char *b = p;
+  const size_t rest = (size_t)(end - p);
+  for (int t = 0; t < nt; ++t) {
+    const char *e = t == nt - 1 ? end : p + (rest * (size_t)(t + 1)) / nt;
+    if (e < b) e = b;
+    if (t < nt - 1) {
+      const char *nl = static_cast<const char *>(memchr(e, '\n', (size_t)(end - e)));
+      e = nl ? nl + 1 : end;
     }
-    coef.push_back(cv);
-    rows.push_back(std::move(feats));
+    ch[t].begin = b;
+    ch[t].end = e;
+    b = e;
   }
-  if (total_sv >= 0 && (long long)rows.size() != total_sv) return TSVM_ERR_IO;
+  parallel_for(nt, [&](int t) { parse_sv_chunk(ch[t]); });
+  size_t nsv = 0;
+  int maxi = 0;
+  std::vector<size_t> row0(nt + 1, 0);
+  for (int t = 0; t < nt; ++t) {
+    if (ch[t].bad) return TSVM_ERR_IO;
+    nsv += ch[t].coef.size();
+    row0[t + 1] = nsv;
+    maxi = std::max(maxi, ch[t].maxi);
+  }
+  if (total_sv >= 0 && (long long)nsv != total_sv) return TSVM_ERR_IO;
   const int d = std::max(maxi, 1);
-  const size_t nsv = rows.size();
   float *S = static_cast<float *>(calloc(std::max<size_t>(nsv * d, 1), sizeof(float)));
   double *cf = static_cast<double *>(malloc(sizeof(double) * std::max<size_t>(nsv, 1)));
   if (!S || !cf) {
@@ -575,10 +633,15 @@ tsvm_status tsvm_read_model(const char *path, tsvm_model_view *m, int32_t *label
     free(cf);
     return TSVM_ERR_OUT_OF_MEMORY;
   }
-  for (size_t i = 0; i < nsv; ++i) {
-    cf[i] = coef[i];
-    for (auto &pr : rows[i]) S[i * d + (pr.first - 1)] = pr.second;
-  }
+  parallel_for(nt, [&](int t) {
+    const SvChunk &c = ch[t];
+    for (size_t r = 0; r < c.coef.size(); ++r) {
+      const size_t i = row0[t] + r;
+      cf[i] = c.coef[r];
+      for (int64_t e = c.row_ptr[r]; e < c.row_ptr[r + 1]; ++e)
+        S[i * d + (size_t)(c.idx[e] - 1)] = c.val[e];
+    }
+  });
   m->d = d;
   m->nsv = (int64_t)nsv;
   m->sv = S;
