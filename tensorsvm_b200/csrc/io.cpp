@@ -63,7 +63,8 @@ void parallel_for(int nt, F &&fn) {
 inline bool is_blank(char c) { return c == ' ' || c == '\t' || c == '\r'; }
 
 // The training file, mapped read-only (the parsing threads fault its pages in, each in its own
-// chunk); a file that cannot be mapped is read into memory instead.
+// chunk); a file that cannot be mapped is read into memory instead.  As with any mapping, a
+// file truncated by another process while it is being parsed raises SIGBUS.
 class FileView {
  public:
   ~FileView() {
