@@ -36,6 +36,14 @@ WORKLOAD = "two_gaussians_rbf"
 N_DEFAULT, D, K, GAMMA, CPEN, NOISE = 1_000_000, 18, 256, 0.05, 32.0, 0.10
 
 
+def workload_config(n: int, world: int) -> dict:
+    """The benchmark workload, named the same way by both arms."""
+    return {"workload": WORKLOAD, "n": n, "d": D, "k": K, "gamma": GAMMA, "C": CPEN,
+            "stop": "rel_gap<=1e-6 and ||rd||,|rp|/(1+sqrt n)<=1e-6",
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": "inputs larger than L2 (Z 1 GiB fp32, kernel operand 0.5 GiB)"}
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -247,10 +255,8 @@ def run_ours(args, world, rank, local):
         "dtype": {"fp16": "f16 (fp32 accum)", "bf16": "bf16 (fp32 accum)", "fp32": "f32"}[prec]
                  + " contractions, f64 k x k + IPM vectors",
         "data": "synthetic (seeded two-Gaussian mixture, 10% label noise)",
-        "config": {"workload": WORKLOAD, "n": n, "d": D, "k": K, "gamma": GAMMA, "C": CPEN,
-                   "precision": prec, "stop": "rel_gap<=1e-6 and ||rd||,|rp|/(1+sqrt n)<=1e-6",
-                   "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "inputs larger than L2 (Z 1 GiB fp32, kernel operand 0.5 GiB)"},
+        "precision": prec,
+        "config": workload_config(n, world),
         "phases_ms": {"sketch": round(fi["ms_sketch"], 2), "pass1": round(fi["ms_pass1"], 2),
                       "ortho": round(fi["ms_ortho"], 2), "pass2": round(fi["ms_pass2"], 2),
                       "project": round(fi["ms_project"], 2), "factor_total": round(fi["ms_total"], 2),
@@ -291,22 +297,33 @@ def decision_values(ctx, Z, alpha, y, k, C):
 
 
 def cpu_baseline(args):
-    """The FP64 oracle (same algorithm, host BLAS/LAPACK) on a bounded sample, scaled to n."""
+    """The FP64 oracle (same algorithm, host BLAS/LAPACK, all host cores) on bounded samples of
+    the same generator, extrapolated to n: the factor time is fitted as a n^2 + b n + c through
+    the samples (its two kernel-block passes are quadratic in n), the IPM is timed on the
+    largest sample and scaled by n."""
     from oracle import oracle as orc
     from tensorsvm_b200 import synth
-    ns = args.cpu_sample
-    X, y = synth.two_gaussians(ns, D, seed=2, noise=NOISE)
-    t0 = time.perf_counter()
-    f = orc.lra(X, y, GAMMA, K)
-    t1 = time.perf_counter()
-    r = orc.mpc(f.U, y, CPEN, kernel="rbf", rel_gap_tol=1e-6)
-    t2 = time.perf_counter()
-    scale = args.n / ns
-    est = (t1 - t0) * scale * scale + (t2 - t1) * scale
-    return {"value": round(est, 1), "unit": "s", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"FP64 oracle (numpy/OpenBLAS) on n={ns} rows of the same generator: "
-                      f"factor {t1 - t0:.2f}s scaled by (n/ns)^2, IPM {t2 - t1:.2f}s "
-                      f"({r.iters} it) scaled by n/ns"}
+    sizes = [int(v) for v in args.cpu_sample.split(",")]
+    cores = os.cpu_count() or 1
+    fac, ipm_s, ipm_it = [], 0.0, 0
+    for ns in sizes:
+        X, y = synth.two_gaussians(ns, D, seed=2, noise=NOISE)
+        t0 = time.perf_counter()
+        f = orc.lra(X, y, GAMMA, K, threads=cores)
+        fac.append(time.perf_counter() - t0)
+        if ns == sizes[-1]:
+            t1 = time.perf_counter()
+            r = orc.mpc(f.U, y, CPEN, kernel="rbf", rel_gap_tol=1e-6)
+            ipm_s, ipm_it = time.perf_counter() - t1, r.iters
+    A = np.array([[float(ns) ** 2, float(ns), 1.0] for ns in sizes])
+    coef = np.linalg.lstsq(A, np.array(fac), rcond=None)[0]
+    n = float(args.n)
+    est = float(coef @ np.array([n * n, n, 1.0])) + ipm_s * n / sizes[-1]
+    return {"value": round(est, 1), "unit": "s", "cores": cores, "kind": "port",
+            "sample": (f"FP64 oracle (numpy/OpenBLAS, {cores} threads) on n in {sizes} rows of the "
+                       f"same generator: factor {[round(t, 2) for t in fac]} s fitted as "
+                       f"a n^2 + b n + c (a={coef[0]:.3e}) and evaluated at n; IPM "
+                       f"{ipm_s:.2f} s ({ipm_it} it) at n={sizes[-1]} scaled by n")}
 
 
 # ------------------------------------------------------------------------------------------
@@ -566,20 +583,44 @@ def run_workload(args, world, rank, local):
 # ------------------------------------------------------------------------------------------
 
 def parse_ref_log(text):
+    """Phase times and the every-5-iterations IPM log of one reference run (tensorsvm-train.cu):
+    file read (line 899), LRA (963) and MPC (987) totals in whole seconds, the model write
+    (1022-1024, timed by the END_TIMER macro of line 53), and (iter, normdx, normdy, pobj,
+    dobj) per logged iterate (1645)."""
     text = re.sub(r"\x1b\[[0-9;]*m", "", text)
     el = [float(v) for v in re.findall(r"elapsed time = ([0-9.]+) seconds", text)]
     read = float(re.search(r"Reading files took ([0-9.]+) seconds", text).group(1))
-    km1 = float(re.search(r"rbf_kermatmul1.*?elapsed time = [0-9.]+ seconds\s*elapsed time = ([0-9.]+)",
-                          text, re.S).group(1))
-    km2 = float(re.search(r"rbf_kermatmul2.*?elapsed time = [0-9.]+ seconds\s*elapsed time = ([0-9.]+)",
-                          text, re.S).group(1))
+    lra = float(re.search(r"LRA elapsed time = ([0-9.]+) seconds", text).group(1))
+    mpc = float(re.search(r"MPC elapsed time = ([0-9.]+) seconds", text).group(1))
     write = el[-1]
-    iters = [ln for ln in re.findall(r"iter (\d+), mu=\S+, normdx=(\S+), normdy=(\S+) max/min\(D\)=\S+ "
-                                     r"pobj=(\S+) dobj=(\S+)", text)]
-    return read, km1, km2, write, iters
+    iters = [(int(i), float(dx), float(dy), float(p), float(d)) for i, dx, dy, p, d in
+             re.findall(r"iter (\d+), mu=\S+, normdx=(\S+), normdy=(\S+) max/min\(D\)=\S+ "
+                        r"pobj=(\S+) dobj=(\S+)", text)]
+    return read, lra, mpc, write, iters
+
+
+def ref_time_to_gap(wall, read, mpc, write, iters, n):
+    """Seconds from the host-resident training set to the first logged iterate that meets the
+    stopping rule of this benchmark (rel_gap <= 1e-6, ||rd||/(1+sqrt n) and |rp|/(1+sqrt n)
+    <= 1e-6): the run's wall time less its file read and model write, less the part of its
+    MPC phase after that iterate (MPC time prorated by iterations; the reference logs every
+    5th iterate, so the first one logged at or after the rule is met is used)."""
+    last = iters[-1][0]
+    hit = last
+    for it, dx, dy, p, d in iters:
+        if (p - d) / max(1.0, abs(p)) <= 1e-6 and dx / (1 + n ** 0.5) <= 1e-6 \
+                and dy / (1 + n ** 0.5) <= 1e-6:
+            hit = it
+            break
+    after = mpc * (last - hit) / (last + 1)
+    return wall - read - write - after, hit
 
 
 def run_reference(args, world, rank):
+    """The reference trainer (oracle/_ref, built from its own source) on the benchmark's full
+    n = 1M workload, run as a process per step on the box's host cores and its GPU.  A run
+    takes about 100 s, so the arm runs as many full-size steps as fit in --ref-budget seconds
+    (at least one, at most --steps) and reports the count it ran."""
     if rank != 0:
         return None
     ref = os.path.join(ROOT, "oracle", "_ref", "tensorsvm-train-ref")
@@ -590,42 +631,49 @@ def run_reference(args, world, rank):
     small = os.path.join(tmp, "small.train")
     X, y = synth.two_gaussians(8192, D, seed=2, noise=NOISE)
     synth.write_libsvm(small, X, y)
-    ns = args.ref_sample
-    big = os.path.join(tmp, "sample.train")
-    X, y = synth.two_gaussians(ns, D, seed=2, noise=NOISE)
+    big = os.path.join(tmp, "full.train")
+    X, y = synth.two_gaussians(args.n, D, seed=replica_seed(0), noise=NOISE)
     synth.write_libsvm(big, X, y)
+    del X, y
     cmd = [ref, "-k", str(K), "-c", str(CPEN), "-g", str(GAMMA), "-t", "2"]
+    # warm-up on a small file: the driver JIT-compiles the reference's compute_70 PTX once
     for _ in range(args.warmup):
         subprocess.run(cmd + [small, small + ".model"], capture_output=True, text=True, timeout=600)
-    ests, walls, details = [], [], []
-    for _ in range(args.steps):
+    vals, walls, details = [], [], []
+    t_start = time.perf_counter()
+    while len(vals) < args.steps:
         t0 = time.perf_counter()
         p = subprocess.run(cmd + [big, big + ".model"], capture_output=True, text=True, timeout=1800)
         wall = time.perf_counter() - t0
-        read, km1, km2, write, iters = parse_ref_log(p.stdout)
-        # time to rel_gap 1e-6: the reference logs every 5 iterations; keep its whole MPC phase
-        # unless an earlier logged iterate already met the criterion (then scale by iterations)
-        rest = wall - read - write - km1 - km2     # sketch, TSQR, C, eig, U, MPC: ~linear in n
-        scale = args.n / ns
-        est = (km1 + km2) * scale * scale + rest * scale
-        ests.append(est)
+        if p.returncode != 0:
+            return {"impl": "reference", "unavailable": f"reference run exited {p.returncode}"}
+        read, lra, mpc, write, iters = parse_ref_log(p.stdout)
+        v, hit = ref_time_to_gap(wall, read, mpc, write, iters, args.n)
+        vals.append(v)
         walls.append(wall)
-        details.append({"wall": round(wall, 2), "read": read, "kermatmul": round(km1 + km2, 3),
-                        "writemodel": write, "iters_logged": len(iters)})
-    value = statistics.mean(ests)
+        details.append({"wall": round(wall, 2), "read": read, "lra": lra, "mpc": mpc,
+                        "writemodel": write, "iters": iters[-1][0], "rule_met_at_iter": hit,
+                        "pobj": iters[-1][3], "dobj": iters[-1][4]})
+        elapsed = time.perf_counter() - t_start
+        if elapsed + statistics.mean(walls) > args.ref_budget:
+            break
+    value = statistics.mean(vals)
     return {
         "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": "s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "n_gpus": world, "steps": len(vals), "steps_requested": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1e3 * statistics.mean(walls), 1), "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 LRA (cuBLAS) + f64 host IPM (OpenBLAS)",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 LRA (cuBLAS) + f64 host IPM (OpenBLAS)",
         "data": "synthetic (seeded two-Gaussian mixture, 10% label noise)",
-        "config": {"workload": WORKLOAD, "n": args.n, "d": D, "k": K, "gamma": GAMMA, "C": CPEN},
+        "config": workload_config(args.n, 1),
         "cpu_baseline": {"value": round(value, 2), "unit": "s", "cores": os.cpu_count(),
                          "kind": "reference",
-                         "sample": f"reference build (oracle/_ref) on n={ns} rows; kernel passes "
-                                   f"scaled (n/ns)^2, other phases n/ns; excludes file read and "
-                                   f"model write"},
-        "e2e": {"value": round(value, 2), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                         "sample": f"reference build (oracle/_ref) on the full n={args.n} file, "
+                                   f"{len(vals)} runs; value = wall time less file read and "
+                                   f"model write and less the MPC iterations after the first "
+                                   f"logged iterate meeting the stopping rule"},
+        "e2e": {"value": round(value, 2), "unit": "s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
         "detail": details,
     }
 
@@ -641,8 +689,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-fp32-form", dest="fp32_form", action="store_false")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample", type=int, default=16384)
-    ap.add_argument("--ref-sample", type=int, default=262144)
+    ap.add_argument("--cpu-sample", default="32768,65536,131072",
+                    help="row counts of the FP64 oracle samples behind cpu_baseline's fit")
+    ap.add_argument("--ref-budget", type=float, default=900.0,
+                    help="reference arm: seconds of full-size reference runs (at least one run)")
     ap.add_argument("--factor-threads", type=int, default=4,
                     help="grid workload: host threads (one context each) for the 64 factors")
     ap.add_argument("--workload", default="two_gaussians", choices=["two_gaussians", "wide", "grid", "hypergrad"],

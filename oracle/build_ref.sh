@@ -9,7 +9,9 @@
 # linked: the reference calls cblas_* directly, which NVBLAS does not intercept.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-SRC="${TSVM_REFERENCE_SRC:-/root/reference/tensorsvm-train.cu}"
+# The reference checkout is looked for beside the repository (../reference), unless
+# TSVM_REFERENCE_SRC names the source file.
+SRC="${TSVM_REFERENCE_SRC:-$HERE/../../reference/tensorsvm-train.cu}"
 OUT="$HERE/_ref"
 if [ ! -f "$SRC" ]; then
   echo "build_ref: reference source not found at $SRC; keeping existing $OUT" >&2

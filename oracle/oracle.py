@@ -160,16 +160,29 @@ def rbf_block(Xi, Xj, yi, yj, gamma):
     return (np.asarray(yi, np.float64)[:, None] * np.asarray(yj, np.float64)[None, :]) * np.exp(-gamma * d2)
 
 
-def kermatmul(X, y, gamma, A, block: int = 2048):
-    """W = (Y K Y) A, K the RBF kernel of X (tensorsvm-train.cu:1999-2063 with 2476-2567)."""
+def kermatmul(X, y, gamma, A, block: int = 2048, threads: int = 1):
+    """W = (Y K Y) A, K the RBF kernel of X (tensorsvm-train.cu:1999-2063 with 2476-2567).
+
+    threads > 1 spreads the row blocks over host threads (numpy's exp and single-threaded BLAS
+    inside each worker); every row block is still summed over the column blocks in order."""
     n = X.shape[0]
     A = np.asarray(A, dtype=np.float64)
     W = np.zeros((n, A.shape[1]), dtype=np.float64)
-    for i in range(0, n, block):
+
+    def row_block(i):
         ib = slice(i, min(n, i + block))
         for j in range(0, n, block):
             jb = slice(j, min(n, j + block))
             W[ib] += rbf_block(X[ib], X[jb], y[ib], y[jb], gamma) @ A[jb]
+
+    if threads <= 1:
+        for i in range(0, n, block):
+            row_block(i)
+        return W
+    from concurrent.futures import ThreadPoolExecutor
+    from threadpoolctl import threadpool_limits
+    with threadpool_limits(limits=1, user_api="blas"), ThreadPoolExecutor(threads) as ex:
+        list(ex.map(row_block, range(0, n, block)))
     return W
 
 
@@ -186,7 +199,7 @@ class LraResult:
     C: np.ndarray = field(repr=False, default=None)
 
 
-def lra(X, y, gamma, k, Q=None, c_as_float32: bool = True) -> LraResult:
+def lra(X, y, gamma, k, Q=None, c_as_float32: bool = True, threads: int = 1) -> LraResult:
     """Randomised range-finder factor of Y K Y (tensorsvm-train.cu:1941-2249), FP64.
 
     Steps: Q = sketch; W = K~ Q; W = orth(W); Q = K~ W; C = W^T Q (stored as float,
@@ -195,9 +208,9 @@ def lra(X, y, gamma, k, Q=None, c_as_float32: bool = True) -> LraResult:
     n = X.shape[0]
     if Q is None:
         Q = polar_sketch(n, k)
-    W = kermatmul(X, y, gamma, Q)
+    W = kermatmul(X, y, gamma, Q, threads=threads)
     W, _ = np.linalg.qr(W)                       # any exact QR: only range(W) matters
-    Q2 = kermatmul(X, y, gamma, W)
+    Q2 = kermatmul(X, y, gamma, W, threads=threads)
     C = W.T @ Q2
     if c_as_float32:
         C32 = C.astype(np.float32)

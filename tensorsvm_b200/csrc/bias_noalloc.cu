@@ -83,8 +83,7 @@ noalloc_bias_final(const float *__restrict__ Z, int64_t ldz, int k, int64_t n,
                    const double *__restrict__ scratch, double *__restrict__ out) {
   __shared__ double v[kNoAllocMaxK];
   __shared__ double bj[kMaxFree];
-  __shared__ int idx[kMaxFree];
-  __shared__ int found;
+  __shared__ int64_t idx[kMaxFree];
   __shared__ int wcnt[32];
   __shared__ double counts[2];
   for (int c = threadIdx.x; c < k; c += blockDim.x) {
@@ -98,11 +97,11 @@ noalloc_bias_final(const float *__restrict__ Z, int64_t ldz, int k, int64_t n,
       s += scratch[(size_t)b * kPartStride + kNoAllocMaxK + threadIdx.x];
     counts[threadIdx.x] = s;
   }
-  if (threadIdx.x == 0) found = 0;
-  __syncthreads();
+  // Every thread keeps its own copy of the running count of free SVs, updated from the same
+  // per-warp counts after the same barrier, so the loop-top test is uniform over the block.
+  int found = 0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int64_t base = 0; base < n; base += blockDim.x) {
-    if (found >= kMaxFree) break;
+  for (int64_t base = 0; base < n && found < kMaxFree; base += blockDim.x) {
     const int64_t i = base + threadIdx.x;
     bool f = false;
     if (i < n) {
@@ -112,17 +111,15 @@ noalloc_bias_final(const float *__restrict__ Z, int64_t ldz, int k, int64_t n,
     const unsigned bal = __ballot_sync(0xffffffffu, f);
     if (lane == 0) wcnt[warp] = __popc(bal);
     __syncthreads();
-    int off = found;
-    for (int w = 0; w < warp; ++w) off += wcnt[w];
-    off += __popc(bal & ((1u << lane) - 1u));
-    if (f && off < kMaxFree) idx[off] = (int)i;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int tot = 0;
-      for (int w = 0; w < nw; ++w) tot += wcnt[w];
-      found += tot;
+    int off = found, tot = 0;
+    for (int w = 0; w < nw; ++w) {
+      if (w < warp) off += wcnt[w];
+      tot += wcnt[w];
     }
-    __syncthreads();
+    off += __popc(bal & ((1u << lane) - 1u));
+    if (f && off < kMaxFree) idx[off] = i;
+    found += tot;
+    __syncthreads();  // wcnt is rewritten by the next round; idx is read after the loop
   }
   const int m = found < kMaxFree ? found : kMaxFree;
   for (int t = warp; t < m; t += nw) {
@@ -180,6 +177,9 @@ extern "C" tsvm_status tsvm_bias_noalloc(const float *Z, int32_t ldz, const floa
   double *scratch = nullptr;
   const tsvm_status st = scratch_address(device, &scratch);
   if (st != TSVM_OK) return st;
+  // An error left by an earlier, unrelated launch of the caller is not this call's failure:
+  // clear it so that the check after the launches reports only these two kernels.
+  (void)cudaGetLastError();
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   noalloc_bias_partial<<<kNoAllocBlocks, kNoAllocThreads, 0, s>>>(Z, ldz, k, n, alpha, C,
                                                                    scratch);

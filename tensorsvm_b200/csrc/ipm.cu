@@ -1282,14 +1282,14 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
 namespace {
 
 __global__ void first_free_kernel(const double *__restrict__ alpha, int64_t n, double C, int want,
-                                  int *__restrict__ idx, int *__restrict__ count) {
-  __shared__ int found;
+                                  int64_t *__restrict__ idx, int *__restrict__ count) {
+  // The first `want` free SVs (1e-6 < alpha < C - 1e-6) in index order.  Each thread keeps its
+  // own running count, updated from the same per-warp counts after the same barrier, so the
+  // loop-top test is uniform over the block.
   __shared__ int wcnt[32];
-  if (threadIdx.x == 0) found = 0;
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int64_t base = 0; base < n; base += blockDim.x) {
-    if (found >= want) break;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int found = 0;
+  for (int64_t base = 0; base < n && found < want; base += blockDim.x) {
     const int64_t i = base + threadIdx.x;
     bool f = false;
     if (i < n) {
@@ -1299,24 +1299,22 @@ __global__ void first_free_kernel(const double *__restrict__ alpha, int64_t n, d
     const unsigned bal = __ballot_sync(0xffffffffu, f);
     if (lane == 0) wcnt[warp] = __popc(bal);
     __syncthreads();
-    int off = found;
-    for (int w = 0; w < warp; ++w) off += wcnt[w];
-    off += __popc(bal & ((1u << lane) - 1u));
-    if (f && off < want) idx[off] = (int)i;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int tot = 0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += wcnt[w];
-      found += tot;
+    int off = found, tot = 0;
+    for (int w = 0; w < nw; ++w) {
+      if (w < warp) off += wcnt[w];
+      tot += wcnt[w];
     }
-    __syncthreads();
+    off += __popc(bal & ((1u << lane) - 1u));
+    if (f && off < want) idx[off] = i;
+    found += tot;
+    __syncthreads();  // wcnt is rewritten by the next round
   }
   if (threadIdx.x == 0) *count = found < want ? found : want;
 }
 
 __global__ void bias_terms_kernel(const float *__restrict__ Z, int64_t ldz, int k,
                                   const float *__restrict__ y, const double *__restrict__ v,
-                                  const int *__restrict__ idx, const int *__restrict__ count,
+                                  const int64_t *__restrict__ idx, const int *__restrict__ count,
                                   double *__restrict__ out) {
   // one warp per selected free SV j: b_j = y_j - y_j (v . Z_j); out[0..1] = mean, std
   __shared__ double bj[64];
@@ -1369,8 +1367,8 @@ tsvm_status bias_rbf(tsvm_context *ctx, const float *Z, int ldz, const float *y,
   run.scal = sbuf;
   double *v = sbuf + kNScal;
   double *out = v + kz;
-  int *idx = reinterpret_cast<int *>(out + 4);
-  int *cnt = idx + 64;
+  int64_t *idx = reinterpret_cast<int64_t *>(out + 4);
+  int *cnt = reinterpret_cast<int *>(idx + 64);
   run.info = cnt + 1;
   run.err = cnt + 2;
   TSVM_CUDA(cudaMemsetAsync(run.err, 0, sizeof(int), ctx->stream));

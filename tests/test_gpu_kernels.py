@@ -191,3 +191,23 @@ def test_kermatmul_tensor_core_exp_split(ctx, npoly, monkeypatch):
                                            _lib.PREC_FP16), "kermatmul_tc")
     ref = orc.kermatmul(X, y, 0.05, A)
     assert np.linalg.norm(W.cpu().numpy() - ref) / np.linalg.norm(ref) < 2e-3
+
+
+@pytest.mark.parametrize("spacing", [1, 700, 1025])
+def test_bias_first_free_svs_spread_over_many_rounds(ctx, spacing):
+    """tsvm_bias with free SVs spread over many 1024-row rounds of its index scan (the 50th
+    beyond 34,000 rows at spacing 700 and 1025), against the oracle's bias (T:355-376)."""
+    from tensorsvm_b200 import api
+    rng = np.random.default_rng(100 + spacing)
+    n, k, C = 60 * spacing + 500, 40, 4.0
+    Zh = rng.standard_normal((n, k)).astype(np.float32)
+    yh = np.where(rng.random(n) < 0.5, 1.0, -1.0).astype(np.float32)
+    ah = np.where(rng.random(n) < 0.5, C, 0.0)
+    free = np.arange(3, n, spacing)[:70]
+    ah[free] = rng.uniform(0.1, C - 0.1, len(free))
+    b_ref, bstd_ref = orc.bias_rbf(Zh, yh, ah, C)
+    b, bstd, nsv, nfree = api.bias(ctx, dev(Zh), dev(yh), dev(ah), k, C)
+    sv, fr = orc.sv_sets(ah, C)
+    assert (nsv, nfree) == (len(sv), len(fr))
+    assert abs(b - b_ref) <= 1e-9 * max(1.0, abs(b_ref))
+    assert abs(bstd - bstd_ref) <= 1e-9 * max(1.0, abs(bstd_ref))
