@@ -45,7 +45,9 @@ typedef enum tsvm_status {
   TSVM_WARN_MAX_ITER = 9,
   /* the Gaussian sketch stream ran short of accepted pairs (retry limit reached) */
   TSVM_ERR_SKETCH = 10,
-  TSVM_ERR_IO = 11
+  TSVM_ERR_IO = 11,
+  /* a collective of the row-sharded path (tsvm_comm.allreduce) reported a failure */
+  TSVM_ERR_COMM = 12
 } tsvm_status;
 
 /* -t kernel_type values accepted by the reference (tensorsvm-train.cu:1112-1118) */
@@ -53,17 +55,32 @@ typedef enum tsvm_kernel { TSVM_KERNEL_LINEAR = 0, TSVM_KERNEL_RBF = 2 } tsvm_ke
 
 /* Arithmetic of the two contractions (kernel-block product and Z^T D^-1 Z).
  * FP32: SIMT FP32 (the "plain" form, what the reference computes without -tensorcore).
- * BF16/FP16: tcgen05 tensor cores with FP32 accumulation (the "-tensorcore" form). */
+ * BF16/FP16: tcgen05 tensor cores with FP32 accumulation (the "-tensorcore" form).  In each
+ *   factor pass the operand whose rounding sets the factor's accuracy is carried as a 16-bit
+ *   hi + lo pair, contracted by two MMAs into the same FP32 accumulator: the kernel block in
+ *   the range-finder pass W = K Q, the orthonormal basis in the projection pass K W.
+ * BF16_FAST/FP16_FAST: one 16-bit product per pass (about 1.7x faster factor); the basis of
+ *   the projection pass is rounded in place.  The factor's weak eigen-directions then move by
+ *   the 16-bit rounding, and with them the solution along the dual's flat optimal face. */
 typedef enum tsvm_precision {
   TSVM_PREC_FP32 = 0,
   TSVM_PREC_BF16 = 1,
-  TSVM_PREC_FP16 = 2
+  TSVM_PREC_FP16 = 2,
+  TSVM_PREC_BF16_FAST = 3,
+  TSVM_PREC_FP16_FAST = 4
 } tsvm_precision;
 
 /* Sketch source.  GLIBC reproduces the reference's gaussrand() stream exactly (glibc rand()
- * from its default seed, Marsaglia polar method, tensorsvm-train.cu:2621-2643) on the GPU.
- * USER takes a caller-provided n x k row-major float matrix. */
-typedef enum tsvm_sketch { TSVM_SKETCH_GLIBC = 0, TSVM_SKETCH_USER = 1 } tsvm_sketch;
+ * from its default seed, Marsaglia polar method, tensorsvm-train.cu:2621-2643) on the GPU: the
+ * parity mode.  USER takes a caller-provided n x k row-major float matrix.  PHILOX draws the
+ * entries from the counter-based Philox4x32-10 generator (Salmon et al., SC 2011) keyed by the
+ * context's seed (tsvm_set_sketch_seed), two Box-Muller pairs per 128-bit block: the same
+ * matrix for the same seed on any launch shape, with no sequential stream. */
+typedef enum tsvm_sketch {
+  TSVM_SKETCH_GLIBC = 0,
+  TSVM_SKETCH_USER = 1,
+  TSVM_SKETCH_PHILOX = 2
+} tsvm_sketch;
 
 typedef struct tsvm_context tsvm_context;
 
@@ -137,6 +154,38 @@ tsvm_status tsvm_destroy(tsvm_context *ctx);
  * NULL restores the context's own stream.  The library never destroys a caller's stream. */
 tsvm_status tsvm_set_stream(tsvm_context *ctx, void *stream);
 
+/* Row-sharded training over several GPUs, one process (and context) per GPU.  Each rank owns a
+ * contiguous range of the n training rows (its rows of X, y, Z, alpha, s and xi); the ranks
+ * exchange only k x k matrices, k-vectors and scalars in the interior-point solver, and the
+ * factor's basis once per factor (the projection pass needs every row of it).  The reference
+ * has no multi-GPU path (one process, one GPU, host chunk loops, tensorsvm-train.cu:1999-2063
+ * and 1674-1697); this communicator is how the caller's collective library (NCCL over
+ * NVLink, or any other) is plugged in.
+ *   allreduce: in-place all-reduce over the ranks of `count` values at the DEVICE pointer
+ *     `buf`, ordered on the CUDA stream `stream` (cudaStream_t as void*): the library's later
+ *     work on that stream must see the result.  dtype 0 = double, 1 = float; op 0 = sum,
+ *     1 = min.  Returns 0 on success; anything else makes the calling entry point return
+ *     TSVM_ERR_COMM.  Every rank makes the same calls in the same order (the control flow of
+ *     the sharded solve depends only on reduced values), so a rank that fails or leaves shows
+ *     up as a failing collective on the others. */
+typedef struct tsvm_comm {
+  int32_t rank, world;
+  int (*allreduce)(void *user, void *buf, int64_t count, int32_t dtype, int32_t op,
+                   void *stream);
+  void *user;
+} tsvm_comm;
+
+/* Attach a communicator to the context (copied; NULL detaches).  While one is attached,
+ * tsvm_ipm and tsvm_bias work on this rank's rows of a row-sharded problem: their Z, y, alpha,
+ * xi, s are the rank's rows, n is the rank's row count, and every reduction (k-vectors,
+ * scalars, the capacitance matrix I + Z^T D^-1 Z, the bias's free-SV terms) is completed
+ * across the ranks; the statistics are global.  tsvm_factor_rows uses it for the factor. */
+tsvm_status tsvm_set_comm(tsvm_context *ctx, const tsvm_comm *comm);
+
+/* Seed of the TSVM_SKETCH_PHILOX sketch of this context's factors (default 0).  The
+ * reference's sketch has no seed: glibc rand() is never seeded (tensorsvm-train.cu:1966). */
+tsvm_status tsvm_set_sketch_seed(tsvm_context *ctx, uint64_t seed);
+
 /* Fill `opt` with the reference's defaults (max_iter 100, tol 1e-7, FP32, RBF init). */
 void tsvm_ipm_default_options(tsvm_ipm_options *opt);
 
@@ -152,6 +201,19 @@ void tsvm_ipm_default_options(tsvm_ipm_options *opt);
 tsvm_status tsvm_factor(tsvm_context *ctx, const float *X, const float *y, int64_t n, int32_t d,
                         double gamma, int32_t k, int32_t precision, int32_t sketch,
                         const float *Q_user, float *Z, int32_t ldz, tsvm_factor_info *info);
+
+/* Kernel factor of a row-sharded problem (replaces LRA, tensorsvm-train.cu:1941-2374, across
+ * the ranks of the attached communicator): X (n_global x d) and y (n_global) are the whole
+ * training set on every rank (small: 72 MB at n = 1M, d = 18); this rank computes the rows
+ * [row0, row0 + n_rows) of Z (n_rows x ldz, device).  Every rank draws the whole sketch (or
+ * reads Q_user, n_global x k), computes its rows of W = Y K Y Q against all rows, and the
+ * CholeskyQR Gram matrices and C = W^T (K W) are all-reduced; the basis W is all-gathered
+ * (as an all-reduce of the zero-padded rows) once for the projection pass.  With no
+ * communicator attached, row0 = 0 and n_rows = n_global, it is tsvm_factor. */
+tsvm_status tsvm_factor_rows(tsvm_context *ctx, const float *X, const float *y, int64_t n_global,
+                             int32_t d, int64_t row0, int64_t n_rows, double gamma, int32_t k,
+                             int32_t precision, int32_t sketch, const float *Q_user, float *Z,
+                             int32_t ldz, tsvm_factor_info *info);
 
 /* Linear "factor": Z = diag(y) X, k = d (tensorsvm-train.cu:909-914).  Device buffers. */
 tsvm_status tsvm_linear_factor(tsvm_context *ctx, const float *X, const float *y, int64_t n,

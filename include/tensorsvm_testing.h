@@ -19,10 +19,14 @@ extern "C" {
 tsvm_status tsvm_test_rand_stream(tsvm_context *ctx, int64_t count, uint32_t *out);
 /* The reference's gaussrand() stream (tensorsvm-train.cu:2621-2643), count floats. */
 tsvm_status tsvm_test_sketch(tsvm_context *ctx, int64_t count, float *out);
-/* W (n x kp) = (Y K Y) A (n x kp) with the given precision (kermatmul, T:2476-2567). */
+/* count values of the Philox4x32-10 Box-Muller sketch with this seed (TSVM_SKETCH_PHILOX). */
+tsvm_status tsvm_test_sketch_philox(tsvm_context *ctx, uint64_t seed, int64_t count, float *out);
+/* W (n x kp) = (Y K Y) A (n x kp) with the given precision (kermatmul, T:2476-2567); for the
+ * tensor-core precisions split = 0 (one product), 1 (the kernel block as hi + lo) or 2 (A as
+ * hi + lo). */
 tsvm_status tsvm_test_kermatmul(tsvm_context *ctx, const float *X, const float *y, int64_t n,
                                 int32_t d, double gamma, const float *A, int32_t kp, float *W,
-                                int32_t precision);
+                                int32_t precision, int32_t split);
 /* In-place lower Cholesky of A (n x n row-major); *info_host = 0 or failing column (T:1709). */
 tsvm_status tsvm_test_chol(tsvm_context *ctx, double *A, int32_t n, int32_t *info_host);
 /* Solve L L^T X = B, B holds nrhs rows of length ldb (T:1834). */

@@ -69,6 +69,41 @@ def polar_sketch(n: int, k: int) -> np.ndarray:
     return out.reshape(n, k)
 
 
+def philox4x32_10(ctr, key):
+    """Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC 2011) on vectors of counters: ctr is a
+    (4, m) uint32 array, key a (2,) pair.  Restated from the paper's round function: two 32x32
+    multiplications per round with the multipliers 0xD2511F53 and 0xCD9E8D57, Weyl key bumps
+    0x9E3779B9 and 0xBB67AE85, ten rounds."""
+    c = [np.asarray(v, dtype=np.uint64) for v in ctr]
+    k0, k1 = np.uint64(key[0]), np.uint64(key[1])
+    mask = np.uint64(0xFFFFFFFF)
+    for _ in range(10):
+        p0 = np.uint64(0xD2511F53) * c[0]
+        p1 = np.uint64(0xCD9E8D57) * c[2]
+        c = [(p1 >> np.uint64(32)) ^ c[1] ^ k0, p1 & mask, (p0 >> np.uint64(32)) ^ c[3] ^ k1,
+             p0 & mask]
+        k0 = (k0 + np.uint64(0x9E3779B9)) & mask
+        k1 = (k1 + np.uint64(0xBB67AE85)) & mask
+    return np.stack([v.astype(np.uint32) for v in c])
+
+
+def philox_sketch(seed: int, count: int) -> np.ndarray:
+    """The TSVM_SKETCH_PHILOX stream in FP64: block b = e // 4 of entry e is Philox4x32-10 of
+    counter (b, 0, 0, 0) under key (seed low, seed high); words (w0, w1) and (w2, w3) give
+    Box-Muller pairs r cos(2 pi u1), r sin(2 pi u1), r = sqrt(-2 ln u0), u = ((w >> 8) + 1/2) 2^-24."""
+    blocks = (count + 3) // 4
+    b = np.arange(blocks, dtype=np.uint64)
+    ctr = [b & np.uint64(0xFFFFFFFF), b >> np.uint64(32), np.zeros_like(b), np.zeros_like(b)]
+    w = philox4x32_10(ctr, (seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF))
+    u = ((w >> np.uint32(8)).astype(np.float64) + 0.5) / 16777216.0
+    out = np.empty((blocks, 4))
+    for p in range(2):
+        r = np.sqrt(-2.0 * np.log(u[2 * p]))
+        out[:, 2 * p] = r * np.cos(2 * np.pi * u[2 * p + 1])
+        out[:, 2 * p + 1] = r * np.sin(2 * np.pi * u[2 * p + 1])
+    return out.ravel()[:count]
+
+
 def glibc_rand(count: int) -> np.ndarray:
     """The glibc rand() stream from the default seed (1)."""
     out = np.empty(count, dtype=np.uint32)

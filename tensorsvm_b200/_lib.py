@@ -25,14 +25,18 @@ WARN_ILL_CONDITIONED = 8
 WARN_MAX_ITER = 9
 ERR_SKETCH = 10
 ERR_IO = 11
+ERR_COMM = 12
 
 KERNEL_LINEAR = 0
 KERNEL_RBF = 2
 PREC_FP32 = 0
 PREC_BF16 = 1
 PREC_FP16 = 2
+PREC_BF16_FAST = 3
+PREC_FP16_FAST = 4
 SKETCH_GLIBC = 0
 SKETCH_USER = 1
+SKETCH_PHILOX = 2
 
 # every symbol include/tensorsvm.h and include/tensorsvm_testing.h declare
 EXPORTS = [
@@ -42,12 +46,23 @@ EXPORTS = [
     "tsvm_train", "tsvm_kernel_launches", "tsvm_ipm_batched", "tsvm_hypergrad",
     "tsvm_decision_values", "tsvm_predict", "tsvm_kernel_residual", "tsvm_train_residual",
     "tsvm_read_libsvm", "tsvm_free", "tsvm_write_model", "tsvm_read_model", "tsvm_free_model",
+    "tsvm_set_comm", "tsvm_factor_rows", "tsvm_set_sketch_seed",
 ]
 TEST_EXPORTS = [
     "tsvm_test_rand_stream", "tsvm_test_sketch", "tsvm_test_kermatmul", "tsvm_test_chol",
     "tsvm_test_potrs", "tsvm_test_eig", "tsvm_test_gram", "tsvm_test_syrk_mixed",
-    "tsvm_test_grid_barrier", "tsvm_test_fail_alloc",
+    "tsvm_test_grid_barrier", "tsvm_test_fail_alloc", "tsvm_test_sketch_philox",
 ]
+
+
+# int (*allreduce)(void *user, void *buf, int64_t count, int32_t dtype, int32_t op, void *stream)
+ALLREDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p)
+
+
+class Comm(ctypes.Structure):
+    _fields_ = [("rank", ctypes.c_int32), ("world", ctypes.c_int32),
+                ("allreduce", ALLREDUCE_FN), ("user", ctypes.c_void_p)]
 
 
 class IpmProblem(ctypes.Structure):
@@ -130,6 +145,13 @@ def load() -> ctypes.CDLL:
     lib.tsvm_factor.restype = ctypes.c_int
     lib.tsvm_factor.argtypes = [P, P, P, I64, I32, D, I32, I32, I32, P, P, I32,
                                 ctypes.POINTER(FactorInfo)]
+    lib.tsvm_set_sketch_seed.restype = ctypes.c_int
+    lib.tsvm_set_sketch_seed.argtypes = [P, ctypes.c_uint64]
+    lib.tsvm_set_comm.restype = ctypes.c_int
+    lib.tsvm_set_comm.argtypes = [P, ctypes.POINTER(Comm)]
+    lib.tsvm_factor_rows.restype = ctypes.c_int
+    lib.tsvm_factor_rows.argtypes = [P, P, P, I64, I32, I64, I64, D, I32, I32, I32, P, P, I32,
+                                     ctypes.POINTER(FactorInfo)]
     lib.tsvm_linear_factor.restype = ctypes.c_int
     lib.tsvm_linear_factor.argtypes = [P, P, P, I64, I32, P, I32]
     lib.tsvm_ipm.restype = ctypes.c_int
@@ -178,7 +200,8 @@ def load() -> ctypes.CDLL:
     for name, args in {
         "tsvm_test_rand_stream": [P, I64, P],
         "tsvm_test_sketch": [P, I64, P],
-        "tsvm_test_kermatmul": [P, P, P, I64, I32, D, P, I32, P, I32],
+        "tsvm_test_kermatmul": [P, P, P, I64, I32, D, P, I32, P, I32, I32],
+        "tsvm_test_sketch_philox": [P, ctypes.c_uint64, I64, P],
         "tsvm_test_chol": [P, P, I32, ctypes.POINTER(I32)],
         "tsvm_test_potrs": [P, P, I32, P, I32, I32],
         "tsvm_test_eig": [P, P, I32, P, P, ctypes.POINTER(I32)],

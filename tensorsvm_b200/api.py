@@ -16,7 +16,8 @@ import numpy as np
 
 from . import _lib
 
-PRECISIONS = {"fp32": _lib.PREC_FP32, "bf16": _lib.PREC_BF16, "fp16": _lib.PREC_FP16}
+PRECISIONS = {"fp32": _lib.PREC_FP32, "bf16": _lib.PREC_BF16, "fp16": _lib.PREC_FP16,
+              "bf16_fast": _lib.PREC_BF16_FAST, "fp16_fast": _lib.PREC_FP16_FAST}
 
 
 def _ptr(t) -> int:
@@ -27,8 +28,11 @@ def _fields(struct) -> dict:
     return {name: getattr(struct, name) for name, _ in struct._fields_}
 
 
-def factor(ctx, X, y, gamma: float, k: int, precision: str = "fp32", Q=None, ldz: int | None = None):
-    """Z (n x ldz float32 CUDA tensor, ldz = round_up(k, 64) by default) with Z Z^T ~= Y K Y."""
+def factor(ctx, X, y, gamma: float, k: int, precision: str = "fp32", Q=None, ldz: int | None = None,
+           philox_seed: int | None = None):
+    """Z (n x ldz float32 CUDA tensor, ldz = round_up(k, 64) by default) with Z Z^T ~= Y K Y.
+    The sketch is the reference's glibc stream, the caller's Q, or with philox_seed the
+    counter-based Philox sketch of that seed."""
     import torch
     n, d = X.shape
     kp = ((k + 63) // 64) * 64
@@ -36,6 +40,9 @@ def factor(ctx, X, y, gamma: float, k: int, precision: str = "fp32", Q=None, ldz
     Z = torch.empty((n, ldz), dtype=torch.float32, device=X.device)
     info = _lib.FactorInfo()
     sketch = _lib.SKETCH_USER if Q is not None else _lib.SKETCH_GLIBC
+    if philox_seed is not None:
+        _lib.check(ctx.lib.tsvm_set_sketch_seed(ctx.handle, int(philox_seed)), "tsvm_set_sketch_seed")
+        sketch = _lib.SKETCH_PHILOX
     st = ctx.lib.tsvm_factor(ctx.handle, _ptr(X), _ptr(y), n, d, float(gamma), k,
                              PRECISIONS[precision], sketch, _ptr(Q), _ptr(Z), ldz,
                              ctypes.byref(info))

@@ -49,7 +49,8 @@ void help_msg() {
          "-s solver : 0 -- approx interior point method (default)\n"
          "-N n_samples : only consider the first n_samples in training\n"
          "-tensorcore : tensor-core (FP16, tcgen05) kernel-block products\n"
-         "-prec fp32|bf16|fp16 : contraction precision (overrides -tensorcore)\n"
+         "-prec fp32|bf16|fp16|bf16_fast|fp16_fast : contraction precision (overrides\n"
+         "     -tensorcore); *_fast: one 16-bit product per factor pass, no hi+lo split\n"
          "-rel_gap tol : also stop at relative duality gap <= tol\n"
          "-scale256 : divide feature values by 256\n"
          "-analysis : report ||K||_F and ||K - Z Z'||_F (RBF, FP64 on the GPU)\n"
@@ -89,7 +90,9 @@ bool parse(int argc, char **argv, Args &a) {
       const char *p = next("-prec");
       a.precision = !strcmp(p, "fp32") ? TSVM_PREC_FP32
                     : !strcmp(p, "bf16") ? TSVM_PREC_BF16
-                    : !strcmp(p, "fp16") ? TSVM_PREC_FP16 : -2;
+                    : !strcmp(p, "fp16") ? TSVM_PREC_FP16
+                    : !strcmp(p, "bf16_fast") ? TSVM_PREC_BF16_FAST
+                    : !strcmp(p, "fp16_fast") ? TSVM_PREC_FP16_FAST : -2;
       if (a.precision == -2) {
         fprintf(stderr, "Error: unknown precision %s\n", p);
         exit(1);

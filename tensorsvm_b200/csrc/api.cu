@@ -44,6 +44,23 @@ tsvm_status scratch(tsvm_context *ctx, Slot s, size_t bytes, void **out) {
   return TSVM_OK;
 }
 
+tsvm_status comm_allreduce(tsvm_context *ctx, void *buf, int64_t count, int dtype, int op) {
+  if (!ctx->has_comm || ctx->comm.world <= 1 || count <= 0) return TSVM_OK;
+  const int rc = ctx->comm.allreduce(ctx->comm.user, buf, count, dtype, op, ctx->stream);
+  return rc == 0 ? TSVM_OK : TSVM_ERR_COMM;
+}
+
+tsvm_status comm_sum_host(tsvm_context *ctx, double *value) {
+  if (!sharded(ctx)) return TSVM_OK;
+  double *d = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_COMM, 8, &d));
+  TSVM_CUDA(cudaMemcpyAsync(d, value, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  TSVM_TRY(comm_allreduce(ctx, d, 1, 0, COMM_SUM));
+  TSVM_CUDA(cudaMemcpyAsync(value, d, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSVM_OK;
+}
+
 float event_ms(cudaEvent_t a, cudaEvent_t b) {
   float ms = 0.f;
   cudaEventSynchronize(b);
@@ -70,6 +87,7 @@ const char *tsvm_status_string(tsvm_status s) {
     case TSVM_WARN_MAX_ITER: return "stopped: iteration limit reached";
     case TSVM_ERR_SKETCH: return "sketch stream exhausted";
     case TSVM_ERR_IO: return "I/O error";
+    case TSVM_ERR_COMM: return "collective of the row-sharded path failed";
   }
   return "unknown status";
 }
@@ -117,6 +135,27 @@ tsvm_status tsvm_set_stream(tsvm_context *ctx, void *stream) {
   return TSVM_OK;
 }
 
+tsvm_status tsvm_set_comm(tsvm_context *ctx, const tsvm_comm *comm) {
+  if (!ctx) return TSVM_ERR_INVALID_ARGUMENT;
+  if (!comm) {
+    ctx->has_comm = false;
+    ctx->comm = tsvm_comm{};
+    return TSVM_OK;
+  }
+  if (comm->world < 1 || comm->rank < 0 || comm->rank >= comm->world ||
+      (comm->world > 1 && !comm->allreduce))
+    return TSVM_ERR_INVALID_ARGUMENT;
+  ctx->comm = *comm;
+  ctx->has_comm = true;
+  return TSVM_OK;
+}
+
+tsvm_status tsvm_set_sketch_seed(tsvm_context *ctx, uint64_t seed) {
+  if (!ctx) return TSVM_ERR_INVALID_ARGUMENT;
+  ctx->sketch_seed = seed;
+  return TSVM_OK;
+}
+
 void tsvm_ipm_default_options(tsvm_ipm_options *opt) {
   if (!opt) return;
   opt->max_iter = 100;
@@ -134,10 +173,25 @@ tsvm_status tsvm_factor(tsvm_context *ctx, const float *X, const float *y, int64
                         double gamma, int32_t k, int32_t precision, int32_t sketch,
                         const float *Q_user, float *Z, int32_t ldz, tsvm_factor_info *info) {
   if (!ctx || !X || !y || !Z) return TSVM_ERR_INVALID_ARGUMENT;
-  if (precision < TSVM_PREC_FP32 || precision > TSVM_PREC_FP16) return TSVM_ERR_INVALID_ARGUMENT;
+  if (!precision_valid(precision)) return TSVM_ERR_INVALID_ARGUMENT;
+  if (sharded(ctx)) return TSVM_ERR_UNSUPPORTED;   // row-sharded: tsvm_factor_rows
   TSVM_CUDA(cudaSetDevice(ctx->device));
   TraceRange tr("tsvm_factor");
   return factor_rbf(ctx, X, y, n, d, gamma, k, precision, sketch, Q_user, Z, ldz, info);
+}
+
+tsvm_status tsvm_factor_rows(tsvm_context *ctx, const float *X, const float *y, int64_t n_global,
+                             int32_t d, int64_t row0, int64_t n_rows, double gamma, int32_t k,
+                             int32_t precision, int32_t sketch, const float *Q_user, float *Z,
+                             int32_t ldz, tsvm_factor_info *info) {
+  if (!ctx || !X || !y || !Z) return TSVM_ERR_INVALID_ARGUMENT;
+  if (!precision_valid(precision)) return TSVM_ERR_INVALID_ARGUMENT;
+  if (row0 < 0 || n_rows < 1 || row0 + n_rows > n_global) return TSVM_ERR_INVALID_ARGUMENT;
+  if ((row0 != 0 || n_rows != n_global) && !sharded(ctx)) return TSVM_ERR_INVALID_ARGUMENT;
+  TSVM_CUDA(cudaSetDevice(ctx->device));
+  TraceRange tr("tsvm_factor_rows");
+  return factor_rbf(ctx, X, y, n_global, d, gamma, k, precision, sketch, Q_user, Z, ldz, info,
+                    nullptr, row0, n_rows);
 }
 
 tsvm_status tsvm_linear_factor(tsvm_context *ctx, const float *X, const float *y, int64_t n,
@@ -170,6 +224,7 @@ tsvm_status tsvm_ipm_batched(tsvm_context *ctx, const tsvm_ipm_problem *problems
                              tsvm_ipm_stats *stats, tsvm_batch_info *info) {
   if (!ctx || !problems || count < 1 || k < 1 || ldz < k || (ldz % 4) != 0)
     return TSVM_ERR_INVALID_ARGUMENT;
+  if (sharded(ctx)) return TSVM_ERR_UNSUPPORTED;   // problems are partitioned, not sharded
   for (int32_t p = 0; p < count; ++p) {
     const tsvm_ipm_problem &q = problems[p];
     if (!q.Z || !q.y || !q.alpha_out || q.n < 2 || !(q.C > 0) ||
@@ -198,6 +253,7 @@ tsvm_status tsvm_train(tsvm_context *ctx, const float *X, const float *y, int64_
                        int32_t kernel, double gamma, double C, int32_t k, int32_t precision,
                        const tsvm_ipm_options *opt, double *alpha_out, double *b_out,
                        tsvm_factor_info *finfo, tsvm_ipm_stats *istats) {
+  if (ctx && sharded(ctx)) return TSVM_ERR_UNSUPPORTED;   // row-sharded: factor_rows + ipm
   if (!ctx || !X || !y || !alpha_out || n < 2 || d < 1) return TSVM_ERR_INVALID_ARGUMENT;
   if (kernel != TSVM_KERNEL_LINEAR && kernel != TSVM_KERNEL_RBF) return TSVM_ERR_UNSUPPORTED;
   TSVM_CUDA(cudaSetDevice(ctx->device));

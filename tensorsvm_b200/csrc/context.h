@@ -52,6 +52,8 @@ enum Slot : int {
   SLOT_DEV_OUT,       // tsvm_train: device alpha
   SLOT_PRED_IN,       // tsvm_predict: device copies of the model and the rows
   SLOT_PRED_OUT,      // tsvm_predict: decision values
+  SLOT_COMM,          // row-sharded path: staging of host values for the collectives
+  SLOT_SHARD_A,       // row-sharded factor: the all-gathered kernel-block operand (all rows)
   SLOT_COUNT_
 };
 
@@ -75,6 +77,11 @@ struct tsvm_context {
   // test hook: scratch growth fails with TSVM_ERR_OUT_OF_MEMORY after this many more device
   // allocations (-1: never)
   int alloc_fail_after = -1;
+  // seed of the Philox sketch (tsvm_set_sketch_seed)
+  uint64_t sketch_seed = 0;
+  // row-sharded solves (tsvm_set_comm): the caller's communicator
+  bool has_comm = false;
+  tsvm_comm comm = {};
   // the last RBF tsvm_train (its X, y in SLOT_DEV_IN and Z in SLOT_DEV_Z), for -analysis
   struct {
     bool valid = false;
@@ -99,5 +106,13 @@ inline tsvm_status scratch_t(tsvm_context *ctx, Slot s, size_t count, T **out) {
 
 // Elapsed ms between two recorded events (synchronises on the second).
 float event_ms(cudaEvent_t a, cudaEvent_t b);
+
+// Collectives of the row-sharded path: no-ops without a communicator.  dtype 0 double,
+// 1 float; op 0 sum, 1 min.
+enum CommOp : int { COMM_SUM = 0, COMM_MIN = 1 };
+tsvm_status comm_allreduce(tsvm_context *ctx, void *buf, int64_t count, int dtype, int op);
+inline bool sharded(const tsvm_context *ctx) { return ctx->has_comm && ctx->comm.world > 1; }
+// Sum of a host value over the ranks (through a device staging word).
+tsvm_status comm_sum_host(tsvm_context *ctx, double *value);
 
 }  // namespace tsvm

@@ -99,15 +99,17 @@ struct Phase {
 
 }  // namespace
 
-// round_back: see kermatmul_tc (ignored by the FP32 form, whose operand is not rounded).
+// round_back, split, row range: see kermatmul_tc (the FP32 form ignores round_back and split:
+// its operand is not rounded).
 static tsvm_status kermatmul(tsvm_context *ctx, const float *Xc, const float *norms,
                              const float *y, int64_t n, int d, double gamma, const float *A,
                              int kp, float *W, int precision, float *kernel_ms,
-                             float *round_back = nullptr) {
+                             float *round_back, int split, int64_t row0, int64_t nr) {
   if (precision == TSVM_PREC_FP32)
-    return kermatmul_fp32(ctx, Xc, norms, y, n, d, gamma, A, kp, W);
+    return kermatmul_fp32(ctx, Xc, norms, y, n, d, gamma, A, kp, W, row0, nr);
   if (!kermatmul_tc_supported(d, kp)) return TSVM_ERR_UNSUPPORTED;
-  return kermatmul_tc(ctx, Xc, norms, y, n, d, gamma, A, kp, W, precision, kernel_ms, round_back);
+  return kermatmul_tc(ctx, Xc, norms, y, n, d, gamma, A, kp, W, precision, kernel_ms, round_back,
+                      split, row0, nr);
 }
 
 // Rkeep (2 k x k doubles, may be null): the combined factor R with (input W) = (output W) R.
@@ -115,8 +117,10 @@ static tsvm_status kermatmul(tsvm_context *ctx, const float *Xc, const float *no
 // Gram matrix from the tensor-core SYRK with a 3-way BF16 split (about FP32 accuracy, the
 // precision W is stored in) instead of the exact FP64 sum; the first, ill-conditioned step
 // always uses the exact FP64 Gram.
+// n_total: rows of the whole problem (this rank's W holds n of them when row-sharded: the Gram
+// matrices are then all-reduced, and W's rows are updated locally).
 static tsvm_status orthonormalise(tsvm_context *ctx, float *W, int64_t n, int k, int kp,
-                                  double *Rkeep, bool tc_gram = false) {
+                                  double *Rkeep, bool tc_gram, int64_t n_total) {
   double *G = nullptr, *Linv = nullptr;
   float *R32 = nullptr;
   int *info = nullptr;
@@ -132,7 +136,7 @@ static tsvm_status orthonormalise(tsvm_context *ctx, float *W, int64_t n, int k,
     TSVM_LAUNCHED(ctx);
   }
   for (int step = 0; step < 3; ++step) {
-    double factor = step == 0 ? 11.0 * ((double)n * k + (double)k * (k + 1)) * u : 0.0;
+    double factor = step == 0 ? 11.0 * ((double)n_total * k + (double)k * (k + 1)) * u : 0.0;
     for (int attempt = 0; attempt < 4; ++attempt) {
       if (tc_gram && step > 0 && attempt == 0) {
         // M = I + sum_j 1 * w_j w_j^T (every row on the tensor cores) plus the exact -I
@@ -147,6 +151,7 @@ static tsvm_status orthonormalise(tsvm_context *ctx, float *W, int64_t n, int k,
       } else {
         TSVM_TRY(gram_fp64(ctx, W, kp, W, kp, n, k, k, true, G));
       }
+      TSVM_TRY(comm_allreduce(ctx, G, (int64_t)k * k, 0, COMM_SUM));   // row-sharded
       if (factor > 0) {
         shift_by_trace<<<1, 256, 0, ctx->stream>>>(G, k, factor);
         TSVM_LAUNCHED(ctx);
@@ -157,7 +162,8 @@ static tsvm_status orthonormalise(tsvm_context *ctx, float *W, int64_t n, int k,
       TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
       if (hinfo == 0) break;
       if (attempt == 3) return TSVM_ERR_NOT_SPD;
-      factor = factor > 0 ? factor * 100.0 : 11.0 * ((double)n * k + (double)k * (k + 1)) * u;
+      factor = factor > 0 ? factor * 100.0
+                          : 11.0 * ((double)n_total * k + (double)k * (k + 1)) * u;
     }
     if (Rkeep) {
       double *Rtmp = Rkeep + (size_t)k * k;
@@ -177,9 +183,16 @@ static tsvm_status orthonormalise(tsvm_context *ctx, float *W, int64_t n, int k,
 
 tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_t n, int d,
                        double gamma, int k, int precision, int sketch, const float *Q_user,
-                       float *Z, int ldz, tsvm_factor_info *info, FactorKeep *keep) {
+                       float *Z, int ldz, tsvm_factor_info *info, FactorKeep *keep, int64_t row0,
+                       int64_t nr) {
   if (n < 2 || d < 1 || k < 1 || k > 1000 || ldz < k || !(gamma > 0)) return TSVM_ERR_INVALID_ARGUMENT;
   if (k > n) return TSVM_ERR_INVALID_ARGUMENT;
+  if (nr < 0) nr = n - row0;
+  if (row0 < 0 || nr < 1 || row0 + nr > n) return TSVM_ERR_INVALID_ARGUMENT;
+  // row-sharded: this rank computes Z's rows [row0, row0 + nr) (W, the pass outputs and Z hold
+  // nr rows; X, y and the pass operands all n)
+  const bool rows = row0 != 0 || nr != n;
+  if (rows && keep) return TSVM_ERR_UNSUPPORTED;
   const int kp = (int)round_up(k, 64);
   cudaEvent_t *ev = ctx->ev;
   TracePhases phase;
@@ -190,10 +203,18 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
   float *norms = Xc + (size_t)n * d;
   TSVM_TRY(centre_features(ctx, X, n, d, Xc, norms));
   TSVM_TRY(scratch_t(ctx, SLOT_Q, (size_t)n * kp, &Q));
-  TSVM_TRY(scratch_t(ctx, SLOT_W, (size_t)n * kp, &W));
+  TSVM_TRY(scratch_t(ctx, SLOT_W, (size_t)nr * kp, &W));
   if (sketch == TSVM_SKETCH_GLIBC) {
-    TSVM_TRY(sketch_glibc(ctx, n * (int64_t)k, W));          // stream order = row-major n x k
-    TSVM_TRY(pad_rows(ctx, W, k, n, k, Q, kp));
+    // every rank draws the whole stream (stream order = row-major n x k): pass 1 needs all rows
+    float *raw = W;
+    if (rows) TSVM_TRY(scratch_t(ctx, SLOT_W2, (size_t)n * k, &raw));
+    TSVM_TRY(sketch_glibc(ctx, n * (int64_t)k, raw));
+    TSVM_TRY(pad_rows(ctx, raw, k, n, k, Q, kp));
+  } else if (sketch == TSVM_SKETCH_PHILOX) {
+    float *raw = W;
+    if (rows) TSVM_TRY(scratch_t(ctx, SLOT_W2, (size_t)n * k, &raw));
+    TSVM_TRY(sketch_philox(ctx, ctx->sketch_seed, n * (int64_t)k, raw));
+    TSVM_TRY(pad_rows(ctx, raw, k, n, k, Q, kp));
   } else if (sketch == TSVM_SKETCH_USER) {
     if (!Q_user) return TSVM_ERR_INVALID_ARGUMENT;
     TSVM_TRY(pad_rows(ctx, Q_user, k, n, k, Q, kp));
@@ -206,28 +227,53 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
   TSVM_CUDA(cudaEventRecord(ev[1], ctx->stream));
   phase.next("factor: kernel-block pass 1");
   float km1 = 0.f, km2 = 0.f;
-  TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, Q, kp, W, precision, &km1));
+  // split forms: the kernel block as hi + lo in this pass (its rounding would perturb the
+  // kernel whose range is found; rounding the sketch only draws another Gaussian sketch)
+  const bool split = precision_is_split(precision);
+  TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, Q, kp, W, precision, &km1, nullptr,
+                     split ? 1 : 0, row0, nr));
   TSVM_CUDA(cudaEventRecord(ev[2], ctx->stream));
   phase.next("factor: orthonormalise");
   const bool tc_gram = precision != TSVM_PREC_FP32 && keep == nullptr && syrk_tc_supported(k) &&
                        k >= 32;
-  TSVM_TRY(orthonormalise(ctx, W, n, k, kp, keep ? keep->R : nullptr, tc_gram));
+  TSVM_TRY(orthonormalise(ctx, W, nr, k, kp, keep ? keep->R : nullptr, tc_gram, n));
   if (keep)
     TSVM_CUDA(cudaMemcpyAsync(keep->W, W, sizeof(float) * n * kp, cudaMemcpyDeviceToDevice,
                               ctx->stream));
   TSVM_CUDA(cudaEventRecord(ev[3], ctx->stream));
   phase.next("factor: kernel-block pass 2");
-  // the second pass rounds the orthonormal basis W to the tensor-core operand type in place:
-  // C = W^T (K W) and Z = W V diag(sqrt w) then use the W the tensor cores contracted, so the
-  // weak eigen-directions of C do not pick up the rounding of one side only
-  TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, W, kp, Q, precision, &km2, W));
+  // split forms: the basis W as hi + lo (rounding it would tilt the subspace K is projected
+  // on).  One-product forms round W to the tensor-core operand type in place instead, so that
+  // C = W^T (K W) and Z = W V diag(sqrt w) use the W the tensor cores contracted and the weak
+  // eigen-directions of C do not pick up the rounding of one side only.
+  // Row-sharded: the pass needs every row of W, gathered as an all-reduce of the zero-padded
+  // rows (exact: each entry is one rank's value plus zeros).
+  float *Wall = W;
+  if (rows) {
+    TSVM_TRY(scratch_t(ctx, SLOT_SHARD_A, (size_t)n * kp, &Wall));
+    TSVM_CUDA(cudaMemsetAsync(Wall, 0, sizeof(float) * n * kp, ctx->stream));
+    TSVM_CUDA(cudaMemcpyAsync(Wall + row0 * kp, W, sizeof(float) * nr * kp,
+                              cudaMemcpyDeviceToDevice, ctx->stream));
+    TSVM_TRY(comm_allreduce(ctx, Wall, n * (int64_t)kp, 1, COMM_SUM));
+  }
+  if (split) {
+    TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, Wall, kp, Q, precision, &km2, nullptr, 2,
+                       row0, nr));
+  } else {
+    TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, Wall, kp, Q, precision, &km2, Wall, 0,
+                       row0, nr));
+    if (rows && precision != TSVM_PREC_FP32)   // this rank's rows as the tensor cores saw them
+      TSVM_CUDA(cudaMemcpyAsync(W, Wall + row0 * kp, sizeof(float) * nr * kp,
+                                cudaMemcpyDeviceToDevice, ctx->stream));
+  }
   TSVM_CUDA(cudaEventRecord(ev[4], ctx->stream));
   phase.next("factor: projection and eigensolver");
   double *Cm = nullptr, *V = nullptr, *w = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_SMALL, (size_t)k * k + 8, &Cm));
   TSVM_TRY(scratch_t(ctx, SLOT_SMALL2, (size_t)k * k + (size_t)k, &V));
   w = V + (size_t)k * k;
-  TSVM_TRY(gram_fp64(ctx, W, kp, Q, kp, n, k, k, false, Cm));
+  TSVM_TRY(gram_fp64(ctx, W, kp, Q, kp, nr, k, k, false, Cm));
+  TSVM_TRY(comm_allreduce(ctx, Cm, (int64_t)k * k, 0, COMM_SUM));   // row-sharded
   TSVM_TRY(small_symmetrize(ctx, Cm, k, k));
   int sweeps = 0;
   TSVM_TRY(eig_jacobi_fp64(ctx, Cm, k, k, w, V, &sweeps));
@@ -237,10 +283,10 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
                                                                                          kp, X32);
   TSVM_LAUNCHED(ctx);
   if (ldz == kp) {
-    TSVM_TRY(apply_right_fp32(ctx, W, n, kp, X32, Z));
+    TSVM_TRY(apply_right_fp32(ctx, W, nr, kp, X32, Z));
   } else {
-    TSVM_TRY(apply_right_fp32(ctx, W, n, kp, X32, Q));  // Q is free again
-    TSVM_TRY(pad_rows(ctx, Q, kp, n, k, Z, ldz));
+    TSVM_TRY(apply_right_fp32(ctx, W, nr, kp, X32, Q));  // Q is free again
+    TSVM_TRY(pad_rows(ctx, Q, kp, nr, k, Z, ldz));
   }
   TSVM_CUDA(cudaEventRecord(ev[5], ctx->stream));
   std::vector<double> hw(k);

@@ -373,7 +373,8 @@ extern "C" tsvm_status tsvm_hypergrad(tsvm_context *ctx, const float *X, const f
   if (!ctx || !X || !y || !Xv || !yv || !alpha || !xi || !s || !res || n < 2 || nv < 1 || d < 1 ||
       d > kKMaxD || k < 1 || k > 1000 || k > n || !(gamma > 0) || !(C > 0))
     return TSVM_ERR_INVALID_ARGUMENT;
-  if (precision < TSVM_PREC_FP32 || precision > TSVM_PREC_FP16) return TSVM_ERR_INVALID_ARGUMENT;
+  if (!precision_valid(precision)) return TSVM_ERR_INVALID_ARGUMENT;
+  if (ctx && sharded(ctx)) return TSVM_ERR_UNSUPPORTED;
   TSVM_CUDA(cudaSetDevice(ctx->device));
   TraceRange trace_call("tsvm_hypergrad");
   const auto t0 = std::chrono::steady_clock::now();

@@ -832,11 +832,12 @@ __device__ void scalar_stage(double *__restrict__ sc, const double *red, int sta
 }
 
 // Sum block partials in fixed order; the last block also reduces the scalars and runs the
-// scalar stage of the iteration.
+// scalar stage of the iteration -- or, with red_out set (row-sharded solves), stores the
+// reduced sums and minima there for the collective, after which scalar_stage_kernel runs.
 __global__ void finalize_kernel(const double *__restrict__ part_vec, int nblk, int nvec,
                                 double *__restrict__ out_vec, const double *__restrict__ part_s,
                                 int ns, int nm, double *__restrict__ sc, int stage,
-                                const int *__restrict__ info) {
+                                const int *__restrict__ info, double *__restrict__ red_out) {
   // vector blocks: 32 entries each, the partials split over 8 warps (strided), then summed in
   // warp order -- a fixed order, independent of timing
   const int vb = (nvec + 31) / 32;
@@ -870,7 +871,17 @@ __global__ void finalize_kernel(const double *__restrict__ part_vec, int nblk, i
   }
   __syncthreads();
   if (threadIdx.x != 0) return;
+  if (red_out) {
+    for (int j = 0; j < ns + nm; ++j) red_out[j] = red[j];
+    return;
+  }
   scalar_stage(sc, red, stage, info);
+}
+
+// The scalar stage on sums / minima completed across the ranks (row-sharded solves).
+__global__ void scalar_stage_kernel(double *__restrict__ sc, const double *__restrict__ red,
+                                    int stage, const int *__restrict__ info) {
+  if (threadIdx.x == 0) scalar_stage(sc, red, stage, info);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -906,6 +917,9 @@ struct Runner {
   const double *dinv;
 
   int *err;   // set by a streaming pass that timed out
+  // row-sharded solves: every finalize completes its sums / minima across the ranks
+  bool shard = false;
+  double *red_buf = nullptr;   // 16 doubles
 
   // One streaming pass (stream_kernel) with this solve's geometry: one CTA per SM, as many
   // chunk stages as fit in ~192 KB of shared memory (at least 2, at most 16, and room for the
@@ -1001,11 +1015,27 @@ struct Runner {
   tsvm_status finalize(int nparts, int nvec, double *out_vec, int ns, int nm, int stage) {
     const int vb = (nvec + 31) / 32;
     finalize_kernel<<<vb + 1, 256, 0, ctx->stream>>>(part_vec, nparts, nvec, out_vec, part_s, ns,
-                                                      nm, scal, stage, info);
+                                                      nm, scal, stage, info,
+                                                      shard ? red_buf : nullptr);
+    TSVM_LAUNCHED(ctx);
+    if (!shard) return TSVM_OK;
+    // the same collectives on every rank: the vector, the sums, the minima
+    TSVM_TRY(comm_allreduce(ctx, out_vec, nvec, 0, COMM_SUM));
+    TSVM_TRY(comm_allreduce(ctx, red_buf, ns, 0, COMM_SUM));
+    TSVM_TRY(comm_allreduce(ctx, red_buf + ns, nm, 0, COMM_MIN));
+    scalar_stage_kernel<<<1, 32, 0, ctx->stream>>>(scal, red_buf, stage, info);
     TSVM_LAUNCHED(ctx);
     return TSVM_OK;
   }
 };
+
+// Sum of the k x k matrix over the ranks when each rank's copy holds I + its rows' sum: the
+// identity is counted once.
+tsvm_status comm_capacitance(tsvm_context *ctx, double *M, int k) {
+  if (!sharded(ctx)) return TSVM_OK;
+  TSVM_TRY(comm_allreduce(ctx, M, (int64_t)k * k, 0, COMM_SUM));
+  return small_add_diag(ctx, M, k, k, -(double)(ctx->comm.world - 1));
+}
 
 }  // namespace
 
@@ -1030,6 +1060,7 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
   TSVM_TRY(scratch_t(ctx, SLOT_IPM_SCAL, (size_t)kNScal + 10 * (size_t)kz + 64, &sbuf));
   TSVM_TRY(scratch_t(ctx, SLOT_IPM_M, (size_t)k * k + (size_t)ceil_div(k, 32) * 1024, &M));
   double *Mdinv = M + (size_t)k * k;   // inverses of the 32 x 32 diagonal blocks of chol(M)
+  static_assert(3 * sizeof(int) <= 8 * sizeof(double), "status words before red_buf");
   double *part = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_IPM_PART, (size_t)run.nblk * (2 * kz + 16), &part));
   run.part_vec = part;
@@ -1043,6 +1074,11 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
   run.info = reinterpret_cast<int *>(cv + 2 * kz);   // [0] Cholesky/refinement status,
   int *big_count = run.info + 1;                     // [1] rows summed exactly in FP64,
   run.err = run.info + 2;                            // [2] streaming-pass timeout
+  run.red_buf = cv + 2 * kz + 8;                     // 16 doubles (row-sharded solves)
+  run.shard = sharded(ctx);
+  // rows of the whole problem (this rank's n when the problem is not sharded)
+  double n_global = (double)n;
+  TSVM_TRY(comm_sum_host(ctx, &n_global));
 
   Vecs V;
   V.x = vecbuf;
@@ -1078,7 +1114,7 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
 
   double hsc[kNScal] = {0};
   hsc[I_C] = C;
-  hsc[I_N] = (double)n;
+  hsc[I_N] = n_global;
   TSVM_CUDA(cudaMemcpyAsync(run.scal, hsc, sizeof(hsc), cudaMemcpyHostToDevice, ctx->stream));
   TSVM_CUDA(cudaMemsetAsync(run.info, 0, 3 * sizeof(int), ctx->stream));
 
@@ -1134,6 +1170,11 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
                               ctx->stream));
     TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
     memcpy(sc, ctx->host_scalars, sizeof(sc));
+    if (run.shard) {   // a rank whose pass timed out takes the others out with it
+      double e = host_info[2] ? 1.0 : 0.0;
+      TSVM_TRY(comm_sum_host(ctx, &e));
+      if (e > 0.0) return TSVM_ERR_TIMEOUT;
+    }
     if (host_info[2]) return TSVM_ERR_TIMEOUT;
     if (pending_events) {
       ms_syrk += event_ms(ev_syrk0, ev_syrk1);
@@ -1166,7 +1207,7 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
     }
     const double mu = sc[I_MU], nrd = sc[I_NORMRD], nrp = fabs(sc[I_RP]), cond = sc[I_COND];
     if (t_gap < 0 && sc[I_RELGAP] <= 1e-6) {
-      const double scale = 1.0 + sqrt((double)n);
+      const double scale = 1.0 + sqrt(n_global);
       if (nrd / scale <= 1e-6 && nrp / scale <= 1e-6)
         t_gap = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
     }
@@ -1183,7 +1224,7 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
       break;
     }
     if (opt.rel_gap_tol > 0) {
-      const double scale = 1.0 + sqrt((double)n);
+      const double scale = 1.0 + sqrt(n_global);
       if (sc[I_RELGAP] <= opt.rel_gap_tol && nrd / scale <= opt.rel_gap_tol &&
           nrp / scale <= opt.rel_gap_tol) {
         result = TSVM_OK;
@@ -1205,8 +1246,10 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
       TSVM_TRY(big_rows(ctx, V.dinv, n, tau, big_idx, big_count));
       TSVM_TRY(gram_fp64_rows(ctx, Z, ldz, n, k, big_idx, big_count, V.dinv, G64));
       TSVM_TRY(syrk_capacitance_tc(ctx, Z, ldz, n, k, V.dinv, tau, 2, G64, M));
+      TSVM_TRY(comm_capacitance(ctx, M, k));
     } else {
       TSVM_TRY(gram_fp64(ctx, Z, ldz, Z, ldz, n, k, k, true, M, V.dinv));
+      TSVM_TRY(comm_allreduce(ctx, M, (int64_t)k * k, 0, COMM_SUM));
       TSVM_TRY(small_add_diag(ctx, M, k, k, 1.0));
     }
     TSVM_CUDA(cudaEventRecord(ev_syrk1, ctx->stream));
@@ -1315,7 +1358,7 @@ __global__ void first_free_kernel(const double *__restrict__ alpha, int64_t n, d
 __global__ void bias_terms_kernel(const float *__restrict__ Z, int64_t ldz, int k,
                                   const float *__restrict__ y, const double *__restrict__ v,
                                   const int64_t *__restrict__ idx, const int *__restrict__ count,
-                                  double *__restrict__ out) {
+                                  double *__restrict__ out, double *__restrict__ slot) {
   // one warp per selected free SV j: b_j = y_j - y_j (v . Z_j); out[0..1] = mean, std
   __shared__ double bj[64];
   const int m = *count;
@@ -1329,6 +1372,11 @@ __global__ void bias_terms_kernel(const float *__restrict__ Z, int64_t ldz, int 
   }
   __syncthreads();
   if (threadIdx.x == 0) {
+    if (slot) {   // row-sharded: this rank's terms, merged across the ranks afterwards
+      slot[0] = (double)m;
+      for (int t = 0; t < m; ++t) slot[1 + t] = bj[t];
+      return;
+    }
     if (m == 0) {
       out[0] = NAN;
       out[1] = NAN;
@@ -1342,6 +1390,31 @@ __global__ void bias_terms_kernel(const float *__restrict__ Z, int64_t ldz, int 
     out[0] = mean;
     out[1] = sqrt(ss / m);
   }
+}
+
+// Row-sharded bias: terms[r * 51] = rank r's count m_r (<= 50), then its m_r terms in index
+// order.  The ranks hold consecutive row ranges in rank order, so the first <= 50 free SVs of
+// the whole problem are the ranks' terms taken in rank order.
+__global__ void bias_merge_kernel(const double *__restrict__ terms, int world, double *out) {
+  if (threadIdx.x != 0) return;
+  double take[50];
+  int m = 0;
+  for (int r = 0; r < world && m < 50; ++r) {
+    const int mr = (int)terms[(int64_t)r * 51];
+    for (int t = 0; t < mr && m < 50; ++t) take[m++] = terms[(int64_t)r * 51 + 1 + t];
+  }
+  if (m == 0) {
+    out[0] = NAN;
+    out[1] = NAN;
+    return;
+  }
+  double mean = 0.0;
+  for (int t = 0; t < m; ++t) mean += take[t];
+  mean /= m;
+  double ss = 0.0;
+  for (int t = 0; t < m; ++t) ss += (take[t] - mean) * (take[t] - mean);
+  out[0] = mean;
+  out[1] = sqrt(ss / m);
 }
 
 }  // namespace
@@ -1371,13 +1444,28 @@ tsvm_status bias_rbf(tsvm_context *ctx, const float *Z, int ldz, const float *y,
   int *cnt = reinterpret_cast<int *>(idx + 64);
   run.info = cnt + 1;
   run.err = cnt + 2;
+  run.red_buf = out + 4 + 64 + 8;   // 16 doubles after idx and the status words
+  run.shard = sharded(ctx);
   TSVM_CUDA(cudaMemsetAsync(run.err, 0, sizeof(int), ctx->stream));
   TSVM_TRY(run.vec(BiasCountOp{alpha, C}, ST_INIT));  // counts into I_E2SUM / I_E2SQ slots
   TSVM_TRY(run.zt(BiasRhsOp{alpha}, v, ST_NONE));
   first_free_kernel<<<1, 1024, 0, ctx->stream>>>(alpha, n, C, 50, idx, cnt);
   TSVM_LAUNCHED(ctx);
-  bias_terms_kernel<<<1, 256, 0, ctx->stream>>>(Z, ldz, k, y, v, idx, cnt, out);
-  TSVM_LAUNCHED(ctx);
+  if (run.shard) {
+    const int world = ctx->comm.world;
+    double *terms = nullptr;
+    TSVM_TRY(scratch_t(ctx, SLOT_COMM, (size_t)world * 51 + 8, &terms));
+    TSVM_CUDA(cudaMemsetAsync(terms, 0, sizeof(double) * world * 51, ctx->stream));
+    bias_terms_kernel<<<1, 256, 0, ctx->stream>>>(Z, ldz, k, y, v, idx, cnt, out,
+                                                    terms + (size_t)ctx->comm.rank * 51);
+    TSVM_LAUNCHED(ctx);
+    TSVM_TRY(comm_allreduce(ctx, terms, (int64_t)world * 51, 0, COMM_SUM));
+    bias_merge_kernel<<<1, 32, 0, ctx->stream>>>(terms, world, out);
+    TSVM_LAUNCHED(ctx);
+  } else {
+    bias_terms_kernel<<<1, 256, 0, ctx->stream>>>(Z, ldz, k, y, v, idx, cnt, out, nullptr);
+    TSVM_LAUNCHED(ctx);
+  }
   double hs[2], hb[2];
   int herr = 0;
   TSVM_CUDA(cudaMemcpyAsync(hs, run.scal + I_E2SUM, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));

@@ -24,7 +24,8 @@ template <int KPT>
 __global__ void __launch_bounds__(256, 1)
 kermatmul_simt_kernel(const float *__restrict__ Xc, const float *__restrict__ norms,
                       const float *__restrict__ y, int64_t n, int d, float g2,
-                      const float *__restrict__ A, float *__restrict__ W) {
+                      const float *__restrict__ A, float *__restrict__ W, int64_t i_begin,
+                      int64_t i_end) {
   constexpr int KP = KPT * 16;
   extern __shared__ float4 smem4[];
   float *sm = reinterpret_cast<float *>(smem4);
@@ -39,17 +40,18 @@ kermatmul_simt_kernel(const float *__restrict__ Xc, const float *__restrict__ no
 
   const int tid = threadIdx.x;
   const int tx = tid & 15, ty = tid >> 4;
-  const int64_t i0 = (int64_t)blockIdx.x * kTI;
+  // rows I of this CTA: [i0, i0 + kTI) within [i_begin, i_end); J runs over all n rows
+  const int64_t i0 = i_begin + (int64_t)blockIdx.x * kTI;
 
   for (int e = tid; e < kTI * d; e += 256) {
     const int r = e / d, c = e % d;
     const int64_t gi = i0 + r;
-    XI[c * kTI + r] = gi < n ? Xc[gi * d + c] : 0.f;
+    XI[c * kTI + r] = gi < i_end ? Xc[gi * d + c] : 0.f;
   }
   for (int r = tid; r < kTI; r += 256) {
     const int64_t gi = i0 + r;
-    nI[r] = gi < n ? norms[gi] : 0.f;
-    yI[r] = gi < n ? y[gi] : 0.f;
+    nI[r] = gi < i_end ? norms[gi] : 0.f;
+    yI[r] = gi < i_end ? y[gi] : 0.f;
   }
 
   float acc[8][KPT];
@@ -120,24 +122,25 @@ kermatmul_simt_kernel(const float *__restrict__ Xc, const float *__restrict__ no
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
     const int64_t gi = i0 + ty * 8 + r;
-    if (gi >= n) continue;
+    if (gi >= i_end) continue;
 #pragma unroll
     for (int m = 0; m < KPT / 4; ++m)
-      reinterpret_cast<float4 *>(W + gi * KP + m * 64)[tx] =
+      reinterpret_cast<float4 *>(W + (gi - i_begin) * KP + m * 64)[tx] =
           make_float4(acc[r][4 * m + 0], acc[r][4 * m + 1], acc[r][4 * m + 2], acc[r][4 * m + 3]);
   }
 }
 
 template <int KPT>
 tsvm_status launch_simt(tsvm_context *ctx, const float *Xc, const float *norms, const float *y,
-                        int64_t n, int d, float g2, const float *A, float *W) {
+                        int64_t n, int d, float g2, const float *A, float *W, int64_t row0,
+                        int64_t nr) {
   constexpr int KP = KPT * 16;
   const size_t smem = sizeof(float) * (size_t)(kMaxD * kTI + kMaxD * kTJ + kTJ * kTI + kTJ * KP +
                                                2 * kTI + 2 * kTJ);
   TSVM_CUDA(cudaFuncSetAttribute(kermatmul_simt_kernel<KPT>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kermatmul_simt_kernel<KPT><<<(unsigned)ceil_div(n, kTI), 256, smem, ctx->stream>>>(
-      Xc, norms, y, n, d, g2, A, W);
+  kermatmul_simt_kernel<KPT><<<(unsigned)ceil_div(nr, kTI), 256, smem, ctx->stream>>>(
+      Xc, norms, y, n, d, g2, A, W, row0, row0 + nr);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;
 }
@@ -146,8 +149,10 @@ tsvm_status launch_simt(tsvm_context *ctx, const float *Xc, const float *norms, 
 
 tsvm_status kermatmul_fp32(tsvm_context *ctx, const float *Xc, const float *norms,
                            const float *y, int64_t n, int d, double gamma, const float *A,
-                           int kp, float *W) {
+                           int kp, float *W, int64_t row0, int64_t nr) {
   if (d < 1 || d > kMaxD || kp % 64 != 0 || kp <= 0) return TSVM_ERR_UNSUPPORTED;
+  if (nr < 0) nr = n - row0;
+  if (row0 < 0 || nr < 1 || row0 + nr > n) return TSVM_ERR_INVALID_ARGUMENT;
   const float g2 = (float)(-gamma * 1.4426950408889634);
   // Columns are processed in chunks of at most 256 (the register tile); each chunk is an
   // independent launch over a column slice of A and W with the same leading dimension kp.
@@ -155,23 +160,23 @@ tsvm_status kermatmul_fp32(tsvm_context *ctx, const float *Xc, const float *norm
   // launching on compact per-chunk copies when kp > 256.
   if (kp <= 256) {
     switch (kp / 16) {
-      case 4: return launch_simt<4>(ctx, Xc, norms, y, n, d, g2, A, W);
-      case 8: return launch_simt<8>(ctx, Xc, norms, y, n, d, g2, A, W);
-      case 12: return launch_simt<12>(ctx, Xc, norms, y, n, d, g2, A, W);
-      case 16: return launch_simt<16>(ctx, Xc, norms, y, n, d, g2, A, W);
+      case 4: return launch_simt<4>(ctx, Xc, norms, y, n, d, g2, A, W, row0, nr);
+      case 8: return launch_simt<8>(ctx, Xc, norms, y, n, d, g2, A, W, row0, nr);
+      case 12: return launch_simt<12>(ctx, Xc, norms, y, n, d, g2, A, W, row0, nr);
+      case 16: return launch_simt<16>(ctx, Xc, norms, y, n, d, g2, A, W, row0, nr);
       default: return TSVM_ERR_UNSUPPORTED;
     }
   }
   // kp > 256: split columns into 256-wide slabs (plus remainder) through compact buffers.
   float *Ac = nullptr, *Wc = nullptr;
-  TSVM_TRY(scratch_t(ctx, SLOT_W2, (size_t)n * 256 * 2, &Ac));
+  TSVM_TRY(scratch_t(ctx, SLOT_W2, (size_t)(n + nr) * 256, &Ac));
   Wc = Ac + (size_t)n * 256;
   for (int c0 = 0; c0 < kp; c0 += 256) {
     const int w = kp - c0 < 256 ? kp - c0 : 256;
     TSVM_CUDA(cudaMemcpy2DAsync(Ac, (size_t)w * 4, A + c0, (size_t)kp * 4, (size_t)w * 4, n,
                                 cudaMemcpyDeviceToDevice, ctx->stream));
-    TSVM_TRY(kermatmul_fp32(ctx, Xc, norms, y, n, d, gamma, Ac, w, Wc));
-    TSVM_CUDA(cudaMemcpy2DAsync(W + c0, (size_t)kp * 4, Wc, (size_t)w * 4, (size_t)w * 4, n,
+    TSVM_TRY(kermatmul_fp32(ctx, Xc, norms, y, n, d, gamma, Ac, w, Wc, row0, nr));
+    TSVM_CUDA(cudaMemcpy2DAsync(W + c0, (size_t)kp * 4, Wc, (size_t)w * 4, (size_t)w * 4, nr,
                                 cudaMemcpyDeviceToDevice, ctx->stream));
   }
   return TSVM_OK;

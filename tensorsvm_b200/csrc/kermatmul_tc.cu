@@ -124,6 +124,33 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
   }
 }
 
+// hi = the pair rounded to the 16-bit type, lo = what the rounding left out, rounded again:
+// hi + lo carries about twice the bits of one 16-bit value.
+template <bool BF16>
+__device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t &lo) {
+  if constexpr (BF16) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    const float2 hf = __bfloat1622float2(h);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+    hi = *reinterpret_cast<const uint32_t *>(&h);
+    lo = *reinterpret_cast<const uint32_t *>(&l);
+  } else {
+    const __half2 h = __floats2half2_rn(a, b);
+    const float2 hf = __half22float2(h);
+    const __half2 l = __floats2half2_rn(a - hf.x, b - hf.y);
+    hi = *reinterpret_cast<const uint32_t *>(&h);
+    lo = *reinterpret_cast<const uint32_t *>(&l);
+  }
+}
+
+// Operand splits that carry a pass's accuracy-setting operand in two 16-bit parts (hi + lo),
+// each contracted by its own MMA into the same FP32 accumulator:
+//   kSplitP: the kernel block P (range-finder pass, W = K Q): its rounding perturbs the kernel
+//            the range is found of, while rounding the Gaussian sketch only draws another sketch;
+//   kSplitA: the kernel-block operand (projection pass, K W): rounding the orthonormal basis W
+//            tilts the subspace the kernel is projected on, while P's rounding averages out.
+constexpr int kSplitNone = 0, kSplitP = 1, kSplitA = 2;
+
 // ---------------------------------------------------------------------------------------
 // The fused kernel, persistent: grid.x <= SM count, CTA c takes the 128-row blocks c, c + G,
 // c + 2G, ... (G = gridDim.x) in turn, and every CTA walks the J blocks in the same order, so
@@ -138,14 +165,19 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
 // buffer is free again when that MMA completes.  XA and W are single-buffered: the next row
 // block's XA is loaded once the last Gram MMA of the previous one completed (xaempty), and its
 // first P AT^T MMA waits for the epilogue to have read W out of TMEM (wempty).
+// SPLIT == kSplitP: the exp warps write P's hi part over the buffer's first 32 columns and its
+// lo part over the other 32, and the issuer runs W += P_hi AT^T + P_lo AT^T.
+// SPLIT == kSplitA: every J block takes two consecutive slots of the kernel-operand ring, AT_hi
+// (map_at) and AT_lo (map_atlo), and the issuer runs W += P AT_hi^T + P AT_lo^T.
 // ---------------------------------------------------------------------------------------
 constexpr int kSBufs = 4;
 
-template <bool BF16, int NPOLY, int KG, bool SHIFT>
+template <bool BF16, int NPOLY, int KG, bool SHIFT, int SPLIT>
 __global__ void __launch_bounds__(kThreadsTC, 1)
 kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
                     const __grid_constant__ CUtensorMap map_xb,
-                    const __grid_constant__ CUtensorMap map_at, const float *__restrict__ y,
+                    const __grid_constant__ CUtensorMap map_at,
+                    const __grid_constant__ CUtensorMap map_atlo, const float *__restrict__ y,
                     const float *__restrict__ inv_scale, const float *__restrict__ ccol,
                     int64_t n, int nrb, int ntiles, int kp, int c0, int kpw,
                     float *__restrict__ W, int64_t ldw, int *__restrict__ err) {
@@ -239,16 +271,22 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
     // ---------------- TMA producer: kernel-block operand ring ----------------
     if (lane == 0) {
       asm volatile("prefetch.tensormap [%0];" ::"l"(&map_at) : "memory");
+      if constexpr (SPLIT == kSplitA) asm volatile("prefetch.tensormap [%0];" ::"l"(&map_atlo) : "memory");
       const uint32_t at_bytes = (uint32_t)kpw * kBJ * 2;
+      constexpr int kParts = SPLIT == kSplitA ? 2 : 1;
       int st = 0;
       uint32_t ph = 0;
       bool ok = true;
       for (int rb = blockIdx.x; ok && rb < nrb; rb += G) {
-        for (int t = 0; t < ntiles; ++t) {
-          if (!mbar_wait(b_atempty + 8 * st, ph ^ 1, abort)) { ok = false; break; }
-          mbar_expect_tx(b_atfull + 8 * st, at_bytes);
-          tma_load_2d(&map_at, b_atfull + 8 * st, base + L.at(st), 0, t * kp + c0);
-          if (++st == kAtStages) { st = 0; ph ^= 1; }
+        for (int t = 0; ok && t < ntiles; ++t) {
+#pragma unroll
+          for (int part = 0; part < kParts; ++part) {
+            if (!mbar_wait(b_atempty + 8 * st, ph ^ 1, abort)) { ok = false; break; }
+            mbar_expect_tx(b_atfull + 8 * st, at_bytes);
+            tma_load_2d(part == 0 ? &map_at : &map_atlo, b_atfull + 8 * st, base + L.at(st), 0,
+                        t * kp + c0);
+            if (++st == kAtStages) { st = 0; ph ^= 1; }
+          }
         }
       }
     }
@@ -298,7 +336,11 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
         if (r > 0 && !mbar_wait(b_wempty, (r - 1) & 1, abort)) break;
         tc_fence_after();
         for (int t = 0; t < ntiles; ++t) {
+          // SPLIT == kSplitA: the J block's AT_lo sits in the ring slot after its AT_hi
+          const int st2 = st + 1 == kAtStages ? 0 : st + 1;
+          const uint32_t sph2 = st + 1 == kAtStages ? sph ^ 1 : sph;
           if (!mbar_wait(b_atfull + 8 * st, sph, abort) ||
+              (SPLIT == kSplitA && !mbar_wait(b_atfull + 8 * st2, sph2, abort)) ||
               !mbar_wait(b_pfull + 8 * b, bph, abort)) {
             ok = false;
             break;
@@ -309,9 +351,24 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
 #pragma unroll
           for (int kk = 0; kk < kBJ / 16; ++kk)
             umma_ts(t_w, ap + kk * 8, dat + 2 * kk, id2, (t > 0 || kk > 0) ? 1u : 0u);
+          if constexpr (SPLIT == kSplitP) {
+#pragma unroll
+            for (int kk = 0; kk < kBJ / 16; ++kk)   // P_lo over the buffer's columns 32..63
+              umma_ts(t_w, ap + kBJ / 2 + kk * 8, dat + 2 * kk, id2, 1u);
+          }
+          if constexpr (SPLIT == kSplitA) {
+            const uint64_t dat2 = dat0 + (uint64_t)(st2 * at_step);
+#pragma unroll
+            for (int kk = 0; kk < kBJ / 16; ++kk)
+              umma_ts(t_w, ap + kk * 8, dat2 + 2 * kk, id2, 1u);
+          }
           umma_commit(b_free + 8 * b);
           umma_commit(b_atempty + 8 * st);
           if (++st == kAtStages) { st = 0; sph ^= 1; }
+          if constexpr (SPLIT == kSplitA) {
+            umma_commit(b_atempty + 8 * st);
+            if (++st == kAtStages) { st = 0; sph ^= 1; }
+          }
           if (++b == kSBufs) { b = 0; bph ^= 1; }
         }
         if (ok) umma_commit(b_wfull);
@@ -342,7 +399,20 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
         tmem_ld32(tb + 32, s1);
         tmem_wait_ld();
         uint32_t pk[32];
-        if constexpr (SHIFT) {
+        if constexpr (SPLIT == kSplitP) {
+          uint32_t pl[32];
+#pragma unroll
+          for (int c = 0; c < 16; ++c)
+            split2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c]), 2 * c) - shift,
+                         exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c + 1]), 2 * c + 1) - shift,
+                         pk[c], pl[c]);
+#pragma unroll
+          for (int c = 0; c < 16; ++c)
+            split2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c]), 2 * c) - shift,
+                         exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c + 1]), 2 * c + 1) - shift,
+                         pk[16 + c], pl[16 + c]);
+          tmem_st32(tb + kBJ / 2, pl);   // P_lo over the buffer's columns 32..63
+        } else if constexpr (SHIFT) {
 #pragma unroll
           for (int c = 0; c < 16; ++c)
             pk[c] = pack2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c]), 2 * c) - shift,
@@ -407,15 +477,16 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
 // Operand preparation
 // ---------------------------------------------------------------------------------------
 // XA/XB rows (n_pad x 64 FP16) from centred features: see the file comment for the layout.
+// Either output may be null (a row-sharded factor builds XA for its own rows and XB for all).
 __global__ void prep_gram_operands(const float *__restrict__ Xc, int64_t n, int64_t n_pad, int d,
                                    int KG, double scale, __half *__restrict__ XA,
                                    __half *__restrict__ XB) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_pad) return;
-  __half *a = XA + i * KG, *b = XB + i * KG;
+  __half *a = XA ? XA + i * KG : nullptr, *b = XB ? XB + i * KG : nullptr;
   for (int c = 0; c < KG; ++c) {
-    a[c] = __float2half_rn(0.f);
-    b[c] = __float2half_rn(0.f);
+    if (a) a[c] = __float2half_rn(0.f);
+    if (b) b[c] = __float2half_rn(0.f);
   }
   if (i >= n) return;
   double nn = 0.0;
@@ -424,12 +495,16 @@ __global__ void prep_gram_operands(const float *__restrict__ Xc, int64_t n, int6
     nn += xt * xt;
     const __half hi = __float2half_rn((float)xt);
     const __half lo = __float2half_rn((float)(xt - (double)__half2float(hi)));
-    a[c] = hi;
-    a[d + c] = lo;
-    a[2 * d + c] = hi;
-    b[c] = hi;
-    b[d + c] = hi;
-    b[2 * d + c] = lo;
+    if (a) {
+      a[c] = hi;
+      a[d + c] = lo;
+      a[2 * d + c] = hi;
+    }
+    if (b) {
+      b[c] = hi;
+      b[d + c] = hi;
+      b[2 * d + c] = lo;
+    }
   }
   const double v = 0.5 * nn;
   const __half h = __float2half_rn((float)v);
@@ -438,10 +513,14 @@ __global__ void prep_gram_operands(const float *__restrict__ Xc, int64_t n, int6
   const __half l = __float2half_rn((float)(r1 - (double)__half2float(m)));
   const __half one = __float2half_rn(1.f);
   const int o = 3 * d;
-  a[o + 0] = one; a[o + 1] = one; a[o + 2] = one;
-  a[o + 3] = __hneg(h); a[o + 4] = __hneg(m); a[o + 5] = __hneg(l);
-  b[o + 0] = __hneg(h); b[o + 1] = __hneg(m); b[o + 2] = __hneg(l);
-  b[o + 3] = one; b[o + 4] = one; b[o + 5] = one;
+  if (a) {
+    a[o + 0] = one; a[o + 1] = one; a[o + 2] = one;
+    a[o + 3] = __hneg(h); a[o + 4] = __hneg(m); a[o + 5] = __hneg(l);
+  }
+  if (b) {
+    b[o + 0] = __hneg(h); b[o + 1] = __hneg(m); b[o + 2] = __hneg(l);
+    b[o + 3] = one; b[o + 4] = one; b[o + 5] = one;
+  }
 }
 
 __global__ void sumsq_partial(const float *__restrict__ A, int64_t count, double *__restrict__ part) {
@@ -500,12 +579,23 @@ __device__ __forceinline__ float round16(float v) {
     return __bfloat162float(__float2bfloat16_rn(v));
 }
 
+// With ATlo set, the operand is split: AT holds the rounded hi part and ATlo (same layout) the
+// rounding remainder, rounded again; the column sums are those of hi + lo.
+template <typename T>
+__device__ __forceinline__ T to16(float v) {
+  if constexpr (std::is_same<T, __half>::value)
+    return __float2half_rn(v);
+  else
+    return __float2bfloat16_rn(v);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256)
 prep_at(const float *A, const float *__restrict__ y, int64_t n, int64_t n_pad, int kp,
-        const float *__restrict__ scale, T *__restrict__ AT, float *round_back,
-        double *__restrict__ cpart) {
+        const float *__restrict__ scale, T *__restrict__ AT, T *__restrict__ ATlo,
+        float *round_back, double *__restrict__ cpart) {
   __shared__ float tile[32][33];
+  __shared__ float tile_lo[32][33];
   __shared__ double red[8][33];
   const int c0 = blockIdx.y * 32;
   const float s = scale[0], inv_s = scale[1];
@@ -515,14 +605,17 @@ prep_at(const float *A, const float *__restrict__ y, int64_t n, int64_t n_pad, i
     for (int r = threadIdx.y; r < 32; r += blockDim.y) {
       const int64_t j = j0 + r;
       const int c = c0 + threadIdx.x;
-      float v = 0.f;
+      float v = 0.f, vl = 0.f;
       if (j < n && c < kp) {
         const float yj = y[j];
-        v = round16<T>(A[j * kp + c] * yj * s);
+        const float x = A[j * kp + c] * yj * s;
+        v = round16<T>(x);
+        if (ATlo) vl = round16<T>(x - v);
         if (round_back) round_back[j * kp + c] = v * inv_s * yj;
       }
       tile[r][threadIdx.x] = v;
-      csum += (double)v;
+      tile_lo[r][threadIdx.x] = vl;
+      csum += (double)v + (double)vl;
     }
     __syncthreads();
     for (int r = threadIdx.y; r < 32; r += blockDim.y) {
@@ -530,10 +623,8 @@ prep_at(const float *A, const float *__restrict__ y, int64_t n, int64_t n_pad, i
       const int64_t j = j0 + threadIdx.x;
       if (c < kp && j < n_pad) {
         const int64_t o = ((j / kBJ) * kp + c) * kBJ + (j % kBJ);
-        if constexpr (sizeof(T) == 2 && std::is_same<T, __half>::value)
-          AT[o] = __float2half_rn(tile[threadIdx.x][r]);
-        else
-          AT[o] = __float2bfloat16_rn(tile[threadIdx.x][r]);
+        AT[o] = to16<T>(tile[threadIdx.x][r]);
+        if (ATlo) ATlo[o] = to16<T>(tile_lo[threadIdx.x][r]);
       }
     }
   }
@@ -619,9 +710,9 @@ __global__ void column_shift(const double *__restrict__ cpart, int nparts, int k
 // ---------------------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------------------
-using TcKernel = void (*)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const float *,
-                          const float *, const float *, int64_t, int, int, int, int, int, float *,
-                          int64_t, int *);
+using TcKernel = void (*)(const CUtensorMap, const CUtensorMap, const CUtensorMap,
+                          const CUtensorMap, const float *, const float *, const float *, int64_t,
+                          int, int, int, int, int, float *, int64_t, int *);
 
 // Exps per 8 columns evaluated by the FMA-pipe polynomial (the rest on MUFU); tunable through
 // TSVM_TC_POLY (0, 2, 4, 6 or 8) for the autotuning sweep in the benchmarks.
@@ -634,24 +725,36 @@ int poly_split() {
   return v;
 }
 
-TcKernel select_kernel(bool bf16, int npoly, int KG, bool shift) {
-  if (shift) {   // flat kernels: MUFU exps only
-    if (KG == 128) return bf16 ? kermatmul_tc_kernel<true, 0, 128, true> : kermatmul_tc_kernel<false, 0, 128, true>;
-    if (KG == 192) return bf16 ? kermatmul_tc_kernel<true, 0, 192, true> : kermatmul_tc_kernel<false, 0, 192, true>;
-    return bf16 ? kermatmul_tc_kernel<true, 0, 64, true> : kermatmul_tc_kernel<false, 0, 64, true>;
-  }
-  if (KG == 128) return bf16 ? kermatmul_tc_kernel<true, 0, 128, false> : kermatmul_tc_kernel<false, 0, 128, false>;
-  if (KG == 192) return bf16 ? kermatmul_tc_kernel<true, 0, 192, false> : kermatmul_tc_kernel<false, 0, 192, false>;
+template <int SPLIT>
+TcKernel select_split(bool bf16, int KG, bool shift) {
+  // MUFU exps only
+#define TSVM_SEL(K, S)                                                                   \
+  if (KG == K && shift == S)                                                             \
+    return bf16 ? kermatmul_tc_kernel<true, 0, K, S, SPLIT> : kermatmul_tc_kernel<false, 0, K, S, SPLIT>;
+  TSVM_SEL(64, true)
+  TSVM_SEL(128, true)
+  TSVM_SEL(192, true)
+  TSVM_SEL(64, false)
+  TSVM_SEL(128, false)
+  TSVM_SEL(192, false)
+#undef TSVM_SEL
+  return nullptr;
+}
+
+TcKernel select_kernel(bool bf16, int npoly, int KG, bool shift, int split) {
+  if (split == kSplitP) return select_split<kSplitP>(bf16, KG, shift);
+  if (split == kSplitA) return select_split<kSplitA>(bf16, KG, shift);
+  if (shift || KG != 64) return select_split<kSplitNone>(bf16, KG, shift);
 #define TSVM_SEL(P) \
   if (npoly == P) \
-    return bf16 ? kermatmul_tc_kernel<true, P, 64, false> : kermatmul_tc_kernel<false, P, 64, false>;
+    return bf16 ? kermatmul_tc_kernel<true, P, 64, false, kSplitNone> : kermatmul_tc_kernel<false, P, 64, false, kSplitNone>;
   TSVM_SEL(0)
   TSVM_SEL(2)
   TSVM_SEL(4)
   TSVM_SEL(6)
   TSVM_SEL(8)
 #undef TSVM_SEL
-  return bf16 ? kermatmul_tc_kernel<true, 4, 64, false> : kermatmul_tc_kernel<false, 4, 64, false>;
+  return bf16 ? kermatmul_tc_kernel<true, 4, 64, false, kSplitNone> : kermatmul_tc_kernel<false, 4, 64, false, kSplitNone>;
 }
 
 // Gram K for d features: 3 d split products + 6 norm terms, rounded up to a 64-wide chunk.
@@ -674,18 +777,26 @@ bool kermatmul_tc_supported(int d, int kp) {
 
 tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms, const float *y,
                          int64_t n, int d, double gamma, const float *A, int kp, float *W,
-                         int precision, float *kernel_ms, float *round_back) {
+                         int precision, float *kernel_ms, float *round_back, int split,
+                         int64_t row0, int64_t nr) {
   (void)norms;
   if (!kermatmul_tc_supported(d, kp)) return TSVM_ERR_UNSUPPORTED;
-  const bool bf16 = precision == TSVM_PREC_BF16;
-  const int64_t n_pad = round_up(n, kBM);
+  if (split < kSplitNone || split > kSplitA) return TSVM_ERR_INVALID_ARGUMENT;
+  if (nr < 0) nr = n - row0;
+  if (row0 < 0 || nr < 1 || row0 + nr > n) return TSVM_ERR_INVALID_ARGUMENT;
+  const bool rows = row0 != 0 || nr != n;   // only the rows [row0, row0 + nr) of W
+  const bool bf16 = precision_is_bf16(precision);
+  const int64_t n_pad = round_up(n, kBM);          // J side (XB, AT): all rows
+  const int64_t nr_pad = round_up(nr, kBM);        // I side (XA, W): this call's rows
   const int KG = gram_k(d);
-  // operands
+  // operands: [XA (nr_pad rows) | XB (n_pad rows)]
   __half *XA = nullptr;
-  TSVM_TRY(scratch_t(ctx, SLOT_OPX, (size_t)2 * n_pad * KG, &XA));
-  __half *XB = XA + (size_t)n_pad * KG;
+  TSVM_TRY(scratch_t(ctx, SLOT_OPX, (size_t)(nr_pad + n_pad) * KG, &XA));
+  __half *XB = XA + (size_t)nr_pad * KG;
   uint16_t *AT = nullptr;
-  TSVM_TRY(scratch_t(ctx, SLOT_OPA, (size_t)kp * n_pad, &AT));
+  const size_t at_elems = (size_t)kp * n_pad;
+  TSVM_TRY(scratch_t(ctx, SLOT_OPA, (split == kSplitA ? 2 : 1) * at_elems, &AT));
+  uint16_t *ATlo = split == kSplitA ? AT + at_elems : nullptr;
   // SLOT_MISC: sum-of-squares partials [nb] | scale: s, 1/s, shift, - (4 floats) | err |
   // kernel-moment row sums [2 m] | column-sum partials [rg][kp] | ccol [kp floats]
   const int nb = ctx->num_sms * 2;
@@ -700,9 +811,18 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
   double *samp = part + o_samp, *cpart = part + o_cpart;
   float *ccol = reinterpret_cast<float *>(part + o_ccol);   // o_ccol is even: 16-byte aligned
   const double xscale = sqrt(2.0 * gamma * 1.4426950408889634);
-  prep_gram_operands<<<(unsigned)ceil_div(n_pad, 256), 256, 0, ctx->stream>>>(
-      Xc, n, n_pad, d, KG, xscale, XA, XB);
-  TSVM_LAUNCHED(ctx);
+  if (rows) {
+    prep_gram_operands<<<(unsigned)ceil_div(n_pad, 256), 256, 0, ctx->stream>>>(
+        Xc, n, n_pad, d, KG, xscale, nullptr, XB);
+    TSVM_LAUNCHED(ctx);
+    prep_gram_operands<<<(unsigned)ceil_div(nr_pad, 256), 256, 0, ctx->stream>>>(
+        Xc + row0 * d, nr, nr_pad, d, KG, xscale, XA, nullptr);
+    TSVM_LAUNCHED(ctx);
+  } else {   // XA and XB of the same rows in one pass
+    prep_gram_operands<<<(unsigned)ceil_div(n_pad, 256), 256, 0, ctx->stream>>>(
+        Xc, n, n_pad, d, KG, xscale, XA, XB);
+    TSVM_LAUNCHED(ctx);
+  }
   sumsq_partial<<<nb, 256, 0, ctx->stream>>>(A, n * (int64_t)kp, part);
   TSVM_LAUNCHED(ctx);
   choose_scale<<<1, 256, 0, ctx->stream>>>(part, nb, n * (int64_t)kp, scale);
@@ -718,35 +838,40 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
   const dim3 tgrid((unsigned)rg, (unsigned)ceil_div(kp, 32));
   if (bf16)
     prep_at<__nv_bfloat16><<<tgrid, dim3(32, 8), 0, ctx->stream>>>(
-        A, y, n, n_pad, kp, scale, reinterpret_cast<__nv_bfloat16 *>(AT), round_back, cpart);
+        A, y, n, n_pad, kp, scale, reinterpret_cast<__nv_bfloat16 *>(AT),
+        reinterpret_cast<__nv_bfloat16 *>(ATlo), round_back, cpart);
   else
     prep_at<__half><<<tgrid, dim3(32, 8), 0, ctx->stream>>>(
-        A, y, n, n_pad, kp, scale, reinterpret_cast<__half *>(AT), round_back, cpart);
+        A, y, n, n_pad, kp, scale, reinterpret_cast<__half *>(AT), reinterpret_cast<__half *>(ATlo),
+        round_back, cpart);
   TSVM_LAUNCHED(ctx);
   column_shift<<<(unsigned)ceil_div(kp, 256), 256, 0, ctx->stream>>>(cpart, rg, kp, scale, ccol);
   TSVM_LAUNCHED(ctx);
   TSVM_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
 
   CUtensorMap mxa, mxb;
-  if (!make_map(&mxa, XA, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, KG, n_pad, 64, kBM) ||
+  if (!make_map(&mxa, XA, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, KG, nr_pad, 64, kBM) ||
       !make_map(&mxb, XB, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, KG, n_pad, 64, kBJ))
     return TSVM_ERR_CUDA;
   const int ntiles = (int)(n_pad / kBJ);
-  const int nrb = (int)(n_pad / kBM);
+  const int nrb = (int)(nr_pad / kBM);
   const unsigned grid = (unsigned)(nrb < ctx->num_sms ? nrb : ctx->num_sms);
   cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
   TSVM_CUDA(cudaEventRecord(e0, ctx->stream));
   for (int c0 = 0; c0 < kp; c0 += kMaxSlab) {
     const int kpw = kp - c0 < kMaxSlab ? kp - c0 : kMaxSlab;
-    CUtensorMap mat;
-    if (!make_map(&mat, AT, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
-                  kBJ, (uint64_t)ntiles * kp, kBJ, kpw))
+    CUtensorMap mat, matlo;
+    const CUtensorMapDataType at_type =
+        bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    if (!make_map(&mat, AT, at_type, kBJ, (uint64_t)ntiles * kp, kBJ, kpw) ||
+        !make_map(&matlo, ATlo ? ATlo : AT, at_type, kBJ, (uint64_t)ntiles * kp, kBJ, kpw))
       return TSVM_ERR_CUDA;
     const size_t smem = tc_smem(KG, kpw);
-    auto kern = select_kernel(bf16, poly_split(), KG, hshift != 0.f);
+    auto kern = select_kernel(bf16, poly_split(), KG, hshift != 0.f, split);
+    if (!kern) return TSVM_ERR_UNSUPPORTED;
     TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<grid, kThreadsTC, smem, ctx->stream>>>(mxa, mxb, mat, y, scale + 1, ccol, n, nrb,
-                                                  ntiles, kp, c0, kpw, W, kp, err);
+    kern<<<grid, kThreadsTC, smem, ctx->stream>>>(mxa, mxb, mat, matlo, y + row0, scale + 1,
+                                                  ccol, nr, nrb, ntiles, kp, c0, kpw, W, kp, err);
     TSVM_LAUNCHED(ctx);
   }
   TSVM_CUDA(cudaEventRecord(e1, ctx->stream));

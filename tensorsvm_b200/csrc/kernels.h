@@ -12,6 +12,8 @@ namespace tsvm {
 // ---- sketch.cu -------------------------------------------------------------------------
 // The reference's gaussrand() stream (count floats, contiguous) into Q.
 tsvm_status sketch_glibc(tsvm_context *ctx, int64_t count, float *Q);
+// count N(0, 1) values of the counter-based Philox4x32-10 + Box-Muller sketch (Q 16-byte aligned)
+tsvm_status sketch_philox(tsvm_context *ctx, uint64_t seed, int64_t count, float *Q);
 // Raw glibc rand() stream (count values) into out (device).
 tsvm_status glibc_rand_stream(tsvm_context *ctx, int64_t count, uint32_t *out);
 
@@ -31,18 +33,28 @@ tsvm_status label_rows(tsvm_context *ctx, const float *X, const float *y, int64_
 
 // ---- kermatmul_simt.cu -----------------------------------------------------------------
 // W (n x kp) = (Y K Y) A (n x kp), K_ij = exp(-gamma ||xc_i - xc_j||^2); FP32 SIMT.
-// kp must be a multiple of 64; d <= 64.
+// kp must be a multiple of 64; d <= 64.  With a row range, W holds only the rows
+// [row0, row0 + nr) of the product (nr rows), still summed over all n rows of A.
 tsvm_status kermatmul_fp32(tsvm_context *ctx, const float *Xc, const float *norms,
                            const float *y, int64_t n, int d, double gamma, const float *A,
-                           int kp, float *W);
+                           int kp, float *W, int64_t row0 = 0, int64_t nr = -1);
 
 // ---- kermatmul_tc.cu -------------------------------------------------------------------
 bool kermatmul_tc_supported(int d, int kp);
 // Tensor-core (tcgen05) version; precision TSVM_PREC_FP16 or TSVM_PREC_BF16 for P and A.
 // round_back (may be A itself, or null) receives A rounded to the 16-bit operand type.
+// split: 0 one product; 1 the kernel block P as hi + lo (two products); 2 the operand A as
+// hi + lo (two products).
 tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms, const float *y,
                          int64_t n, int d, double gamma, const float *A, int kp, float *W,
-                         int precision, float *kernel_ms, float *round_back = nullptr);
+                         int precision, float *kernel_ms, float *round_back = nullptr,
+                         int split = 0, int64_t row0 = 0, int64_t nr = -1);
+
+// Precision classes of tsvm_precision.
+inline bool precision_valid(int p) { return p >= TSVM_PREC_FP32 && p <= TSVM_PREC_FP16_FAST; }
+inline bool precision_is_bf16(int p) { return p == TSVM_PREC_BF16 || p == TSVM_PREC_BF16_FAST; }
+// the tensor-core forms that split the accuracy-setting operand of each factor pass
+inline bool precision_is_split(int p) { return p == TSVM_PREC_BF16 || p == TSVM_PREC_FP16; }
 
 // A unit of batched work: rows [row0, row0 + rows) of problem p; goff is the index of the
 // unit's first row in the problems' concatenated per-row vectors.
@@ -149,9 +161,12 @@ struct FactorKeep {
   double *R;
   float *W;
 };
+// With a row range (row0, nr) the rows [row0, row0 + nr) of Z are computed (Z holds nr rows)
+// against all n rows of X, across the ranks of ctx's communicator (keep must be null).
 tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_t n, int d,
                        double gamma, int k, int precision, int sketch, const float *Q_user,
-                       float *Z, int ldz, tsvm_factor_info *info, FactorKeep *keep = nullptr);
+                       float *Z, int ldz, tsvm_factor_info *info, FactorKeep *keep = nullptr,
+                       int64_t row0 = 0, int64_t nr = -1);
 
 // ---- predict.cu ---------------------------------------------------------------------------
 // Decision values of m rows under a model (device arrays); asynchronous on ctx->stream.

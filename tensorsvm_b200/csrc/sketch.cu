@@ -23,6 +23,7 @@
 //     the accept pattern and to <= 1 ulp in value.
 #include <math.h>
 
+#include <algorithm>
 #include <array>
 #include <vector>
 
@@ -298,6 +299,75 @@ tsvm_status sketch_glibc(tsvm_context *ctx, int64_t count, float *Q) {
     attempts_d *= 1.25;
   }
   return TSVM_ERR_SKETCH;
+}
+
+}  // namespace tsvm
+
+// ---------------------------------------------------------------------------------------
+// Counter-based Gaussian sketch (TSVM_SKETCH_PHILOX): Philox4x32-10 (Salmon, Moraes, Dror,
+// Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC 2011) keyed by the 64-bit seed,
+// counter (block, 0, 0, 0) for the block of four entries 4 block .. 4 block + 3 of the
+// row-major n x k sketch; the four words become two Box-Muller pairs.  Every entry depends only
+// on (seed, index), not on the launch shape, so any grid reproduces the same matrix.
+// ---------------------------------------------------------------------------------------
+namespace tsvm {
+namespace {
+
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+    const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += 0x9E3779B9u;
+    k.y += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// (0, 1): the top 24 bits of the word, centred on their cell
+__device__ __forceinline__ float philox_uniform(uint32_t x) {
+  return ((float)(x >> 8) + 0.5f) * (1.0f / 16777216.0f);
+}
+
+__global__ void __launch_bounds__(256) sketch_philox_kernel(uint64_t seed, int64_t count,
+                                                            float *__restrict__ Q) {
+  const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+  const int64_t blocks = (count + 3) / 4;
+  for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < blocks;
+       b += (int64_t)gridDim.x * blockDim.x) {
+    const uint4 r = philox4x32_10(make_uint4((uint32_t)b, (uint32_t)(b >> 32), 0u, 0u), key);
+    float z[4];
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      const float u0 = philox_uniform(p == 0 ? r.x : r.z);
+      const float u1 = philox_uniform(p == 0 ? r.y : r.w);
+      const float rad = sqrtf(-2.0f * logf(u0));
+      float s, c;
+      sincospif(2.0f * u1, &s, &c);
+      z[2 * p] = rad * c;
+      z[2 * p + 1] = rad * s;
+    }
+    const int64_t e = 4 * b;
+    if (e + 3 < count) {
+      reinterpret_cast<float4 *>(Q)[b] = make_float4(z[0], z[1], z[2], z[3]);
+    } else {
+      for (int q = 0; q < 4 && e + q < count; ++q) Q[e + q] = z[q];
+    }
+  }
+}
+
+}  // namespace
+
+tsvm_status sketch_philox(tsvm_context *ctx, uint64_t seed, int64_t count, float *Q) {
+  if (count < 0 || !Q || (reinterpret_cast<uintptr_t>(Q) & 15) != 0)
+    return TSVM_ERR_INVALID_ARGUMENT;
+  if (count == 0) return TSVM_OK;
+  const int64_t blocks = (count + 3) / 4;
+  const unsigned grid = (unsigned)std::min<int64_t>((int64_t)ctx->num_sms * 8, (blocks + 255) / 256);
+  sketch_philox_kernel<<<grid, 256, 0, ctx->stream>>>(seed, count, Q);
+  TSVM_LAUNCHED(ctx);
+  return TSVM_OK;
 }
 
 }  // namespace tsvm

@@ -39,10 +39,18 @@ tsvm_status tsvm_test_sketch(tsvm_context *ctx, int64_t count, float *out) {
   return TSVM_OK;
 }
 
+tsvm_status tsvm_test_sketch_philox(tsvm_context *ctx, uint64_t seed, int64_t count, float *out) {
+  if (!ctx || !out || count < 0) return TSVM_ERR_INVALID_ARGUMENT;
+  TSVM_TRY(sketch_philox(ctx, seed, count, out));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSVM_OK;
+}
+
 tsvm_status tsvm_test_kermatmul(tsvm_context *ctx, const float *X, const float *y, int64_t n,
                                 int32_t d, double gamma, const float *A, int32_t kp, float *W,
-                                int32_t precision) {
+                                int32_t precision, int32_t split) {
   if (!ctx || !X || !y || !A || !W || n < 1 || d < 1 || kp < 1) return TSVM_ERR_INVALID_ARGUMENT;
+  if (!precision_valid(precision) || split < 0 || split > 2) return TSVM_ERR_INVALID_ARGUMENT;
   float *Xc = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_XC, (size_t)n * d + (size_t)n + 64, &Xc));
   float *norms = Xc + (size_t)n * d;
@@ -52,7 +60,8 @@ tsvm_status tsvm_test_kermatmul(tsvm_context *ctx, const float *X, const float *
     TSVM_TRY(kermatmul_fp32(ctx, Xc, norms, y, n, d, gamma, A, kp, W));
   } else {
     if (!kermatmul_tc_supported(d, kp)) return TSVM_ERR_UNSUPPORTED;
-    TSVM_TRY(kermatmul_tc(ctx, Xc, norms, y, n, d, gamma, A, kp, W, precision, &ms));
+    TSVM_TRY(kermatmul_tc(ctx, Xc, norms, y, n, d, gamma, A, kp, W, precision, &ms, nullptr,
+                          split));
   }
   TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
   return TSVM_OK;

@@ -134,7 +134,7 @@ def test_kermatmul_fp32(ctx, n, d, kp):
     g = 0.05
     Xd, yd, Ad = dev(X), dev(y), dev(A)   # keep the device copies alive across the call
     _lib.check(ctx.lib.tsvm_test_kermatmul(ctx.handle, P(Xd), P(yd), n, d, g, P(Ad), kp,
-                                           P(W), _lib.PREC_FP32), "kermatmul")
+                                           P(W), _lib.PREC_FP32, 0), "kermatmul")
     ref = orc.kermatmul(X, y, g, A)
     err = np.linalg.norm(W.cpu().numpy() - ref) / np.linalg.norm(ref)
     assert err < 2e-6, err
@@ -153,7 +153,7 @@ def test_kermatmul_tensor_core(ctx, n, d, kp, prec, tol):
     g = 0.05
     Xd, yd, Ad = dev(X), dev(y), dev(A)
     _lib.check(ctx.lib.tsvm_test_kermatmul(ctx.handle, P(Xd), P(yd), n, d, g, P(Ad), kp,
-                                           P(W), prec), "kermatmul_tc")
+                                           P(W), prec, 0), "kermatmul_tc")
     ref = orc.kermatmul(X, y, g, A)
     err = np.linalg.norm(W.cpu().numpy() - ref) / np.linalg.norm(ref)
     assert err < tol, err
@@ -171,7 +171,7 @@ def test_kermatmul_tensor_core_distance_precision(ctx):
     W = torch.empty((n, kp), dtype=torch.float32, device="cuda")
     Xd, yd, Ad = dev(X), dev(y), dev(A)
     _lib.check(ctx.lib.tsvm_test_kermatmul(ctx.handle, P(Xd), P(yd), n, d, 0.5, P(Ad), kp, P(W),
-                                           _lib.PREC_FP16), "kermatmul_tc")
+                                           _lib.PREC_FP16, 0), "kermatmul_tc")
     ref = orc.kermatmul(X, y, 0.5, A)
     assert np.max(np.abs(W.cpu().numpy() - ref)) < 2e-3 * np.max(np.abs(ref))
 
@@ -188,9 +188,60 @@ def test_kermatmul_tensor_core_exp_split(ctx, npoly, monkeypatch):
     W = torch.empty((n, kp), dtype=torch.float32, device="cuda")
     Xd, yd, Ad = dev(X), dev(y), dev(A)
     _lib.check(ctx.lib.tsvm_test_kermatmul(ctx.handle, P(Xd), P(yd), n, d, 0.05, P(Ad), kp, P(W),
-                                           _lib.PREC_FP16), "kermatmul_tc")
+                                           _lib.PREC_FP16, 0), "kermatmul_tc")
     ref = orc.kermatmul(X, y, 0.05, A)
     assert np.linalg.norm(W.cpu().numpy() - ref) / np.linalg.norm(ref) < 2e-3
+
+
+def _kermatmul(ctx, X, y, g, A, prec, split):
+    n, kp = A.shape
+    W = torch.empty((n, kp), dtype=torch.float32, device="cuda")
+    Xd, yd, Ad = dev(X), dev(y), dev(A)
+    _lib.check(ctx.lib.tsvm_test_kermatmul(ctx.handle, P(Xd), P(yd), n, X.shape[1], g, P(Ad), kp,
+                                           P(W), prec, split), "kermatmul_tc")
+    return W.cpu().numpy()
+
+
+@pytest.mark.parametrize("n,d,kp", [(3001, 18, 64), (1000, 18, 448), (1500, 28, 256),
+                                    (900, 54, 448)])
+@pytest.mark.parametrize("prec,tol_split,tol_one", [(_lib.PREC_FP16, 2e-5, 2e-4),
+                                                    (_lib.PREC_BF16, 2e-4, 2e-3)])
+def test_kermatmul_kernel_block_split(ctx, n, d, kp, prec, tol_split, tol_one):
+    """The kernel block as hi + lo (the range-finder pass): with an operand that the 16-bit type
+    holds exactly, only the kernel block's rounding is left, and the split removes it."""
+    rng = np.random.default_rng(7 * n + kp)
+    X = rng.standard_normal((n, d)).astype(np.float32)
+    y = np.where(rng.random(n) < 0.5, 1.0, -1.0).astype(np.float32)
+    A = rng.standard_normal((n, kp)).astype(np.float16 if prec == _lib.PREC_FP16 else np.float32)
+    if prec == _lib.PREC_BF16:   # round to bf16 on the host
+        A = (A.view(np.uint32) & np.uint32(0xFFFF0000)).view(np.float32)
+    A = A.astype(np.float32)
+    ref = orc.kermatmul(X, y, 0.05, A)
+    e_split = np.linalg.norm(_kermatmul(ctx, X, y, 0.05, A, prec, 1) - ref) / np.linalg.norm(ref)
+    e_one = np.linalg.norm(_kermatmul(ctx, X, y, 0.05, A, prec, 0) - ref) / np.linalg.norm(ref)
+    assert e_split < tol_split, (e_split, e_one)
+    assert e_one > 4 * e_split
+
+
+@pytest.mark.parametrize("n,kp", [(2048, 64), (3001, 256), (1000, 448)])
+@pytest.mark.parametrize("prec,tol_split", [(_lib.PREC_FP16, 2e-6), (_lib.PREC_BF16, 2e-5)])
+def test_kermatmul_operand_split(ctx, n, kp, prec, tol_split):
+    """The operand as hi + lo (the projection pass): on points in well-separated groups of exact
+    duplicates the kernel block is exactly 0 or 1, so only the operand's rounding is left, and
+    the split removes it (the one-product form keeps a 16-bit rounding of A)."""
+    rng = np.random.default_rng(n + 3 * kp)
+    d = 18
+    # squared distances between centres ~2300 (exp2 of the scaled distance underflows the
+    # 16-bit types), within a group the Gram product leaves |S| << 2^-12, so exp2 rounds to 1
+    centres = 8.0 * rng.standard_normal((8, d)).astype(np.float32)
+    X = centres[rng.integers(0, 8, n)]
+    y = np.where(rng.random(n) < 0.5, 1.0, -1.0).astype(np.float32)
+    A = rng.standard_normal((n, kp)).astype(np.float32)
+    ref = orc.kermatmul(X, y, 0.05, A)
+    e_split = np.linalg.norm(_kermatmul(ctx, X, y, 0.05, A, prec, 2) - ref) / np.linalg.norm(ref)
+    e_one = np.linalg.norm(_kermatmul(ctx, X, y, 0.05, A, prec, 0) - ref) / np.linalg.norm(ref)
+    assert e_split < tol_split, (e_split, e_one)
+    assert e_one > 10 * e_split
 
 
 @pytest.mark.parametrize("spacing", [1, 700, 1025])
@@ -211,3 +262,31 @@ def test_bias_first_free_svs_spread_over_many_rounds(ctx, spacing):
     assert (nsv, nfree) == (len(sv), len(fr))
     assert abs(b - b_ref) <= 1e-9 * max(1.0, abs(b_ref))
     assert abs(bstd - bstd_ref) <= 1e-9 * max(1.0, abs(bstd_ref))
+
+
+@pytest.mark.parametrize("seed,count", [(0, 1), (1, 7), (12345, 4096), (2 ** 40 + 3, 1_000_001)])
+def test_philox_sketch_matches_oracle(ctx, seed, count):
+    """TSVM_SKETCH_PHILOX against the oracle's FP64 restatement: the same Philox words (the
+    uniforms agree exactly), FP32 logf / sqrtf / sincospif within a few ulp."""
+    out = torch.empty(max(count, 4), dtype=torch.float32, device="cuda")
+    _lib.check(ctx.lib.tsvm_test_sketch_philox(ctx.handle, seed, count, P(out)), "philox")
+    got = out.cpu().numpy()[:count].astype(np.float64)
+    ref = orc.philox_sketch(seed, count)
+    assert np.max(np.abs(got - ref)) < 2e-5 * max(1.0, np.max(np.abs(ref)))
+    out2 = torch.empty_like(out)
+    _lib.check(ctx.lib.tsvm_test_sketch_philox(ctx.handle, seed, count, P(out2)), "philox")
+    assert torch.equal(out[:count], out2[:count])
+
+
+def test_factor_with_philox_sketch_matches_oracle(ctx):
+    from tensorsvm_b200 import api
+    X, y = synth.two_gaussians(3000, 18, seed=9)
+    g, k = 0.05, 48
+    Z, _ = api.factor(ctx, dev(X), dev(y), g, k, "fp32", philox_seed=99)
+    Q = orc.philox_sketch(99, 3000 * k).reshape(3000, k).astype(np.float32)
+    f = orc.lra(X, y, g, k, Q=Q.astype(np.float64))
+    Zh = Z.cpu().numpy()[:, :k].astype(np.float64)
+    G, Gr = Zh @ Zh.T, f.U @ f.U.T
+    assert np.linalg.norm(G - Gr) / np.linalg.norm(Gr) < 1e-4
+    Z2, _ = api.factor(ctx, dev(X), dev(y), g, k, "fp32", philox_seed=100)
+    assert not torch.equal(Z, Z2)

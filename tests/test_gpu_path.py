@@ -193,7 +193,13 @@ def test_cli_end_to_end(tmp_path):
     assert np.mean(np.sign(dv) == np.sign(dv_o)) >= 0.995
 
 
-@pytest.mark.parametrize("prec", ["fp16", "bf16"])
+# Z Z^T of the tensor-core factor against the FP64 oracle's.  Split forms (the kernel block as
+# hi + lo in the range-finder pass, the basis as hi + lo in the projection pass): about FP32
+# accuracy; one-product forms: the 16-bit rounding of both operands.
+FACTOR_TOL = {"fp16": 5e-5, "bf16": 5e-4, "fp16_fast": 2e-3, "bf16_fast": 2e-2}
+
+
+@pytest.mark.parametrize("prec", ["fp16", "bf16", "fp16_fast", "bf16_fast"])
 def test_factor_tensor_core_matches_oracle(ctx, c1, prec):
     X, y, g, C, k = c1
     Z, info = api.factor(ctx, dev(X), dev(y), g, k, prec)
@@ -201,10 +207,10 @@ def test_factor_tensor_core_matches_oracle(ctx, c1, prec):
     f = orc.lra(X, y, g, k)
     G, Gr = Zh @ Zh.T, f.U @ f.U.T
     err = np.linalg.norm(G - Gr) / np.linalg.norm(Gr)
-    assert err < (2e-3 if prec == "fp16" else 2e-2), err
+    assert err < FACTOR_TOL[prec], err
 
 
-@pytest.mark.parametrize("prec", ["fp16", "bf16"])
+@pytest.mark.parametrize("prec", ["fp16", "bf16", "fp16_fast", "bf16_fast"])
 def test_factor_tensor_core_wide_features(ctx, prec):
     # d = 54 (the covtype-shaped config): Gram K = 192 on the tensor cores
     X, y, g, C, k = synth.make("c3", n=3000)
@@ -214,22 +220,28 @@ def test_factor_tensor_core_wide_features(ctx, prec):
     f = orc.lra(X, y, g, k)
     G, Gr = Zh @ Zh.T, f.U @ f.U.T
     err = np.linalg.norm(G - Gr) / np.linalg.norm(Gr)
-    assert err < (2e-3 if prec == "fp16" else 2e-2), err
+    assert err < FACTOR_TOL[prec], err
 
 
-def test_train_tensor_core_against_fp64_oracle(ctx, c1):
+# Against the FP64 oracle (same sketch, same algorithm) on config 1's test split: objective
+# and decision-value signs of the exact-kernel model (the model file's decision function).
+# The FP16 split form is held to the bars of the tensor-core form (objective 1e-5, >= 99.9%
+# signs); the others are held to what they measure, stated here.
+@pytest.mark.parametrize("prec,pobj_tol,signs", [("fp16", 1e-5, 0.999), ("bf16", 2e-5, 0.99),
+                                                 ("fp16_fast", 1e-4, 0.98)])
+def test_train_tensor_core_against_fp64_oracle(ctx, c1, prec, pobj_tol, signs):
     X, y, g, C, k = c1
-    m = api.train(ctx, X, y, _lib.KERNEL_RBF, g, C, k, "fp16")
+    m = api.train(ctx, X, y, _lib.KERNEL_RBF, g, C, k, prec)
     f, r, b = orc.train_rbf(X, y, g, C, k)
     st = m.ipm_stats
-    assert abs(st["pobj"] - r.log[-1][5]) / abs(r.log[-1][5]) < 1e-3
+    assert abs(st["pobj"] - r.log[-1][5]) / abs(r.log[-1][5]) < pobj_tol
     Xt = synth.make("c1_test")[0]
     dv = orc.decision_values_dense(m.alpha, y, X, g, m.b, Xt)
     dv_o = orc.decision_values_dense(r.x, y, X, g, b, Xt)
-    # k = 32 keeps eigen-directions down to 3.6e-4 of the largest; FP16 rounding of the kernel
-    # block and the operand moves the weakest ones, and the flat rank-32 dual moves alpha along
-    # them: 98.7% sign agreement measured on this split (100% for the FP32 form)
-    assert np.mean(np.sign(dv) == np.sign(dv_o)) >= 0.98
+    # k = 32 keeps eigen-directions down to 3.6e-4 of the largest; the flat rank-32 dual moves
+    # alpha along them when the factor's weak directions move, which the 16-bit rounding of
+    # the kernel block (range finder) and of the basis (projection) does in the fast form
+    assert np.mean(np.sign(dv) == np.sign(dv_o)) >= signs
 
 
 @pytest.fixture(scope="module")
@@ -243,7 +255,9 @@ def flat_kernel_oracle():
     return X, y, g, C, k, f.eigvals, r.log[-1][5], fv
 
 
-@pytest.mark.parametrize("prec,pobj_tol,eig_tol", [("fp16", 3e-4, 0.05), ("bf16", 5e-2, 0.7)])
+@pytest.mark.parametrize("prec,pobj_tol,eig_tol", [("fp16", 5e-5, 0.01), ("bf16", 1e-3, 0.05),
+                                                   ("fp16_fast", 3e-4, 0.05),
+                                                   ("bf16_fast", 5e-2, 0.7)])
 def test_flat_kernel_tensor_core_against_fp64_oracle(ctx, flat_kernel_oracle, prec, pobj_tol,
                                                      eig_tol):
     # 16-bit rounding of entries near 1 would put noise of ~2 sigma sqrt(n) = 0.04 on the kernel,
@@ -260,5 +274,30 @@ def test_flat_kernel_tensor_core_against_fp64_oracle(ctx, flat_kernel_oracle, pr
     Zk = Z[:, :k].double()
     fv = (Zk @ (Zk.T @ (a * yd.double())) + b).cpu().numpy()
     assert np.mean(np.sign(fv) == np.sign(fv_o)) >= 0.999
-    if prec == "fp16":
+    if prec in ("fp16", "fp16_fast"):
         assert np.max(np.abs(fv - fv_o)) <= 2e-3 * np.max(np.abs(fv_o))
+
+
+def test_full_size_two_gaussians_against_reference_run(ctx):
+    """The benchmark workload itself (n = 1M, d = 18, k = 256, gamma 0.05, C 32, seed 2, 10%
+    label noise) through the FP16 tensor-core form, against the reference build's own run on
+    the same file (tests/golden/ref_c2_1000000.log and .model.head): its last logged iterate
+    pobj -2.481707792e7 / dobj -2.481707797e7 (T:1645), 785,145 SVs (19,396 free) and rho
+    0.060243 (T:384-396).  The reference file's first label is -1, which it maps to +1
+    (T:880-895): its labels are ours negated, the dual (alpha, objective) is the same and its
+    b is ours negated, so its rho (= -b_ref) is our b."""
+    X, y, g, C, k = synth.make("c2")
+    m = api.train(ctx, X, y, _lib.KERNEL_RBF, g, C, k, "fp16")
+    last = ref_log("ref_c2_1000000")[-1]
+    st = m.ipm_stats
+    assert abs(st["pobj"] - last[5]) / abs(last[5]) < 1e-5, (st["pobj"], last[5])
+    assert abs(st["dobj"] - last[6]) / abs(last[6]) < 1e-5, (st["dobj"], last[6])
+    sv, free = orc.sv_sets(m.alpha, C)
+    with open(os.path.join(os.path.dirname(__file__), "golden", "ref_c2_1000000.model.head")) as f:
+        head = dict(ln.split(" ", 1) for ln in f.read().split("\n") if " " in ln)
+    nsv_ref = int(head["total_sv"])
+    nfree_ref = int(head["nr_sv"].split()[0])
+    assert abs(len(sv) - nsv_ref) <= 1e-3 * nsv_ref, (len(sv), nsv_ref)
+    assert abs(len(free) - nfree_ref) <= 0.02 * nfree_ref, (len(free), nfree_ref)
+    # b is a mean over the first 50 free SVs, whose spread is 0.014 in the reference's run
+    assert abs(m.b - float(head["rho"])) < 0.01, (m.b, head["rho"])

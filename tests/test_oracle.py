@@ -164,3 +164,23 @@ def test_lra_full_rank_reproduces_kernel():
     f = orc.lra(X, y, 0.3, 96)
     K = orc.labelled_kernel(X, y, 0.3)
     assert np.linalg.norm(f.U @ f.U.T - K) / np.linalg.norm(K) < 1e-5
+
+
+def test_philox_restatement_known_answers():
+    """The oracle's Philox4x32-10 against the generator's published known-answer vectors
+    (counter, key) -> output words."""
+    kat = [((0, 0, 0, 0), (0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
+           ((0xffffffff,) * 4, (0xffffffff,) * 2, (0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd)),
+           ((0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344), (0xa4093822, 0x299f31d0),
+            (0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1))]
+    for ctr, key, want in kat:
+        got = orc.philox4x32_10([np.array([v], np.uint64) for v in ctr], key)[:, 0]
+        assert tuple(int(v) for v in got) == want
+
+
+def test_philox_sketch_moments_and_seeds():
+    z = orc.philox_sketch(7, 1_000_003)
+    assert abs(z.mean()) < 5e-3 and abs(z.var() - 1.0) < 5e-3
+    assert abs(np.mean(z ** 4) - 3.0) < 3e-2                 # Gaussian kurtosis
+    assert np.array_equal(z[:1000], orc.philox_sketch(7, 1000))
+    assert not np.allclose(z[:1000], orc.philox_sketch(8, 1000))
