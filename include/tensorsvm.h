@@ -215,6 +215,25 @@ tsvm_status tsvm_factor_rows(tsvm_context *ctx, const float *X, const float *y, 
                              int32_t precision, int32_t sketch, const float *Q_user, float *Z,
                              int32_t ldz, tsvm_factor_info *info);
 
+/* One problem of a batched factorisation. */
+typedef struct tsvm_factor_problem {
+  const float *X;      /* device, n x d row-major */
+  const float *y;      /* device, n labels in {+1, -1} */
+  int64_t n;
+  double gamma;
+  float *Z;            /* device, n x ldz output (ldz = k rounded up to 64) */
+} tsvm_factor_problem;
+
+/* Kernel factors of `count` independent problems of the same d, k and precision (replaces
+ * running LRA, tensorsvm-train.cu:1941-2374, once per problem; the reference trains one problem
+ * per process).  Each problem runs its sketch, kernel-block passes, CholeskyQR and projection
+ * C = W^T (K W); then the eigen-decompositions of all the C's are one launch (one CTA per
+ * problem for k <= 128, side by side on their own SMs), and every Z = W V diag(sqrt(w+)) is
+ * formed in place.  infos[count] (may be NULL) receive each problem's factor statistics. */
+tsvm_status tsvm_factor_batched(tsvm_context *ctx, const tsvm_factor_problem *problems,
+                                int32_t count, int32_t d, int32_t k, int32_t precision,
+                                int32_t sketch, int32_t ldz, tsvm_factor_info *infos);
+
 /* Linear "factor": Z = diag(y) X, k = d (tensorsvm-train.cu:909-914).  Device buffers. */
 tsvm_status tsvm_linear_factor(tsvm_context *ctx, const float *X, const float *y, int64_t n,
                                int32_t d, float *Z, int32_t ldz);

@@ -46,7 +46,7 @@ EXPORTS = [
     "tsvm_train", "tsvm_kernel_launches", "tsvm_ipm_batched", "tsvm_hypergrad",
     "tsvm_decision_values", "tsvm_predict", "tsvm_kernel_residual", "tsvm_train_residual",
     "tsvm_read_libsvm", "tsvm_free", "tsvm_write_model", "tsvm_read_model", "tsvm_free_model",
-    "tsvm_set_comm", "tsvm_factor_rows", "tsvm_set_sketch_seed",
+    "tsvm_set_comm", "tsvm_factor_rows", "tsvm_set_sketch_seed", "tsvm_factor_batched",
 ]
 TEST_EXPORTS = [
     "tsvm_test_rand_stream", "tsvm_test_sketch", "tsvm_test_kermatmul", "tsvm_test_chol",
@@ -63,6 +63,11 @@ ALLREDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, 
 class Comm(ctypes.Structure):
     _fields_ = [("rank", ctypes.c_int32), ("world", ctypes.c_int32),
                 ("allreduce", ALLREDUCE_FN), ("user", ctypes.c_void_p)]
+
+
+class FactorProblem(ctypes.Structure):
+    _fields_ = [("X", ctypes.c_void_p), ("y", ctypes.c_void_p), ("n", ctypes.c_int64),
+                ("gamma", ctypes.c_double), ("Z", ctypes.c_void_p)]
 
 
 class IpmProblem(ctypes.Structure):
@@ -147,6 +152,9 @@ def load() -> ctypes.CDLL:
                                 ctypes.POINTER(FactorInfo)]
     lib.tsvm_set_sketch_seed.restype = ctypes.c_int
     lib.tsvm_set_sketch_seed.argtypes = [P, ctypes.c_uint64]
+    lib.tsvm_factor_batched.restype = ctypes.c_int
+    lib.tsvm_factor_batched.argtypes = [P, ctypes.POINTER(FactorProblem), I32, I32, I32, I32,
+                                        I32, I32, ctypes.POINTER(FactorInfo)]
     lib.tsvm_set_comm.restype = ctypes.c_int
     lib.tsvm_set_comm.argtypes = [P, ctypes.POINTER(Comm)]
     lib.tsvm_factor_rows.restype = ctypes.c_int

@@ -50,6 +50,24 @@ def factor(ctx, X, y, gamma: float, k: int, precision: str = "fp32", Q=None, ldz
     return Z, _fields(info)
 
 
+def factor_batched(ctx, Xs, ys, gammas, k: int, precision: str = "fp32"):
+    """Factors of many problems (tsvm_factor_batched): lists of CUDA tensors X (n_p x d), y and
+    gammas; returns the list of Z (n_p x round_up(k, 64)) and of factor statistics."""
+    import torch
+    kp = ((k + 63) // 64) * 64
+    count = len(Xs)
+    d = Xs[0].shape[1]
+    Zs = [torch.empty((X.shape[0], kp), dtype=torch.float32, device=X.device) for X in Xs]
+    probs = (_lib.FactorProblem * count)()
+    for p, (X, y, g, Z) in enumerate(zip(Xs, ys, gammas, Zs)):
+        probs[p] = _lib.FactorProblem(_ptr(X), _ptr(y), X.shape[0], float(g), _ptr(Z))
+    infos = (_lib.FactorInfo * count)()
+    st = ctx.lib.tsvm_factor_batched(ctx.handle, probs, count, d, k, PRECISIONS[precision],
+                                     _lib.SKETCH_GLIBC, kp, infos)
+    _lib.check(st, "tsvm_factor_batched")
+    return Zs, [_fields(i) for i in infos]
+
+
 def ipm(ctx, Z, y, k: int, C: float, kernel: int = _lib.KERNEL_RBF, want_xi: bool = False, **opts):
     """Solve the dual with Q = Z Z^T; returns (alpha f64 CUDA tensor, xi or None, y_mult, stats).
     With want_xi the multipliers s of alpha >= 0 are returned as stats["s"] as well."""

@@ -194,6 +194,21 @@ tsvm_status tsvm_factor_rows(tsvm_context *ctx, const float *X, const float *y, 
                     nullptr, row0, n_rows);
 }
 
+tsvm_status tsvm_factor_batched(tsvm_context *ctx, const tsvm_factor_problem *problems,
+                                int32_t count, int32_t d, int32_t k, int32_t precision,
+                                int32_t sketch, int32_t ldz, tsvm_factor_info *infos) {
+  if (!ctx || !problems || count < 1 || d < 1 || k < 1) return TSVM_ERR_INVALID_ARGUMENT;
+  if (!precision_valid(precision) || (sketch != TSVM_SKETCH_GLIBC && sketch != TSVM_SKETCH_PHILOX))
+    return TSVM_ERR_INVALID_ARGUMENT;
+  for (int p = 0; p < count; ++p)
+    if (!problems[p].X || !problems[p].y || !problems[p].Z || problems[p].n < 2)
+      return TSVM_ERR_INVALID_ARGUMENT;
+  if (sharded(ctx)) return TSVM_ERR_UNSUPPORTED;
+  TSVM_CUDA(cudaSetDevice(ctx->device));
+  TraceRange tr("tsvm_factor_batched");
+  return factor_rbf_batched(ctx, problems, count, d, k, precision, sketch, ldz, infos, nullptr);
+}
+
 tsvm_status tsvm_linear_factor(tsvm_context *ctx, const float *X, const float *y, int64_t n,
                                int32_t d, float *Z, int32_t ldz) {
   if (!ctx || !X || !y || !Z || n < 1 || d < 1 || ldz < d) return TSVM_ERR_INVALID_ARGUMENT;

@@ -52,6 +52,8 @@ enum Slot : int {
   SLOT_DEV_OUT,       // tsvm_train: device alpha
   SLOT_PRED_IN,       // tsvm_predict: device copies of the model and the rows
   SLOT_PRED_OUT,      // tsvm_predict: decision values
+  SLOT_B_EIG,         // batched factor: projections C, eigenvectors, eigenvalues
+  SLOT_B_EIGSW,       // batched factor: per-problem sweep counts
   SLOT_COMM,          // row-sharded path: staging of host values for the collectives
   SLOT_SHARD_A,       // row-sharded factor: the all-gathered kernel-block operand (all rows)
   SLOT_COUNT_

@@ -8,6 +8,8 @@
 // where noted.
 #include <math.h>
 
+#include <vector>
+
 #include "common.cuh"
 #include "context.h"
 #include "kernels.h"
@@ -453,10 +455,17 @@ __device__ __forceinline__ void round_pair(int m, int round, int ne, int &p, int
   q = 1 + b;
 }
 
+// Batched launches (grid.x problems): problem b reads A + b strideA and writes w + b strideW,
+// V + b strideV and sweeps_out[b]; the strides are 0 for a single problem.
 __global__ void __launch_bounds__(1024, 1)
 jacobi_small_kernel(const double *__restrict__ A, int n, int lda, int ne, int max_sweeps,
                     double tol, double *__restrict__ w, double *__restrict__ V,
-                    int *__restrict__ sweeps_out) {
+                    int *__restrict__ sweeps_out, int64_t strideA, int64_t strideW,
+                    int64_t strideV) {
+  A += blockIdx.x * strideA;
+  w += blockIdx.x * strideW;
+  V += blockIdx.x * strideV;
+  sweeps_out += blockIdx.x;
   extern __shared__ double2 jsh2[];
   const int np = ne / 2;
   double2 *rot = jsh2;                                    // [2][np] (c, s), by round parity
@@ -689,7 +698,7 @@ tsvm_status eig_jacobi_fp64(tsvm_context *ctx, double *A, int n, int lda, double
     TSVM_CUDA(cudaFuncSetAttribute(jacobi_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
     jacobi_small_kernel<<<1, 1024, smem, ctx->stream>>>(A, n, lda, ne, 40, 1e-13, w, V,
-                                                         sweeps_dev);
+                                                         sweeps_dev, 0, 0, 0);
     TSVM_LAUNCHED(ctx);
     int sweeps = 0;
     TSVM_CUDA(cudaMemcpyAsync(&sweeps, sweeps_dev, sizeof(int), cudaMemcpyDeviceToHost,
@@ -730,6 +739,45 @@ tsvm_status eig_jacobi_fp64(tsvm_context *ctx, double *A, int n, int lda, double
   TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
   if (sweeps_out) *sweeps_out = sweeps;
   if (sweeps < 0) return TSVM_ERR_TIMEOUT;
+  return TSVM_OK;
+}
+
+// count eigenproblems of width n (A: count x n x n row-major, contiguous; w: count x n;
+// V: count x n x n): one CTA per problem in one launch for n <= kJacobiSmallNe (the CTAs run
+// side by side on their own SMs), else one grid eigensolver after the other.
+tsvm_status eig_jacobi_fp64_batched(tsvm_context *ctx, double *A, int n, int count, double *w,
+                                    double *V, int *max_sweeps_out) {
+  if (n < 1 || n > 1024 || count < 1) return TSVM_ERR_UNSUPPORTED;
+  int ne = n + (n & 1);
+  if (ne < 2) ne = 2;
+  const int64_t nn = (int64_t)n * n;
+  if (ne > kJacobiSmallNe) {
+    int worst = 0;
+    for (int b = 0; b < count; ++b) {
+      int sw = 0;
+      TSVM_TRY(eig_jacobi_fp64(ctx, A + b * nn, n, n, w + (int64_t)b * n, V + b * nn, &sw));
+      worst = sw > worst ? sw : worst;
+    }
+    if (max_sweeps_out) *max_sweeps_out = worst;
+    return TSVM_OK;
+  }
+  int *sweeps_dev = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_B_EIGSW, (size_t)count, &sweeps_dev));
+  const int np = ne / 2;
+  const size_t smem = sizeof(double2) * 2 * np +
+                      sizeof(double) * (64 + (size_t)ne * (ne + 1) / 2 + (size_t)ne * ne);
+  TSVM_CUDA(cudaFuncSetAttribute(jacobi_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  jacobi_small_kernel<<<count, 1024, smem, ctx->stream>>>(A, n, n, ne, 40, 1e-13, w, V,
+                                                           sweeps_dev, nn, n, nn);
+  TSVM_LAUNCHED(ctx);
+  std::vector<int> sw(count);
+  TSVM_CUDA(cudaMemcpyAsync(sw.data(), sweeps_dev, sizeof(int) * count, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  int worst = 0;
+  for (int v : sw) worst = v > worst ? v : worst;
+  if (max_sweeps_out) *max_sweeps_out = worst;
   return TSVM_OK;
 }
 

@@ -184,7 +184,7 @@ static tsvm_status orthonormalise(tsvm_context *ctx, float *W, int64_t n, int k,
 tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_t n, int d,
                        double gamma, int k, int precision, int sketch, const float *Q_user,
                        float *Z, int ldz, tsvm_factor_info *info, FactorKeep *keep, int64_t row0,
-                       int64_t nr) {
+                       int64_t nr, double *C_out) {
   if (n < 2 || d < 1 || k < 1 || k > 1000 || ldz < k || !(gamma > 0)) return TSVM_ERR_INVALID_ARGUMENT;
   if (k > n) return TSVM_ERR_INVALID_ARGUMENT;
   if (nr < 0) nr = n - row0;
@@ -193,6 +193,7 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
   // nr rows; X, y and the pass operands all n)
   const bool rows = row0 != 0 || nr != n;
   if (rows && keep) return TSVM_ERR_UNSUPPORTED;
+  if (C_out && (rows || keep || ldz != (int)round_up(k, 64))) return TSVM_ERR_UNSUPPORTED;
   const int kp = (int)round_up(k, 64);
   cudaEvent_t *ev = ctx->ev;
   TracePhases phase;
@@ -275,6 +276,31 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
   TSVM_TRY(gram_fp64(ctx, W, kp, Q, kp, nr, k, k, false, Cm));
   TSVM_TRY(comm_allreduce(ctx, Cm, (int64_t)k * k, 0, COMM_SUM));   // row-sharded
   TSVM_TRY(small_symmetrize(ctx, Cm, k, k));
+  if (C_out) {   // stop here: the batched factor solves the eigenproblems of all problems at once
+    TSVM_CUDA(cudaMemcpyAsync(C_out, Cm, sizeof(double) * k * k, cudaMemcpyDeviceToDevice,
+                              ctx->stream));
+    TSVM_CUDA(cudaMemcpyAsync(Z, W, sizeof(float) * n * kp, cudaMemcpyDeviceToDevice,
+                              ctx->stream));
+    TSVM_CUDA(cudaEventRecord(ev[5], ctx->stream));
+    TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (info) {
+      info->n = n;
+      info->d = d;
+      info->k = k;
+      info->k_padded = kp;
+      info->precision = precision;
+      info->ms_sketch = event_ms(ev[0], ev[1]);
+      info->ms_pass1 = event_ms(ev[1], ev[2]);
+      info->ms_ortho = event_ms(ev[2], ev[3]);
+      info->ms_pass2 = event_ms(ev[3], ev[4]);
+      info->ms_project = event_ms(ev[4], ev[5]);
+      info->ms_total = event_ms(ev[0], ev[5]);
+      info->ms_kermatmul_kernel =
+          precision == TSVM_PREC_FP32 ? info->ms_pass1 + info->ms_pass2 : (double)km1 + km2;
+      info->flops_kermatmul = 2.0 * (2.0 * (double)n * n * k + 2.0 * (double)n * n * d);
+    }
+    return TSVM_OK;
+  }
   int sweeps = 0;
   TSVM_TRY(eig_jacobi_fp64(ctx, Cm, k, k, w, V, &sweeps));
   float *X32 = nullptr;
@@ -318,6 +344,61 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
         precision == TSVM_PREC_FP32 ? info->ms_pass1 + info->ms_pass2 : (double)km1 + km2;
     info->flops_kermatmul = 2.0 * (2.0 * (double)n * n * k + 2.0 * (double)n * n * d);
   }
+  return TSVM_OK;
+}
+
+tsvm_status factor_finish(tsvm_context *ctx, float *Z, int64_t n, int k, const double *V,
+                          const double *w, tsvm_factor_info *info) {
+  const int kp = (int)round_up(k, 64);
+  float *X32 = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_IPM_M, (size_t)kp * kp, &X32));
+  eigfactor_to_fp32<<<(unsigned)ceil_div((int64_t)kp * kp, 256), 256, 0, ctx->stream>>>(V, w, k,
+                                                                                         kp, X32);
+  TSVM_LAUNCHED(ctx);
+  // in place: every block reads all of its 128 rows before it writes them
+  TSVM_TRY(apply_right_fp32(ctx, Z, n, kp, X32, Z));
+  if (info) {
+    std::vector<double> hw(k);
+    TSVM_CUDA(cudaMemcpyAsync(hw.data(), w, sizeof(double) * k, cudaMemcpyDeviceToHost,
+                              ctx->stream));
+    TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+    int realk = 0;
+    double wmax = -INFINITY, wmin = INFINITY;
+    for (int i = 0; i < k; ++i) {
+      realk += hw[i] > 0.0;
+      wmax = fmax(wmax, hw[i]);
+      wmin = fmin(wmin, hw[i]);
+    }
+    info->realk = realk;
+    info->eig_max = wmax;
+    info->eig_min = wmin;
+  }
+  return TSVM_OK;
+}
+
+tsvm_status factor_rbf_batched(tsvm_context *ctx, const tsvm_factor_problem *pr, int count, int d,
+                               int k, int precision, int sketch, int ldz,
+                               tsvm_factor_info *infos, double *ms_eig) {
+  const int kp = (int)round_up(k, 64);
+  if (count < 1 || ldz != kp) return TSVM_ERR_INVALID_ARGUMENT;
+  double *buf = nullptr;   // [count][k][k] C, then [count][k][k] V, then [count][k] w
+  const size_t kk = (size_t)k * k;
+  TSVM_TRY(scratch_t(ctx, SLOT_B_EIG, (2 * kk + (size_t)k) * count, &buf));
+  double *Cb = buf, *Vb = buf + kk * count, *wb = Vb + kk * count;
+  for (int p = 0; p < count; ++p)
+    TSVM_TRY(factor_rbf(ctx, pr[p].X, pr[p].y, pr[p].n, d, pr[p].gamma, k, precision, sketch,
+                        nullptr, pr[p].Z, ldz, infos ? infos + p : nullptr, nullptr, 0, -1,
+                        Cb + kk * p));
+  cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
+  TSVM_CUDA(cudaEventRecord(e0, ctx->stream));
+  int sweeps = 0;
+  TSVM_TRY(eig_jacobi_fp64_batched(ctx, Cb, k, count, wb, Vb, &sweeps));
+  TSVM_CUDA(cudaEventRecord(e1, ctx->stream));
+  for (int p = 0; p < count; ++p)
+    TSVM_TRY(factor_finish(ctx, pr[p].Z, pr[p].n, k, Vb + kk * p, wb + (size_t)k * p,
+                           infos ? infos + p : nullptr));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (ms_eig) *ms_eig = event_ms(e0, e1);
   return TSVM_OK;
 }
 

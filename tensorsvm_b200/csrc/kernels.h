@@ -111,6 +111,10 @@ tsvm_status trinv_lower_fp64(tsvm_context *ctx, const double *L, int n, int lda,
 // the eigenvalues, V (n x n row-major) the eigenvectors as COLUMNS.
 tsvm_status eig_jacobi_fp64(tsvm_context *ctx, double *A, int n, int lda, double *w, double *V,
                             int *sweeps_out);
+// count problems (A count x n x n, w count x n, V count x n x n, contiguous) in one launch when
+// n <= 128 (one CTA each); *max_sweeps_out = the most sweeps any problem took.
+tsvm_status eig_jacobi_fp64_batched(tsvm_context *ctx, double *A, int n, int count, double *w,
+                                    double *V, int *max_sweeps_out);
 // Elementwise helpers on small matrices (device kernels, defined in dense.cu).
 tsvm_status small_add_diag(tsvm_context *ctx, double *A, int n, int lda, double shift);
 tsvm_status small_symmetrize(tsvm_context *ctx, double *A, int n, int lda);
@@ -166,7 +170,17 @@ struct FactorKeep {
 tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_t n, int d,
                        double gamma, int k, int precision, int sketch, const float *Q_user,
                        float *Z, int ldz, tsvm_factor_info *info, FactorKeep *keep = nullptr,
-                       int64_t row0 = 0, int64_t nr = -1);
+                       int64_t row0 = 0, int64_t nr = -1, double *C_out = nullptr);
+// With C_out set, factor_rbf stops after the projection: C_out (k x k FP64) holds the symmetrised
+// C = W^T (K W) and Z (ldz = kp) the orthonormal basis W; factor_finish then forms
+// Z = W V diag(sqrt(max(w, 0))) in place from C's eigen-decomposition (V k x k row-major, w k).
+tsvm_status factor_finish(tsvm_context *ctx, float *Z, int64_t n, int k, const double *V,
+                          const double *w, tsvm_factor_info *info);
+// Factors of `count` independent problems (shared d, k, precision): every problem through the
+// projection, one batched eigensolver launch, then every Z.  ms_eig: the eigensolver launch.
+tsvm_status factor_rbf_batched(tsvm_context *ctx, const tsvm_factor_problem *pr, int count, int d,
+                               int k, int precision, int sketch, int ldz,
+                               tsvm_factor_info *infos, double *ms_eig);
 
 // ---- predict.cu ---------------------------------------------------------------------------
 // Decision values of m rows under a model (device arrays); asynchronous on ctx->stream.

@@ -62,3 +62,21 @@ def test_batched_single_problem_and_launch_count(ctx, grid):
     assert stats[0]["status"] == _lib.OK
     # every iteration is one replay of the captured graph: launches grow with iterations
     assert ctx.launches - l0 > 10 * stats[0]["iters"]
+
+
+@pytest.mark.parametrize("prec,k", [("fp32", 64), ("fp16", 128), ("fp16_fast", 128), ("fp32", 130)])
+def test_factor_batched_matches_single(ctx, prec, k):
+    """tsvm_factor_batched (every problem through its projection, the eigenproblems in one
+    launch, Z formed in place) gives the factor of tsvm_factor for each problem: the same
+    kernels on the same data, the same eigensolver per problem (k = 130 takes the grid
+    eigensolver one problem after the other)."""
+    probs = synth.grid_problems(count=6, lo=700, hi=6000, seed=11)
+    Xs = [dev(X) for X, _, _, _ in probs]
+    ys = [dev(y) for _, y, _, _ in probs]
+    gs = [g for _, _, g, _ in probs]
+    Zb, infos = api.factor_batched(ctx, Xs, ys, gs, k, prec)
+    for X, y, g, Z, info in zip(Xs, ys, gs, Zb, infos):
+        Z1, info1 = api.factor(ctx, X, y, g, k, prec)
+        assert info["realk"] == info1["realk"]
+        assert abs(info["eig_min"] - info1["eig_min"]) <= 1e-9 * abs(info1["eig_max"])
+        assert torch.allclose(Z, Z1, rtol=0, atol=1e-6 * float(Z1.abs().max()))
