@@ -46,14 +46,63 @@ __device__ void tri_inverse_block(const double *Dg, double *Di, int nb, const do
   __syncthreads();
 }
 
-// Right-looking blocked Cholesky in one CTA of 1024 threads, 32-column panels:
-//  (a) the diagonal block is factored in shared memory with one thread per element (thread 0
-//      takes each pivot's square root and reciprocal once); (b) its inverse Di is formed and
-//      stored in Dinv (block jb/32, 32 x 32 row-major) for the triangular solves; (c) the panel
-//      below becomes A_below Di^T (one warp per row, the row broadcast by shuffles), kept
-//      transposed in shared memory; (d) the trailing lower triangle is updated with the panel
-//      (4 x 4 register tiles per thread).
-__global__ void __launch_bounds__(1024) chol_kernel(double *__restrict__ A, int n, int lda,
+// Factor the nb x nb diagonal block held in Dg (lower part, zeros above the diagonal and past
+// nb) in place by one warp, and form its inverse Di: lane r keeps row r in registers for the
+// factorisation (each pivot broadcast by a shuffle, every lane taking the square root and
+// reciprocal itself), then lane c forward-substitutes column c of the inverse,
+// Di[r][c] = (delta_rc - sum_{m<r} L[r][m] Di[m][c]) / L[r][r], reading L's rows as shared-memory
+// broadcasts.  No block barrier inside.  Returns 0, or 1 + the failing column.
+__device__ int diag_block_warp(double *Dg, double *Di, int nb, double *rdiag) {
+  const int lane = threadIdx.x & 31;
+  double a[kNB];
+#pragma unroll
+  for (int c = 0; c < kNB; ++c) a[c] = Dg[lane * kDP + c];
+  int bad = 0;
+#pragma unroll
+  for (int c = 0; c < kNB; ++c) {
+    if (c < nb && bad == 0) {
+      const double d = __shfl_sync(0xffffffffu, a[c], c);
+      if (!(d > 0.0)) {
+        bad = c + 1;
+      } else {
+        const double sq = sqrt(d), inv = 1.0 / sq;
+        const double l = lane > c ? a[c] * inv : (lane == c ? sq : a[c]);
+        a[c] = l;
+        if (lane == 0) rdiag[c] = inv;
+#pragma unroll
+        for (int s = c + 1; s < kNB; ++s) {
+          const double ls = __shfl_sync(0xffffffffu, l, s);
+          if (lane >= s) a[s] = fma(-l, ls, a[s]);
+        }
+      }
+    }
+  }
+  if (bad) return bad;
+#pragma unroll
+  for (int c = 0; c < kNB; ++c) Dg[lane * kDP + c] = (lane < nb && c <= lane) ? a[c] : 0.0;
+  __syncwarp();
+  double x[kNB];
+#pragma unroll
+  for (int r = 0; r < kNB; ++r) {
+    double t = r == lane ? 1.0 : 0.0;
+#pragma unroll
+    for (int m = 0; m < r; ++m) t = fma(-Dg[r * kDP + m], x[m], t);
+    x[r] = (r < nb && lane < nb && r >= lane) ? t * rdiag[r] : 0.0;
+  }
+#pragma unroll
+  for (int r = 0; r < kNB; ++r) Di[r * kDP + lane] = x[r];
+  return 0;
+}
+
+// Right-looking blocked Cholesky in one CTA, 32-column panels:
+//  (a, b) one warp factors the diagonal block in registers and forms its inverse Di (stored in
+//      Dinv, block jb/32, 32 x 32 row-major, for the triangular solves; diag_block_warp);
+//  (c) the panel below becomes A_below Di^T (four rows per warp at a time, each row broadcast by
+//      shuffles), kept transposed in shared memory;
+//  (d) the trailing lower triangle is updated with the panel (4 x 4 register tiles per thread).
+// Batched launches run one CTA per problem.
+constexpr int kCholThreads = 512;   // 128 registers a thread: the diagonal block's rows fit
+__global__ void __launch_bounds__(kCholThreads) chol_kernel(double *__restrict__ A, int n, int lda,
                                                     double *__restrict__ Dinv,
                                                     int *__restrict__ info, int64_t strideA,
                                                     int64_t strideD,
@@ -65,7 +114,7 @@ __global__ void __launch_bounds__(1024) chol_kernel(double *__restrict__ A, int 
   info += blockIdx.x;
   extern __shared__ double PT[];  // [kNB][ldp] panel, transposed: PT[c][i] = L[r0 + i][jb + c]
   __shared__ double Dg[kNB * kDP], Di[kNB * kDP];
-  __shared__ double piv[2], rdiag[kNB];
+  __shared__ double rdiag[kNB];
   __shared__ int fail;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int ldp = n > kNB ? n - kNB : 1;
@@ -73,60 +122,50 @@ __global__ void __launch_bounds__(1024) chol_kernel(double *__restrict__ A, int 
   __syncthreads();
   for (int jb = 0; jb < n; jb += kNB) {
     const int nb = min(kNB, n - jb), m = n - jb - nb, r0 = jb + nb;
-    {
-      const int r = tid >> 5, c = tid & 31;
+    for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+      const int r = e >> 5, c = e & 31;
       Dg[r * kDP + c] = (r < nb && c <= r) ? A[(int64_t)(jb + r) * lda + jb + c] : 0.0;
     }
     __syncthreads();
-    // (a) thread (r, s) owns Dg[r][s]
-    {
-      const int r = tid >> 5, sidx = tid & 31;
-      for (int c = 0; c < nb; ++c) {
-        if (tid == 0) {
-          const double dcc = Dg[c * kDP + c];
-          if (!(dcc > 0.0)) {
-            fail = jb + c + 1;
-          } else {
-            const double sq = sqrt(dcc);
-            piv[0] = sq;
-            piv[1] = 1.0 / sq;
-            rdiag[c] = piv[1];
-          }
-        }
-        __syncthreads();
-        if (fail) break;
-        const double sq = piv[0], inv = piv[1];
-        const double lrc = Dg[r * kDP + c] * inv, lsc = Dg[sidx * kDP + c] * inv;
-        __syncthreads();
-        if (r < nb) {
-          if (sidx == c && r >= c) Dg[r * kDP + c] = r == c ? sq : lrc;
-          else if (sidx > c && sidx <= r) Dg[r * kDP + sidx] -= lrc * lsc;
-        }
-        __syncthreads();
-      }
+    // (a) + (b): the diagonal block and its inverse, one warp
+    if (warp == 0) {
+      const int bad = diag_block_warp(Dg, Di, nb, rdiag);
+      if (lane == 0 && bad) fail = jb + bad;
     }
     __syncthreads();
     if (fail) break;
-    // (b)
-    tri_inverse_block(Dg, Di, nb, rdiag);
     {
       double *Dblk = Dinv + (int64_t)(jb / kNB) * kNB * kNB;
-      const int r = tid >> 5, c = tid & 31;
-      Dblk[tid] = Di[r * kDP + c];
-      if (r < nb && c <= r) A[(int64_t)(jb + r) * lda + jb + c] = Dg[r * kDP + c];
+      for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+        const int r = e >> 5, c = e & 31;
+        Dblk[e] = Di[r * kDP + c];
+        if (r < nb && c <= r) A[(int64_t)(jb + r) * lda + jb + c] = Dg[r * kDP + c];
+      }
     }
-    // (c) L[r0 + i][jb + c] = sum_{q <= c} A[r0 + i][jb + q] Di[c][q]
-    for (int i = warp; i < m; i += (int)(blockDim.x >> 5)) {
-      const double a = lane < nb ? A[(int64_t)(r0 + i) * lda + jb + lane] : 0.0;
-      double v = 0.0;
+    // (c) L[r0 + i][jb + c] = sum_{q <= c} A[r0 + i][jb + q] Di[c][q], four rows per warp at a
+    // time (independent accumulation chains)
+    const int nwarps = (int)(blockDim.x >> 5);
+    for (int i0 = 4 * warp; i0 < m; i0 += 4 * nwarps) {
+      double a4[4], v4[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + u;
+        a4[u] = (lane < nb && i < m) ? A[(int64_t)(r0 + i) * lda + jb + lane] : 0.0;
+        v4[u] = 0.0;
+      }
 #pragma unroll 8
       for (int q = 0; q < kNB; ++q) {
-        const double aq = __shfl_sync(0xffffffffu, a, q);
-        if (q <= lane) v = fma(aq, Di[lane * kDP + q], v);
+        const double dq = q <= lane ? Di[lane * kDP + q] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v4[u] = fma(__shfl_sync(0xffffffffu, a4[u], q), dq, v4[u]);
       }
-      if (lane < nb) {
-        PT[lane * ldp + i] = v;
-        A[(int64_t)(r0 + i) * lda + jb + lane] = v;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + u;
+        if (lane < nb && i < m) {
+          PT[lane * ldp + i] = v4[u];
+          A[(int64_t)(r0 + i) * lda + jb + lane] = v4[u];
+        }
       }
     }
     __syncthreads();
@@ -615,7 +654,7 @@ tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_de
   const size_t smem = sizeof(double) * (size_t)kNB * (size_t)(n > kNB ? n - kNB : 1);
   TSVM_CUDA(cudaFuncSetAttribute(chol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
-  chol_kernel<<<1, 1024, smem, ctx->stream>>>(A, n, lda, Dinv, info_dev, 0, 0, nullptr);
+  chol_kernel<<<1, kCholThreads, smem, ctx->stream>>>(A, n, lda, Dinv, info_dev, 0, 0, nullptr);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;
 }
@@ -627,7 +666,7 @@ tsvm_status chol_fp64_batched(tsvm_context *ctx, double *A, int n, int lda, int6
   const size_t smem = sizeof(double) * (size_t)kNB * (size_t)(n > kNB ? n - kNB : 1);
   TSVM_CUDA(cudaFuncSetAttribute(chol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
-  chol_kernel<<<count, 1024, smem, ctx->stream>>>(A, n, lda, Dinv, info_dev, strideA, strideD,
+  chol_kernel<<<count, kCholThreads, smem, ctx->stream>>>(A, n, lda, Dinv, info_dev, strideA, strideD,
                                                   active);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;

@@ -235,6 +235,228 @@ syrk_tc_kernel(const __grid_constant__ CUtensorMap map, int T, float *__restrict
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// Fused 2-way SYRK for k <= 256 (one column window, ldz <= KP): the rows of Z arrive as FP32 by
+// bulk copies and are scaled by sqrt(dinv), split into BF16 hi + lo and written into the
+// swizzled K-major operand tiles by the converter warps inside the kernel, so the operand never
+// goes through HBM (syrk_prep + syrk_tc_kernel read Z, write the BF16 parts and read them back).
+//   warp 0      bulk copies of 32-row half-chunks of Z into a 3-slot FP32 ring
+//   warp 1      TMEM owner and MMA issuer (as syrk_tc_kernel), 2 operand stages of 64 rows
+//   warps 2-5   converters (warp w handles the 8-row groups w - 2 of each half-chunk), then
+//               the epilogue (TMEM -> per-CTA FP32 partials)
+// Element (c, j) of a part tile (Z column c, row j of the 64-row chunk) sits at byte
+// c * 128 + ((j / 8) ^ (c % 8)) * 16 + (j % 8) * 2: the layout the 128-byte-swizzle TMA load of
+// syrk_tc_kernel produces, read by the same MMA descriptors.
+template <int KP>
+struct FusedCfg {
+  static constexpr uint32_t kTile = KP * kSJ * 2;           // one BF16 part tile
+  static constexpr uint32_t kPartStage = 2 * kTile;         // hi + lo
+  static constexpr int kParts = 2;
+  static constexpr uint32_t kHalfRows = 32;
+  static constexpr uint32_t kHalf = kHalfRows * KP * 4;     // FP32 half-chunk (ldz <= KP)
+  static constexpr int kHalves = 3;
+  static constexpr int kSegs = KP / 128;
+  static constexpr uint32_t kTmemCols = KP == 256 ? 512 : 128;
+  static constexpr uint32_t kStaging = kParts * kPartStage;
+  static constexpr uint32_t kBars = kStaging + kHalves * kHalf;
+  static constexpr uint32_t kSmem = kBars + 256 + 1024;
+};
+
+template <int KP>
+__global__ void __launch_bounds__(kSyrkThreads, 1)
+syrk_fused_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, int T,
+                  const double *__restrict__ dinv, double tau, float *__restrict__ part,
+                  int *__restrict__ err) {
+  using Cfg = FusedCfg<KP>;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  const uint32_t raw = su32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t *sbase = smem_raw + (base - raw);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sbase + Cfg::kBars);
+  const uint32_t b_hfull = su32(bars);                       // [kHalves] FP32 half-chunk landed
+  const uint32_t b_hempty = b_hfull + 8 * Cfg::kHalves;      // [kHalves] converted
+  const uint32_t b_pfull = b_hempty + 8 * Cfg::kHalves;      // [kParts] operand stage written
+  const uint32_t b_pempty = b_pfull + 8 * Cfg::kParts;       // [kParts] operand stage consumed
+  const uint32_t b_done = b_pempty + 8 * Cfg::kParts;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * Cfg::kHalves + 2 * Cfg::kParts + 1);
+  volatile int *abort = reinterpret_cast<volatile int *>(tmem_slot + 1);
+  const float *staging = reinterpret_cast<const float *>(sbase + Cfg::kStaging);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int G = gridDim.x;
+  const int t0 = (int)((int64_t)T * blockIdx.x / G), t1 = (int)((int64_t)T * (blockIdx.x + 1) / G);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < Cfg::kHalves; ++s) {
+      mbar_init(b_hfull + 8 * s, 1);
+      mbar_init(b_hempty + 8 * s, 4);
+    }
+    for (int s = 0; s < Cfg::kParts; ++s) {
+      mbar_init(b_pfull + 8 * s, 4);
+      mbar_init(b_pempty + 8 * s, 1);
+    }
+    mbar_init(b_done, 1);
+    *abort = 0;
+    fence_barrier_init();
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     su32(tmem_slot)),
+                 "r"(Cfg::kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      bool ok = true;
+      for (int t = t0; ok && t < t1; ++t) {
+        for (int h = 0; h < 2; ++h) {
+          if (!mbar_wait(b_hempty + 8 * s, ph ^ 1, abort)) { ok = false; break; }
+          const int64_t r0 = (int64_t)t * kSJ + h * Cfg::kHalfRows;
+          const int64_t rows = n - r0 < (int64_t)Cfg::kHalfRows ? n - r0 : Cfg::kHalfRows;
+          if (rows > 0) {
+            const uint32_t bytes = (uint32_t)(rows * ldz * 4);
+            mbar_expect_tx(b_hfull + 8 * s, bytes);
+            bulk_load(base + Cfg::kStaging + s * Cfg::kHalf, Z + r0 * ldz, bytes, b_hfull + 8 * s);
+          } else {
+            mbar_arrive(b_hfull + 8 * s);   // nothing to copy: the converters zero these rows
+          }
+          if (++s == Cfg::kHalves) { s = 0; ph ^= 1; }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint64_t d0 = desc_sw128(base);
+      int st = 0;
+      uint32_t ph = 0;
+      bool first = true, ok = true;
+      for (int t = t0; t < t1; ++t) {
+        if (!mbar_wait(b_pfull + 8 * st, ph, abort)) { ok = false; break; }
+        tc_fence_after();
+        const uint64_t ds = d0 + (uint64_t)((st * Cfg::kPartStage) >> 4);
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+          for (int b = 0; a + b < 2; ++b)
+#pragma unroll
+            for (int mb = 0; mb < Cfg::kSegs; ++mb) {
+              const uint32_t idesc = idesc_f16(128, (mb + 1) * 128, 1u);
+              const uint64_t da = ds + (uint64_t)((a * Cfg::kTile + mb * 128 * 128) >> 4);
+              const uint64_t db = ds + (uint64_t)((b * Cfg::kTile) >> 4);
+              const uint32_t dt = tmem + (mb == 0 ? 0u : 128u);
+#pragma unroll
+              for (int kk = 0; kk < kSJ / 16; ++kk)
+                umma(dt, da + 2 * kk, db + 2 * kk, idesc,
+                     (first && a == 0 && b == 0 && kk == 0) ? 0u : 1u);
+            }
+        first = false;
+        umma_commit(b_pempty + 8 * st);
+        if (++st == Cfg::kParts) { st = 0; ph ^= 1; }
+      }
+      if (ok) umma_commit(b_done);
+    }
+  } else {
+    // converters: warp g = warp - 2 takes rows 8 g .. 8 g + 7 of each half-chunk, lane = column
+    // within each 32-column block
+    const int g = warp - 2;
+    int hs = 0, ps = 0;
+    uint32_t hph = 0, pph = 0;
+    bool ok = true;
+    for (int t = t0; ok && t < t1; ++t) {
+      if (!mbar_wait(b_pempty + 8 * ps, pph ^ 1, abort)) { ok = false; break; }
+      uint8_t *tile = sbase + ps * Cfg::kPartStage;
+      for (int h = 0; h < 2; ++h) {
+        if (!mbar_wait(b_hfull + 8 * hs, hph, abort)) { ok = false; break; }
+        const int64_t r0 = (int64_t)t * kSJ + h * Cfg::kHalfRows + 8 * g;   // this warp's rows
+        float wr = 0.f;   // lane l < 8: the weight of row r0 + l (0 for exact rows and padding)
+        if (lane < 8 && r0 + lane < n) {
+          const double dv = dinv[r0 + lane];
+          if (dv <= tau) wr = (float)sqrt(dv);
+        }
+        float wj[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) wj[q] = __shfl_sync(0xffffffffu, wr, q);
+        const float *src = staging + (size_t)hs * (Cfg::kHalf / 4) + (size_t)(8 * g) * ldz;
+        const int jg = h * 4 + g;   // 8-row group of the 64-row chunk
+#pragma unroll 2
+        for (int cb = 0; cb < KP; cb += 32) {
+          const int c = cb + lane;
+          float v[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const float x = c < k ? src[(size_t)q * ldz + c] : 0.f;
+            v[q] = wj[q] != 0.f ? x * wj[q] : 0.f;   // select: padding rows may hold anything
+          }
+          uint32_t hi[4], lo[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const __nv_bfloat162 hv = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+            const float2 hf = __bfloat1622float2(hv);
+            const __nv_bfloat162 lv = __floats2bfloat162_rn(v[2 * q] - hf.x, v[2 * q + 1] - hf.y);
+            hi[q] = *reinterpret_cast<const uint32_t *>(&hv);
+            lo[q] = *reinterpret_cast<const uint32_t *>(&lv);
+          }
+          const uint32_t off = (uint32_t)c * 128u + (uint32_t)((jg ^ (c & 7)) << 4);
+          *reinterpret_cast<uint4 *>(tile + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+          *reinterpret_cast<uint4 *>(tile + Cfg::kTile + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(b_hempty + 8 * hs);
+        if (++hs == Cfg::kHalves) { hs = 0; hph ^= 1; }
+      }
+      if (!ok) break;
+      // the generic-proxy stores must be visible to the tensor cores' async-proxy reads
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(b_pfull + 8 * ps);
+      if (++ps == Cfg::kParts) { ps = 0; pph ^= 1; }
+    }
+    // epilogue (lane quarter q = warp % 4)
+    const int q = warp & 3;
+    const uint32_t lane_off = (uint32_t)(q * 32) << 16;
+    const bool have = t1 > t0;
+    if (ok && (!have || mbar_wait(b_done, 0, abort))) {
+      tc_fence_after();
+      float *P = part + (size_t)blockIdx.x * KP * KP;
+#pragma unroll
+      for (int mb = 0; mb < Cfg::kSegs; ++mb) {
+        const int r = mb * 128 + q * 32 + lane;
+        const uint32_t tcol = tmem + (mb == 0 ? 0u : 128u);
+        for (int c0 = 0; c0 < (mb + 1) * 128; c0 += 32) {
+          uint32_t v[32];
+          if (have) {
+            tmem_ld32(tcol + c0 + lane_off, v);
+            tmem_wait_ld();
+          } else {
+#pragma unroll
+            for (int i = 0; i < 32; ++i) v[i] = 0u;
+          }
+          float4 *dst = reinterpret_cast<float4 *>(P + (size_t)r * KP + c0);
+#pragma unroll
+          for (int i = 0; i < 8; ++i)
+            dst[i] = make_float4(__uint_as_float(v[4 * i]), __uint_as_float(v[4 * i + 1]),
+                                 __uint_as_float(v[4 * i + 2]), __uint_as_float(v[4 * i + 3]));
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (threadIdx.x == 0 && *abort) atomicExch(err, 1);
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(Cfg::kTmemCols));
+  }
+}
+
 // M[R][C] = M[C][R] = (R == C) + G64[R][C] + sum_g part[g][r][c] (FP64, CTA order) for the
 // window entries r >= c, R = cols[r], C = cols[c] (identity when cols is null), k the full width,
 // wl the window's.  With a window plan only the entries whose group pair this window owns
@@ -362,6 +584,19 @@ tsvm_status launch_syrk_tc(tsvm_context *ctx, const CUtensorMap &map, int T, int
   return TSVM_OK;
 }
 
+template <int KP>
+tsvm_status launch_syrk_fused(tsvm_context *ctx, const float *Z, int64_t ldz, int k, int64_t n,
+                              int T, const double *dinv, double tau, int G, float *part,
+                              int *err) {
+  using Cfg = FusedCfg<KP>;
+  auto kern = syrk_fused_kernel<KP>;
+  TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)Cfg::kSmem));
+  kern<<<G, kSyrkThreads, Cfg::kSmem, ctx->stream>>>(Z, ldz, k, n, T, dinv, tau, part, err);
+  TSVM_LAUNCHED(ctx);
+  return TSVM_OK;
+}
+
 }  // namespace
 
 bool syrk_tc_supported(int k) { return k >= 1 && k <= kSyrkMaxK && tc::encode_fn() != nullptr; }
@@ -421,6 +656,24 @@ tsvm_status syrk_capacitance_tc(tsvm_context *ctx, const float *Z, int ldz, int6
   for (int w = 0; w < plan.nw; ++w) wmax = std::max(wmax, wl[w]);
   const int KPmax = wmax <= 128 ? 128 : 256;
   const int64_t T = ceil_div(n, (int64_t)kSJ);
+  // One window, 2-way split, rows of at most KP floats on 16-byte boundaries: scale and split
+  // inside the tensor-core kernel (no BF16 operand in HBM).
+  if (ways == 2 && plan.nw == 1 && ldz <= KPmax && ldz % 4 == 0 &&
+      (reinterpret_cast<uintptr_t>(Z) & 15) == 0 && T <= (int64_t)INT32_MAX) {
+    const int G = (int)std::min<int64_t>(ctx->num_sms, T);
+    float *part = nullptr;
+    TSVM_TRY(scratch_t(ctx, SLOT_SYRK_PART, (size_t)G * KPmax * KPmax + 64, &part));
+    int *err = reinterpret_cast<int *>(part + (size_t)G * KPmax * KPmax);
+    TSVM_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
+    const tsvm_status st =
+        KPmax == 128 ? launch_syrk_fused<128>(ctx, Z, ldz, k, n, (int)T, dinv, tau, G, part, err)
+                     : launch_syrk_fused<256>(ctx, Z, ldz, k, n, (int)T, dinv, tau, G, part, err);
+    if (st != TSVM_OK) return st;
+    syrk_reduce<<<(unsigned)ceil_div((int64_t)k * k, 256), 256, 0, ctx->stream>>>(
+        part, G, KPmax, k, k, nullptr, nullptr, nullptr, plan.ng, 0, G64, err, M);
+    TSVM_LAUNCHED(ctx);
+    return TSVM_OK;
+  }
   if ((int64_t)ways * T * KPmax > (int64_t)INT32_MAX) return TSVM_ERR_UNSUPPORTED;
   __nv_bfloat16 *parts = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_SYRK_OP, (size_t)ways * T * KPmax * kSJ, &parts));

@@ -42,7 +42,7 @@ def test_sketch_matches_reference_stream(ctx, n, k):
     assert np.mean(ulp != 0) < 5e-3
 
 
-@pytest.mark.parametrize("k", [1, 32, 50, 256, 400])
+@pytest.mark.parametrize("k", [1, 32, 33, 50, 97, 256, 400])
 def test_cholesky_and_solve(ctx, k):
     rng = np.random.default_rng(k)
     A = rng.standard_normal((k, k + 5))
@@ -59,13 +59,15 @@ def test_cholesky_and_solve(ctx, k):
     assert np.allclose(Bd.cpu().numpy(), np.linalg.solve(M, B.T).T, rtol=1e-8, atol=1e-10)
 
 
-def test_cholesky_reports_indefinite(ctx):
-    M = np.eye(40)
-    M[17, 17] = -1.0
+@pytest.mark.parametrize("n,bad", [(40, 17), (100, 70), (100, 0), (65, 64)])
+def test_cholesky_reports_indefinite(ctx, n, bad):
+    # the first failing pivot's 1-based column, in the first panel and in later ones
+    M = np.eye(n)
+    M[bad, bad] = -1.0
     L = dev(M)
     info = ctypes.c_int32(0)
-    _lib.check(ctx.lib.tsvm_test_chol(ctx.handle, P(L), 40, ctypes.byref(info)), "chol")
-    assert info.value == 18
+    _lib.check(ctx.lib.tsvm_test_chol(ctx.handle, P(L), n, ctypes.byref(info)), "chol")
+    assert info.value == bad + 1
 
 
 # k <= 128: the one-CTA packed solver; above: the cooperative-grid one

@@ -53,6 +53,27 @@ def test_syrk_mixed_accuracy(ctx, n, k, ways, tau):
     assert err < tol, err
 
 
+@pytest.mark.parametrize("n,k", [(70001, 256), (130, 256), (5000, 128), (3001, 250), (64, 64)])
+@pytest.mark.parametrize("tau", [100.0, float("inf")])
+def test_syrk_fused_matches_two_kernel_path(ctx, n, k, tau):
+    """With ldz <= 256 the 2-way SYRK scales and splits Z inside the tensor-core kernel; with a
+    wider ldz it runs the separate split kernel and the TMA-fed SYRK.  Both feed the same BF16
+    parts to the same MMAs over the same row ranges, so M must agree bit for bit, and both must
+    meet the FP64 bound."""
+    rng = np.random.default_rng(3 * n + k)
+    ldz_fused = (k + 3) // 4 * 4
+    Z = rng.standard_normal((n, ldz_fused + 260)).astype(np.float32)
+    dinv = np.exp(rng.uniform(np.log(1e-4), np.log(1e4), n))
+    Mf, cf = syrk_mixed(ctx, np.ascontiguousarray(Z[:, :ldz_fused]), k, dinv, tau, 2)
+    Mp, cp = syrk_mixed(ctx, Z, k, dinv, tau, 2)
+    assert cf == cp
+    assert np.array_equal(Mf, Mp)
+    Zk = Z[:, :k].astype(np.float64)
+    ref = np.eye(k) + (Zk * dinv[:, None]).T @ Zk
+    scale = np.sqrt(np.outer(np.diag(ref), np.diag(ref)))
+    assert np.max(np.abs(Mf - ref) / scale) < 1e-4
+
+
 @pytest.fixture(scope="module")
 def prob(ctx):
     X, y = synth.two_gaussians(20000, 18, seed=2, noise=0.1)
