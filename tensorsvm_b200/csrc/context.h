@@ -47,6 +47,8 @@ enum Slot : int {
   SLOT_HG_R,          // hypergradient: combined CholeskyQR factor and k-vectors
   SLOT_HG_KPART,      // hypergradient: per-split partial kernel-vector products
   SLOT_HG_W,          // hypergradient: the factor's orthonormal basis before rounding
+  SLOT_HG_TC,         // hypergradient: centred rows, FP32 operand and product of the tensor-core
+                      // kernel-vector products
   SLOT_DEV_IN,        // tsvm_train: device copies of host inputs
   SLOT_DEV_Z,         // tsvm_train: factor Z
   SLOT_DEV_OUT,       // tsvm_train: device alpha

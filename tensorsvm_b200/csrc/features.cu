@@ -56,7 +56,7 @@ __global__ void centre_rows(const float *__restrict__ X, int64_t n, int d,
     Xc[r * d + c] = v;
     s += (double)v * (double)v;
   }
-  norms[r] = (float)s;
+  if (norms) norms[r] = (float)s;
 }
 
 __global__ void pad_rows_kernel(const float *__restrict__ src, int64_t lds, int64_t n, int k,
@@ -84,6 +84,24 @@ tsvm_status centre_features(tsvm_context *ctx, const float *X, int64_t n, int d,
   colmean_finish<<<(unsigned)ceil_div(d, 64), 64, 0, ctx->stream>>>(part, nb, d, n, mean);
   TSVM_LAUNCHED(ctx);
   centre_rows<<<(unsigned)ceil_div(n, 256), 256, 0, ctx->stream>>>(X, n, d, mean, Xc, norms);
+  TSVM_LAUNCHED(ctx);
+  return TSVM_OK;
+}
+
+tsvm_status centre_pair(tsvm_context *ctx, const float *XJ, int64_t nj, const float *XI,
+                        int64_t ni, int d, float *XJc, float *XIc) {
+  const int nb = (int)std::min<int64_t>(ctx->num_sms * 2, ceil_div(nj, 256));
+  const int64_t rpb = ceil_div(nj, nb);
+  double *part = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_MISC, (size_t)nb * d + 2 * (size_t)d, &part));
+  float *mean = reinterpret_cast<float *>(part + (size_t)nb * d);
+  colsum_partial<<<nb, 256, 0, ctx->stream>>>(XJ, nj, d, rpb, part);
+  TSVM_LAUNCHED(ctx);
+  colmean_finish<<<(unsigned)ceil_div(d, 64), 64, 0, ctx->stream>>>(part, nb, d, nj, mean);
+  TSVM_LAUNCHED(ctx);
+  centre_rows<<<(unsigned)ceil_div(nj, 256), 256, 0, ctx->stream>>>(XJ, nj, d, mean, XJc, nullptr);
+  TSVM_LAUNCHED(ctx);
+  centre_rows<<<(unsigned)ceil_div(ni, 256), 256, 0, ctx->stream>>>(XI, ni, d, mean, XIc, nullptr);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;
 }

@@ -204,6 +204,49 @@ tsvm_status kprod(tsvm_context *ctx, const float *A, int64_t na, const float *B,
   return kprod_launch<64, R64, NU, DERIV>(ctx, A, na, B, nb, d, gl2, U, nu_total, out);
 }
 
+// U (nb x nu FP64) -> Uf (nb x kp FP32, zero columns past nu)
+__global__ void u_to_float(const double *__restrict__ U, int64_t nb, int nu, int kp,
+                           float *__restrict__ Uf) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nb * kp) return;
+  const int64_t j = e / kp;
+  const int c = (int)(e % kp);
+  Uf[e] = c < nu ? (float)U[j * nu + c] : 0.f;
+}
+// out (na x nu FP64) = scale * W (na x kp FP32)
+__global__ void w_to_out(const float *__restrict__ W, int64_t na, int kp, int nu, double scale,
+                         double *__restrict__ out) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= na * nu) return;
+  const int64_t i = e / nu;
+  const int c = (int)(e % nu);
+  out[e] = scale * (double)W[i * kp + c];
+}
+
+// The kernel-vector product of kprod on the tensor cores (kermatmul_tc_core with the kernel
+// block and U both split hi + lo, FP32 accumulation): out = [K or K'](A, B) U.  Both row sets
+// are centred by B's mean; K' = -||a - b||^2 K is the kernel's S exp2(S) entries
+// (S = -gamma log2(e) ||a - b||^2) divided by gamma log2 e.
+tsvm_status kprod_tc(tsvm_context *ctx, const float *A, int64_t na, const float *B, int64_t nb,
+                     int d, double gamma, const double *U, int nu, double *out, bool deriv) {
+  const int kp = (int)round_up(nu, 64);
+  const size_t oa = 0, ob = round_up((size_t)na * d, 64), ou = ob + round_up((size_t)nb * d, 64);
+  const size_t ow = ou + round_up((size_t)nb * kp, 64);
+  float *buf = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_HG_TC, ow + (size_t)na * kp, &buf));
+  float *Ac = buf + oa, *Bc = buf + ob, *Uf = buf + ou, *Wt = buf + ow;
+  TSVM_TRY(centre_pair(ctx, B, nb, A, na, d, Bc, Ac));
+  u_to_float<<<(unsigned)ceil_div(nb * kp, 256), 256, 0, ctx->stream>>>(U, nb, nu, kp, Uf);
+  TSVM_LAUNCHED(ctx);
+  TSVM_TRY(kermatmul_tc_core(ctx, Ac, nullptr, na, Bc, nullptr, nb, d, gamma, Uf, kp, Wt,
+                             TSVM_PREC_FP16, nullptr, nullptr, 3, deriv));
+  const double scale = deriv ? 1.0 / (gamma * 1.4426950408889634) : 1.0;
+  w_to_out<<<(unsigned)ceil_div(na * (int64_t)nu, 256), 256, 0, ctx->stream>>>(Wt, na, kp, nu,
+                                                                              scale, out);
+  TSVM_LAUNCHED(ctx);
+  return TSVM_OK;
+}
+
 __global__ void beta_kernel(const double *alpha, const float *y, int64_t n, double *beta) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) beta[i] = alpha[i] * (double)y[i];
@@ -418,6 +461,17 @@ extern "C" tsvm_status tsvm_hypergrad(tsvm_context *ctx, const float *X, const f
     TSVM_CUDA(cudaMemcpyAsync(dF, F.data(), sizeof(int64_t) * F.size(), cudaMemcpyHostToDevice, st));
   const int nf = (int)F.size();
 
+  // kernel-vector products: the tensor cores for the 16-bit precisions (the FP32 form keeps the
+  // SIMT products); the loss's own forward product below stays on the FP64-accumulating SIMT
+  // kernel, which holds the loss to ~1e-7
+  const bool tc_products = precision != TSVM_PREC_FP32 && kermatmul_tc_supported(d, 64);
+  auto kp1 = [&](const float *A_, int64_t na_, const float *B_, int64_t nb_, const double *U_,
+                 double *out_, bool deriv) -> tsvm_status {
+    if (tc_products) return kprod_tc(ctx, A_, na_, B_, nb_, d, gamma, U_, 1, out_, deriv);
+    return deriv ? kprod<1, true>(ctx, A_, na_, B_, nb_, d, gamma, U_, 1, out_)
+                 : kprod<1, false>(ctx, A_, na_, B_, nb_, d, gamma, U_, 1, out_);
+  };
+
   // forward on the validation set: f = K(Xv, X) beta + b, loss, g
   beta_kernel<<<gn, 256, 0, st>>>(alpha, y, n, beta);
   TSVM_LAUNCHED(ctx);
@@ -426,7 +480,7 @@ extern "C" tsvm_status tsvm_hypergrad(tsvm_context *ctx, const float *X, const f
   TSVM_LAUNCHED(ctx);
   std::vector<double> hg(nv);
   TSVM_CUDA(cudaMemcpyAsync(hg.data(), g, sizeof(double) * nv, cudaMemcpyDeviceToHost, st));
-  TSVM_TRY((kprod<1, false>(ctx, X, n, Xv, nv, d, gamma, g, 1, tmp)));
+  TSVM_TRY(kp1(X, n, Xv, nv, g, tmp, false));
   TSVM_CUDA(cudaStreamSynchronize(st));
   double Gb = 0.0;
   for (double v : hg) Gb += v;
@@ -445,7 +499,7 @@ extern "C" tsvm_status tsvm_hypergrad(tsvm_context *ctx, const float *X, const f
   TSVM_TRY(ro.P(alpha, u));                                              // u = P alpha
   yscale_kernel<<<gn, 256, 0, st>>>(u, y, n, tmp);
   TSVM_LAUNCHED(ctx);
-  TSVM_TRY((kprod<1, false>(ctx, X, n, X, n, d, gamma, tmp, 1, E1)));
+  TSVM_TRY(kp1(X, n, X, n, tmp, E1, false));
   yscale_kernel<<<gn, 256, 0, st>>>(E1, y, n, E1);                       // E1 = Ky u
   TSVM_LAUNCHED(ctx);
   // the five vectors dKy is applied to: Om B+ E1, (I-P) E1, u, Om B+ alpha, (I-P) alpha
@@ -462,7 +516,10 @@ extern "C" tsvm_status tsvm_hypergrad(tsvm_context *ctx, const float *X, const f
   axpy_kernel<<<gn, 256, 0, st>>>(alpha, -1.0, u, n, tmp);
   pack_col<<<gn, 256, 0, st>>>(tmp, y, n, U5, 5, 4);
   TSVM_LAUNCHED(ctx);
-  TSVM_TRY((kprod<8, true>(ctx, X, n, X, n, d, gamma, U5, 5, D5)));       // D_j = K' (Y v_j)
+  if (tc_products)                                                       // D_j = K' (Y v_j)
+    TSVM_TRY(kprod_tc(ctx, X, n, X, n, d, gamma, U5, 5, D5, true));
+  else
+    TSVM_TRY((kprod<8, true>(ctx, X, n, X, n, d, gamma, U5, 5, D5)));
   // s2 = (I-P) D4 + B+^T Om^T D5 ; E2 = Ky s2
   unpack_col<<<gn, 256, 0, st>>>(D5, y, n, 5, 3, tmp);
   TSVM_LAUNCHED(ctx);
@@ -474,7 +531,7 @@ extern "C" tsvm_status tsvm_hypergrad(tsvm_context *ctx, const float *X, const f
   axpy_kernel<<<gn, 256, 0, st>>>(s2, 1.0, t2, n, s2);
   yscale_kernel<<<gn, 256, 0, st>>>(s2, y, n, tmp);
   TSVM_LAUNCHED(ctx);
-  TSVM_TRY((kprod<1, false>(ctx, X, n, X, n, d, gamma, tmp, 1, s2)));
+  TSVM_TRY(kp1(X, n, X, n, tmp, s2, false));
   yscale_kernel<<<gn, 256, 0, st>>>(s2, y, n, s2);                       // s2 <- E2 = Ky s2
   TSVM_LAUNCHED(ctx);
   // r = (I-P) D1 + B+^T Om^T D2 + P D3 + P E2
@@ -495,7 +552,7 @@ extern "C" tsvm_status tsvm_hypergrad(tsvm_context *ctx, const float *X, const f
   TSVM_LAUNCHED(ctx);
 
   // validation-kernel gamma term: t_v = sum_i beta_i K'_iv
-  TSVM_TRY((kprod<1, true>(ctx, Xv, nv, X, n, d, gamma, beta, 1, tv)));
+  TSVM_TRY(kp1(Xv, nv, X, n, beta, tv, true));
   dots_kernel<<<nb, 256, 0, st>>>(lam, xi, alpha, C, r, n, lossv, g, tv, nv, part);
   TSVM_LAUNCHED(ctx);
   std::vector<double> hp(4 * nb), hr(nf > 0 ? nf : 1);
@@ -512,7 +569,10 @@ extern "C" tsvm_status tsvm_hypergrad(tsvm_context *ctx, const float *X, const f
     S = bx + (size_t)n * (d + 1);
     beta_x_kernel<<<gn, 256, 0, st>>>(beta, X, n, d, bx);
     TSVM_LAUNCHED(ctx);
-    TSVM_TRY((kprod<32, false>(ctx, Xv, nv, X, n, d, gamma, bx, d + 1, S)));
+    if (tc_products)
+      TSVM_TRY(kprod_tc(ctx, Xv, nv, X, n, d, gamma, bx, d + 1, S, false));
+    else
+      TSVM_TRY((kprod<32, false>(ctx, Xv, nv, X, n, d, gamma, bx, d + 1, S)));
     dxv_kernel<<<gv, 256, 0, st>>>(S, Xv, g, nv, d, gamma, dXv);
     TSVM_LAUNCHED(ctx);
   }

@@ -149,7 +149,11 @@ __device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t 
 //            the range is found of, while rounding the Gaussian sketch only draws another sketch;
 //   kSplitA: the kernel-block operand (projection pass, K W): rounding the orthonormal basis W
 //            tilts the subspace the kernel is projected on, while P's rounding averages out.
-constexpr int kSplitNone = 0, kSplitP = 1, kSplitA = 2;
+//   kSplitPA: both (three products P_hi A_hi + P_lo A_hi + P_hi A_lo), for kernel-vector products
+//            that need about FP32 accuracy (the hypergradient's).
+constexpr int kSplitNone = 0, kSplitP = 1, kSplitA = 2, kSplitPA = 3;
+__host__ __device__ constexpr bool split_p(int s) { return s == kSplitP || s == kSplitPA; }
+__host__ __device__ constexpr bool split_a(int s) { return s == kSplitA || s == kSplitPA; }
 
 // ---------------------------------------------------------------------------------------
 // The fused kernel, persistent: grid.x <= SM count, CTA c takes the 128-row blocks c, c + G,
@@ -169,10 +173,12 @@ constexpr int kSplitNone = 0, kSplitP = 1, kSplitA = 2;
 // lo part over the other 32, and the issuer runs W += P_hi AT^T + P_lo AT^T.
 // SPLIT == kSplitA: every J block takes two consecutive slots of the kernel-operand ring, AT_hi
 // (map_at) and AT_lo (map_atlo), and the issuer runs W += P AT_hi^T + P AT_lo^T.
+// DERIV: the kernel block's entries are S exp2(S) = -gamma log2(e) ||x_i - x_j||^2 K_ij (the
+// caller divides W by -gamma log2 e for dK/dgamma = -||x_i - x_j||^2 K).
 // ---------------------------------------------------------------------------------------
 constexpr int kSBufs = 4;
 
-template <bool BF16, int NPOLY, int KG, bool SHIFT, int SPLIT>
+template <bool BF16, int NPOLY, int KG, bool SHIFT, int SPLIT, bool DERIV>
 __global__ void __launch_bounds__(kThreadsTC, 1)
 kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
                     const __grid_constant__ CUtensorMap map_xb,
@@ -271,9 +277,9 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
     // ---------------- TMA producer: kernel-block operand ring ----------------
     if (lane == 0) {
       asm volatile("prefetch.tensormap [%0];" ::"l"(&map_at) : "memory");
-      if constexpr (SPLIT == kSplitA) asm volatile("prefetch.tensormap [%0];" ::"l"(&map_atlo) : "memory");
+      if constexpr (split_a(SPLIT)) asm volatile("prefetch.tensormap [%0];" ::"l"(&map_atlo) : "memory");
       const uint32_t at_bytes = (uint32_t)kpw * kBJ * 2;
-      constexpr int kParts = SPLIT == kSplitA ? 2 : 1;
+      constexpr int kParts = split_a(SPLIT) ? 2 : 1;
       int st = 0;
       uint32_t ph = 0;
       bool ok = true;
@@ -340,7 +346,7 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
           const int st2 = st + 1 == kAtStages ? 0 : st + 1;
           const uint32_t sph2 = st + 1 == kAtStages ? sph ^ 1 : sph;
           if (!mbar_wait(b_atfull + 8 * st, sph, abort) ||
-              (SPLIT == kSplitA && !mbar_wait(b_atfull + 8 * st2, sph2, abort)) ||
+              (split_a(SPLIT) && !mbar_wait(b_atfull + 8 * st2, sph2, abort)) ||
               !mbar_wait(b_pfull + 8 * b, bph, abort)) {
             ok = false;
             break;
@@ -351,12 +357,12 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
 #pragma unroll
           for (int kk = 0; kk < kBJ / 16; ++kk)
             umma_ts(t_w, ap + kk * 8, dat + 2 * kk, id2, (t > 0 || kk > 0) ? 1u : 0u);
-          if constexpr (SPLIT == kSplitP) {
+          if constexpr (split_p(SPLIT)) {
 #pragma unroll
             for (int kk = 0; kk < kBJ / 16; ++kk)   // P_lo over the buffer's columns 32..63
               umma_ts(t_w, ap + kBJ / 2 + kk * 8, dat + 2 * kk, id2, 1u);
           }
-          if constexpr (SPLIT == kSplitA) {
+          if constexpr (split_a(SPLIT)) {
             const uint64_t dat2 = dat0 + (uint64_t)(st2 * at_step);
 #pragma unroll
             for (int kk = 0; kk < kBJ / 16; ++kk)
@@ -365,7 +371,7 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
           umma_commit(b_free + 8 * b);
           umma_commit(b_atempty + 8 * st);
           if (++st == kAtStages) { st = 0; sph ^= 1; }
-          if constexpr (SPLIT == kSplitA) {
+          if constexpr (split_a(SPLIT)) {
             umma_commit(b_atempty + 8 * st);
             if (++st == kAtStages) { st = 0; sph ^= 1; }
           }
@@ -399,18 +405,22 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
         tmem_ld32(tb + 32, s1);
         tmem_wait_ld();
         uint32_t pk[32];
-        if constexpr (SPLIT == kSplitP) {
+        // the kernel block's entry from the scaled distance x = S_ij: exp2(x) (less the shift),
+        // or x exp2(x) for the derivative
+        auto pv = [&](uint32_t raw, int e) -> float {
+          const float x = __uint_as_float(raw);
+          if constexpr (DERIV) return x * exp2_mixed<NPOLY>(x, e);
+          else return exp2_mixed<NPOLY>(x, e) - shift;
+        };
+        if constexpr (split_p(SPLIT)) {
           uint32_t pl[32];
 #pragma unroll
           for (int c = 0; c < 16; ++c)
-            split2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c]), 2 * c) - shift,
-                         exp2_mixed<NPOLY>(__uint_as_float(s0[2 * c + 1]), 2 * c + 1) - shift,
-                         pk[c], pl[c]);
+            split2<BF16>(pv(s0[2 * c], 2 * c), pv(s0[2 * c + 1], 2 * c + 1), pk[c], pl[c]);
 #pragma unroll
           for (int c = 0; c < 16; ++c)
-            split2<BF16>(exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c]), 2 * c) - shift,
-                         exp2_mixed<NPOLY>(__uint_as_float(s1[2 * c + 1]), 2 * c + 1) - shift,
-                         pk[16 + c], pl[16 + c]);
+            split2<BF16>(pv(s1[2 * c], 2 * c), pv(s1[2 * c + 1], 2 * c + 1), pk[16 + c],
+                         pl[16 + c]);
           tmem_st32(tb + kBJ / 2, pl);   // P_lo over the buffer's columns 32..63
         } else if constexpr (SHIFT) {
 #pragma unroll
@@ -441,7 +451,7 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
       if (!ok || !mbar_wait(b_wfull, r & 1, abort)) break;
       tc_fence_after();
       const int64_t gi = (int64_t)rb * kBM + row;
-      const float sc = gi < n ? y[gi] * inv_scale[0] : 0.f;
+      const float sc = gi < n ? (y ? y[gi] : 1.f) * inv_scale[0] : 0.f;
       for (int cc = g * half; cc < (g + 1) * half; cc += 32) {
         uint32_t v[32];
         tmem_ld32(t_w + cc + lane_off, v);
@@ -607,7 +617,7 @@ prep_at(const float *A, const float *__restrict__ y, int64_t n, int64_t n_pad, i
       const int c = c0 + threadIdx.x;
       float v = 0.f, vl = 0.f;
       if (j < n && c < kp) {
-        const float yj = y[j];
+        const float yj = y ? y[j] : 1.f;
         const float x = A[j * kp + c] * yj * s;
         v = round16<T>(x);
         if (ATlo) vl = round16<T>(x - v);
@@ -730,7 +740,8 @@ TcKernel select_split(bool bf16, int KG, bool shift) {
   // MUFU exps only
 #define TSVM_SEL(K, S)                                                                   \
   if (KG == K && shift == S)                                                             \
-    return bf16 ? kermatmul_tc_kernel<true, 0, K, S, SPLIT> : kermatmul_tc_kernel<false, 0, K, S, SPLIT>;
+    return bf16 ? kermatmul_tc_kernel<true, 0, K, S, SPLIT, false>                       \
+                : kermatmul_tc_kernel<false, 0, K, S, SPLIT, false>;
   TSVM_SEL(64, true)
   TSVM_SEL(128, true)
   TSVM_SEL(192, true)
@@ -741,20 +752,30 @@ TcKernel select_split(bool bf16, int KG, bool shift) {
   return nullptr;
 }
 
-TcKernel select_kernel(bool bf16, int npoly, int KG, bool shift, int split) {
+TcKernel select_kernel(bool bf16, int npoly, int KG, bool shift, int split, bool deriv) {
+  if (deriv) {   // FP16, all splits, no shift (the derivative's entries are not flat)
+    if (bf16 || shift || split != kSplitPA) return nullptr;
+    if (KG == 64) return kermatmul_tc_kernel<false, 0, 64, false, kSplitPA, true>;
+    if (KG == 128) return kermatmul_tc_kernel<false, 0, 128, false, kSplitPA, true>;
+    if (KG == 192) return kermatmul_tc_kernel<false, 0, 192, false, kSplitPA, true>;
+    return nullptr;
+  }
   if (split == kSplitP) return select_split<kSplitP>(bf16, KG, shift);
   if (split == kSplitA) return select_split<kSplitA>(bf16, KG, shift);
+  if (split == kSplitPA) return select_split<kSplitPA>(bf16, KG, shift);
   if (shift || KG != 64) return select_split<kSplitNone>(bf16, KG, shift);
 #define TSVM_SEL(P) \
   if (npoly == P) \
-    return bf16 ? kermatmul_tc_kernel<true, P, 64, false, kSplitNone> : kermatmul_tc_kernel<false, P, 64, false, kSplitNone>;
+    return bf16 ? kermatmul_tc_kernel<true, P, 64, false, kSplitNone, false> \
+                : kermatmul_tc_kernel<false, P, 64, false, kSplitNone, false>;
   TSVM_SEL(0)
   TSVM_SEL(2)
   TSVM_SEL(4)
   TSVM_SEL(6)
   TSVM_SEL(8)
 #undef TSVM_SEL
-  return bf16 ? kermatmul_tc_kernel<true, 4, 64, false, kSplitNone> : kermatmul_tc_kernel<false, 4, 64, false, kSplitNone>;
+  return bf16 ? kermatmul_tc_kernel<true, 4, 64, false, kSplitNone, false>
+              : kermatmul_tc_kernel<false, 4, 64, false, kSplitNone, false>;
 }
 
 // Gram K for d features: 3 d split products + 6 norm terms, rounded up to a 64-wide chunk.
@@ -780,14 +801,28 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
                          int precision, float *kernel_ms, float *round_back, int split,
                          int64_t row0, int64_t nr) {
   (void)norms;
-  if (!kermatmul_tc_supported(d, kp)) return TSVM_ERR_UNSUPPORTED;
-  if (split < kSplitNone || split > kSplitA) return TSVM_ERR_INVALID_ARGUMENT;
   if (nr < 0) nr = n - row0;
   if (row0 < 0 || nr < 1 || row0 + nr > n) return TSVM_ERR_INVALID_ARGUMENT;
-  const bool rows = row0 != 0 || nr != n;   // only the rows [row0, row0 + nr) of W
+  if (split < kSplitNone || split > kSplitA) return TSVM_ERR_INVALID_ARGUMENT;
+  const bool rows = row0 != 0 || nr != n;
+  return kermatmul_tc_core(ctx, rows ? Xc + row0 * d : Xc, y + row0, nr, Xc, y, n, d, gamma, A,
+                           kp, W, precision, kernel_ms, round_back, split, false);
+}
+
+// The general form: W (ni x kp) = Y_I K(X_I, X_J) Y_J A with the I rows XI (ni x d, labels yI) and
+// the J rows XJ (nj x d, labels yJ; A is nj x kp), both centred by the same vector; a null label
+// vector means all ones.  XI may be XJ itself.
+tsvm_status kermatmul_tc_core(tsvm_context *ctx, const float *XI, const float *yI, int64_t ni,
+                              const float *XJ, const float *yJ, int64_t nj, int d, double gamma,
+                              const float *A, int kp, float *W, int precision, float *kernel_ms,
+                              float *round_back, int split, bool deriv) {
+  if (!kermatmul_tc_supported(d, kp)) return TSVM_ERR_UNSUPPORTED;
+  if (split < kSplitNone || split > kSplitPA || ni < 1 || nj < 1) return TSVM_ERR_INVALID_ARGUMENT;
+  if (deriv && split != kSplitPA) return TSVM_ERR_UNSUPPORTED;
+  const bool same = XI == XJ && ni == nj;
   const bool bf16 = precision_is_bf16(precision);
-  const int64_t n_pad = round_up(n, kBM);          // J side (XB, AT): all rows
-  const int64_t nr_pad = round_up(nr, kBM);        // I side (XA, W): this call's rows
+  const int64_t n_pad = round_up(nj, kBM);         // J side (XB, AT)
+  const int64_t nr_pad = round_up(ni, kBM);        // I side (XA, W)
   const int KG = gram_k(d);
   // operands: [XA (nr_pad rows) | XB (n_pad rows)]
   __half *XA = nullptr;
@@ -795,12 +830,12 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
   __half *XB = XA + (size_t)nr_pad * KG;
   uint16_t *AT = nullptr;
   const size_t at_elems = (size_t)kp * n_pad;
-  TSVM_TRY(scratch_t(ctx, SLOT_OPA, (split == kSplitA ? 2 : 1) * at_elems, &AT));
-  uint16_t *ATlo = split == kSplitA ? AT + at_elems : nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_OPA, (split_a(split) ? 2 : 1) * at_elems, &AT));
+  uint16_t *ATlo = split_a(split) ? AT + at_elems : nullptr;
   // SLOT_MISC: sum-of-squares partials [nb] | scale: s, 1/s, shift, - (4 floats) | err |
   // kernel-moment row sums [2 m] | column-sum partials [rg][kp] | ccol [kp floats]
   const int nb = ctx->num_sms * 2;
-  const int m = n < kStageMax / 2 ? (int)n : kStageMax / 2;
+  const int m = nj < kStageMax / 2 ? (int)nj : kStageMax / 2;
   const int rg = (int)(n_pad / 32 < (int64_t)nb ? n_pad / 32 : nb);
   const size_t o_samp = (size_t)nb + 8, o_cpart = o_samp + 2048;
   const size_t o_ccol = o_cpart + (size_t)rg * kp;
@@ -811,38 +846,42 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
   double *samp = part + o_samp, *cpart = part + o_cpart;
   float *ccol = reinterpret_cast<float *>(part + o_ccol);   // o_ccol is even: 16-byte aligned
   const double xscale = sqrt(2.0 * gamma * 1.4426950408889634);
-  if (rows) {
+  if (!same) {
     prep_gram_operands<<<(unsigned)ceil_div(n_pad, 256), 256, 0, ctx->stream>>>(
-        Xc, n, n_pad, d, KG, xscale, nullptr, XB);
+        XJ, nj, n_pad, d, KG, xscale, nullptr, XB);
     TSVM_LAUNCHED(ctx);
     prep_gram_operands<<<(unsigned)ceil_div(nr_pad, 256), 256, 0, ctx->stream>>>(
-        Xc + row0 * d, nr, nr_pad, d, KG, xscale, XA, nullptr);
+        XI, ni, nr_pad, d, KG, xscale, XA, nullptr);
     TSVM_LAUNCHED(ctx);
   } else {   // XA and XB of the same rows in one pass
     prep_gram_operands<<<(unsigned)ceil_div(n_pad, 256), 256, 0, ctx->stream>>>(
-        Xc, n, n_pad, d, KG, xscale, XA, XB);
+        XJ, nj, n_pad, d, KG, xscale, XA, XB);
     TSVM_LAUNCHED(ctx);
   }
-  sumsq_partial<<<nb, 256, 0, ctx->stream>>>(A, n * (int64_t)kp, part);
+  sumsq_partial<<<nb, 256, 0, ctx->stream>>>(A, nj * (int64_t)kp, part);
   TSVM_LAUNCHED(ctx);
-  choose_scale<<<1, 256, 0, ctx->stream>>>(part, nb, n * (int64_t)kp, scale);
+  choose_scale<<<1, 256, 0, ctx->stream>>>(part, nb, nj * (int64_t)kp, scale);
   TSVM_LAUNCHED(ctx);
-  kernel_mean_rows<<<m, 256, 0, ctx->stream>>>(Xc, n, d, m, (float)gamma, samp);
-  TSVM_LAUNCHED(ctx);
-  kernel_mean_finish<<<1, 256, 0, ctx->stream>>>(samp, m, scale);
-  TSVM_LAUNCHED(ctx);
-  float hshift = 0.f;   // picks the kernel instantiation
-  TSVM_CUDA(cudaMemcpyAsync(&hshift, scale + 2, sizeof(float), cudaMemcpyDeviceToHost,
-                            ctx->stream));
-  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  float hshift = 0.f;   // picks the kernel instantiation (the derivative's entries are not flat)
+  if (!deriv) {
+    kernel_mean_rows<<<m, 256, 0, ctx->stream>>>(XJ, nj, d, m, (float)gamma, samp);
+    TSVM_LAUNCHED(ctx);
+    kernel_mean_finish<<<1, 256, 0, ctx->stream>>>(samp, m, scale);
+    TSVM_LAUNCHED(ctx);
+    TSVM_CUDA(cudaMemcpyAsync(&hshift, scale + 2, sizeof(float), cudaMemcpyDeviceToHost,
+                              ctx->stream));
+    TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  } else {
+    TSVM_CUDA(cudaMemsetAsync(scale + 2, 0, sizeof(float), ctx->stream));
+  }
   const dim3 tgrid((unsigned)rg, (unsigned)ceil_div(kp, 32));
   if (bf16)
     prep_at<__nv_bfloat16><<<tgrid, dim3(32, 8), 0, ctx->stream>>>(
-        A, y, n, n_pad, kp, scale, reinterpret_cast<__nv_bfloat16 *>(AT),
+        A, yJ, nj, n_pad, kp, scale, reinterpret_cast<__nv_bfloat16 *>(AT),
         reinterpret_cast<__nv_bfloat16 *>(ATlo), round_back, cpart);
   else
     prep_at<__half><<<tgrid, dim3(32, 8), 0, ctx->stream>>>(
-        A, y, n, n_pad, kp, scale, reinterpret_cast<__half *>(AT), reinterpret_cast<__half *>(ATlo),
+        A, yJ, nj, n_pad, kp, scale, reinterpret_cast<__half *>(AT), reinterpret_cast<__half *>(ATlo),
         round_back, cpart);
   TSVM_LAUNCHED(ctx);
   column_shift<<<(unsigned)ceil_div(kp, 256), 256, 0, ctx->stream>>>(cpart, rg, kp, scale, ccol);
@@ -867,11 +906,11 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
         !make_map(&matlo, ATlo ? ATlo : AT, at_type, kBJ, (uint64_t)ntiles * kp, kBJ, kpw))
       return TSVM_ERR_CUDA;
     const size_t smem = tc_smem(KG, kpw);
-    auto kern = select_kernel(bf16, poly_split(), KG, hshift != 0.f, split);
+    auto kern = select_kernel(bf16, poly_split(), KG, hshift != 0.f, split, deriv);
     if (!kern) return TSVM_ERR_UNSUPPORTED;
     TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<grid, kThreadsTC, smem, ctx->stream>>>(mxa, mxb, mat, matlo, y + row0, scale + 1,
-                                                  ccol, nr, nrb, ntiles, kp, c0, kpw, W, kp, err);
+    kern<<<grid, kThreadsTC, smem, ctx->stream>>>(mxa, mxb, mat, matlo, yI, scale + 1, ccol, ni,
+                                                  nrb, ntiles, kp, c0, kpw, W, kp, err);
     TSVM_LAUNCHED(ctx);
   }
   TSVM_CUDA(cudaEventRecord(e1, ctx->stream));

@@ -21,6 +21,9 @@ tsvm_status glibc_rand_stream(tsvm_context *ctx, int64_t count, uint32_t *out);
 // Centre X (n x d row-major) by its column means into Xc (n x d), write row norms ||xc||^2.
 tsvm_status centre_features(tsvm_context *ctx, const float *X, int64_t n, int d, float *Xc,
                             float *norms);
+// XJc, XIc = XJ, XI less the column means of XJ (one centre for both point sets).
+tsvm_status centre_pair(tsvm_context *ctx, const float *XJ, int64_t nj, const float *XI,
+                        int64_t ni, int d, float *XJc, float *XIc);
 // Copy src (n x k, leading dim lds) into dst (n x ldd), zero columns k..ldd-1.
 tsvm_status pad_rows(tsvm_context *ctx, const float *src, int64_t lds, int64_t n, int k,
                      float *dst, int64_t ldd);
@@ -49,6 +52,15 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
                          int64_t n, int d, double gamma, const float *A, int kp, float *W,
                          int precision, float *kernel_ms, float *round_back = nullptr,
                          int split = 0, int64_t row0 = 0, int64_t nr = -1);
+
+// W (ni x kp) = Y_I K(X_I, X_J) Y_J A on the tensor cores, I rows XI (ni x d) and J rows XJ
+// (nj x d; A nj x kp), both centred by the same vector; null labels mean all ones; XI may be XJ.
+// split: 0..2 as kermatmul_tc, 3 = both the kernel block and A as hi + lo (about FP32 accuracy);
+// deriv (split 3, FP16 only): the entries are -gamma log2(e) ||x_i - x_j||^2 K_ij.
+tsvm_status kermatmul_tc_core(tsvm_context *ctx, const float *XI, const float *yI, int64_t ni,
+                              const float *XJ, const float *yJ, int64_t nj, int d, double gamma,
+                              const float *A, int kp, float *W, int precision, float *kernel_ms,
+                              float *round_back, int split, bool deriv);
 
 // Precision classes of tsvm_precision.
 inline bool precision_valid(int p) { return p >= TSVM_PREC_FP32 && p <= TSVM_PREC_FP16_FAST; }
