@@ -27,6 +27,11 @@ tsvm_status tsvm_test_sketch_philox(tsvm_context *ctx, uint64_t seed, int64_t co
 tsvm_status tsvm_test_kermatmul(tsvm_context *ctx, const float *X, const float *y, int64_t n,
                                 int32_t d, double gamma, const float *A, int32_t kp, float *W,
                                 int32_t precision, int32_t split);
+/* out (na x nu, FP64) = sum_j w_ij exp(-gamma ||a_i - b_j||^2) U[j][:], w = 1 or (deriv)
+ * -||a_i - b_j||^2, by the hypergradient's SIMT products or (tensor_cores) the tcgen05 form. */
+tsvm_status tsvm_test_kprod(tsvm_context *ctx, const float *A, int64_t na, const float *B,
+                            int64_t nb, int32_t d, double gamma, const double *U, int32_t nu,
+                            double *out, int32_t deriv, int32_t tensor_cores);
 /* In-place lower Cholesky of A (n x n row-major); *info_host = 0 or failing column (T:1709). */
 tsvm_status tsvm_test_chol(tsvm_context *ctx, double *A, int32_t n, int32_t *info_host);
 /* Solve L L^T X = B, B holds nrhs rows of length ldb (T:1834). */

@@ -369,6 +369,26 @@ __global__ void unpack_col(const double *U, const float *y, int64_t n, int nu, i
 }
 
 }  // namespace
+
+// Test hook (tsvm_test_kprod): out = [K or K'](A, B) U by the SIMT or the tensor-core products.
+tsvm_status kprod_any(tsvm_context *ctx, const float *A, int64_t na, const float *B, int64_t nb,
+                      int d, double gamma, const double *U, int nu, double *out, bool deriv,
+                      bool tc) {
+  if (tc) {
+    if (!kermatmul_tc_supported(d, 64)) return TSVM_ERR_UNSUPPORTED;
+    return kprod_tc(ctx, A, na, B, nb, d, gamma, U, nu, out, deriv);
+  }
+  if (d > kKMaxD) return TSVM_ERR_UNSUPPORTED;
+  if (nu == 1)
+    return deriv ? kprod<1, true>(ctx, A, na, B, nb, d, gamma, U, nu, out)
+                 : kprod<1, false>(ctx, A, na, B, nb, d, gamma, U, nu, out);
+  if (nu <= 8)
+    return deriv ? kprod<8, true>(ctx, A, na, B, nb, d, gamma, U, nu, out)
+                 : kprod<8, false>(ctx, A, na, B, nb, d, gamma, U, nu, out);
+  return deriv ? kprod<32, true>(ctx, A, na, B, nb, d, gamma, U, nu, out)
+               : kprod<32, false>(ctx, A, na, B, nb, d, gamma, U, nu, out);
+}
+
 }  // namespace tsvm
 
 using namespace tsvm;

@@ -62,6 +62,12 @@ tsvm_status kermatmul_tc_core(tsvm_context *ctx, const float *XI, const float *y
                               const float *A, int kp, float *W, int precision, float *kernel_ms,
                               float *round_back, int split, bool deriv);
 
+// Kernel-vector products of the hypergradient (hypergrad.cu): out (na x nu, FP64) =
+// [K or K' = -||a - b||^2 K](A, B) U with U nb x nu FP64, on the SIMT kernel or the tensor cores.
+tsvm_status kprod_any(tsvm_context *ctx, const float *A, int64_t na, const float *B, int64_t nb,
+                      int d, double gamma, const double *U, int nu, double *out, bool deriv,
+                      bool tc);
+
 // Precision classes of tsvm_precision.
 inline bool precision_valid(int p) { return p >= TSVM_PREC_FP32 && p <= TSVM_PREC_FP16_FAST; }
 inline bool precision_is_bf16(int p) { return p == TSVM_PREC_BF16 || p == TSVM_PREC_BF16_FAST; }

@@ -46,6 +46,16 @@ tsvm_status tsvm_test_sketch_philox(tsvm_context *ctx, uint64_t seed, int64_t co
   return TSVM_OK;
 }
 
+tsvm_status tsvm_test_kprod(tsvm_context *ctx, const float *A, int64_t na, const float *B,
+                            int64_t nb, int32_t d, double gamma, const double *U, int32_t nu,
+                            double *out, int32_t deriv, int32_t tensor_cores) {
+  if (!ctx || !A || !B || !U || !out || na < 1 || nb < 1 || d < 1 || nu < 1 || nu > 64)
+    return TSVM_ERR_INVALID_ARGUMENT;
+  TSVM_TRY(kprod_any(ctx, A, na, B, nb, d, gamma, U, nu, out, deriv != 0, tensor_cores != 0));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSVM_OK;
+}
+
 tsvm_status tsvm_test_kermatmul(tsvm_context *ctx, const float *X, const float *y, int64_t n,
                                 int32_t d, double gamma, const float *A, int32_t kp, float *W,
                                 int32_t precision, int32_t split) {

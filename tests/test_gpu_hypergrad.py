@@ -119,3 +119,30 @@ def test_hypergrad_autograd_matches_central_differences(ctx, data):
     scale = 1e-3 * float(loss.detach())
     assert abs(float(lc.grad) - fd_c) <= 2e-2 * max(abs(fd_c), scale), (float(lc.grad), fd_c)
     assert abs(float(lg.grad) - fd_g) <= 2e-2 * max(abs(fd_g), scale), (float(lg.grad), fd_g)
+
+
+@pytest.mark.parametrize("na,nb,nu,deriv", [(2000, 2000, 1, False), (3001, 1777, 5, True),
+                                            (500, 4000, 29, False), (1000, 1000, 1, True)])
+def test_kernel_vector_products_tc_and_simt(ctx, na, nb, nu, deriv):
+    """The hypergradient's kernel-vector products, SIMT and tensor-core forms, against FP64:
+    out = sum_j w_ij K(a_i, b_j) U_j, w = 1 or -||a_i - b_j||^2 (dK/dgamma), rectangular row
+    sets included."""
+    import ctypes
+    rng = np.random.default_rng(na + nb + nu)
+    A = rng.standard_normal((na, D)).astype(np.float32)
+    B = rng.standard_normal((nb, D)).astype(np.float32) + 0.3
+    U = rng.standard_normal((nb, nu))
+    gamma = 0.03
+    d2 = ((A.astype(np.float64)[:, None, :] - B.astype(np.float64)[None, :, :]) ** 2).sum(-1)
+    Kab = np.exp(-gamma * d2)
+    ref = ((-d2 * Kab) if deriv else Kab) @ U
+    Ad, Bd, Ud = dev(A), dev(B), dev(U)
+    for tc, tol in ((0, 1e-5), (1, 2e-5)):
+        out = torch.empty((na, nu), dtype=torch.float64, device="cuda")
+        _lib.check(ctx.lib.tsvm_test_kprod(ctx.handle, ctypes.c_void_p(Ad.data_ptr()), na,
+                                           ctypes.c_void_p(Bd.data_ptr()), nb, D, gamma,
+                                           ctypes.c_void_p(Ud.data_ptr()), nu,
+                                           ctypes.c_void_p(out.data_ptr()), int(deriv), tc),
+                   "kprod")
+        err = np.linalg.norm(out.cpu().numpy() - ref) / np.linalg.norm(ref)
+        assert err < tol, (tc, err)
