@@ -48,7 +48,7 @@ def test_two_gloo_ranks_max_over_ranks_and_distinct_replicas():
     assert be0 == be1 == "gloo"
 
 
-# ---- row-sharded training restated in FP64 on gloo ranks ----------------------
+# ---- row-sharded training restated in FP64 on gloo ranks --------------------------------
 
 def _sharded_rank(rank, world, port, out, n, k):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(world),
