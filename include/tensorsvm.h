@@ -186,6 +186,14 @@ tsvm_status tsvm_set_comm(tsvm_context *ctx, const tsvm_comm *comm);
  * reference's sketch has no seed: glibc rand() is never seeded (tensorsvm-train.cu:1966). */
 tsvm_status tsvm_set_sketch_seed(tsvm_context *ctx, uint64_t seed);
 
+/* With keep = 1, every tsvm_factor of this context with the glibc sketch keeps what the
+ * hypergradient needs of it in the context (the sketch, the CholeskyQR factor, the basis before
+ * its 16-bit rounding and Z: about 3 n k_padded floats), and tsvm_hypergrad on the same X, y, n, d,
+ * gamma, k and precision reuses them instead of recomputing the factor.  Off (0) by default: when
+ * memory is tight the hypergradient recomputes the factor.  The kept factor's orthonormalisation
+ * uses exact FP64 Gram matrices (as the recomputation does). */
+tsvm_status tsvm_set_factor_keep(tsvm_context *ctx, int32_t keep);
+
 /* Fill `opt` with the reference's defaults (max_iter 100, tol 1e-7, FP32, RBF init). */
 void tsvm_ipm_default_options(tsvm_ipm_options *opt);
 
@@ -278,6 +286,7 @@ typedef struct tsvm_hypergrad_result {
   double dloss_dlog_C;
   int32_t n_free_bias;       /* free SVs the bias was averaged over (<= 50) */
   double ms;
+  int32_t factor_reused;     /* 1: the factor kept by tsvm_factor was reused, 0: recomputed */
 } tsvm_hypergrad_result;
 
 /* Hypergradient of the validation squared-hinge loss of a trained RBF SVM (no counterpart in
@@ -285,7 +294,8 @@ typedef struct tsvm_hypergrad_result {
  * training set (X n x d, labels y), gamma, C, k and the factor precision used for training,
  * the solution of tsvm_ipm (alpha, xi, s, the equality multiplier ymult) and the bias b of
  * tsvm_bias, the model is f(x) = sum_i alpha_i y_i exp(-gamma ||x_i - x||^2) + b.  The factor
- * is recomputed (same sketch, same Z as training), the KKT system of the dual is differentiated
+ * is reused when tsvm_factor kept it (tsvm_set_factor_keep) for the same inputs, else recomputed
+ * (same sketch, same Z as training), the KKT system of the dual is differentiated
  * implicitly with one adjoint solve through I + Z^T D^-1 Z (SMW, as the IPM's Newton step),
  * and the gamma derivative goes through the range finder with the sketch held fixed.  dXv
  * (device, nv x d, may be NULL) receives dL/dXv.  All arrays are device pointers; d <= 64. */

@@ -47,6 +47,7 @@ EXPORTS = [
     "tsvm_decision_values", "tsvm_predict", "tsvm_kernel_residual", "tsvm_train_residual",
     "tsvm_read_libsvm", "tsvm_free", "tsvm_write_model", "tsvm_read_model", "tsvm_free_model",
     "tsvm_set_comm", "tsvm_factor_rows", "tsvm_set_sketch_seed", "tsvm_factor_batched",
+    "tsvm_set_factor_keep",
 ]
 TEST_EXPORTS = [
     "tsvm_test_rand_stream", "tsvm_test_sketch", "tsvm_test_kermatmul", "tsvm_test_chol",
@@ -86,7 +87,7 @@ class BatchInfo(ctypes.Structure):
 class HypergradResult(ctypes.Structure):
     _fields_ = [("loss", ctypes.c_double), ("dloss_dlog_gamma", ctypes.c_double),
                 ("dloss_dlog_C", ctypes.c_double), ("n_free_bias", ctypes.c_int32),
-                ("ms", ctypes.c_double)]
+                ("ms", ctypes.c_double), ("factor_reused", ctypes.c_int32)]
 
 
 class ModelView(ctypes.Structure):
@@ -151,6 +152,8 @@ def load() -> ctypes.CDLL:
     lib.tsvm_factor.restype = ctypes.c_int
     lib.tsvm_factor.argtypes = [P, P, P, I64, I32, D, I32, I32, I32, P, P, I32,
                                 ctypes.POINTER(FactorInfo)]
+    lib.tsvm_set_factor_keep.restype = ctypes.c_int
+    lib.tsvm_set_factor_keep.argtypes = [P, I32]
     lib.tsvm_set_sketch_seed.restype = ctypes.c_int
     lib.tsvm_set_sketch_seed.argtypes = [P, ctypes.c_uint64]
     lib.tsvm_factor_batched.restype = ctypes.c_int
@@ -272,6 +275,10 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def set_factor_keep(self, on: bool) -> None:
+        """Keep each factor's state for tsvm_hypergrad (tsvm_set_factor_keep)."""
+        check(self.lib.tsvm_set_factor_keep(self.handle, 1 if on else 0), "tsvm_set_factor_keep")
 
     def set_stream(self, stream_handle: int) -> None:
         """Issue all work on the given cudaStream_t (e.g. torch.cuda.Stream().cuda_stream)."""

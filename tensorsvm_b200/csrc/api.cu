@@ -150,6 +150,12 @@ tsvm_status tsvm_set_comm(tsvm_context *ctx, const tsvm_comm *comm) {
   return TSVM_OK;
 }
 
+tsvm_status tsvm_set_factor_keep(tsvm_context *ctx, int32_t keep) {
+  if (!ctx || keep < 0 || keep > 1) return TSVM_ERR_INVALID_ARGUMENT;
+  ctx->keep_factor = keep;
+  return TSVM_OK;
+}
+
 tsvm_status tsvm_set_sketch_seed(tsvm_context *ctx, uint64_t seed) {
   if (!ctx) return TSVM_ERR_INVALID_ARGUMENT;
   ctx->sketch_seed = seed;
@@ -177,6 +183,8 @@ tsvm_status tsvm_factor(tsvm_context *ctx, const float *X, const float *y, int64
   if (sharded(ctx)) return TSVM_ERR_UNSUPPORTED;   // row-sharded: tsvm_factor_rows
   TSVM_CUDA(cudaSetDevice(ctx->device));
   TraceRange tr("tsvm_factor");
+  if (ctx->keep_factor && sketch == TSVM_SKETCH_GLIBC && k >= 1 && n >= 2 && ldz >= k)
+    return factor_rbf_keep(ctx, X, y, n, d, gamma, k, precision, Z, ldz, info);
   return factor_rbf(ctx, X, y, n, d, gamma, k, precision, sketch, Q_user, Z, ldz, info);
 }
 

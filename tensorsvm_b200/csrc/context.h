@@ -47,6 +47,7 @@ enum Slot : int {
   SLOT_HG_R,          // hypergradient: combined CholeskyQR factor and k-vectors
   SLOT_HG_KPART,      // hypergradient: per-split partial kernel-vector products
   SLOT_HG_W,          // hypergradient: the factor's orthonormal basis before rounding
+  SLOT_HG_Z,          // hypergradient: the factor Z it differentiates (kept or recomputed)
   SLOT_HG_TC,         // hypergradient: centred rows, FP32 operand and product of the tensor-core
                       // kernel-vector products
   SLOT_DEV_IN,        // tsvm_train: device copies of host inputs
@@ -86,6 +87,16 @@ struct tsvm_context {
   // row-sharded solves (tsvm_set_comm): the caller's communicator
   bool has_comm = false;
   tsvm_comm comm = {};
+  // tsvm_set_factor_keep: tsvm_factor keeps what tsvm_hypergrad needs of the factor (sketch,
+  // CholeskyQR R, unrounded basis, Z in SLOT_HG_*), and which inputs it belongs to
+  int keep_factor = 0;
+  struct {
+    bool valid = false;
+    const float *X = nullptr, *y = nullptr;
+    int64_t n = 0;
+    int d = 0, k = 0, precision = 0;
+    double gamma = 0.0;
+  } kept;
   // the last RBF tsvm_train (its X, y in SLOT_DEV_IN and Z in SLOT_DEV_Z), for -analysis
   struct {
     bool valid = false;

@@ -402,4 +402,37 @@ tsvm_status factor_rbf_batched(tsvm_context *ctx, const tsvm_factor_problem *pr,
   return TSVM_OK;
 }
 
+tsvm_status factor_rbf_keep(tsvm_context *ctx, const float *X, const float *y, int64_t n, int d,
+                            double gamma, int k, int precision, float *Z, int ldz,
+                            tsvm_factor_info *info) {
+  const int kp = (int)round_up(k, 64);
+  float *Zk = nullptr, *Om = nullptr, *Wk = nullptr;
+  double *Rbuf = nullptr;
+  ctx->kept.valid = false;
+  TSVM_TRY(scratch_t(ctx, SLOT_HG_Z, (size_t)n * kp, &Zk));
+  TSVM_TRY(scratch_t(ctx, SLOT_HG_OMEGA, (size_t)n * kp, &Om));
+  TSVM_TRY(scratch_t(ctx, SLOT_HG_R, (size_t)2 * k * k + 2 * (size_t)kp + 64, &Rbuf));
+  TSVM_TRY(scratch_t(ctx, SLOT_HG_W, (size_t)n * kp, &Wk));
+  FactorKeep keep{Om, Rbuf, Wk};
+  TSVM_TRY(factor_rbf(ctx, X, y, n, d, gamma, k, precision, TSVM_SKETCH_GLIBC, nullptr, Zk, kp,
+                      info, &keep));
+  if (Z && Z != Zk)
+    TSVM_CUDA(cudaMemcpy2DAsync(Z, sizeof(float) * ldz, Zk, sizeof(float) * kp,
+                                sizeof(float) * (ldz < kp ? ldz : kp), n, cudaMemcpyDeviceToDevice,
+                                ctx->stream));
+  if (Z && ldz > kp)
+    TSVM_CUDA(cudaMemset2DAsync(Z + kp, sizeof(float) * ldz, 0, sizeof(float) * (ldz - kp), n,
+                                ctx->stream));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->kept.valid = true;
+  ctx->kept.X = X;
+  ctx->kept.y = y;
+  ctx->kept.n = n;
+  ctx->kept.d = d;
+  ctx->kept.k = k;
+  ctx->kept.precision = precision;
+  ctx->kept.gamma = gamma;
+  return TSVM_OK;
+}
+
 }  // namespace tsvm

@@ -443,18 +443,20 @@ extern "C" tsvm_status tsvm_hypergrad(tsvm_context *ctx, const float *X, const f
   const auto t0 = std::chrono::steady_clock::now();
   cudaStream_t st = ctx->stream;
   const int kp = (int)round_up(k, 64);
-  // recompute the factorisation, keeping Omega, R and W
-  float *Zf = nullptr, *Om = nullptr;
-  ctx->last_train.valid = false;   // the factor below overwrites tsvm_train's Z
-  TSVM_TRY(scratch_t(ctx, SLOT_DEV_Z, (size_t)n * kp, &Zf));
-  TSVM_TRY(scratch_t(ctx, SLOT_HG_OMEGA, (size_t)n * kp, &Om));
+  // the factorisation with its sketch Omega, R and unrounded W: kept by tsvm_factor (with
+  // tsvm_set_factor_keep) for these very inputs, or recomputed here
+  const bool reuse = ctx->kept.valid && ctx->kept.X == X && ctx->kept.y == y && ctx->kept.n == n &&
+                     ctx->kept.d == d && ctx->kept.k == k && ctx->kept.precision == precision &&
+                     ctx->kept.gamma == gamma;
+  if (!reuse) TSVM_TRY(factor_rbf_keep(ctx, X, y, n, d, gamma, k, precision, nullptr, kp, nullptr));
+  float *Zf = nullptr, *Om = nullptr, *Wk = nullptr;
   double *Rbuf = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_HG_Z, (size_t)n * kp, &Zf));
+  TSVM_TRY(scratch_t(ctx, SLOT_HG_OMEGA, (size_t)n * kp, &Om));
   TSVM_TRY(scratch_t(ctx, SLOT_HG_R, (size_t)2 * k * k + 2 * (size_t)kp + 64, &Rbuf));
-  float *Wk = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_HG_W, (size_t)n * kp, &Wk));
   FactorKeep keep{Om, Rbuf, Wk};
-  TSVM_TRY(factor_rbf(ctx, X, y, n, d, gamma, k, precision, TSVM_SKETCH_GLIBC, nullptr, Zf, kp,
-                      nullptr, &keep));
+  res->factor_reused = reuse ? 1 : 0;
   // scratch: n-vectors beta, c, lam, u, E1, tmp, t2, s2, r + U5/D5 (5 n each); nv-vectors
   const int nb = 148;
   double *buf = nullptr;

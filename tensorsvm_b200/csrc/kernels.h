@@ -192,6 +192,11 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
 // With C_out set, factor_rbf stops after the projection: C_out (k x k FP64) holds the symmetrised
 // C = W^T (K W) and Z (ldz = kp) the orthonormal basis W; factor_finish then forms
 // Z = W V diag(sqrt(max(w, 0))) in place from C's eigen-decomposition (V k x k row-major, w k).
+// factor_rbf keeping the hypergradient's factor state in the context (SLOT_HG_OMEGA / _R / _W /
+// _Z, ctx->kept); Z (ldz) receives the factor as from factor_rbf.
+tsvm_status factor_rbf_keep(tsvm_context *ctx, const float *X, const float *y, int64_t n, int d,
+                            double gamma, int k, int precision, float *Z, int ldz,
+                            tsvm_factor_info *info);
 tsvm_status factor_finish(tsvm_context *ctx, float *Z, int64_t n, int k, const double *V,
                           const double *w, tsvm_factor_info *info);
 // Factors of `count` independent problems (shared d, k, precision): every problem through the

@@ -146,3 +146,23 @@ def test_kernel_vector_products_tc_and_simt(ctx, na, nb, nu, deriv):
                    "kprod")
         err = np.linalg.norm(out.cpu().numpy() - ref) / np.linalg.norm(ref)
         assert err < tol, (tc, err)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+def test_hypergrad_reuses_kept_factor(ctx, data, prec):
+    """With tsvm_set_factor_keep the backward reuses the forward's factor (sketch, R, unrounded
+    basis, Z) instead of recomputing it, with the same result as the recomputing call."""
+    X, y, Xv, yv = data
+    gamma, C = 0.03, 16.0
+    Xd, yd, Xvd, yvd = dev(X), dev(y), dev(Xv), dev(yv)
+    with _lib.Context(0) as c2:
+        c2.set_factor_keep(True)
+        Z, alpha, xi, ym, b = train(c2, Xd, yd, gamma, C, prec)
+        kept, _ = api.hypergrad(c2, Xd, yd, Xvd, yvd, gamma, C, K, alpha, xi[0], xi[1], ym, b,
+                                precision=prec)
+    with _lib.Context(0) as c3:   # no kept factor: recomputed
+        fresh, _ = api.hypergrad(c3, Xd, yd, Xvd, yvd, gamma, C, K, alpha, xi[0], xi[1], ym, b,
+                                 precision=prec)
+    assert kept["factor_reused"] == 1 and fresh["factor_reused"] == 0
+    for key in ("loss", "dloss_dlog_gamma", "dloss_dlog_C"):
+        assert abs(kept[key] - fresh[key]) <= 1e-10 * max(1.0, abs(fresh[key])), key
