@@ -460,7 +460,7 @@ extern "C" tsvm_status tsvm_hypergrad(tsvm_context *ctx, const float *X, const f
   // scratch: n-vectors beta, c, lam, u, E1, tmp, t2, s2, r + U5/D5 (5 n each); nv-vectors
   const int nb = 148;
   double *buf = nullptr;
-  const size_t need = (size_t)19 * n + (size_t)4 * nv + (size_t)k + 4 * nb + 64;
+  const size_t need = (size_t)19 * n + (size_t)4 * nv + (size_t)k + 4 * nb + 64 + 64;
   TSVM_TRY(scratch_t(ctx, SLOT_DEV_OUT, need, &buf));
   double *beta = buf, *c = beta + n, *lam = c + n, *u = lam + n, *E1 = u + n, *tmp = E1 + n;
   double *t2 = tmp + n, *s2 = t2 + n, *r = s2 + n, *U5 = r + n, *D5 = U5 + 5 * n;
@@ -477,8 +477,9 @@ extern "C" tsvm_status tsvm_hypergrad(tsvm_context *ctx, const float *X, const f
   std::vector<int64_t> F;
   for (int64_t i = 0; i < n && F.size() < 50; ++i)
     if (ha[i] > 1e-6 && ha[i] < C - 1e-6) F.push_back(i);
-  int64_t *dF = nullptr;
-  TSVM_TRY(scratch_t(ctx, SLOT_MISC, (size_t)64, &dF));
+  // the free-set indices live in this call's own buffer: the kernel-vector products below grow
+  // the shared scratch slots (a regrown slot is freed and reallocated)
+  int64_t *dF = reinterpret_cast<int64_t *>(part + 4 * nb);
   if (!F.empty())
     TSVM_CUDA(cudaMemcpyAsync(dF, F.data(), sizeof(int64_t) * F.size(), cudaMemcpyHostToDevice, st));
   const int nf = (int)F.size();
