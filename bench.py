@@ -153,6 +153,21 @@ def tc_traffic(n: int) -> float:
     return round(TC_BYTES_PER_TILE * tiles, -6)
 
 
+def tc_executed(n: int, k: int, d: int, split: bool) -> dict:
+    """Tensor-core flops the two kernel-block launches execute (128 x 64 tiles; Gram K of
+    3 d + 6 rounded up to 64; the split forms run two P A products per tile), against the
+    algorithmic 2 n^2 k + 2 n^2 d per product: the range-finder pass takes every tile, the
+    projection pass (half product) the tiles from the diagonal on."""
+    nrb, ntl = -(-n // 128), 2 * -(-n // 128)
+    kp = -(-k // 64) * 64
+    kg = 64 if 3 * d + 6 <= 64 else 128 if 3 * d + 6 <= 128 else 192
+    per_tile = 2.0 * 128 * 64 * kg + (2 if split else 1) * 2.0 * 128 * 64 * kp
+    full = nrb * ntl
+    half = sum(ntl - 2 * rb for rb in range(nrb))
+    return {"pass1_tiles": full, "pass2_tiles": half, "pass1_flops": full * per_tile,
+            "pass2_flops": half * per_tile}
+
+
 def run_ours(args, world, rank, local):
     import torch
     from tensorsvm_b200 import _lib, api, synth
@@ -258,6 +273,18 @@ def run_ours(args, world, rank, local):
         # FP32 SIMT FMA peak: 148 SMs x 128 lanes x 2 flops x 1.965 GHz (nominal, no measured copy)
         peak, unit, pname, pk_kind = 148 * 128 * 2 * 1.965e9 / 1e12, "TFLOP/s", "fp32_simt_nominal", "nominal"
     achieved = km_flops / (km_ms / 1e3) / 1e12
+    passes = None
+    if tensor:
+        ex = tc_executed(n, K, D, prec in ("fp16", "bf16"))
+        passes = {}
+        for name, key, tiles, fl in (("range_finder", "ms_pass1", ex["pass1_tiles"], ex["pass1_flops"]),
+                                      ("projection_half", "ms_pass2", ex["pass2_tiles"], ex["pass2_flops"])):
+            ms = fi[key]
+            passes[name] = {"phase_ms": round(ms, 2), "tiles": tiles,
+                            "algorithmic_tflops": round(km_flops / (ms / 1e3) / 1e12, 1),
+                            "executed_flops": fl,
+                            "executed_tflops": round(fl / (ms / 1e3) / 1e12, 1),
+                            "executed_frac": round(fl / (ms / 1e3) / 1e12 / peak, 4)}
     st = stats[-1]
     line = {
         "metric": METRIC,
@@ -290,7 +317,8 @@ def run_ours(args, world, rank, local):
                      "traffic_source": ("dram__bytes_read.sum + dram__bytes_write.sum of one launch "
                                         "at n=262144 (2.649 GB over 2048x4096 tiles), scaled by "
                                         "the tile count" if tensor else None),
-                     "flops_per_launch": km_flops, "ms_per_launch": round(km_ms, 3)},
+                     "flops_per_launch": km_flops, "ms_per_launch": round(km_ms, 3),
+                     "passes": passes},
         "e2e": {"value": round(e2e_s, 4), "unit": "s",
                 "h2d_bytes_per_step": int(X.nbytes + y.nbytes), "d2h_bytes_per_step": int(8 * n + 8)},
         "gpu_launches": int(launches),

@@ -27,6 +27,13 @@ tsvm_status tsvm_test_sketch_philox(tsvm_context *ctx, uint64_t seed, int64_t co
 tsvm_status tsvm_test_kermatmul(tsvm_context *ctx, const float *X, const float *y, int64_t n,
                                 int32_t d, double gamma, const float *A, int32_t kp, float *W,
                                 int32_t precision, int32_t split);
+/* The half product of a symmetric projection on the tensor cores: R (n x kp) = Y (K o H) Y A with
+ * H_ij = 1 (j > i), 1/2 (j == i), 0 (j < i), and sym (kp + 1 doubles) = [s, A^T y] such that
+ * A^T (Y K Y) A = A^T R + R^T A + s (A^T y)(A^T y)^T (s: the kernel-mean shift, or 0).  split 0
+ * or 2 (A as hi + lo) as tsvm_test_kermatmul. */
+tsvm_status tsvm_test_kermatmul_half(tsvm_context *ctx, const float *X, const float *y, int64_t n,
+                                     int32_t d, double gamma, const float *A, int32_t kp,
+                                     float *R, double *sym, int32_t precision, int32_t split);
 /* out (na x nu, FP64) = sum_j w_ij exp(-gamma ||a_i - b_j||^2) U[j][:], w = 1 or (deriv)
  * -||a_i - b_j||^2, by the hypergradient's SIMT products or (tensor_cores) the tcgen05 form. */
 tsvm_status tsvm_test_kprod(tsvm_context *ctx, const float *A, int64_t na, const float *B,

@@ -24,6 +24,18 @@
 namespace tsvm {
 namespace {
 
+// C <- C + C^T + s u u^T with s = sym[0], u = sym[1..k]: the projection W^T K W from the half
+// product's C = W^T R (pairs i <= j, one thread each)
+__global__ void half_projection_finish(double *C, int k, const double *__restrict__ sym) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)k * k) return;
+  const int i = (int)(e / k), j = (int)(e % k);
+  if (i > j) return;
+  const double v = C[(int64_t)i * k + j] + C[(int64_t)j * k + i] + sym[0] * sym[1 + i] * sym[1 + j];
+  C[(int64_t)i * k + j] = v;
+  C[(int64_t)j * k + i] = v;
+}
+
 // G[i][i] += factor * trace(G)   (one block)
 __global__ void shift_by_trace(double *G, int k, double factor) {
   __shared__ double sh[32];
@@ -257,7 +269,17 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
                               cudaMemcpyDeviceToDevice, ctx->stream));
     TSVM_TRY(comm_allreduce(ctx, Wall, n * (int64_t)kp, 1, COMM_SUM));
   }
-  if (split) {
+  // The projection needs only C = W^T K W: on one device the tensor-core forms take the half
+  // product R over the J blocks from the diagonal on (about half the tiles) and
+  // C = W^T R + R^T W + s u u^T.
+  double *Cm = nullptr, *V = nullptr, *w = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_SMALL, (size_t)k * k + 8 + (size_t)kp + 8, &Cm));
+  double *sym = Cm + (size_t)k * k + 8;
+  const bool half = precision != TSVM_PREC_FP32 && !rows;
+  if (half) {
+    TSVM_TRY(kermatmul_tc_half(ctx, Xc, y, n, d, gamma, W, kp, Q, precision, &km2,
+                               split ? nullptr : W, split ? 2 : 0, sym));
+  } else if (split) {
     TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, Wall, kp, Q, precision, &km2, nullptr, 2,
                        row0, nr));
   } else {
@@ -269,13 +291,17 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
   }
   TSVM_CUDA(cudaEventRecord(ev[4], ctx->stream));
   phase.next("factor: projection and eigensolver");
-  double *Cm = nullptr, *V = nullptr, *w = nullptr;
-  TSVM_TRY(scratch_t(ctx, SLOT_SMALL, (size_t)k * k + 8, &Cm));
   TSVM_TRY(scratch_t(ctx, SLOT_SMALL2, (size_t)k * k + (size_t)k, &V));
   w = V + (size_t)k * k;
   TSVM_TRY(gram_fp64(ctx, W, kp, Q, kp, nr, k, k, false, Cm));
-  TSVM_TRY(comm_allreduce(ctx, Cm, (int64_t)k * k, 0, COMM_SUM));   // row-sharded
-  TSVM_TRY(small_symmetrize(ctx, Cm, k, k));
+  if (half) {
+    half_projection_finish<<<(unsigned)ceil_div((int64_t)k * k, 256), 256, 0, ctx->stream>>>(
+        Cm, k, sym);
+    TSVM_LAUNCHED(ctx);
+  } else {
+    TSVM_TRY(comm_allreduce(ctx, Cm, (int64_t)k * k, 0, COMM_SUM));   // row-sharded
+    TSVM_TRY(small_symmetrize(ctx, Cm, k, k));
+  }
   if (C_out) {   // stop here: the batched factor solves the eigenproblems of all problems at once
     TSVM_CUDA(cudaMemcpyAsync(C_out, Cm, sizeof(double) * k * k, cudaMemcpyDeviceToDevice,
                               ctx->stream));

@@ -175,8 +175,22 @@ __host__ __device__ constexpr bool split_a(int s) { return s == kSplitA || s == 
 // (map_at) and AT_lo (map_atlo), and the issuer runs W += P AT_hi^T + P AT_lo^T.
 // DERIV: the kernel block's entries are S exp2(S) = -gamma log2(e) ||x_i - x_j||^2 K_ij (the
 // caller divides W by -gamma log2 e for dK/dgamma = -||x_i - x_j||^2 K).
+// tri (I and J the same rows): the half product R = Y (K o H) Y A with H_ij = 1 for j > i, 1/2 for
+// j == i and 0 for j < i, over the J blocks from the diagonal on (about half of the tiles), for a
+// symmetric projection A^T K A = A^T R + R^T A.  The kernel-mean shift is not restored here: the
+// caller adds shift (A^T y)(A^T y)^T to the projection instead.
 // ---------------------------------------------------------------------------------------
 constexpr int kSBufs = 4;
+
+// Row block of round r for this CTA.  The half product (tri) walks the rounds in alternating
+// directions, so that the CTA with the longest row (the lowest row block) of one round has the
+// shortest of the next.
+__device__ __forceinline__ int row_block(int r, int G, int tri) {
+  return r * G + ((tri && (r & 1)) ? G - 1 - (int)blockIdx.x : (int)blockIdx.x);
+}
+// First J block of row block rb: all of them, or for the half product the first one that
+// reaches column rb * kBM (the diagonal).
+__device__ __forceinline__ int first_tile(int rb, int tri) { return tri ? rb * (kBM / kBJ) : 0; }
 
 template <bool BF16, int NPOLY, int KG, bool SHIFT, int SPLIT, bool DERIV>
 __global__ void __launch_bounds__(kThreadsTC, 1)
@@ -185,7 +199,7 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
                     const __grid_constant__ CUtensorMap map_at,
                     const __grid_constant__ CUtensorMap map_atlo, const float *__restrict__ y,
                     const float *__restrict__ inv_scale, const float *__restrict__ ccol,
-                    int64_t n, int nrb, int ntiles, int kp, int c0, int kpw,
+                    int64_t n, int nrb, int ntiles, int kp, int c0, int kpw, int tri,
                     float *__restrict__ W, int64_t ldw, int *__restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   const uint32_t raw = su32(smem_raw);
@@ -256,13 +270,13 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
       int st = 0;
       uint32_t ph = 0;
       bool ok = true;
-      for (int rb = blockIdx.x, r = 0; ok && rb < nrb; rb += G, ++r) {
+      for (int r = 0, rb = row_block(0, G, tri); ok && rb < nrb; rb = row_block(++r, G, tri)) {
         if (r > 0 && !mbar_wait(b_xaempty, (r - 1) & 1, abort)) break;
         mbar_expect_tx(b_xafull, kXaBytes);
 #pragma unroll
         for (int kc = 0; kc < KG / 64; ++kc)   // one 128-byte-wide chunk of K per box
           tma_load_2d(&map_xa, b_xafull, base + L.xa() + kc * (kBM * 128), kc * 64, rb * kBM);
-        for (int t = 0; t < ntiles; ++t) {
+        for (int t = first_tile(rb, tri); t < ntiles; ++t) {
           if (!mbar_wait(b_xbempty + 8 * st, ph ^ 1, abort)) { ok = false; break; }
           mbar_expect_tx(b_xbfull + 8 * st, kXbBytes);
 #pragma unroll
@@ -283,8 +297,8 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
       int st = 0;
       uint32_t ph = 0;
       bool ok = true;
-      for (int rb = blockIdx.x; ok && rb < nrb; rb += G) {
-        for (int t = 0; ok && t < ntiles; ++t) {
+      for (int r = 0, rb = row_block(0, G, tri); ok && rb < nrb; rb = row_block(++r, G, tri)) {
+        for (int t = first_tile(rb, tri); ok && t < ntiles; ++t) {
 #pragma unroll
           for (int part = 0; part < kParts; ++part) {
             if (!mbar_wait(b_atempty + 8 * st, ph ^ 1, abort)) { ok = false; break; }
@@ -305,9 +319,9 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
       int st = 0, b = 0;
       uint32_t sph = 0, bph = 0;  // ring / buffer phase parities
       bool ok = true;
-      for (int rb = blockIdx.x, r = 0; ok && rb < nrb; rb += G, ++r) {
+      for (int r = 0, rb = row_block(0, G, tri); ok && rb < nrb; rb = row_block(++r, G, tri)) {
         if (!mbar_wait(b_xafull, r & 1, abort)) break;
-        for (int t = 0; t < ntiles; ++t) {
+        for (int t = first_tile(rb, tri); t < ntiles; ++t) {
           if (!mbar_wait(b_xbfull + 8 * st, sph, abort) ||
               !mbar_wait(b_free + 8 * b, bph ^ 1, abort)) {
             ok = false;
@@ -338,10 +352,11 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
       int st = 0, b = 0;
       uint32_t sph = 0, bph = 0;
       bool ok = true;
-      for (int rb = blockIdx.x, r = 0; ok && rb < nrb; rb += G, ++r) {
+      for (int r = 0, rb = row_block(0, G, tri); ok && rb < nrb; rb = row_block(++r, G, tri)) {
         if (r > 0 && !mbar_wait(b_wempty, (r - 1) & 1, abort)) break;
         tc_fence_after();
-        for (int t = 0; t < ntiles; ++t) {
+        const int tb0 = first_tile(rb, tri);
+        for (int t = tb0; t < ntiles; ++t) {
           // SPLIT == kSplitA: the J block's AT_lo sits in the ring slot after its AT_hi
           const int st2 = st + 1 == kAtStages ? 0 : st + 1;
           const uint32_t sph2 = st + 1 == kAtStages ? sph ^ 1 : sph;
@@ -356,7 +371,7 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
           const uint32_t ap = tmem + b * kBJ;
 #pragma unroll
           for (int kk = 0; kk < kBJ / 16; ++kk)
-            umma_ts(t_w, ap + kk * 8, dat + 2 * kk, id2, (t > 0 || kk > 0) ? 1u : 0u);
+            umma_ts(t_w, ap + kk * 8, dat + 2 * kk, id2, (t > tb0 || kk > 0) ? 1u : 0u);
           if constexpr (split_p(SPLIT)) {
 #pragma unroll
             for (int kk = 0; kk < kBJ / 16; ++kk)   // P_lo over the buffer's columns 32..63
@@ -392,11 +407,13 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
     // of 1.33 GHz under the power cap (the same cycles per tile, more energy per cycle).
     const float shift = SHIFT ? inv_scale[1] : 0.f;
     bool ok = true;
-    for (int rb = blockIdx.x, r = 0; ok && rb < nrb; rb += G, ++r) {
-      const uint32_t T0 = (uint32_t)r * (uint32_t)ntiles;   // flat index of the first J block
-      for (uint32_t T = T0 + ((T0 & 1u) != (uint32_t)g ? 1u : 0u); T < T0 + (uint32_t)ntiles;
-           T += 2) {
+    uint32_t T0 = 0;   // flat index (over this CTA's row blocks) of the row block's first J block
+    for (int r = 0, rb = row_block(0, G, tri); ok && rb < nrb; rb = row_block(++r, G, tri)) {
+      const int tb0 = first_tile(rb, tri);
+      const uint32_t cnt = (uint32_t)(ntiles - tb0);
+      for (uint32_t T = T0 + ((T0 & 1u) != (uint32_t)g ? 1u : 0u); T < T0 + cnt; T += 2) {
         const uint32_t b = T & (kSBufs - 1);
+        const int t = tb0 + (int)(T - T0);
         if (!mbar_wait(b_sfull + 8 * b, (T / kSBufs) & 1u, abort)) { ok = false; break; }
         tc_fence_after();
         const uint32_t tb = tmem + b * kBJ + lane_off;
@@ -412,7 +429,31 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
           if constexpr (DERIV) return x * exp2_mixed<NPOLY>(x, e);
           else return exp2_mixed<NPOLY>(x, e) - shift;
         };
-        if constexpr (split_p(SPLIT)) {
+        if (tri && t < tb0 + kBM / kBJ) {
+          // a tile across the diagonal of the half-product: entry (i, j) weighs 1 for j > i, 1/2
+          // for j == i and 0 for j < i (dj = j - i of the tile's column 0)
+          const int dj = t * kBJ - (rb * kBM + row);
+          float f[2 * 32];
+#pragma unroll
+          for (int e = 0; e < 32; ++e) {
+            f[e] = pv(s0[e], e);
+            f[32 + e] = pv(s1[e], e);
+          }
+#pragma unroll
+          for (int e = 0; e < 64; ++e) {
+            const int dd = dj + e;
+            f[e] = dd > 0 ? f[e] : dd == 0 ? 0.5f * f[e] : 0.f;
+          }
+          if constexpr (split_p(SPLIT)) {
+            uint32_t pl[32];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) split2<BF16>(f[2 * c], f[2 * c + 1], pk[c], pl[c]);
+            tmem_st32(tb + kBJ / 2, pl);
+          } else {
+#pragma unroll
+            for (int c = 0; c < 32; ++c) pk[c] = pack2<BF16>(f[2 * c], f[2 * c + 1]);
+          }
+        } else if constexpr (split_p(SPLIT)) {
           uint32_t pl[32];
 #pragma unroll
           for (int c = 0; c < 16; ++c)
@@ -447,6 +488,7 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
         tc_fence_before();
         mbar_arrive(b_pfull + 8 * b);
       }
+      T0 += cnt;
       // epilogue: W rows of this block, half of the slab per warpgroup
       if (!ok || !mbar_wait(b_wfull, r & 1, abort)) break;
       tc_fence_after();
@@ -462,7 +504,7 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
           const float4 *cs = reinterpret_cast<const float4 *>(ccol + c0 + cc);
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
-            const float4 a = SHIFT ? cs[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 a = SHIFT && !tri ? cs[j] : make_float4(0.f, 0.f, 0.f, 0.f);
             dst[j] = make_float4((__uint_as_float(v[4 * j]) + a.x) * sc,
                                  (__uint_as_float(v[4 * j + 1]) + a.y) * sc,
                                  (__uint_as_float(v[4 * j + 2]) + a.z) * sc,
@@ -717,12 +759,24 @@ __global__ void column_shift(const double *__restrict__ cpart, int nparts, int k
   ccol[c] = (float)((double)scale[2] * t);
 }
 
+// For the half product: out[0] = the kernel-mean shift, out[1 + c] = sum_j y_j A[j][c] over the
+// operand as the tensor cores see it (hi + lo), for the shift's rank-one term of A^T K A.
+__global__ void sym_shift_terms(const double *__restrict__ cpart, int nparts, int kp,
+                                const float *__restrict__ scale, double *__restrict__ out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c == 0) out[0] = (double)scale[2];
+  if (c >= kp) return;
+  double t = 0.0;
+  for (int x = 0; x < nparts; ++x) t += cpart[(int64_t)x * kp + c];
+  out[1 + c] = t * (double)scale[1];   // 1/s, a power of two
+}
+
 // ---------------------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------------------
 using TcKernel = void (*)(const CUtensorMap, const CUtensorMap, const CUtensorMap,
                           const CUtensorMap, const float *, const float *, const float *, int64_t,
-                          int, int, int, int, int, float *, int64_t, int *);
+                          int, int, int, int, int, int, float *, int64_t, int *);
 
 // Exps per 8 columns evaluated by the FMA-pipe polynomial (the rest on MUFU); tunable through
 // TSVM_TC_POLY (0, 2, 4, 6 or 8) for the autotuning sweep in the benchmarks.
@@ -809,17 +863,27 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
                            kp, W, precision, kernel_ms, round_back, split, false);
 }
 
+tsvm_status kermatmul_tc_half(tsvm_context *ctx, const float *Xc, const float *y, int64_t n, int d,
+                              double gamma, const float *A, int kp, float *R, int precision,
+                              float *kernel_ms, float *round_back, int split, double *sym) {
+  if (split < kSplitNone || split > kSplitA || sym == nullptr) return TSVM_ERR_INVALID_ARGUMENT;
+  return kermatmul_tc_core(ctx, Xc, y, n, Xc, y, n, d, gamma, A, kp, R, precision, kernel_ms,
+                           round_back, split, false, sym);
+}
+
 // The general form: W (ni x kp) = Y_I K(X_I, X_J) Y_J A with the I rows XI (ni x d, labels yI) and
 // the J rows XJ (nj x d, labels yJ; A is nj x kp), both centred by the same vector; a null label
 // vector means all ones.  XI may be XJ itself.
 tsvm_status kermatmul_tc_core(tsvm_context *ctx, const float *XI, const float *yI, int64_t ni,
                               const float *XJ, const float *yJ, int64_t nj, int d, double gamma,
                               const float *A, int kp, float *W, int precision, float *kernel_ms,
-                              float *round_back, int split, bool deriv) {
+                              float *round_back, int split, bool deriv, double *sym) {
   if (!kermatmul_tc_supported(d, kp)) return TSVM_ERR_UNSUPPORTED;
   if (split < kSplitNone || split > kSplitPA || ni < 1 || nj < 1) return TSVM_ERR_INVALID_ARGUMENT;
   if (deriv && split != kSplitPA) return TSVM_ERR_UNSUPPORTED;
   const bool same = XI == XJ && ni == nj;
+  const int tri = sym != nullptr ? 1 : 0;
+  if (tri && (!same || yI != yJ)) return TSVM_ERR_INVALID_ARGUMENT;
   const bool bf16 = precision_is_bf16(precision);
   const int64_t n_pad = round_up(nj, kBM);         // J side (XB, AT)
   const int64_t nr_pad = round_up(ni, kBM);        // I side (XA, W)
@@ -886,6 +950,10 @@ tsvm_status kermatmul_tc_core(tsvm_context *ctx, const float *XI, const float *y
   TSVM_LAUNCHED(ctx);
   column_shift<<<(unsigned)ceil_div(kp, 256), 256, 0, ctx->stream>>>(cpart, rg, kp, scale, ccol);
   TSVM_LAUNCHED(ctx);
+  if (tri) {
+    sym_shift_terms<<<(unsigned)ceil_div(kp, 256), 256, 0, ctx->stream>>>(cpart, rg, kp, scale, sym);
+    TSVM_LAUNCHED(ctx);
+  }
   TSVM_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
 
   CUtensorMap mxa, mxb;
@@ -910,7 +978,7 @@ tsvm_status kermatmul_tc_core(tsvm_context *ctx, const float *XI, const float *y
     if (!kern) return TSVM_ERR_UNSUPPORTED;
     TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<grid, kThreadsTC, smem, ctx->stream>>>(mxa, mxb, mat, matlo, yI, scale + 1, ccol, ni,
-                                                  nrb, ntiles, kp, c0, kpw, W, kp, err);
+                                                  nrb, ntiles, kp, c0, kpw, tri, W, kp, err);
     TSVM_LAUNCHED(ctx);
   }
   TSVM_CUDA(cudaEventRecord(e1, ctx->stream));

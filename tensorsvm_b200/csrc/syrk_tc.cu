@@ -457,29 +457,54 @@ syrk_fused_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, in
   }
 }
 
-// M[R][C] = M[C][R] = (R == C) + G64[R][C] + sum_g part[g][r][c] (FP64, CTA order) for the
-// window entries r >= c, R = cols[r], C = cols[c] (identity when cols is null), k the full width,
-// wl the window's.  With a window plan only the entries whose group pair this window owns
+// M[R][C] = M[C][R] = (R == C) + G64[R][C] + sum_g part[g][r][c] (FP64) for the window entries
+// r >= c, R = cols[r], C = cols[c] (identity when cols is null), k the full width, wl the
+// window's.  With a window plan only the entries whose group pair this window owns
 // (owner[gid[R] * ng + gid[C]] == win) are written.  A timed-out tensor-core launch (err set)
-// poisons M with NaN.
-__global__ void syrk_reduce(const float *__restrict__ part, int G, int KP, int k, int wl,
-                            const int *__restrict__ cols, const int *__restrict__ gid,
-                            const int *__restrict__ owner, int ng, int win,
-                            const double *__restrict__ G64, const int *__restrict__ err,
-                            double *__restrict__ M) {
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (int64_t)wl * wl) return;
-  const int r = (int)(e / wl), c = (int)(e % wl);
-  if (c > r) return;
+// poisons M with NaN.  A block takes 32 consecutive entries (coalesced rows of the partials);
+// its 8 warps sum the CTA partials g = w, w + 8, ... (four loads in flight per thread), and the
+// eight sums are added in warp order: the same order on every run.
+constexpr int kReduceEntries = 32;
+__global__ void __launch_bounds__(256)
+syrk_reduce(const float *__restrict__ part, int G, int KP, int k, int wl,
+            const int *__restrict__ cols, const int *__restrict__ gid,
+            const int *__restrict__ owner, int ng, int win, const double *__restrict__ G64,
+            const int *__restrict__ err, double *__restrict__ M) {
+  __shared__ double red[8][kReduceEntries + 1];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int64_t e = (int64_t)blockIdx.x * kReduceEntries + tx;
+  const bool valid = e < (int64_t)wl * wl;
+  const int r = valid ? (int)(e / wl) : 0, c = valid ? (int)(e % wl) : 0;
+  const bool want = valid && c <= r;
+  double s = 0.0;
+  if (want) {
+    const float *p = part + (size_t)r * KP + c;
+    const size_t stride = (size_t)KP * KP;
+    int g = ty;
+    for (; g + 24 < G; g += 32) {
+      const float a0 = __ldcs(p + (size_t)g * stride), a1 = __ldcs(p + (size_t)(g + 8) * stride);
+      const float a2 = __ldcs(p + (size_t)(g + 16) * stride);
+      const float a3 = __ldcs(p + (size_t)(g + 24) * stride);
+      s += (double)a0;
+      s += (double)a1;
+      s += (double)a2;
+      s += (double)a3;
+    }
+    for (; g < G; g += 8) s += (double)__ldcs(p + (size_t)g * stride);
+  }
+  red[ty][tx] = s;
+  __syncthreads();
+  if (ty != 0 || !want) return;
   const int R = cols ? cols[r] : r, C = cols ? cols[c] : c;
   if (owner && owner[gid[R] * ng + gid[C]] != win) return;
-  double s = 0.0;
-  for (int g = 0; g < G; ++g) s += (double)part[((size_t)g * KP + r) * KP + c];
-  if (G64) s += G64[(size_t)R * k + C];
-  if (R == C) s += 1.0;
-  if (*err) s = NAN;
-  M[(size_t)R * k + C] = s;
-  M[(size_t)C * k + R] = s;
+  double t = 0.0;
+#pragma unroll
+  for (int w = 0; w < 8; ++w) t += red[w][tx];
+  if (G64) t += G64[(size_t)R * k + C];
+  if (R == C) t += 1.0;
+  if (*err) t = NAN;
+  M[(size_t)R * k + C] = t;
+  M[(size_t)C * k + R] = t;
 }
 
 // Rows with dinv > tau, in index order: per-block counts over contiguous row ranges, then each
@@ -669,7 +694,7 @@ tsvm_status syrk_capacitance_tc(tsvm_context *ctx, const float *Z, int ldz, int6
         KPmax == 128 ? launch_syrk_fused<128>(ctx, Z, ldz, k, n, (int)T, dinv, tau, G, part, err)
                      : launch_syrk_fused<256>(ctx, Z, ldz, k, n, (int)T, dinv, tau, G, part, err);
     if (st != TSVM_OK) return st;
-    syrk_reduce<<<(unsigned)ceil_div((int64_t)k * k, 256), 256, 0, ctx->stream>>>(
+    syrk_reduce<<<(unsigned)ceil_div((int64_t)k * k, kReduceEntries), 256, 0, ctx->stream>>>(
         part, G, KPmax, k, k, nullptr, nullptr, nullptr, plan.ng, 0, G64, err, M);
     TSVM_LAUNCHED(ctx);
     return TSVM_OK;
@@ -705,7 +730,8 @@ tsvm_status syrk_capacitance_tc(tsvm_context *ctx, const float *Z, int ldz, int6
       st = KP == 128 ? launch_syrk_tc<3, 128>(ctx, map, (int)T, G, part, err)
                      : launch_syrk_tc<3, 256>(ctx, map, (int)T, G, part, err);
     if (st != TSVM_OK) return st;
-    syrk_reduce<<<(unsigned)ceil_div((int64_t)wl[w] * wl[w], 256), 256, 0, ctx->stream>>>(
+    syrk_reduce<<<(unsigned)ceil_div((int64_t)wl[w] * wl[w], kReduceEntries), 256, 0,
+                  ctx->stream>>>(
         part, G, KP, k, wl[w], cols, dgid, downer, plan.ng, w, G64, err, M);
     TSVM_LAUNCHED(ctx);
   }

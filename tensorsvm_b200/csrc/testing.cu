@@ -77,6 +77,25 @@ tsvm_status tsvm_test_kermatmul(tsvm_context *ctx, const float *X, const float *
   return TSVM_OK;
 }
 
+tsvm_status tsvm_test_kermatmul_half(tsvm_context *ctx, const float *X, const float *y, int64_t n,
+                                     int32_t d, double gamma, const float *A, int32_t kp,
+                                     float *R, double *sym, int32_t precision, int32_t split) {
+  if (!ctx || !X || !y || !A || !R || !sym || n < 1 || d < 1 || kp < 1)
+    return TSVM_ERR_INVALID_ARGUMENT;
+  if (!precision_valid(precision) || precision == TSVM_PREC_FP32 || split < 0 || split > 2)
+    return TSVM_ERR_INVALID_ARGUMENT;
+  if (!kermatmul_tc_supported(d, kp)) return TSVM_ERR_UNSUPPORTED;
+  float *Xc = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_XC, (size_t)n * d + (size_t)n + 64, &Xc));
+  float *norms = Xc + (size_t)n * d;
+  TSVM_TRY(centre_features(ctx, X, n, d, Xc, norms));
+  float ms = 0.f;
+  TSVM_TRY(kermatmul_tc_half(ctx, Xc, y, n, d, gamma, A, kp, R, precision, &ms, nullptr, split,
+                             sym));
+  TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TSVM_OK;
+}
+
 tsvm_status tsvm_test_chol(tsvm_context *ctx, double *A, int32_t n, int32_t *info_host) {
   if (!ctx || !A || n < 1) return TSVM_ERR_INVALID_ARGUMENT;
   int *info = nullptr;

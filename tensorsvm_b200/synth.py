@@ -100,6 +100,7 @@ CONFIGS = {
     "c1": (two_gaussians, dict(n=8192, d=18, seed=1), 0.01, 32.0, 32),
     "c1_test": (two_gaussians, dict(n=2048, d=18, seed=101), 0.01, 32.0, 32),
     "c2": (two_gaussians, dict(n=1_000_000, d=18, seed=2, noise=0.10), 0.05, 32.0, 256),
+    "c2_test": (two_gaussians, dict(n=20_000, d=18, seed=102, noise=0.10), 0.05, 32.0, 256),
     "c3": (mixed_onehot, dict(n=500_000, seed=3, noise=0.05), 0.02, 32.0, 400),
     "c5": (tanh_teacher, dict(n=200_000, d=28, seed=5), 0.03, 16.0, 256),
     "c5_val": (tanh_teacher, dict(n=50_000, d=28, seed=55), 0.03, 16.0, 256),

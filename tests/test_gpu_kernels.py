@@ -226,11 +226,13 @@ def test_kermatmul_kernel_block_split(ctx, n, d, kp, prec, tol_split, tol_one):
 
 
 @pytest.mark.parametrize("n,kp", [(2048, 64), (3001, 256), (1000, 448)])
-@pytest.mark.parametrize("prec,tol_split", [(_lib.PREC_FP16, 2e-6), (_lib.PREC_BF16, 2e-5)])
+@pytest.mark.parametrize("prec,tol_split", [(_lib.PREC_FP16, 5e-6), (_lib.PREC_BF16, 2e-5)])
 def test_kermatmul_operand_split(ctx, n, kp, prec, tol_split):
     """The operand as hi + lo (the projection pass): on points in well-separated groups of exact
     duplicates the kernel block is exactly 0 or 1, so only the operand's rounding is left, and
-    the split removes it (the one-product form keeps a 16-bit rounding of A)."""
+    the split removes it (the one-product form keeps a 16-bit rounding of A).  What remains is
+    the FP32 accumulation over ~n/8 unit terms per group, ~sqrt(n) 2^-24 relative (measured
+    2.3e-6 at n = 2048 and 3.2e-6 at n = 3001 for FP16, against 1.9e-4 and 2.0e-4 unsplit)."""
     rng = np.random.default_rng(n + 3 * kp)
     d = 18
     # squared distances between centres ~2300 (exp2 of the scaled distance underflows the
