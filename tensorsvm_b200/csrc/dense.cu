@@ -65,7 +65,7 @@ __device__ int diag_block_warp(double *Dg, double *Di, int nb, double *rdiag) {
       if (!(d > 0.0)) {
         bad = c + 1;
       } else {
-        const double sq = sqrt(d), inv = 1.0 / sq;
+        const double inv = rsqrt(d), sq = d * inv;   // one call on the pivot's chain
         const double l = lane > c ? a[c] * inv : (lane == c ? sq : a[c]);
         a[c] = l;
         if (lane == 0) rdiag[c] = inv;
@@ -84,10 +84,11 @@ __device__ int diag_block_warp(double *Dg, double *Di, int nb, double *rdiag) {
   double x[kNB];
 #pragma unroll
   for (int r = 0; r < kNB; ++r) {
-    double t = r == lane ? 1.0 : 0.0;
+    // four independent partial sums: the substitution's chain is then r / 4 FMAs long
+    double t[4] = {r == lane ? 1.0 : 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int m = 0; m < r; ++m) t = fma(-Dg[r * kDP + m], x[m], t);
-    x[r] = (r < nb && lane < nb && r >= lane) ? t * rdiag[r] : 0.0;
+    for (int m = 0; m < r; ++m) t[m & 3] = fma(-Dg[r * kDP + m], x[m], t[m & 3]);
+    x[r] = (r < nb && lane < nb && r >= lane) ? ((t[0] + t[1]) + (t[2] + t[3])) * rdiag[r] : 0.0;
   }
 #pragma unroll
   for (int r = 0; r < kNB; ++r) Di[r * kDP + lane] = x[r];
@@ -214,6 +215,158 @@ __global__ void __launch_bounds__(kCholThreads) chol_kernel(double *__restrict__
   if (tid == 0) *info = fail;
 }
 
+// Trailing update of one 32 x 32 block (ti, tj) (relative to row r0) with the panel PT (nb columns),
+// by one warp, lane = column: A[r][c] -= sum_q L[r][jb + q] L[c][jb + q].  The lane's panel row
+// stays in registers; the block's rows are read four at a time as 16-byte broadcasts.  With Dout
+// (the next diagonal block, its current entries staged in Dout by the caller) the result goes
+// into Dout instead (lower part, zeros elsewhere).
+__device__ __forceinline__ void la_update_block(double *__restrict__ A, int lda, int n,
+                                                const double *__restrict__ PT, int ldp, int nb,
+                                                int r0, int ti, int tj, double *Dout, int lane) {
+  const int gi0 = r0 + ti * kNB, col = r0 + tj * kNB + lane;
+  const bool colok = col < n;
+  double bj[kNB];
+#pragma unroll
+  for (int c = 0; c < kNB; ++c) bj[c] = (c < nb && colok) ? PT[c * ldp + (col - r0)] : 0.0;
+  // the block's current entries: from Dout (staged there by the caller) or from A, loaded one
+  // 4-row step ahead so that the L2 round trip overlaps the step before
+  auto load4 = [&](int i0, double *a) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int row = gi0 + i0 + u;
+      a[u] = Dout ? Dout[(i0 + u) * kDP + lane]
+                  : ((row < n && colok) ? A[(int64_t)row * lda + col] : 0.0);
+    }
+  };
+  double an[4];
+  load4(0, an);
+#pragma unroll 1
+  for (int i0 = 0; i0 < kNB; i0 += 4) {
+    double a[4], acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int u = 0; u < 4; ++u) a[u] = an[u];
+    if (i0 + 4 < kNB) load4(i0 + 4, an);
+    const double *pr = PT + (gi0 - r0) + i0;
+#pragma unroll
+    for (int c = 0; c < kNB; ++c) {
+      if (c < nb) {
+        const double2 v0 = *reinterpret_cast<const double2 *>(pr + c * ldp);
+        const double2 v1 = *reinterpret_cast<const double2 *>(pr + c * ldp + 2);
+        acc[0] = fma(v0.x, bj[c], acc[0]);
+        acc[1] = fma(v0.y, bj[c], acc[1]);
+        acc[2] = fma(v1.x, bj[c], acc[2]);
+        acc[3] = fma(v1.y, bj[c], acc[3]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int r = i0 + u, row = gi0 + r;
+      const bool in = row < n && colok && (ti != tj || lane <= r);
+      if (Dout) Dout[r * kDP + lane] = in ? a[u] - acc[u] : 0.0;
+      else if (in) A[(int64_t)row * lda + col] = a[u] - acc[u];
+    }
+  }
+}
+
+// Right-looking blocked Cholesky in one CTA with a one-panel lookahead, 32-column panels.  Step j:
+//  (1) warps 1..: the panel below diagonal block j, L_ij = A_ij Di_j^T (Di_j formed in the step
+//      before), into A and, transposed, into shared memory (four rows per warp at a time), while
+//      warp 0 loads the next diagonal block;
+//  (2) warp 0 updates the next diagonal block with the panel, factors it and forms its inverse
+//      (diag_block_warp) while the other warps update the rest of the trailing lower triangle,
+//      one 32 x 32 block per warp at a time (la_update_block).
+// So the chain of diagonal factorisations runs beside the trailing updates instead of between
+// them.  Three barriers a step.
+constexpr int kCholLAThreads = 512;
+constexpr int kCholLAWarps = kCholLAThreads / 32;
+__global__ void __launch_bounds__(kCholLAThreads, 1)
+chol_la_kernel(double *__restrict__ A, int n, int lda, double *__restrict__ Dinv,
+               int *__restrict__ info) {
+  extern __shared__ __align__(16) double PTs[];   // [kNB][ldp] (+ slack): PT[c][i] = L[r0 + i][jb + c]
+  __shared__ double Dg[kNB * kDP], Di[kNB * kDP];
+  __shared__ double rdiag[kNB];
+  __shared__ int fail;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ldp = ((n > kNB ? n - kNB : 1) + 1) & ~1;   // even: rows of 16-byte pairs
+  const int nblk = (n + kNB - 1) / kNB;
+  if (tid == 0) fail = 0;
+  {
+    const int nb = min(kNB, n);
+    for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+      const int r = e >> 5, c = e & 31;
+      Dg[r * kDP + c] = (r < nb && c <= r) ? A[(int64_t)r * lda + c] : 0.0;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      const int bad = diag_block_warp(Dg, Di, nb, rdiag);
+      if (lane == 0 && bad) fail = bad;
+    }
+    __syncthreads();
+  }
+  for (int j = 0; j < nblk; ++j) {
+    if (fail) break;
+    const int jb = j * kNB, nb = min(kNB, n - jb), r0 = jb + nb, m = n - r0;
+    {
+      double *Dblk = Dinv + (int64_t)j * kNB * kNB;
+      for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+        const int r = e >> 5, c = e & 31;
+        Dblk[e] = Di[r * kDP + c];
+        if (r < nb && c <= r) A[(int64_t)(jb + r) * lda + jb + c] = Dg[r * kDP + c];
+      }
+    }
+    if (m <= 0) break;
+    __syncthreads();   // Dg has been read: warp 0 stages the next diagonal block there
+    if (warp == 0) {
+      // the next diagonal block's entries (lane = column), loaded while the panel is formed
+#pragma unroll
+      for (int r = 0; r < kNB; ++r)
+        Dg[r * kDP + lane] =
+            (r < m && lane < m && lane <= r) ? A[(int64_t)(r0 + r) * lda + r0 + lane] : 0.0;
+    }
+    // (1) L[r0 + i][jb + c] = sum_{q <= c} A[r0 + i][jb + q] Di[c][q], warps 1..
+    for (int i0 = 4 * (warp - 1); warp > 0 && i0 < m; i0 += 4 * (kCholLAWarps - 1)) {
+      double a4[4], v4[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + u;
+        a4[u] = (lane < nb && i < m) ? A[(int64_t)(r0 + i) * lda + jb + lane] : 0.0;
+        v4[u] = 0.0;
+      }
+#pragma unroll 8
+      for (int q = 0; q < kNB; ++q) {
+        const double dq = q <= lane ? Di[lane * kDP + q] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v4[u] = fma(__shfl_sync(0xffffffffu, a4[u], q), dq, v4[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + u;
+        if (lane < nb && i < m) {
+          PTs[lane * ldp + i] = v4[u];
+          A[(int64_t)(r0 + i) * lda + jb + lane] = v4[u];
+        }
+      }
+    }
+    __syncthreads();
+    // (2) the next diagonal block (warp 0) beside the rest of the trailing update
+    const int nt = (m + kNB - 1) / kNB, ntot = nt * (nt + 1) / 2;
+    if (warp == 0) {
+      la_update_block(A, lda, n, PTs, ldp, nb, r0, 0, 0, Dg, lane);
+      __syncwarp();
+      const int bad = diag_block_warp(Dg, Di, min(kNB, m), rdiag);
+      if (lane == 0 && bad) fail = r0 + bad;
+    } else {
+      for (int b = warp; b < ntot; b += kCholLAWarps - 1) {
+        int ti = 0;
+        while ((ti + 1) * (ti + 2) / 2 <= b) ++ti;
+        la_update_block(A, lda, n, PTs, ldp, nb, r0, ti, b - ti * (ti + 1) / 2, nullptr, lane);
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0) *info = fail;
+}
+
 // Dinv blocks of an existing lower factor L: one CTA per 32 x 32 diagonal block.
 __global__ void __launch_bounds__(1024) diag_inverse_kernel(const double *__restrict__ L, int n,
                                                             int lda, double *__restrict__ Dinv) {
@@ -269,16 +422,23 @@ __global__ void __launch_bounds__(1024) potrs_kernel(const double *__restrict__ 
       }
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const double v = warp_sum(s[q]);
-        if (lane == 0 && q < nrhs) t[q][warp] = y[q * n + jb + warp] - v;
+        if (q < nrhs) {   // uniform over the warp
+          const double v = warp_sum(s[q]);
+          if (lane == 0) t[q][warp] = y[q * n + jb + warp] - v;
+        }
       }
     }
     __syncthreads();
     if (tid < nrhs * nb) {
+      // the 32-term product with the inverted diagonal block, unrolled into four independent
+      // chains (the loads issue together; a serial chain of shared-memory loads and FMAs was
+      // the longest step of each block)
       const int q = tid / nb, r = tid % nb;
-      double v = 0.0;
-      for (int c = 0; c <= r; ++c) v = fma(Ds[r * kDP + c], t[q][c], v);
-      y[q * n + jb + r] = v;
+      double v[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int c = 0; c < kNB; ++c)
+        if (c <= r) v[c & 3] = fma(Ds[r * kDP + c], t[q][c], v[c & 3]);
+      y[q * n + jb + r] = (v[0] + v[1]) + (v[2] + v[3]);
     }
     __syncthreads();
   }
@@ -303,16 +463,19 @@ __global__ void __launch_bounds__(1024) potrs_kernel(const double *__restrict__ 
     __syncthreads();
     if (tid < nrhs * nb) {
       const int q = tid / nb, r = tid % nb;
-      double v = 0.0;
-      for (int w = 0; w < 32; ++w) v += part[(w * 4 + q) * kNB + r];
-      t[q][r] = y[q * n + jb + r] - v;
+      double v[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int w = 0; w < 32; ++w) v[w & 3] += part[(w * 4 + q) * kNB + r];
+      t[q][r] = y[q * n + jb + r] - ((v[0] + v[1]) + (v[2] + v[3]));
     }
     __syncthreads();
     if (tid < nrhs * nb) {
       const int q = tid / nb, r = tid % nb;
-      double v = 0.0;
-      for (int c = r; c < nb; ++c) v = fma(Ds[c * kDP + r], t[q][c], v);
-      y[q * n + jb + r] = v;
+      double v[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int c = 0; c < kNB; ++c)
+        if (c >= r && c < nb) v[c & 3] = fma(Ds[c * kDP + r], t[q][c], v[c & 3]);
+      y[q * n + jb + r] = (v[0] + v[1]) + (v[2] + v[3]);
     }
     __syncthreads();
   }
@@ -651,10 +814,13 @@ __global__ void eig_pack_out(const double *__restrict__ A0, const double *__rest
 
 tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_dev, double *Dinv) {
   if (n < 1 || n > kMaxDense) return TSVM_ERR_UNSUPPORTED;  // panel must fit shared memory
-  const size_t smem = sizeof(double) * (size_t)kNB * (size_t)(n > kNB ? n - kNB : 1);
-  TSVM_CUDA(cudaFuncSetAttribute(chol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  // the panel rows padded to an even length, plus the slack the 4-row reads of a ragged last
+  // block run into
+  const size_t ldp = ((size_t)(n > kNB ? n - kNB : 1) + 1) & ~(size_t)1;
+  const size_t smem = sizeof(double) * ((size_t)kNB * ldp + 64);
+  TSVM_CUDA(cudaFuncSetAttribute(chol_la_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
-  chol_kernel<<<1, kCholThreads, smem, ctx->stream>>>(A, n, lda, Dinv, info_dev, 0, 0, nullptr);
+  chol_la_kernel<<<1, kCholLAThreads, smem, ctx->stream>>>(A, n, lda, Dinv, info_dev);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;
 }

@@ -41,6 +41,7 @@ using namespace tc;
 constexpr int kSJ = 64;              // rows of Z per chunk (MMA K of one chunk, 4 x 16)
 constexpr int kSyrkMaxK = 425;       // widest capacitance matrix the windows cover
 constexpr int kSyrkThreads = 192;
+constexpr int kSyrkFusedThreads = 320;   // producer, MMA issuer, 8 converter warps
 
 template <int WAYS, int KP>
 struct SyrkCfg {
@@ -242,7 +243,8 @@ syrk_tc_kernel(const __grid_constant__ CUtensorMap map, int T, float *__restrict
 // goes through HBM (syrk_prep + syrk_tc_kernel read Z, write the BF16 parts and read them back).
 //   warp 0      bulk copies of 32-row half-chunks of Z into a 3-slot FP32 ring
 //   warp 1      TMEM owner and MMA issuer (as syrk_tc_kernel), 2 operand stages of 64 rows
-//   warps 2-5   converters (warp w handles the 8-row groups w - 2 of each half-chunk), then
+//   warps 2-9   converters (warp w handles 8-row group (w - 2) % 4 of half-chunk (w - 2) / 4
+//               of every chunk; four converter warps could not keep the tensor pipe busy), then
 //               the epilogue (TMEM -> per-CTA FP32 partials)
 // Element (c, j) of a part tile (Z column c, row j of the 64-row chunk) sits at byte
 // c * 128 + ((j / 8) ^ (c % 8)) * 16 + (j % 8) * 2: the layout the 128-byte-swizzle TMA load of
@@ -263,7 +265,7 @@ struct FusedCfg {
 };
 
 template <int KP>
-__global__ void __launch_bounds__(kSyrkThreads, 1)
+__global__ void __launch_bounds__(kSyrkFusedThreads, 1)
 syrk_fused_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, int T,
                   const double *__restrict__ dinv, double tau, float *__restrict__ part,
                   int *__restrict__ err) {
@@ -292,7 +294,7 @@ syrk_fused_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, in
       mbar_init(b_hempty + 8 * s, 4);
     }
     for (int s = 0; s < Cfg::kParts; ++s) {
-      mbar_init(b_pfull + 8 * s, 4);
+      mbar_init(b_pfull + 8 * s, 8);
       mbar_init(b_pempty + 8 * s, 1);
     }
     mbar_init(b_done, 1);
@@ -363,23 +365,33 @@ syrk_fused_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, in
       if (ok) umma_commit(b_done);
     }
   } else {
-    // converters: warp g = warp - 2 takes rows 8 g .. 8 g + 7 of each half-chunk, lane = column
-    // within each 32-column block
-    const int g = warp - 2;
-    int hs = 0, ps = 0;
-    uint32_t hph = 0, pph = 0;
+    // converters: warp cw = warp - 2 takes rows 8 g .. 8 g + 7 (g = cw % 4) of half h = cw / 4 of
+    // every chunk, lane = column within each 32-column block
+    const int cw = warp - 2, g = cw & 3, h = cw >> 2;
+    int ps = 0;
+    uint32_t pph = 0;
     bool ok = true;
+    // lane l < 8 holds dinv of row l of this warp's 8-row group in chunk tt, loaded one chunk
+    // ahead so that the load is off the conversion's path
+    auto fetch = [&](int tt) -> double {
+      const int64_t row = (int64_t)tt * kSJ + h * Cfg::kHalfRows + 8 * g + lane;
+      return (lane < 8 && tt < t1 && row < n) ? dinv[row] : 0.0;
+    };
+    double dv_next = fetch(t0);
     for (int t = t0; ok && t < t1; ++t) {
+      const double dv = dv_next;
+      dv_next = fetch(t + 1);
       if (!mbar_wait(b_pempty + 8 * ps, pph ^ 1, abort)) { ok = false; break; }
       uint8_t *tile = sbase + ps * Cfg::kPartStage;
-      for (int h = 0; h < 2; ++h) {
+      {
+        // this half-chunk's slot of the 3-slot ring (half-chunks in the order (t, 0), (t, 1), ...)
+        const int hidx = 2 * (t - t0) + h;
+        const int hs = hidx % Cfg::kHalves;
+        const uint32_t hph = (uint32_t)((hidx / Cfg::kHalves) & 1);
         if (!mbar_wait(b_hfull + 8 * hs, hph, abort)) { ok = false; break; }
         const int64_t r0 = (int64_t)t * kSJ + h * Cfg::kHalfRows + 8 * g;   // this warp's rows
         float wr = 0.f;   // lane l < 8: the weight of row r0 + l (0 for exact rows and padding)
-        if (lane < 8 && r0 + lane < n) {
-          const double dv = dinv[r0 + lane];
-          if (dv <= tau) wr = (float)sqrt(dv);
-        }
+        if (lane < 8 && r0 + lane < n && dv <= tau) wr = (float)sqrt(dv);
         float wj[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) wj[q] = __shfl_sync(0xffffffffu, wr, q);
@@ -409,16 +421,15 @@ syrk_fused_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, in
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(b_hempty + 8 * hs);
-        if (++hs == Cfg::kHalves) { hs = 0; hph ^= 1; }
       }
-      if (!ok) break;
       // the generic-proxy stores must be visible to the tensor cores' async-proxy reads
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(b_pfull + 8 * ps);
       if (++ps == Cfg::kParts) { ps = 0; pph ^= 1; }
     }
-    // epilogue (lane quarter q = warp % 4)
+    // epilogue (lane quarter q = warp % 4; the two warps of a quarter take alternate 32-column
+    // blocks)
     const int q = warp & 3;
     const uint32_t lane_off = (uint32_t)(q * 32) << 16;
     const bool have = t1 > t0;
@@ -429,7 +440,7 @@ syrk_fused_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, in
       for (int mb = 0; mb < Cfg::kSegs; ++mb) {
         const int r = mb * 128 + q * 32 + lane;
         const uint32_t tcol = tmem + (mb == 0 ? 0u : 128u);
-        for (int c0 = 0; c0 < (mb + 1) * 128; c0 += 32) {
+        for (int c0 = 32 * h; c0 < (mb + 1) * 128; c0 += 64) {
           uint32_t v[32];
           if (have) {
             tmem_ld32(tcol + c0 + lane_off, v);
@@ -617,7 +628,7 @@ tsvm_status launch_syrk_fused(tsvm_context *ctx, const float *Z, int64_t ldz, in
   auto kern = syrk_fused_kernel<KP>;
   TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)Cfg::kSmem));
-  kern<<<G, kSyrkThreads, Cfg::kSmem, ctx->stream>>>(Z, ldz, k, n, T, dinv, tau, part, err);
+  kern<<<G, kSyrkFusedThreads, Cfg::kSmem, ctx->stream>>>(Z, ldz, k, n, T, dinv, tau, part, err);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;
 }

@@ -42,7 +42,7 @@ def test_sketch_matches_reference_stream(ctx, n, k):
     assert np.mean(ulp != 0) < 5e-3
 
 
-@pytest.mark.parametrize("k", [1, 32, 33, 50, 97, 256, 400])
+@pytest.mark.parametrize("k", [1, 32, 33, 50, 64, 97, 129, 256, 400, 864])
 def test_cholesky_and_solve(ctx, k):
     rng = np.random.default_rng(k)
     A = rng.standard_normal((k, k + 5))
