@@ -142,15 +142,20 @@ def barrier(world):
 # our arm
 # ------------------------------------------------------------------------------------------
 
-# DRAM bytes (read + write) per 128 x 64 tile of the tensor-core kernel-block product at k = 256,
-# from one ncu capture at n = 262144 (2.390 GB read + 0.259 GB written, 2048 x 4096 tiles): the
-# J-side operands are re-read once per round of 148 row blocks, so traffic grows with the tiles.
-TC_BYTES_PER_TILE = (2.390065e9 + 0.259050e9) / (2048 * 4096)
+# DRAM bytes (read + write) per 128 x 64 tile of the two tensor-core kernel-block launches of
+# the split form at k = 256, from one ncu capture at n = 262144: the range finder (every tile,
+# 2.747 GB read + 0.260 GB written over 8,388,608 tiles) and the projection half product (W as
+# hi + lo, 2.186 GB + 0.226 GB over 4,196,352 tiles).  The J-side operands are re-read once per
+# round of 148 row blocks, so traffic grows with the tiles.
+TC_BYTES_PER_TILE = {"range_finder": (2.747472e9 + 0.260303e9) / 8388608,
+                     "projection_half": (2.185915e9 + 0.225879e9) / 4196352}
 
 
-def tc_traffic(n: int) -> float:
-    tiles = -(-n // 128) * -(-n // 64)
-    return round(TC_BYTES_PER_TILE * tiles, -6)
+def tc_traffic(n: int) -> dict:
+    nrb = -(-n // 128)
+    full, half = nrb * 2 * nrb, nrb * (nrb + 1)   # tiles of the full pass and of the half product
+    return {"range_finder": round(TC_BYTES_PER_TILE["range_finder"] * full, -6),
+            "projection_half": round(TC_BYTES_PER_TILE["projection_half"] * half, -6)}
 
 
 def tc_executed(n: int, k: int, d: int, split: bool) -> dict:
@@ -281,6 +286,7 @@ def run_ours(args, world, rank, local):
                                       ("projection_half", "ms_pass2", ex["pass2_tiles"], ex["pass2_flops"])):
             ms = fi[key]
             passes[name] = {"phase_ms": round(ms, 2), "tiles": tiles,
+                            "traffic": tc_traffic(n)[name],
                             "algorithmic_tflops": round(km_flops / (ms / 1e3) / 1e12, 1),
                             "executed_flops": fl,
                             "executed_tflops": round(fl / (ms / 1e3) / 1e12, 1),
@@ -313,10 +319,10 @@ def run_ours(args, world, rank, local):
         "roofline": {"bound": "tensor" if tensor else "fp32-simt", "kernel": "kermatmul (fused kernel-block product)",
                      "achieved": round(achieved, 2), "peak": round(peak, 1), "unit": unit,
                      "frac": round(achieved / peak, 4), "peak_source": f"{pk_kind} {pname}",
-                     "traffic": tc_traffic(n) if tensor else None,
-                     "traffic_source": ("dram__bytes_read.sum + dram__bytes_write.sum of one launch "
-                                        "at n=262144 (2.649 GB over 2048x4096 tiles), scaled by "
-                                        "the tile count" if tensor else None),
+                     "traffic": (round(sum(tc_traffic(n).values()) / 2, -6) if tensor else None),
+                     "traffic_source": ("dram__bytes_read.sum + dram__bytes_write.sum per launch "
+                                        "(mean of the two launches), from one ncu capture at "
+                                        "n=262144 scaled by the tile count" if tensor else None),
                      "flops_per_launch": km_flops, "ms_per_launch": round(km_ms, 3),
                      "passes": passes},
         "e2e": {"value": round(e2e_s, 4), "unit": "s",
@@ -536,8 +542,10 @@ def run_grid(args, ctx, stream):
     (alphas, bstats, info) = api.ipm_batched(ctx, Zs, ys, k, Cs, rel_gap_tol=1e-6)
     seq_stats, t_seq_ipm = _timed(stream, lambda: sequential(Zs, _lib.PREC_BF16))
     del Zs
-    Z32, t_fac32 = _timed(stream, lambda: factors("fp32"))
-    st32, t_ipm32 = _timed(stream, lambda: sequential(Z32, _lib.PREC_FP32))
+    t_fac32 = t_ipm32 = None
+    if args.fp32_form:
+        Z32, t_fac32 = _timed(stream, lambda: factors("fp32"))
+        st32, t_ipm32 = _timed(stream, lambda: sequential(Z32, _lib.PREC_FP32))
     sec = statistics.mean(times)
     line = _base_line(args, "s for a 64-problem (C, gamma) grid: factors + batched IPM to rel. gap 1e-6",
                       sec, {"workload": "tanh_teacher_grid", "problems": 64, "rows_total": rows,
@@ -554,7 +562,8 @@ def run_grid(args, ctx, stream):
                      "graph_used": info["graph_used"], "iters_max": info["iters_max"]},
         "sequential_same_factors": {"ipm_s": round(t_seq_ipm, 3), "total_s": round(t_fac + t_seq_ipm, 3),
                                     "speedup_batched_ipm": round(t_seq_ipm / statistics.mean(ipm_times), 2)},
-        "plain_fp32_sequential": {"factors_s": round(t_fac32, 3), "ipm_s": round(t_ipm32, 3),
+        "plain_fp32_sequential": None if t_fac32 is None else
+                                 {"factors_s": round(t_fac32, 3), "ipm_s": round(t_ipm32, 3),
                                   "total_s": round(t_fac32 + t_ipm32, 3),
                                   "speedup": round((t_fac32 + t_ipm32) / sec, 2)},
         "iters": {"batched": [s["iters"] for s in bstats], "sequential": [s["iters"] for s in seq_stats]},

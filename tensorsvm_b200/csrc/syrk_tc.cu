@@ -241,10 +241,10 @@ syrk_tc_kernel(const __grid_constant__ CUtensorMap map, int T, float *__restrict
 // bulk copies and are scaled by sqrt(dinv), split into BF16 hi + lo and written into the
 // swizzled K-major operand tiles by the converter warps inside the kernel, so the operand never
 // goes through HBM (syrk_prep + syrk_tc_kernel read Z, write the BF16 parts and read them back).
-//   warp 0      bulk copies of 32-row half-chunks of Z into a 3-slot FP32 ring
+//   warp 0      bulk copies of 16-row sub-chunks of Z into a 6-slot FP32 ring
 //   warp 1      TMEM owner and MMA issuer (as syrk_tc_kernel), 2 operand stages of 64 rows
-//   warps 2-9   converters (warp w handles 8-row group (w - 2) % 4 of half-chunk (w - 2) / 4
-//               of every chunk; four converter warps could not keep the tensor pipe busy), then
+//   warps 2-9   converters (warp w handles 8-row group (w - 2) % 2 of sub-chunk (w - 2) / 2 of
+//               every chunk; four converter warps could not keep the tensor pipe busy), then
 //               the epilogue (TMEM -> per-CTA FP32 partials)
 // Element (c, j) of a part tile (Z column c, row j of the 64-row chunk) sits at byte
 // c * 128 + ((j / 8) ^ (c % 8)) * 16 + (j % 8) * 2: the layout the 128-byte-swizzle TMA load of
@@ -254,9 +254,13 @@ struct FusedCfg {
   static constexpr uint32_t kTile = KP * kSJ * 2;           // one BF16 part tile
   static constexpr uint32_t kPartStage = 2 * kTile;         // hi + lo
   static constexpr int kParts = 2;
-  static constexpr uint32_t kHalfRows = 32;
-  static constexpr uint32_t kHalf = kHalfRows * KP * 4;     // FP32 half-chunk (ldz <= KP)
-  static constexpr int kHalves = 3;
+  // FP32 sub-chunks of 16 rows in a 6-slot ring: finer slots than half-chunks keep more of the
+  // ring's 96 KB in flight (a slot is held while it is converted)
+  static constexpr uint32_t kHalfRows = 16;
+  static constexpr uint32_t kHalf = kHalfRows * KP * 4;     // FP32 sub-chunk (ldz <= KP)
+  static constexpr int kHalves = 6;
+  static constexpr int kSubs = kSJ / kHalfRows;             // sub-chunks per 64-row chunk
+  static constexpr int kSubWarps = kHalfRows / 8;           // converter warps per sub-chunk
   static constexpr int kSegs = KP / 128;
   static constexpr uint32_t kTmemCols = KP == 256 ? 512 : 128;
   static constexpr uint32_t kStaging = kParts * kPartStage;
@@ -291,7 +295,7 @@ syrk_fused_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, in
   if (threadIdx.x == 0) {
     for (int s = 0; s < Cfg::kHalves; ++s) {
       mbar_init(b_hfull + 8 * s, 1);
-      mbar_init(b_hempty + 8 * s, 4);
+      mbar_init(b_hempty + 8 * s, Cfg::kSubWarps);
     }
     for (int s = 0; s < Cfg::kParts; ++s) {
       mbar_init(b_pfull + 8 * s, 8);
@@ -318,7 +322,7 @@ syrk_fused_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, in
       uint32_t ph = 0;
       bool ok = true;
       for (int t = t0; ok && t < t1; ++t) {
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < Cfg::kSubs; ++h) {
           if (!mbar_wait(b_hempty + 8 * s, ph ^ 1, abort)) { ok = false; break; }
           const int64_t r0 = (int64_t)t * kSJ + h * Cfg::kHalfRows;
           const int64_t rows = n - r0 < (int64_t)Cfg::kHalfRows ? n - r0 : Cfg::kHalfRows;
@@ -365,9 +369,9 @@ syrk_fused_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, in
       if (ok) umma_commit(b_done);
     }
   } else {
-    // converters: warp cw = warp - 2 takes rows 8 g .. 8 g + 7 (g = cw % 4) of half h = cw / 4 of
-    // every chunk, lane = column within each 32-column block
-    const int cw = warp - 2, g = cw & 3, h = cw >> 2;
+    // converters: warp cw = warp - 2 takes rows 8 g .. 8 g + 7 (g = cw % 2) of sub-chunk h = cw / 2
+    // of every chunk, lane = column within each 32-column block
+    const int cw = warp - 2, g = cw % Cfg::kSubWarps, h = cw / Cfg::kSubWarps;
     int ps = 0;
     uint32_t pph = 0;
     bool ok = true;
@@ -383,45 +387,43 @@ syrk_fused_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, in
       dv_next = fetch(t + 1);
       if (!mbar_wait(b_pempty + 8 * ps, pph ^ 1, abort)) { ok = false; break; }
       uint8_t *tile = sbase + ps * Cfg::kPartStage;
-      {
-        // this half-chunk's slot of the 3-slot ring (half-chunks in the order (t, 0), (t, 1), ...)
-        const int hidx = 2 * (t - t0) + h;
-        const int hs = hidx % Cfg::kHalves;
-        const uint32_t hph = (uint32_t)((hidx / Cfg::kHalves) & 1);
-        if (!mbar_wait(b_hfull + 8 * hs, hph, abort)) { ok = false; break; }
-        const int64_t r0 = (int64_t)t * kSJ + h * Cfg::kHalfRows + 8 * g;   // this warp's rows
-        float wr = 0.f;   // lane l < 8: the weight of row r0 + l (0 for exact rows and padding)
-        if (lane < 8 && r0 + lane < n && dv <= tau) wr = (float)sqrt(dv);
-        float wj[8];
+      // this sub-chunk's slot of the ring (sub-chunks in the order (t, 0), (t, 1), ...)
+      const int hidx = Cfg::kSubs * (t - t0) + h;
+      const int hs = hidx % Cfg::kHalves;
+      const uint32_t hph = (uint32_t)((hidx / Cfg::kHalves) & 1);
+      if (!mbar_wait(b_hfull + 8 * hs, hph, abort)) { ok = false; break; }
+      const int64_t r0 = (int64_t)t * kSJ + h * Cfg::kHalfRows + 8 * g;   // this warp's rows
+      float wr = 0.f;   // lane l < 8: the weight of row r0 + l (0 for exact rows and padding)
+      if (lane < 8 && r0 + lane < n && dv <= tau) wr = (float)sqrt(dv);
+      float wj[8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) wj[q] = __shfl_sync(0xffffffffu, wr, q);
-        const float *src = staging + (size_t)hs * (Cfg::kHalf / 4) + (size_t)(8 * g) * ldz;
-        const int jg = h * 4 + g;   // 8-row group of the 64-row chunk
+      for (int q = 0; q < 8; ++q) wj[q] = __shfl_sync(0xffffffffu, wr, q);
+      const float *src = staging + (size_t)hs * (Cfg::kHalf / 4) + (size_t)(8 * g) * ldz;
+      const int jg = h * Cfg::kSubWarps + g;   // 8-row group of the 64-row chunk
 #pragma unroll 2
-        for (int cb = 0; cb < KP; cb += 32) {
-          const int c = cb + lane;
-          float v[8];
+      for (int cb = 0; cb < KP; cb += 32) {
+        const int c = cb + lane;
+        float v[8];
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const float x = c < k ? src[(size_t)q * ldz + c] : 0.f;
-            v[q] = wj[q] != 0.f ? x * wj[q] : 0.f;   // select: padding rows may hold anything
-          }
-          uint32_t hi[4], lo[4];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const __nv_bfloat162 hv = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
-            const float2 hf = __bfloat1622float2(hv);
-            const __nv_bfloat162 lv = __floats2bfloat162_rn(v[2 * q] - hf.x, v[2 * q + 1] - hf.y);
-            hi[q] = *reinterpret_cast<const uint32_t *>(&hv);
-            lo[q] = *reinterpret_cast<const uint32_t *>(&lv);
-          }
-          const uint32_t off = (uint32_t)c * 128u + (uint32_t)((jg ^ (c & 7)) << 4);
-          *reinterpret_cast<uint4 *>(tile + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-          *reinterpret_cast<uint4 *>(tile + Cfg::kTile + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        for (int q = 0; q < 8; ++q) {
+          const float x = c < k ? src[(size_t)q * ldz + c] : 0.f;
+          v[q] = wj[q] != 0.f ? x * wj[q] : 0.f;   // select: padding rows may hold anything
         }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(b_hempty + 8 * hs);
+        uint32_t hi[4], lo[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const __nv_bfloat162 hv = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+          const float2 hf = __bfloat1622float2(hv);
+          const __nv_bfloat162 lv = __floats2bfloat162_rn(v[2 * q] - hf.x, v[2 * q + 1] - hf.y);
+          hi[q] = *reinterpret_cast<const uint32_t *>(&hv);
+          lo[q] = *reinterpret_cast<const uint32_t *>(&lv);
+        }
+        const uint32_t off = (uint32_t)c * 128u + (uint32_t)((jg ^ (c & 7)) << 4);
+        *reinterpret_cast<uint4 *>(tile + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+        *reinterpret_cast<uint4 *>(tile + Cfg::kTile + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
       }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(b_hempty + 8 * hs);
       // the generic-proxy stores must be visible to the tensor cores' async-proxy reads
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
@@ -440,7 +442,7 @@ syrk_fused_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, in
       for (int mb = 0; mb < Cfg::kSegs; ++mb) {
         const int r = mb * 128 + q * 32 + lane;
         const uint32_t tcol = tmem + (mb == 0 ? 0u : 128u);
-        for (int c0 = 32 * h; c0 < (mb + 1) * 128; c0 += 64) {
+        for (int c0 = 32 * (cw >> 2); c0 < (mb + 1) * 128; c0 += 64) {
           uint32_t v[32];
           if (have) {
             tmem_ld32(tcol + c0 + lane_off, v);
