@@ -277,8 +277,10 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
   double *sym = Cm + (size_t)k * k + 8;
   const bool half = precision != TSVM_PREC_FP32 && !rows;
   if (half) {
+    // the range-finder pass above built the Gram operands of the same rows and gamma (nothing
+    // in between touches them)
     TSVM_TRY(kermatmul_tc_half(ctx, Xc, y, n, d, gamma, W, kp, Q, precision, &km2,
-                               split ? nullptr : W, split ? 2 : 0, sym));
+                               split ? nullptr : W, split ? 2 : 0, sym, true));
   } else if (split) {
     TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, Wall, kp, Q, precision, &km2, nullptr, 2,
                        row0, nr));

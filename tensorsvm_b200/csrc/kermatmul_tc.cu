@@ -530,48 +530,61 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
 // ---------------------------------------------------------------------------------------
 // XA/XB rows (n_pad x 64 FP16) from centred features: see the file comment for the layout.
 // Either output may be null (a row-sharded factor builds XA for its own rows and XB for all).
-__global__ void prep_gram_operands(const float *__restrict__ Xc, int64_t n, int64_t n_pad, int d,
-                                   int KG, double scale, __half *__restrict__ XA,
-                                   __half *__restrict__ XB) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_pad) return;
-  __half *a = XA ? XA + i * KG : nullptr, *b = XB ? XB + i * KG : nullptr;
+// One block of 32 threads builds 32 rows (thread = row) in shared memory, rows padded by one
+// 4-byte word so that the threads' stores fall in distinct banks, then writes them out as one
+// contiguous span with coalesced 4-byte stores (n_pad is a multiple of 32; rows past n are
+// zero).
+constexpr int kPrepRows = 32;
+constexpr int kPrepPad = kMaxKG + 2;   // halves per staged row, at most
+__global__ void __launch_bounds__(kPrepRows)
+prep_gram_operands(const float *__restrict__ Xc, int64_t n, int64_t n_pad, int d, int KG,
+                   double scale, __half *__restrict__ XA, __half *__restrict__ XB) {
+  __shared__ __align__(16) __half sa[kPrepRows * kPrepPad], sb[kPrepRows * kPrepPad];
+  const int t = threadIdx.x, SP = KG + 2;
+  const int64_t r0 = (int64_t)blockIdx.x * kPrepRows, i = r0 + t;
+  __half *a = sa + t * SP, *b = sb + t * SP;
+  const __half zero = __float2half_rn(0.f);
   for (int c = 0; c < KG; ++c) {
-    if (a) a[c] = __float2half_rn(0.f);
-    if (b) b[c] = __float2half_rn(0.f);
+    a[c] = zero;
+    b[c] = zero;
   }
-  if (i >= n) return;
-  double nn = 0.0;
-  for (int c = 0; c < d; ++c) {
-    const double xt = (double)Xc[i * d + c] * scale;
-    nn += xt * xt;
-    const __half hi = __float2half_rn((float)xt);
-    const __half lo = __float2half_rn((float)(xt - (double)__half2float(hi)));
-    if (a) {
+  if (i < n) {
+    double nn = 0.0;
+    for (int c = 0; c < d; ++c) {
+      const double xt = (double)Xc[i * d + c] * scale;
+      nn += xt * xt;
+      const __half hi = __float2half_rn((float)xt);
+      const __half lo = __float2half_rn((float)(xt - (double)__half2float(hi)));
       a[c] = hi;
       a[d + c] = lo;
       a[2 * d + c] = hi;
-    }
-    if (b) {
       b[c] = hi;
       b[d + c] = hi;
       b[2 * d + c] = lo;
     }
-  }
-  const double v = 0.5 * nn;
-  const __half h = __float2half_rn((float)v);
-  const double r1 = v - (double)__half2float(h);
-  const __half m = __float2half_rn((float)r1);
-  const __half l = __float2half_rn((float)(r1 - (double)__half2float(m)));
-  const __half one = __float2half_rn(1.f);
-  const int o = 3 * d;
-  if (a) {
+    const double v = 0.5 * nn;
+    const __half h = __float2half_rn((float)v);
+    const double r1 = v - (double)__half2float(h);
+    const __half m = __float2half_rn((float)r1);
+    const __half l = __float2half_rn((float)(r1 - (double)__half2float(m)));
+    const __half one = __float2half_rn(1.f);
+    const int o = 3 * d;
     a[o + 0] = one; a[o + 1] = one; a[o + 2] = one;
     a[o + 3] = __hneg(h); a[o + 4] = __hneg(m); a[o + 5] = __hneg(l);
-  }
-  if (b) {
     b[o + 0] = __hneg(h); b[o + 1] = __hneg(m); b[o + 2] = __hneg(l);
     b[o + 3] = one; b[o + 4] = one; b[o + 5] = one;
+  }
+  __syncthreads();
+  if (r0 >= n_pad) return;
+  const int rw = KG / 2, sw = SP / 2;        // 4-byte words per global row / staged row
+  const uint32_t *va = reinterpret_cast<const uint32_t *>(sa);
+  const uint32_t *vb = reinterpret_cast<const uint32_t *>(sb);
+  uint32_t *ga = XA ? reinterpret_cast<uint32_t *>(XA + r0 * KG) : nullptr;
+  uint32_t *gb = XB ? reinterpret_cast<uint32_t *>(XB + r0 * KG) : nullptr;
+  for (int w = t; w < kPrepRows * rw; w += kPrepRows) {
+    const int s_ = (w / rw) * sw + w % rw;
+    if (ga) ga[w] = va[s_];
+    if (gb) gb[w] = vb[s_];
   }
 }
 
@@ -865,10 +878,11 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
 
 tsvm_status kermatmul_tc_half(tsvm_context *ctx, const float *Xc, const float *y, int64_t n, int d,
                               double gamma, const float *A, int kp, float *R, int precision,
-                              float *kernel_ms, float *round_back, int split, double *sym) {
+                              float *kernel_ms, float *round_back, int split, double *sym,
+                              bool reuse_gram) {
   if (split < kSplitNone || split > kSplitA || sym == nullptr) return TSVM_ERR_INVALID_ARGUMENT;
   return kermatmul_tc_core(ctx, Xc, y, n, Xc, y, n, d, gamma, A, kp, R, precision, kernel_ms,
-                           round_back, split, false, sym);
+                           round_back, split, false, sym, reuse_gram);
 }
 
 // The general form: W (ni x kp) = Y_I K(X_I, X_J) Y_J A with the I rows XI (ni x d, labels yI) and
@@ -877,7 +891,8 @@ tsvm_status kermatmul_tc_half(tsvm_context *ctx, const float *Xc, const float *y
 tsvm_status kermatmul_tc_core(tsvm_context *ctx, const float *XI, const float *yI, int64_t ni,
                               const float *XJ, const float *yJ, int64_t nj, int d, double gamma,
                               const float *A, int kp, float *W, int precision, float *kernel_ms,
-                              float *round_back, int split, bool deriv, double *sym) {
+                              float *round_back, int split, bool deriv, double *sym,
+                              bool reuse_gram) {
   if (!kermatmul_tc_supported(d, kp)) return TSVM_ERR_UNSUPPORTED;
   if (split < kSplitNone || split > kSplitPA || ni < 1 || nj < 1) return TSVM_ERR_INVALID_ARGUMENT;
   if (deriv && split != kSplitPA) return TSVM_ERR_UNSUPPORTED;
@@ -910,15 +925,18 @@ tsvm_status kermatmul_tc_core(tsvm_context *ctx, const float *XI, const float *y
   double *samp = part + o_samp, *cpart = part + o_cpart;
   float *ccol = reinterpret_cast<float *>(part + o_ccol);   // o_ccol is even: 16-byte aligned
   const double xscale = sqrt(2.0 * gamma * 1.4426950408889634);
-  if (!same) {
-    prep_gram_operands<<<(unsigned)ceil_div(n_pad, 256), 256, 0, ctx->stream>>>(
+  if (reuse_gram && same) {
+    // XA and XB of these rows, this gamma and this Gram width are still in SLOT_OPX from the
+    // call before (the range-finder pass of the same factor)
+  } else if (!same) {
+    prep_gram_operands<<<(unsigned)(n_pad / kPrepRows), kPrepRows, 0, ctx->stream>>>(
         XJ, nj, n_pad, d, KG, xscale, nullptr, XB);
     TSVM_LAUNCHED(ctx);
-    prep_gram_operands<<<(unsigned)ceil_div(nr_pad, 256), 256, 0, ctx->stream>>>(
+    prep_gram_operands<<<(unsigned)(nr_pad / kPrepRows), kPrepRows, 0, ctx->stream>>>(
         XI, ni, nr_pad, d, KG, xscale, XA, nullptr);
     TSVM_LAUNCHED(ctx);
   } else {   // XA and XB of the same rows in one pass
-    prep_gram_operands<<<(unsigned)ceil_div(n_pad, 256), 256, 0, ctx->stream>>>(
+    prep_gram_operands<<<(unsigned)(n_pad / kPrepRows), kPrepRows, 0, ctx->stream>>>(
         XJ, nj, n_pad, d, KG, xscale, XA, XB);
     TSVM_LAUNCHED(ctx);
   }

@@ -60,15 +60,19 @@ tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms,
 tsvm_status kermatmul_tc_core(tsvm_context *ctx, const float *XI, const float *yI, int64_t ni,
                               const float *XJ, const float *yJ, int64_t nj, int d, double gamma,
                               const float *A, int kp, float *W, int precision, float *kernel_ms,
-                              float *round_back, int split, bool deriv, double *sym = nullptr);
+                              float *round_back, int split, bool deriv, double *sym = nullptr,
+                              bool reuse_gram = false);
 
 // Half product for a symmetric projection (same rows on both sides): R = Y (K o H) Y A with
 // H_ij = 1 (j > i), 1/2 (j == i), 0 (j < i), so that A^T (Y K Y) A = A^T R + R^T A + s u u^T with
 // sym[0] = s (the kernel-mean shift the tensor-core form took off) and sym[1..kp] = u = A^T y
-// (kp + 1 doubles, written by this call).  About half the tiles of kermatmul_tc.
+// (kp + 1 doubles, written by this call).  About half the tiles of kermatmul_tc.  reuse_gram:
+// the call just before on this context was a kermatmul_tc over the same rows Xc with the same
+// gamma, so its Gram operands are reused instead of rebuilt.
 tsvm_status kermatmul_tc_half(tsvm_context *ctx, const float *Xc, const float *y, int64_t n, int d,
                               double gamma, const float *A, int kp, float *R, int precision,
-                              float *kernel_ms, float *round_back, int split, double *sym);
+                              float *kernel_ms, float *round_back, int split, double *sym,
+                              bool reuse_gram = false);
 
 // Kernel-vector products of the hypergradient (hypergrad.cu): out (na x nu, FP64) =
 // [K or K' = -||a - b||^2 K](A, B) U with U nb x nu FP64, on the SIMT kernel or the tensor cores.
