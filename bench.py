@@ -768,7 +768,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", default="32768,65536,131072",
                     help="row counts of the FP64 oracle samples behind cpu_baseline's fit")
-    ap.add_argument("--ref-budget", type=float, default=900.0,
+    ap.add_argument("--ref-budget", type=float, default=300.0,
                     help="reference arm: seconds of full-size reference runs (at least one run)")
     ap.add_argument("--factor-threads", type=int, default=4,
                     help="grid workload: host threads (one context each) for the 64 factors")

@@ -108,9 +108,10 @@ def test_grid_barrier_wait_runs_out_and_context_stays_usable(ctx):
     assert np.allclose(np.sort(w.cpu().numpy()), np.arange(1.0, 9.0))
 
 
-# symmetric and general, narrow and wide (k = 400: seven 64-column tiles), ld > k
+# symmetric and general, narrow and wide (k = 400: seven 64-column tiles, the last ragged), ld > k
 @pytest.mark.parametrize("sym,ka,kb", [(True, 70, 70), (False, 70, 33), (True, 256, 256),
-                                       (False, 256, 256), (True, 400, 400), (False, 130, 200)])
+                                       (False, 256, 256), (True, 400, 400), (False, 130, 200),
+                                       (True, 128, 128), (False, 127, 300), (True, 129, 129)])
 def test_gram_fp64_exact_products(ctx, sym, ka, kb):
     rng = np.random.default_rng(7 + ka)
     n = 10007

@@ -86,6 +86,9 @@ def test_train_end_to_end_matches_reference(ctx, c1):
     assert abs(st["dobj"] - last[6]) / abs(last[6]) < 1e-5
     idx, coef, rho, _ = ref_fixture("ref_c1_rbf")
     sv, _ = orc.sv_sets(m.alpha, C)
+    # the FP64 oracle itself agrees with the reference build on SV Jaccard 0.9958 here (alpha
+    # moves along the dual's nearly flat optimal face with the factor's rounding), so 0.999
+    # would hold no exact solver; the prediction bar below is the 99.9 % one
     assert jaccard(sv, idx) > 0.99
     ref_alpha = np.zeros(len(X))
     ref_alpha[idx] = coef * y[idx]
