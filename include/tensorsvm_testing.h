@@ -34,6 +34,16 @@ tsvm_status tsvm_test_kermatmul(tsvm_context *ctx, const float *X, const float *
 tsvm_status tsvm_test_kermatmul_half(tsvm_context *ctx, const float *X, const float *y, int64_t n,
                                      int32_t d, double gamma, const float *A, int32_t kp,
                                      float *R, double *sym, int32_t precision, int32_t split);
+/* The two products above when only the first kw columns of A may be nonzero (the rest zero):
+ * above 256 columns, kw rounded up to 16 at most 416 runs the product as one launch over kw
+ * columns (the other columns of the output written as zeros), otherwise in 256-column slabs. */
+tsvm_status tsvm_test_kermatmul_cols(tsvm_context *ctx, const float *X, const float *y, int64_t n,
+                                     int32_t d, double gamma, const float *A, int32_t kp,
+                                     int32_t kw, float *W, int32_t precision, int32_t split);
+tsvm_status tsvm_test_kermatmul_half_cols(tsvm_context *ctx, const float *X, const float *y,
+                                          int64_t n, int32_t d, double gamma, const float *A,
+                                          int32_t kp, int32_t kw, float *R, double *sym,
+                                          int32_t precision, int32_t split);
 /* out (na x nu, FP64) = sum_j w_ij exp(-gamma ||a_i - b_j||^2) U[j][:], w = 1 or (deriv)
  * -||a_i - b_j||^2, by the hypergradient's SIMT products or (tensor_cores) the tcgen05 form. */
 tsvm_status tsvm_test_kprod(tsvm_context *ctx, const float *A, int64_t na, const float *B,

@@ -105,6 +105,13 @@ tsvm_status tsvm_create(tsvm_context **out, int device) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
   ctx->stream = ctx->own_stream;
   for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreate(&ctx->ev[i]);
+  if (e == cudaSuccess) {
+    int lo = 0, hi = 0;
+    e = cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    if (e == cudaSuccess)
+      e = cudaStreamCreateWithPriority(&ctx->side_stream, cudaStreamNonBlocking, hi);
+  }
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMallocHost(&ctx->host_scalars, 4096);
   if (e != cudaSuccess) {
     tsvm_destroy(ctx);
@@ -118,11 +125,14 @@ tsvm_status tsvm_destroy(tsvm_context *ctx) {
   if (!ctx) return TSVM_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->side_stream) cudaStreamSynchronize(ctx->side_stream);
   for (int i = 0; i < SLOT_COUNT_; ++i)
     if (ctx->buf[i]) cudaFree(ctx->buf[i]);
   for (int i = 0; i < 8; ++i)
     if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+  if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   if (ctx->host_scalars) cudaFreeHost(ctx->host_scalars);
+  if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return TSVM_OK;

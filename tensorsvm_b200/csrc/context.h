@@ -69,6 +69,10 @@ struct tsvm_context {
   int num_sms = 0;
   cudaStream_t stream = nullptr;      // stream all work is issued on
   cudaStream_t own_stream = nullptr;  // the context's own stream
+  // high-priority side stream (and the event that forks it off `stream`): the interior-point
+  // iteration's k x k Cholesky runs there beside the next streaming pass over Z
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t fork_ev = nullptr;
   int64_t launches = 0;
   void *buf[tsvm::SLOT_COUNT_] = {};
   size_t bytes[tsvm::SLOT_COUNT_] = {};

@@ -812,7 +812,8 @@ __global__ void eig_pack_out(const double *__restrict__ A0, const double *__rest
 
 }  // namespace
 
-tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_dev, double *Dinv) {
+tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_dev, double *Dinv,
+                      cudaStream_t stream) {
   if (n < 1 || n > kMaxDense) return TSVM_ERR_UNSUPPORTED;  // panel must fit shared memory
   // the panel rows padded to an even length, plus the slack the 4-row reads of a ragged last
   // block run into
@@ -820,7 +821,8 @@ tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_de
   const size_t smem = sizeof(double) * ((size_t)kNB * ldp + 64);
   TSVM_CUDA(cudaFuncSetAttribute(chol_la_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
-  chol_la_kernel<<<1, kCholLAThreads, smem, ctx->stream>>>(A, n, lda, Dinv, info_dev);
+  chol_la_kernel<<<1, kCholLAThreads, smem, stream ? stream : ctx->stream>>>(A, n, lda, Dinv,
+                                                                             info_dev);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;
 }

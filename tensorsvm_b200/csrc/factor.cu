@@ -116,12 +116,12 @@ struct Phase {
 static tsvm_status kermatmul(tsvm_context *ctx, const float *Xc, const float *norms,
                              const float *y, int64_t n, int d, double gamma, const float *A,
                              int kp, float *W, int precision, float *kernel_ms,
-                             float *round_back, int split, int64_t row0, int64_t nr) {
+                             float *round_back, int split, int64_t row0, int64_t nr, int kw) {
   if (precision == TSVM_PREC_FP32)
     return kermatmul_fp32(ctx, Xc, norms, y, n, d, gamma, A, kp, W, row0, nr);
   if (!kermatmul_tc_supported(d, kp)) return TSVM_ERR_UNSUPPORTED;
   return kermatmul_tc(ctx, Xc, norms, y, n, d, gamma, A, kp, W, precision, kernel_ms, round_back,
-                      split, row0, nr);
+                      split, row0, nr, kw);
 }
 
 // Rkeep (2 k x k doubles, may be null): the combined factor R with (input W) = (output W) R.
@@ -244,7 +244,7 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
   // kernel whose range is found; rounding the sketch only draws another Gaussian sketch)
   const bool split = precision_is_split(precision);
   TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, Q, kp, W, precision, &km1, nullptr,
-                     split ? 1 : 0, row0, nr));
+                     split ? 1 : 0, row0, nr, k));
   TSVM_CUDA(cudaEventRecord(ev[2], ctx->stream));
   phase.next("factor: orthonormalise");
   const bool tc_gram = precision != TSVM_PREC_FP32 && keep == nullptr && syrk_tc_supported(k) &&
@@ -280,13 +280,13 @@ tsvm_status factor_rbf(tsvm_context *ctx, const float *X, const float *y, int64_
     // the range-finder pass above built the Gram operands of the same rows and gamma (nothing
     // in between touches them)
     TSVM_TRY(kermatmul_tc_half(ctx, Xc, y, n, d, gamma, W, kp, Q, precision, &km2,
-                               split ? nullptr : W, split ? 2 : 0, sym, true));
+                               split ? nullptr : W, split ? 2 : 0, sym, true, k));
   } else if (split) {
     TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, Wall, kp, Q, precision, &km2, nullptr, 2,
-                       row0, nr));
+                       row0, nr, k));
   } else {
     TSVM_TRY(kermatmul(ctx, Xc, norms, y, n, d, gamma, Wall, kp, Q, precision, &km2, Wall, 0,
-                       row0, nr));
+                       row0, nr, k));
     if (rows && precision != TSVM_PREC_FP32)   // this rank's rows as the tensor cores saw them
       TSVM_CUDA(cudaMemcpyAsync(W, Wall + row0 * kp, sizeof(float) * nr * kp,
                                 cudaMemcpyDeviceToDevice, ctx->stream));

@@ -917,6 +917,8 @@ struct Runner {
   const double *dinv;
 
   int *err;   // set by a streaming pass that timed out
+  // SMs left free by the streaming passes (1 while the k x k Cholesky runs beside one)
+  int sm_reserve = 0;
   // row-sharded solves: every finalize completes its sums / minima across the ranks
   bool shard = false;
   double *red_buf = nullptr;   // 16 doubles
@@ -936,7 +938,8 @@ struct Runner {
     const size_t smem = stages * chunk + 8 * (2 * stages + 2);
     auto kern = stream_kernel<MODE, Op, R, CR, LPR, CPL>;
     TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int grid = (int)std::min<int64_t>(std::min(nblk, ctx->num_sms), ceil_div(n, CR));
+    const int grid = (int)std::max<int64_t>(
+        1, std::min<int64_t>(std::min(nblk, ctx->num_sms - sm_reserve), ceil_div(n, CR)));
     kern<<<grid, kSThreads, smem, ctx->stream>>>(Z, ldz, k, n, op, scal, w, dinv, geo.kz,
                                                  (int)stages, part_vec, part_s, err, nullptr,
                                                  nullptr, nullptr);
@@ -1253,11 +1256,25 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
       TSVM_TRY(small_add_diag(ctx, M, k, k, 1.0));
     }
     TSVM_CUDA(cudaEventRecord(ev_syrk1, ctx->stream));
-    TSVM_TRY(chol_fp64(ctx, M, k, k, run.info, Mdinv));
-    TSVM_CUDA(cudaEventRecord(ev_chol1, ctx->stream));
+    // predictor: r7 = SMW(r5), b = SMW(a) in one pair of passes.  The right-hand sides
+    // Z^T [r5/D, a/D] do not need M: the Cholesky (one CTA, latency-bound) runs on the side
+    // stream on one SM while that pass streams Z on the others.
+    if (!run.shard) {
+      TSVM_CUDA(cudaEventRecord(ctx->fork_ev, ctx->stream));
+      TSVM_CUDA(cudaStreamWaitEvent(ctx->side_stream, ctx->fork_ev, 0));
+      TSVM_TRY(chol_fp64(ctx, M, k, k, run.info, Mdinv, ctx->side_stream));
+      TSVM_CUDA(cudaEventRecord(ev_chol1, ctx->side_stream));
+      run.sm_reserve = 1;
+      const tsvm_status st_rhs = run.zt(SmwRhs2Op{V}, h, ST_NONE);
+      run.sm_reserve = 0;
+      TSVM_CUDA(cudaStreamWaitEvent(ctx->stream, ev_chol1, 0));
+      TSVM_TRY(st_rhs);
+    } else {
+      TSVM_TRY(chol_fp64(ctx, M, k, k, run.info, Mdinv));
+      TSVM_CUDA(cudaEventRecord(ev_chol1, ctx->stream));
+      TSVM_TRY(run.zt(SmwRhs2Op{V}, h, ST_NONE));
+    }
     pending_events = true;
-    // predictor: r7 = SMW(r5), b = SMW(a) in one pair of passes
-    TSVM_TRY(run.zt(SmwRhs2Op{V}, h, ST_NONE));
     if (sweeps)
       TSVM_CUDA(cudaMemcpyAsync(h0, h, sizeof(double) * 2 * kz, cudaMemcpyDeviceToDevice,
                                 ctx->stream));

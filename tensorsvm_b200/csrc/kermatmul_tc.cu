@@ -54,35 +54,46 @@ constexpr int kMaxKG = 192;       // widest Gram K (3 d + 6 <= 192: d <= 62)
 
 // Gram K (split features + norms, zero padded to 64, 128 or 192) and the ring depths that
 // fit 227 KB of shared memory with it: 16 + 6x8 + 5x32, 32 + 4x16 + 4x32, 48 + 3x24 + 3x32 KB.
-template <int KG>
+// HALF (wide slabs, kpw in (256, 416]): the J blocks are taken in 32-row units, so that the S/P
+// buffers need 32 TMEM columns each and W up to 416; the kernel-block operand ring then holds
+// one 32-row K slice (kpw x 64 B, 64-byte swizzle) per slot.  16 + 6x8 + 6x26, 32 + 3x16 +
+// 5x26, 48 + 3x24 + 4x26 KB at kpw = 416.
+template <int KG, bool HALF = false>
 struct GramCfg {
   static constexpr uint32_t kXaBytes = kBM * KG * 2;   // XA tile, KG/64 128-byte-wide chunks
   static constexpr uint32_t kXbBytes = kBJ * KG * 2;
-  static constexpr int kXbStages = KG == 64 ? 6 : KG == 128 ? 4 : 3;
-  static constexpr int kAtStages = KG == 64 ? 5 : KG == 128 ? 4 : 3;
+  static constexpr int kXbStages = KG == 64 ? 6 : KG == 128 ? (HALF ? 3 : 4) : 3;
+  static constexpr int kAtStages =
+      HALF ? (KG == 64 ? 6 : KG == 128 ? 5 : 4) : (KG == 64 ? 5 : KG == 128 ? 4 : 3);
+  static constexpr int kUnit = HALF ? 32 : 64;           // J rows per S/P buffer
+  static constexpr int kUnits = kBJ / kUnit;             // units per J block
+  static constexpr int kSBufs = HALF ? 3 : 4;            // S/P buffers in TMEM
+  static constexpr int kSCol0 = HALF ? 416 : 0;          // first S/P column
+  static constexpr int kWCol0 = HALF ? 0 : 256;          // first W column
 };
+constexpr int kMaxHalfW = 416;   // W columns of one HALF launch (512 TMEM columns - 3 x 32)
 
 __host__ __device__ constexpr uint32_t align1k(uint32_t v) { return (v + 1023u) & ~1023u; }
 
 // Shared-memory layout, all operand tiles 1024-byte aligned (128B swizzle atoms):
-// [XA][XB ring][AT ring: kpw*128 B each][barriers].  P lives in TMEM.  Offsets are computed
-// arithmetically (no arrays), so they stay in registers.
-template <int KG>
+// [XA][XB ring][AT ring: kpw*128 B each (kpw*64 B for HALF)][barriers].  P lives in TMEM.
+// Offsets are computed arithmetically (no arrays), so they stay in registers.
+template <int KG, bool HALF = false>
 struct SmemLayout {
   uint32_t at0, at_bytes, bars, total;
   __host__ __device__ uint32_t xa() const { return 0; }
   __host__ __device__ uint32_t xb(int s) const {
-    return GramCfg<KG>::kXaBytes + (uint32_t)s * GramCfg<KG>::kXbBytes;
+    return GramCfg<KG, HALF>::kXaBytes + (uint32_t)s * GramCfg<KG, HALF>::kXbBytes;
   }
   __host__ __device__ uint32_t at(int s) const { return at0 + (uint32_t)s * at_bytes; }
 };
 
-template <int KG>
-__host__ __device__ inline SmemLayout<KG> smem_layout(int kpw) {
-  using C = GramCfg<KG>;
-  SmemLayout<KG> L{};
+template <int KG, bool HALF = false>
+__host__ __device__ inline SmemLayout<KG, HALF> smem_layout(int kpw) {
+  using C = GramCfg<KG, HALF>;
+  SmemLayout<KG, HALF> L{};
   L.at0 = C::kXaBytes + C::kXbStages * C::kXbBytes;
-  L.at_bytes = align1k((uint32_t)kpw * kBJ * 2);
+  L.at_bytes = align1k((uint32_t)kpw * C::kUnit * 2);
   L.bars = L.at0 + C::kAtStages * L.at_bytes;
   L.total = L.bars + 512;
   return L;
@@ -179,8 +190,12 @@ __host__ __device__ constexpr bool split_a(int s) { return s == kSplitA || s == 
 // j == i and 0 for j < i, over the J blocks from the diagonal on (about half of the tiles), for a
 // symmetric projection A^T K A = A^T R + R^T A.  The kernel-mean shift is not restored here: the
 // caller adds shift (A^T y)(A^T y)^T to the projection instead.
+// HALF (kpw in (256, 416], one launch instead of two column slabs that would each recompute S
+// and P): W takes TMEM columns 0..kpw-1 and the S/P buffers, three of 32 columns, 416..511; every
+// J block is taken as two 32-row units (Gram MMA N = 32 on half the XB tile, P AT^T with K = 32
+// from a 32-row K slice of the kernel-block operand in its own ring slot, 64-byte swizzle), and
+// P AT^T runs as two MMAs, N = 256 and N = kpw - 256.
 // ---------------------------------------------------------------------------------------
-constexpr int kSBufs = 4;
 
 // Row block of round r for this CTA.  The half product (tri) walks the rounds in alternating
 // directions, so that the CTA with the longest row (the lowest row block) of one round has the
@@ -192,7 +207,7 @@ __device__ __forceinline__ int row_block(int r, int G, int tri) {
 // reaches column rb * kBM (the diagonal).
 __device__ __forceinline__ int first_tile(int rb, int tri) { return tri ? rb * (kBM / kBJ) : 0; }
 
-template <bool BF16, int NPOLY, int KG, bool SHIFT, int SPLIT, bool DERIV>
+template <bool BF16, int NPOLY, int KG, bool SHIFT, int SPLIT, bool DERIV, bool HALF>
 __global__ void __launch_bounds__(kThreadsTC, 1)
 kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
                     const __grid_constant__ CUtensorMap map_xb,
@@ -205,10 +220,12 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
   const uint32_t raw = su32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   uint8_t *sbase = smem_raw + (base - raw);
-  using Cfg = GramCfg<KG>;
+  using Cfg = GramCfg<KG, HALF>;
   constexpr int kXbStages = Cfg::kXbStages, kAtStages = Cfg::kAtStages;
   constexpr uint32_t kXaBytes = Cfg::kXaBytes, kXbBytes = Cfg::kXbBytes;
-  const SmemLayout<KG> L = smem_layout<KG>(kpw);
+  constexpr int kSBufs = Cfg::kSBufs, kUnit = Cfg::kUnit, kUnits = Cfg::kUnits;
+  static_assert(!(HALF && DERIV), "the derivative runs at kp <= 256");
+  const SmemLayout<KG, HALF> L = smem_layout<KG, HALF>(kpw);
   uint64_t *bars = reinterpret_cast<uint64_t *>(sbase + L.bars);
   // barrier slots (8 bytes each)
   const uint32_t b_xbfull = su32(bars);                  // [kXbStages] Gram operand loaded
@@ -260,7 +277,8 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const uint32_t t_w = tmem + kSBufs * kBJ;   // W accumulator columns
+  const uint32_t t_w = tmem + Cfg::kWCol0;   // W accumulator columns
+  const uint32_t t_s = tmem + Cfg::kSCol0;   // S/P buffer b at t_s + b * kUnit
 
   if (warp == 0) {
     // ---------------- TMA producer: XA per row block, then its Gram operand ring ----------
@@ -292,20 +310,31 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
     if (lane == 0) {
       asm volatile("prefetch.tensormap [%0];" ::"l"(&map_at) : "memory");
       if constexpr (split_a(SPLIT)) asm volatile("prefetch.tensormap [%0];" ::"l"(&map_atlo) : "memory");
-      const uint32_t at_bytes = (uint32_t)kpw * kBJ * 2;
+      const uint32_t at_bytes = (uint32_t)kpw * kUnit * 2;
       constexpr int kParts = split_a(SPLIT) ? 2 : 1;
       int st = 0;
       uint32_t ph = 0;
       bool ok = true;
       for (int r = 0, rb = row_block(0, G, tri); ok && rb < nrb; rb = row_block(++r, G, tri)) {
         for (int t = first_tile(rb, tri); ok && t < ntiles; ++t) {
+          for (int h = 0; ok && h < kUnits; ++h) {
 #pragma unroll
-          for (int part = 0; part < kParts; ++part) {
-            if (!mbar_wait(b_atempty + 8 * st, ph ^ 1, abort)) { ok = false; break; }
-            mbar_expect_tx(b_atfull + 8 * st, at_bytes);
-            tma_load_2d(part == 0 ? &map_at : &map_atlo, b_atfull + 8 * st, base + L.at(st), 0,
-                        t * kp + c0);
-            if (++st == kAtStages) { st = 0; ph ^= 1; }
+            for (int part = 0; part < kParts; ++part) {
+              if (!mbar_wait(b_atempty + 8 * st, ph ^ 1, abort)) { ok = false; break; }
+              mbar_expect_tx(b_atfull + 8 * st, at_bytes);
+              const CUtensorMap *m = part == 0 ? &map_at : &map_atlo;
+              if constexpr (HALF) {
+                // the unit's 32-element K slice of all kpw rows, as two boxes of kpw / 2 rows
+                // (a box has at most 256 rows); x = 32 h elements = 64 h bytes
+                const int hr = kpw / 2;
+                tma_load_2d(m, b_atfull + 8 * st, base + L.at(st), h * kUnit, t * kp + c0);
+                tma_load_2d(m, b_atfull + 8 * st, base + L.at(st) + (uint32_t)hr * kUnit * 2,
+                            h * kUnit, t * kp + c0 + hr);
+              } else {
+                tma_load_2d(m, b_atfull + 8 * st, base + L.at(st), 0, t * kp + c0);
+              }
+              if (++st == kAtStages) { st = 0; ph ^= 1; }
+            }
           }
         }
       }
@@ -313,7 +342,7 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
   } else if (warp == 1) {
     // ---------------- Gram MMA issuer: S_T = XA XB_t^T into buffer T % 4 ----------------
     if (lane == 0) {
-      constexpr uint32_t idg = idesc_f16(kBM, kBJ, 0);  // Gram: FP16 always
+      constexpr uint32_t idg = idesc_f16(kBM, kUnit, 0);  // Gram: FP16 always
       const uint64_t dxa = desc_sw128(base + L.xa());
       const uint64_t dxb0 = desc_sw128(base + L.xb(0));
       int st = 0, b = 0;
@@ -322,23 +351,26 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
       for (int r = 0, rb = row_block(0, G, tri); ok && rb < nrb; rb = row_block(++r, G, tri)) {
         if (!mbar_wait(b_xafull, r & 1, abort)) break;
         for (int t = first_tile(rb, tri); t < ntiles; ++t) {
-          if (!mbar_wait(b_xbfull + 8 * st, sph, abort) ||
-              !mbar_wait(b_free + 8 * b, bph ^ 1, abort)) {
-            ok = false;
-            break;
-          }
-          tc_fence_after();
+          if (!mbar_wait(b_xbfull + 8 * st, sph, abort)) { ok = false; break; }
           const uint64_t dxb = dxb0 + (uint64_t)((st * kXbBytes) >> 4);
 #pragma unroll
-          for (int kk = 0; kk < KG / 16; ++kk) {   // chunk kk/4 of K, 32-byte step kk%4 in it
-            const uint64_t oa = (uint64_t)(((kk >> 2) * (kBM * 128)) >> 4) + 2 * (kk & 3);
-            const uint64_t ob = (uint64_t)(((kk >> 2) * (kBJ * 128)) >> 4) + 2 * (kk & 3);
-            umma(tmem + b * kBJ, dxa + oa, dxb + ob, idg, kk > 0 ? 1u : 0u);
+          for (int h = 0; h < kUnits; ++h) {
+            if (!mbar_wait(b_free + 8 * b, bph ^ 1, abort)) { ok = false; break; }
+            tc_fence_after();
+#pragma unroll
+            for (int kk = 0; kk < KG / 16; ++kk) {   // chunk kk/4 of K, 32-byte step kk%4 in it
+              const uint64_t oa = (uint64_t)(((kk >> 2) * (kBM * 128)) >> 4) + 2 * (kk & 3);
+              // unit h: rows h * kUnit.. of the J tile (whole 8-row swizzle atoms)
+              const uint64_t ob = (uint64_t)(((kk >> 2) * (kBJ * 128) + h * (kUnit * 128)) >> 4) +
+                                  2 * (kk & 3);
+              umma(t_s + b * kUnit, dxa + oa, dxb + ob, idg, kk > 0 ? 1u : 0u);
+            }
+            umma_commit(b_sfull + 8 * b);
+            if (++b == kSBufs) { b = 0; bph ^= 1; }
           }
-          umma_commit(b_sfull + 8 * b);
+          if (!ok) break;
           umma_commit(b_xbempty + 8 * st);
           if (++st == kXbStages) { st = 0; sph ^= 1; }
-          if (++b == kSBufs) { b = 0; bph ^= 1; }
         }
         if (ok) umma_commit(b_xaempty);
       }
@@ -346,9 +378,17 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
   } else if (warp == 11) {
     // ---------------- P AT^T issuer: W += P_T AT_t^T, P from TMEM ----------------
     if (lane == 0) {
-      const uint32_t id2 = idesc_f16(kBM, kpw, BF16 ? 1u : 0u);
-      const uint64_t dat0 = desc_sw128(base + L.at(0));
+      // HALF: W += P AT^T as two MMAs, columns 0..255 and 256..kpw-1 (B rows 256.. of the slot)
+      const bool two = HALF && kpw > 256;
+      const uint32_t id2 = idesc_f16(kBM, two ? 256 : kpw, BF16 ? 1u : 0u);
+      const uint32_t id2b = idesc_f16(kBM, two ? kpw - 256 : 16, BF16 ? 1u : 0u);
+      constexpr uint32_t kRow256 = (256u * kUnit * 2) >> 4;
+      const uint64_t dat0 = HALF ? desc_sw64(base + L.at(0)) : desc_sw128(base + L.at(0));
       const uint32_t at_step = L.at_bytes >> 4;
+      auto mma = [&](uint32_t a, uint64_t bd, uint32_t acc) {
+        umma_ts(t_w, a, bd, id2, acc);
+        if (HALF && two) umma_ts(t_w + 256, a, bd + kRow256, id2b, acc);
+      };
       int st = 0, b = 0;
       uint32_t sph = 0, bph = 0;
       bool ok = true;
@@ -356,41 +396,43 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
         if (r > 0 && !mbar_wait(b_wempty, (r - 1) & 1, abort)) break;
         tc_fence_after();
         const int tb0 = first_tile(rb, tri);
-        for (int t = tb0; t < ntiles; ++t) {
-          // SPLIT == kSplitA: the J block's AT_lo sits in the ring slot after its AT_hi
-          const int st2 = st + 1 == kAtStages ? 0 : st + 1;
-          const uint32_t sph2 = st + 1 == kAtStages ? sph ^ 1 : sph;
-          if (!mbar_wait(b_atfull + 8 * st, sph, abort) ||
-              (split_a(SPLIT) && !mbar_wait(b_atfull + 8 * st2, sph2, abort)) ||
-              !mbar_wait(b_pfull + 8 * b, bph, abort)) {
-            ok = false;
-            break;
-          }
-          tc_fence_after();
-          const uint64_t dat = dat0 + (uint64_t)(st * at_step);
-          const uint32_t ap = tmem + b * kBJ;
+        for (int t = tb0; ok && t < ntiles; ++t) {
+          for (int h = 0; h < kUnits; ++h) {
+            // SPLIT == kSplitA: the unit's AT_lo sits in the ring slot after its AT_hi
+            const int st2 = st + 1 == kAtStages ? 0 : st + 1;
+            const uint32_t sph2 = st + 1 == kAtStages ? sph ^ 1 : sph;
+            if (!mbar_wait(b_atfull + 8 * st, sph, abort) ||
+                (split_a(SPLIT) && !mbar_wait(b_atfull + 8 * st2, sph2, abort)) ||
+                !mbar_wait(b_pfull + 8 * b, bph, abort)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint64_t dat = dat0 + (uint64_t)(st * at_step);
+            const uint32_t ap = t_s + b * kUnit;
+            const bool first = t == tb0 && h == 0;
 #pragma unroll
-          for (int kk = 0; kk < kBJ / 16; ++kk)
-            umma_ts(t_w, ap + kk * 8, dat + 2 * kk, id2, (t > tb0 || kk > 0) ? 1u : 0u);
-          if constexpr (split_p(SPLIT)) {
+            for (int kk = 0; kk < kUnit / 16; ++kk)
+              mma(ap + kk * 8, dat + 2 * kk, (!first || kk > 0) ? 1u : 0u);
+            if constexpr (split_p(SPLIT)) {
 #pragma unroll
-            for (int kk = 0; kk < kBJ / 16; ++kk)   // P_lo over the buffer's columns 32..63
-              umma_ts(t_w, ap + kBJ / 2 + kk * 8, dat + 2 * kk, id2, 1u);
-          }
-          if constexpr (split_a(SPLIT)) {
-            const uint64_t dat2 = dat0 + (uint64_t)(st2 * at_step);
+              for (int kk = 0; kk < kUnit / 16; ++kk)   // P_lo over the buffer's second half
+                mma(ap + kUnit / 2 + kk * 8, dat + 2 * kk, 1u);
+            }
+            if constexpr (split_a(SPLIT)) {
+              const uint64_t dat2 = dat0 + (uint64_t)(st2 * at_step);
 #pragma unroll
-            for (int kk = 0; kk < kBJ / 16; ++kk)
-              umma_ts(t_w, ap + kk * 8, dat2 + 2 * kk, id2, 1u);
-          }
-          umma_commit(b_free + 8 * b);
-          umma_commit(b_atempty + 8 * st);
-          if (++st == kAtStages) { st = 0; sph ^= 1; }
-          if constexpr (split_a(SPLIT)) {
+              for (int kk = 0; kk < kUnit / 16; ++kk) mma(ap + kk * 8, dat2 + 2 * kk, 1u);
+            }
+            umma_commit(b_free + 8 * b);
             umma_commit(b_atempty + 8 * st);
             if (++st == kAtStages) { st = 0; sph ^= 1; }
+            if constexpr (split_a(SPLIT)) {
+              umma_commit(b_atempty + 8 * st);
+              if (++st == kAtStages) { st = 0; sph ^= 1; }
+            }
+            if (++b == kSBufs) { b = 0; bph ^= 1; }
           }
-          if (++b == kSBufs) { b = 0; bph ^= 1; }
         }
         if (ok) umma_commit(b_wfull);
       }
@@ -410,18 +452,14 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
     uint32_t T0 = 0;   // flat index (over this CTA's row blocks) of the row block's first J block
     for (int r = 0, rb = row_block(0, G, tri); ok && rb < nrb; rb = row_block(++r, G, tri)) {
       const int tb0 = first_tile(rb, tri);
-      const uint32_t cnt = (uint32_t)(ntiles - tb0);
+      const uint32_t cnt = (uint32_t)(ntiles - tb0) * kUnits;   // units of this row block
       for (uint32_t T = T0 + ((T0 & 1u) != (uint32_t)g ? 1u : 0u); T < T0 + cnt; T += 2) {
-        const uint32_t b = T & (kSBufs - 1);
-        const int t = tb0 + (int)(T - T0);
+        const uint32_t b = T % kSBufs;
+        const int t = tb0 + (int)((T - T0) / kUnits);
+        const int h = (int)((T - T0) % kUnits);
         if (!mbar_wait(b_sfull + 8 * b, (T / kSBufs) & 1u, abort)) { ok = false; break; }
         tc_fence_after();
-        const uint32_t tb = tmem + b * kBJ + lane_off;
-        uint32_t s0[32], s1[32];
-        tmem_ld32(tb, s0);
-        tmem_ld32(tb + 32, s1);
-        tmem_wait_ld();
-        uint32_t pk[32];
+        const uint32_t tb = t_s + b * kUnit + lane_off;
         // the kernel block's entry from the scaled distance x = S_ij: exp2(x) (less the shift),
         // or x exp2(x) for the derivative
         auto pv = [&](uint32_t raw, int e) -> float {
@@ -429,6 +467,43 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
           if constexpr (DERIV) return x * exp2_mixed<NPOLY>(x, e);
           else return exp2_mixed<NPOLY>(x, e) - shift;
         };
+        if constexpr (HALF) {
+          // a 32-row unit: 32 S columns -> 16 columns of packed P (hi), and lo beside it
+          uint32_t s0[32];
+          tmem_ld32(tb, s0);
+          tmem_wait_ld();
+          float f[32];
+#pragma unroll
+          for (int e = 0; e < 32; ++e) f[e] = pv(s0[e], e);
+          if (tri && t < tb0 + kBM / kBJ) {   // weights of a unit across the diagonal (below)
+            const int dj = t * kBJ + h * kUnit - (rb * kBM + row);
+#pragma unroll
+            for (int e = 0; e < 32; ++e) {
+              const int dd = dj + e;
+              f[e] = dd > 0 ? f[e] : dd == 0 ? 0.5f * f[e] : 0.f;
+            }
+          }
+          uint32_t ph16[16];
+          if constexpr (split_p(SPLIT)) {
+            uint32_t pl16[16];
+#pragma unroll
+            for (int c = 0; c < 16; ++c) split2<BF16>(f[2 * c], f[2 * c + 1], ph16[c], pl16[c]);
+            tmem_st16(tb + kUnit / 2, pl16);
+          } else {
+#pragma unroll
+            for (int c = 0; c < 16; ++c) ph16[c] = pack2<BF16>(f[2 * c], f[2 * c + 1]);
+          }
+          tmem_st16(tb, ph16);
+          tmem_wait_st();
+          tc_fence_before();
+          mbar_arrive(b_pfull + 8 * b);
+          continue;
+        }
+        uint32_t s0[32], s1[32];
+        tmem_ld32(tb, s0);
+        tmem_ld32(tb + 32, s1);
+        tmem_wait_ld();
+        uint32_t pk[32];
         if (tri && t < tb0 + kBM / kBJ) {
           // a tile across the diagonal of the half-product: entry (i, j) weighs 1 for j > i, 1/2
           // for j == i and 0 for j < i (dj = j - i of the tile's column 0)
@@ -494,7 +569,33 @@ kermatmul_tc_kernel(const __grid_constant__ CUtensorMap map_xa,
       tc_fence_after();
       const int64_t gi = (int64_t)rb * kBM + row;
       const float sc = gi < n ? (y ? y[gi] : 1.f) * inv_scale[0] : 0.f;
-      for (int cc = g * half; cc < (g + 1) * half; cc += 32) {
+      if constexpr (HALF) {
+        // 16-column chunks, alternating between the warpgroups; columns kpw..kp-1 (zero rows of
+        // the operand) are written as zeros
+        for (int cc = g * 16; cc < kp; cc += 32) {
+          float4 *dst = reinterpret_cast<float4 *>(W + gi * ldw + c0 + cc);
+          if (cc < kpw) {
+            uint32_t v[16];
+            tmem_ld16(t_w + cc + lane_off, v);
+            tmem_wait_ld();
+            if (gi < n) {
+              const float4 *cs = reinterpret_cast<const float4 *>(ccol + c0 + cc);
+#pragma unroll
+              for (int j = 0; j < 4; ++j) {
+                const float4 a = SHIFT && !tri ? cs[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+                dst[j] = make_float4((__uint_as_float(v[4 * j]) + a.x) * sc,
+                                     (__uint_as_float(v[4 * j + 1]) + a.y) * sc,
+                                     (__uint_as_float(v[4 * j + 2]) + a.z) * sc,
+                                     (__uint_as_float(v[4 * j + 3]) + a.w) * sc);
+              }
+            }
+          } else if (gi < n) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) dst[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+        }
+      }
+      for (int cc = g * half; !HALF && cc < (g + 1) * half; cc += 32) {
         uint32_t v[32];
         tmem_ld32(t_w + cc + lane_off, v);
         tmem_wait_ld();
@@ -802,13 +903,13 @@ int poly_split() {
   return v;
 }
 
-template <int SPLIT>
+template <int SPLIT, bool HALF = false>
 TcKernel select_split(bool bf16, int KG, bool shift) {
   // MUFU exps only
 #define TSVM_SEL(K, S)                                                                   \
   if (KG == K && shift == S)                                                             \
-    return bf16 ? kermatmul_tc_kernel<true, 0, K, S, SPLIT, false>                       \
-                : kermatmul_tc_kernel<false, 0, K, S, SPLIT, false>;
+    return bf16 ? kermatmul_tc_kernel<true, 0, K, S, SPLIT, false, HALF>                 \
+                : kermatmul_tc_kernel<false, 0, K, S, SPLIT, false, HALF>;
   TSVM_SEL(64, true)
   TSVM_SEL(128, true)
   TSVM_SEL(192, true)
@@ -819,12 +920,19 @@ TcKernel select_split(bool bf16, int KG, bool shift) {
   return nullptr;
 }
 
-TcKernel select_kernel(bool bf16, int npoly, int KG, bool shift, int split, bool deriv) {
+TcKernel select_kernel(bool bf16, int npoly, int KG, bool shift, int split, bool deriv,
+                       bool half) {
   if (deriv) {   // FP16, all splits, no shift (the derivative's entries are not flat)
-    if (bf16 || shift || split != kSplitPA) return nullptr;
-    if (KG == 64) return kermatmul_tc_kernel<false, 0, 64, false, kSplitPA, true>;
-    if (KG == 128) return kermatmul_tc_kernel<false, 0, 128, false, kSplitPA, true>;
-    if (KG == 192) return kermatmul_tc_kernel<false, 0, 192, false, kSplitPA, true>;
+    if (bf16 || shift || split != kSplitPA || half) return nullptr;
+    if (KG == 64) return kermatmul_tc_kernel<false, 0, 64, false, kSplitPA, true, false>;
+    if (KG == 128) return kermatmul_tc_kernel<false, 0, 128, false, kSplitPA, true, false>;
+    if (KG == 192) return kermatmul_tc_kernel<false, 0, 192, false, kSplitPA, true, false>;
+    return nullptr;
+  }
+  if (half) {   // one launch over more than 256 columns (the factor's passes at k > 256)
+    if (split == kSplitP) return select_split<kSplitP, true>(bf16, KG, shift);
+    if (split == kSplitA) return select_split<kSplitA, true>(bf16, KG, shift);
+    if (split == kSplitNone) return select_split<kSplitNone, true>(bf16, KG, shift);
     return nullptr;
   }
   if (split == kSplitP) return select_split<kSplitP>(bf16, KG, shift);
@@ -833,16 +941,16 @@ TcKernel select_kernel(bool bf16, int npoly, int KG, bool shift, int split, bool
   if (shift || KG != 64) return select_split<kSplitNone>(bf16, KG, shift);
 #define TSVM_SEL(P) \
   if (npoly == P) \
-    return bf16 ? kermatmul_tc_kernel<true, P, 64, false, kSplitNone, false> \
-                : kermatmul_tc_kernel<false, P, 64, false, kSplitNone, false>;
+    return bf16 ? kermatmul_tc_kernel<true, P, 64, false, kSplitNone, false, false> \
+                : kermatmul_tc_kernel<false, P, 64, false, kSplitNone, false, false>;
   TSVM_SEL(0)
   TSVM_SEL(2)
   TSVM_SEL(4)
   TSVM_SEL(6)
   TSVM_SEL(8)
 #undef TSVM_SEL
-  return bf16 ? kermatmul_tc_kernel<true, 4, 64, false, kSplitNone, false>
-              : kermatmul_tc_kernel<false, 4, 64, false, kSplitNone, false>;
+  return bf16 ? kermatmul_tc_kernel<true, 4, 64, false, kSplitNone, false, false>
+              : kermatmul_tc_kernel<false, 4, 64, false, kSplitNone, false, false>;
 }
 
 // Gram K for d features: 3 d split products + 6 norm terms, rounded up to a 64-wide chunk.
@@ -851,7 +959,12 @@ int gram_k(int d) {
   return need <= 64 ? 64 : need <= 128 ? 128 : 192;
 }
 
-size_t tc_smem(int KG, int kpw) {
+size_t tc_smem(int KG, int kpw, bool half) {
+  if (half) {
+    if (KG == 128) return smem_layout<128, true>(kpw).total + 1024;
+    if (KG == 192) return smem_layout<192, true>(kpw).total + 1024;
+    return smem_layout<64, true>(kpw).total + 1024;
+  }
   if (KG == 128) return smem_layout<128>(kpw).total + 1024;
   if (KG == 192) return smem_layout<192>(kpw).total + 1024;
   return smem_layout<64>(kpw).total + 1024;
@@ -866,23 +979,24 @@ bool kermatmul_tc_supported(int d, int kp) {
 tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms, const float *y,
                          int64_t n, int d, double gamma, const float *A, int kp, float *W,
                          int precision, float *kernel_ms, float *round_back, int split,
-                         int64_t row0, int64_t nr) {
+                         int64_t row0, int64_t nr, int kw) {
   (void)norms;
   if (nr < 0) nr = n - row0;
   if (row0 < 0 || nr < 1 || row0 + nr > n) return TSVM_ERR_INVALID_ARGUMENT;
   if (split < kSplitNone || split > kSplitA) return TSVM_ERR_INVALID_ARGUMENT;
   const bool rows = row0 != 0 || nr != n;
   return kermatmul_tc_core(ctx, rows ? Xc + row0 * d : Xc, y + row0, nr, Xc, y, n, d, gamma, A,
-                           kp, W, precision, kernel_ms, round_back, split, false);
+                           kp, W, precision, kernel_ms, round_back, split, false, nullptr, false,
+                           kw);
 }
 
 tsvm_status kermatmul_tc_half(tsvm_context *ctx, const float *Xc, const float *y, int64_t n, int d,
                               double gamma, const float *A, int kp, float *R, int precision,
                               float *kernel_ms, float *round_back, int split, double *sym,
-                              bool reuse_gram) {
+                              bool reuse_gram, int kw) {
   if (split < kSplitNone || split > kSplitA || sym == nullptr) return TSVM_ERR_INVALID_ARGUMENT;
   return kermatmul_tc_core(ctx, Xc, y, n, Xc, y, n, d, gamma, A, kp, R, precision, kernel_ms,
-                           round_back, split, false, sym, reuse_gram);
+                           round_back, split, false, sym, reuse_gram, kw);
 }
 
 // The general form: W (ni x kp) = Y_I K(X_I, X_J) Y_J A with the I rows XI (ni x d, labels yI) and
@@ -892,7 +1006,7 @@ tsvm_status kermatmul_tc_core(tsvm_context *ctx, const float *XI, const float *y
                               const float *XJ, const float *yJ, int64_t nj, int d, double gamma,
                               const float *A, int kp, float *W, int precision, float *kernel_ms,
                               float *round_back, int split, bool deriv, double *sym,
-                              bool reuse_gram) {
+                              bool reuse_gram, int kw) {
   if (!kermatmul_tc_supported(d, kp)) return TSVM_ERR_UNSUPPORTED;
   if (split < kSplitNone || split > kSplitPA || ni < 1 || nj < 1) return TSVM_ERR_INVALID_ARGUMENT;
   if (deriv && split != kSplitPA) return TSVM_ERR_UNSUPPORTED;
@@ -983,21 +1097,34 @@ tsvm_status kermatmul_tc_core(tsvm_context *ctx, const float *XI, const float *y
   const unsigned grid = (unsigned)(nrb < ctx->num_sms ? nrb : ctx->num_sms);
   cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
   TSVM_CUDA(cudaEventRecord(e0, ctx->stream));
+  // More than 256 columns: one launch in 32-row units when the nonzero columns (kw, rounded to
+  // 16) fit 416 TMEM columns, else column slabs of at most 256 that each recompute S and P.
+  const int kw16 = (int)round_up(kw > 0 && kw < kp ? kw : kp, 16);
+  const bool half = !deriv && kp > kMaxSlab && kw16 <= kMaxHalfW;
+  const CUtensorMapDataType at_type =
+      bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
   for (int c0 = 0; c0 < kp; c0 += kMaxSlab) {
-    const int kpw = kp - c0 < kMaxSlab ? kp - c0 : kMaxSlab;
+    const int kpw = half ? kw16 : kp - c0 < kMaxSlab ? kp - c0 : kMaxSlab;
     CUtensorMap mat, matlo;
-    const CUtensorMapDataType at_type =
-        bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
-    if (!make_map(&mat, AT, at_type, kBJ, (uint64_t)ntiles * kp, kBJ, kpw) ||
-        !make_map(&matlo, ATlo ? ATlo : AT, at_type, kBJ, (uint64_t)ntiles * kp, kBJ, kpw))
+    if (half) {   // boxes of one 32-row K slice x kpw / 2 rows, 64-byte swizzle
+      if (!make_map(&mat, AT, at_type, kBJ, (uint64_t)ntiles * kp, 32, kpw / 2,
+                    CU_TENSOR_MAP_SWIZZLE_64B) ||
+          !make_map(&matlo, ATlo ? ATlo : AT, at_type, kBJ, (uint64_t)ntiles * kp, 32, kpw / 2,
+                    CU_TENSOR_MAP_SWIZZLE_64B))
+        return TSVM_ERR_CUDA;
+    } else if (!make_map(&mat, AT, at_type, kBJ, (uint64_t)ntiles * kp, kBJ, kpw) ||
+               !make_map(&matlo, ATlo ? ATlo : AT, at_type, kBJ, (uint64_t)ntiles * kp, kBJ,
+                         kpw)) {
       return TSVM_ERR_CUDA;
-    const size_t smem = tc_smem(KG, kpw);
-    auto kern = select_kernel(bf16, poly_split(), KG, hshift != 0.f, split, deriv);
+    }
+    const size_t smem = tc_smem(KG, kpw, half);
+    auto kern = select_kernel(bf16, poly_split(), KG, hshift != 0.f, split, deriv, half);
     if (!kern) return TSVM_ERR_UNSUPPORTED;
     TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<grid, kThreadsTC, smem, ctx->stream>>>(mxa, mxb, mat, matlo, yI, scale + 1, ccol, ni,
                                                   nrb, ntiles, kp, c0, kpw, tri, W, kp, err);
     TSVM_LAUNCHED(ctx);
+    if (half) break;
   }
   TSVM_CUDA(cudaEventRecord(e1, ctx->stream));
   int herr = 0;

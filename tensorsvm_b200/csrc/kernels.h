@@ -47,11 +47,13 @@ bool kermatmul_tc_supported(int d, int kp);
 // Tensor-core (tcgen05) version; precision TSVM_PREC_FP16 or TSVM_PREC_BF16 for P and A.
 // round_back (may be A itself, or null) receives A rounded to the 16-bit operand type.
 // split: 0 one product; 1 the kernel block P as hi + lo (two products); 2 the operand A as
-// hi + lo (two products).
+// hi + lo (two products).  kw (0: kp): the columns of A that may be nonzero (the rest are zero);
+// above 256 columns, when kw rounded up to 16 is at most 416 the product runs as one launch
+// (else in column slabs of 256 that each recompute the kernel block).
 tsvm_status kermatmul_tc(tsvm_context *ctx, const float *Xc, const float *norms, const float *y,
                          int64_t n, int d, double gamma, const float *A, int kp, float *W,
                          int precision, float *kernel_ms, float *round_back = nullptr,
-                         int split = 0, int64_t row0 = 0, int64_t nr = -1);
+                         int split = 0, int64_t row0 = 0, int64_t nr = -1, int kw = 0);
 
 // W (ni x kp) = Y_I K(X_I, X_J) Y_J A on the tensor cores, I rows XI (ni x d) and J rows XJ
 // (nj x d; A nj x kp), both centred by the same vector; null labels mean all ones; XI may be XJ.
@@ -61,7 +63,7 @@ tsvm_status kermatmul_tc_core(tsvm_context *ctx, const float *XI, const float *y
                               const float *XJ, const float *yJ, int64_t nj, int d, double gamma,
                               const float *A, int kp, float *W, int precision, float *kernel_ms,
                               float *round_back, int split, bool deriv, double *sym = nullptr,
-                              bool reuse_gram = false);
+                              bool reuse_gram = false, int kw = 0);
 
 // Half product for a symmetric projection (same rows on both sides): R = Y (K o H) Y A with
 // H_ij = 1 (j > i), 1/2 (j == i), 0 (j < i), so that A^T (Y K Y) A = A^T R + R^T A + s u u^T with
@@ -72,7 +74,7 @@ tsvm_status kermatmul_tc_core(tsvm_context *ctx, const float *XI, const float *y
 tsvm_status kermatmul_tc_half(tsvm_context *ctx, const float *Xc, const float *y, int64_t n, int d,
                               double gamma, const float *A, int kp, float *R, int precision,
                               float *kernel_ms, float *round_back, int split, double *sym,
-                              bool reuse_gram = false);
+                              bool reuse_gram = false, int kw = 0);
 
 // Kernel-vector products of the hypergradient (hypergrad.cu): out (na x nu, FP64) =
 // [K or K' = -||a - b||^2 K](A, B) U with U nb x nu FP64, on the SIMT kernel or the tensor cores.
@@ -120,7 +122,8 @@ tsvm_status apply_right_fp32(tsvm_context *ctx, const float *A, int64_t n, int k
 // or the 1-based failing column.  Dinv (ceil(n/32) blocks of 32 x 32 doubles) receives the
 // inverses of the diagonal 32 x 32 blocks of L, used by potrs_fp64 and trinv_lower_fp64.
 // The upper triangle is left untouched.
-tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_dev, double *Dinv);
+tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_dev, double *Dinv,
+                      cudaStream_t stream = nullptr);
 // Dinv of an existing lower factor L (as chol_fp64 writes it).
 tsvm_status tri_diag_inverse(tsvm_context *ctx, const double *L, int n, int lda, double *Dinv);
 // Solve (L L^T) X = B for nrhs (<= 4) right-hand sides stored as rows of B (nrhs x ldb).

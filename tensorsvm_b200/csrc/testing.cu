@@ -59,7 +59,14 @@ tsvm_status tsvm_test_kprod(tsvm_context *ctx, const float *A, int64_t na, const
 tsvm_status tsvm_test_kermatmul(tsvm_context *ctx, const float *X, const float *y, int64_t n,
                                 int32_t d, double gamma, const float *A, int32_t kp, float *W,
                                 int32_t precision, int32_t split) {
+  return tsvm_test_kermatmul_cols(ctx, X, y, n, d, gamma, A, kp, 0, W, precision, split);
+}
+
+tsvm_status tsvm_test_kermatmul_cols(tsvm_context *ctx, const float *X, const float *y, int64_t n,
+                                     int32_t d, double gamma, const float *A, int32_t kp,
+                                     int32_t kw, float *W, int32_t precision, int32_t split) {
   if (!ctx || !X || !y || !A || !W || n < 1 || d < 1 || kp < 1) return TSVM_ERR_INVALID_ARGUMENT;
+  if (kw < 0 || kw > kp) return TSVM_ERR_INVALID_ARGUMENT;
   if (!precision_valid(precision) || split < 0 || split > 2) return TSVM_ERR_INVALID_ARGUMENT;
   float *Xc = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_XC, (size_t)n * d + (size_t)n + 64, &Xc));
@@ -71,7 +78,7 @@ tsvm_status tsvm_test_kermatmul(tsvm_context *ctx, const float *X, const float *
   } else {
     if (!kermatmul_tc_supported(d, kp)) return TSVM_ERR_UNSUPPORTED;
     TSVM_TRY(kermatmul_tc(ctx, Xc, norms, y, n, d, gamma, A, kp, W, precision, &ms, nullptr,
-                          split));
+                          split, 0, -1, kw));
   }
   TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
   return TSVM_OK;
@@ -80,7 +87,15 @@ tsvm_status tsvm_test_kermatmul(tsvm_context *ctx, const float *X, const float *
 tsvm_status tsvm_test_kermatmul_half(tsvm_context *ctx, const float *X, const float *y, int64_t n,
                                      int32_t d, double gamma, const float *A, int32_t kp,
                                      float *R, double *sym, int32_t precision, int32_t split) {
-  if (!ctx || !X || !y || !A || !R || !sym || n < 1 || d < 1 || kp < 1)
+  return tsvm_test_kermatmul_half_cols(ctx, X, y, n, d, gamma, A, kp, 0, R, sym, precision,
+                                       split);
+}
+
+tsvm_status tsvm_test_kermatmul_half_cols(tsvm_context *ctx, const float *X, const float *y,
+                                          int64_t n, int32_t d, double gamma, const float *A,
+                                          int32_t kp, int32_t kw, float *R, double *sym,
+                                          int32_t precision, int32_t split) {
+  if (!ctx || !X || !y || !A || !R || !sym || n < 1 || d < 1 || kp < 1 || kw < 0 || kw > kp)
     return TSVM_ERR_INVALID_ARGUMENT;
   if (!precision_valid(precision) || precision == TSVM_PREC_FP32 || split < 0 || split > 2)
     return TSVM_ERR_INVALID_ARGUMENT;
@@ -91,7 +106,7 @@ tsvm_status tsvm_test_kermatmul_half(tsvm_context *ctx, const float *X, const fl
   TSVM_TRY(centre_features(ctx, X, n, d, Xc, norms));
   float ms = 0.f;
   TSVM_TRY(kermatmul_tc_half(ctx, Xc, y, n, d, gamma, A, kp, R, precision, &ms, nullptr, split,
-                             sym));
+                             sym, false, kw));
   TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
   return TSVM_OK;
 }
