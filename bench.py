@@ -655,6 +655,22 @@ def run_workload(args, world, rank, local):
     return line
 
 
+def run_other_workloads(args, local):
+    """The wide-feature, batched-grid and hypergradient lines (their full-size workloads, three
+    warm-up and up to three timed steps each), nested in the default line so that one run
+    records all of them; a workload that fails records its error instead."""
+    import copy
+    out = {}
+    for name in ("wide", "grid", "hypergrad"):
+        sub = copy.copy(args)
+        sub.workload, sub.n, sub.steps, sub.warmup = name, N_DEFAULT, min(args.steps, 3), 3
+        try:
+            out[name] = run_workload(sub, 1, 0, local)
+        except Exception as e:   # keep the headline line whatever happens here
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+    return out
+
+
 # ------------------------------------------------------------------------------------------
 # reference arm: the reference trainer built from its own source (oracle/_ref)
 # ------------------------------------------------------------------------------------------
@@ -772,6 +788,9 @@ def main():
                     help="reference arm: seconds of full-size reference runs (at least one run)")
     ap.add_argument("--factor-threads", type=int, default=4,
                     help="grid workload: host threads (one context each) for the 64 factors")
+    ap.add_argument("--no-workloads", dest="workloads", action="store_false",
+                    help="default line at N=1: skip the wide / grid / hypergrad lines that are "
+                         "otherwise appended under 'workloads'")
     ap.add_argument("--workload", default="two_gaussians", choices=["two_gaussians", "wide", "grid", "hypergrad"],
                     help="two_gaussians (default): the benchmark line; wide: n=500k d=54 k=400; "
                          "grid: 64-problem batched (C, gamma) grid; hypergrad: validation-loss "
@@ -784,6 +803,8 @@ def main():
         line = run_reference(args, world, rank)
     else:
         line = run_ours(args, world, rank, local)
+        if line is not None and world == 1 and args.workloads:
+            line["workloads"] = run_other_workloads(args, local)
     if line is not None and rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -258,7 +258,9 @@ def flat_kernel_oracle():
     return X, y, g, C, k, f.eigvals, r.log[-1][5], fv
 
 
-@pytest.mark.parametrize("prec,pobj_tol,eig_tol", [("fp16", 5e-5, 0.01), ("bf16", 1e-3, 0.05),
+# fp16 is held to the bar of the tensor-core form (objective 1e-5; measured 6.8e-6 with the
+# one-launch wide kernel, eigenvalue 0.05160 against 0.05163); bf16 measured 5.5e-5
+@pytest.mark.parametrize("prec,pobj_tol,eig_tol", [("fp16", 1e-5, 0.01), ("bf16", 1e-4, 0.05),
                                                    ("fp16_fast", 3e-4, 0.05),
                                                    ("bf16_fast", 5e-2, 0.7)])
 def test_flat_kernel_tensor_core_against_fp64_oracle(ctx, flat_kernel_oracle, prec, pobj_tol,
