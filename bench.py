@@ -512,8 +512,13 @@ def run_grid(args, ctx, stream):
         # every problem's factor through its projection, the 64 eigenproblems in one launch,
         # then the batched IPM
         Zs = api.factor_batched(ctx, Xs, ys, gs, k, args.precision)[0]
-        _, t_ipm = _timed(stream, lambda: api.ipm_batched(ctx, Zs, ys, k, Cs, rel_gap_tol=1e-6))
+        _, t_ipm = _timed(stream, lambda: api.ipm_batched(ctx, Zs, ys, k, Cs, rel_gap_tol=1e-6,
+                                                          precision=ipm_prec))
         return Zs, t_ipm
+
+    # the 16-bit forms' mixed-precision capacitance matrices in the batched and the one-by-one
+    # solves alike
+    ipm_prec = _lib.PREC_FP32 if args.precision == "fp32" else _lib.PREC_BF16
 
     def sequential(Zs, prec):
         out = []
@@ -539,8 +544,9 @@ def run_grid(args, ctx, stream):
     _, t_fac_thr = _timed(stream, lambda: factors_parallel(args.precision))
     factors(args.precision)   # the main context's scratch, sized before it is timed
     _, t_fac_seq = _timed(stream, lambda: factors(args.precision))
-    (alphas, bstats, info) = api.ipm_batched(ctx, Zs, ys, k, Cs, rel_gap_tol=1e-6)
-    seq_stats, t_seq_ipm = _timed(stream, lambda: sequential(Zs, _lib.PREC_BF16))
+    (alphas, bstats, info) = api.ipm_batched(ctx, Zs, ys, k, Cs, rel_gap_tol=1e-6,
+                                             precision=ipm_prec)
+    seq_stats, t_seq_ipm = _timed(stream, lambda: sequential(Zs, ipm_prec))
     del Zs
     t_fac32 = t_ipm32 = None
     if args.fp32_form:
@@ -553,7 +559,8 @@ def run_grid(args, ctx, stream):
                             "d": 28, "k": k, "precision": args.precision,
                             "factor_threads": nthreads})
     line.update({
-        "dtype": f"{args.precision} kernel-block product, f32/f64 IPM",
+        "dtype": f"{args.precision} kernel-block product; IPM f64 vectors, capacitance matrices "
+                 f"{'bf16 hi+lo tensor-core + exact f64 rows, refined' if ipm_prec != _lib.PREC_FP32 else 'f64'}",
         "phases_s": {"factors": round(t_fac, 3), "factors_one_thread": round(t_fac_seq, 3),
                      "factors_threads": round(t_fac_thr, 3),
                      "batched_ipm": round(statistics.mean(ipm_times), 3),

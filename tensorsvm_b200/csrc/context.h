@@ -43,6 +43,9 @@ enum Slot : int {
   SLOT_B_M,           // batched IPM: per-problem capacitance matrices and factors
   SLOT_B_GPART,       // batched IPM: per-unit partial Gram matrices
   SLOT_B_PART,        // batched IPM: per-unit streaming partial sums
+  SLOT_B_SYRK,        // batched mixed IPM: per-unit tensor-core partials, error flag, exact-row
+                      // counts, per-problem tau
+  SLOT_B_IDX,         // batched mixed IPM: exactly summed rows of every unit
   SLOT_HG_OMEGA,      // hypergradient: copy of the factor's sketch
   SLOT_HG_R,          // hypergradient: combined CholeskyQR factor and k-vectors
   SLOT_HG_KPART,      // hypergradient: per-split partial kernel-vector products

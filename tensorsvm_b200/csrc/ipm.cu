@@ -37,7 +37,9 @@ enum ScalarIdx : int {
   I_C = 0, I_N, I_Y, I_MU, I_RP, I_DMAX, I_DMIN, I_COND, I_SUMX, I_SUMXI,
   I_NORMRD, I_XQX, I_POBJ, I_DOBJ, I_RELGAP,
   I_ATR7, I_ATB, I_DYA, I_ALPHA_AFF, I_MUAFF, I_SIGMA, I_ATR7C, I_DYC, I_ALPHA,
-  I_E2SUM, I_E2SQ, I_INFO, I_RESMAX, I_RESPREV, I_COUNT
+  I_E2SUM, I_E2SQ, I_INFO, I_RESMAX, I_RESPREV,
+  I_TAU, I_TAUIT,   // batched mixed-precision solves: the iteration's tau, iterations counted
+  I_COUNT
 };
 constexpr int kNScal = 32;
 
@@ -719,10 +721,10 @@ stream_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, Op op,
 // c = h0 - (g + w) (the residual h0 - M g of the capacitance solve, M g = g + Z^T D^-1 Z g);
 // with `record`, the relative residual max_r ||c_r|| / ||h0_r|| goes into I_RESMAX, and a value
 // above 0.5 (refinement cannot be trusted to converge) marks the iteration as failed.
-__global__ void refine_resid_kernel(const double *__restrict__ h0, const double *__restrict__ g,
-                                    const double *__restrict__ w, double *__restrict__ c, int R,
-                                    int kz, int k, double *__restrict__ sc, int *__restrict__ info,
-                                    int record) {
+__device__ void refine_resid_block(const double *__restrict__ h0, const double *__restrict__ g,
+                                   const double *__restrict__ w, double *__restrict__ c, int R,
+                                   int kz, int k, double *__restrict__ sc, int *__restrict__ info,
+                                   int record) {
   __shared__ double red[2][8];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double worst = 0.0;
@@ -760,6 +762,48 @@ __global__ void refine_resid_kernel(const double *__restrict__ h0, const double 
       sc[I_INFO] = -1.0;
     }
   }
+}
+
+__global__ void refine_resid_kernel(const double *__restrict__ h0, const double *__restrict__ g,
+                                    const double *__restrict__ w, double *__restrict__ c, int R,
+                                    int kz, int k, double *__restrict__ sc, int *__restrict__ info,
+                                    int record) {
+  refine_resid_block(h0, g, w, c, R, kz, k, sc, info, record);
+}
+
+// The same per problem of a batch (block p; R kz entries per problem).
+__global__ void refine_resid_batched(const double *__restrict__ h0, const double *__restrict__ g,
+                                     const double *__restrict__ w, double *__restrict__ c, int R,
+                                     int kz, int k, double *__restrict__ sc, int *__restrict__ info,
+                                     const int *__restrict__ active) {
+  const int p = blockIdx.x;
+  if (active && !active[p]) return;
+  const size_t o = (size_t)p * R * kz;
+  refine_resid_block(h0 + o, g + o, w + o, c + o, R, kz, k, sc + (size_t)p * kNScal, info + p, 1);
+}
+
+// tau of each problem of a batched mixed-precision solve, as the single-problem solver adapts
+// it: 64 at the first iteration; after a failed step (Cholesky or refinement, the step not
+// taken) tau / 64 (0 below 1e-6: every row exact); else / 8 above a refinement residual of 1e-4
+// and x 2 below 1e-6.  Also kept in the problem's scalars (I_TAU) for the host.
+__global__ void tau_update_batched(double *__restrict__ sc, double *__restrict__ taus, int P,
+                                   const int *__restrict__ active) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P || (active && !active[p])) return;
+  double *s = sc + (size_t)p * kNScal;
+  double tau = taus[p];
+  if (s[I_TAUIT] == 0.0) {
+    tau = 64.0;
+  } else if (s[I_INFO] != 0.0) {
+    tau = tau > 1e-6 ? tau / 64.0 : 0.0;
+  } else {
+    const double r = s[I_RESPREV];
+    if (r > 1e-4) tau /= 8.0;
+    else if (r < 1e-6 && tau < 1e30) tau *= 2.0;
+  }
+  taus[p] = tau;
+  s[I_TAU] = tau;
+  s[I_TAUIT] += 1.0;
 }
 
 __global__ void kvec_add(double *__restrict__ g, const double *__restrict__ c, int count) {
@@ -1711,6 +1755,30 @@ __global__ void gram_units_reduce(const double *__restrict__ part, const int *__
   Mp[(int64_t)c * k + r] = s;
 }
 
+// Mixed-precision capacitance matrices of a batch: M_p = I + sum over the units of p of the
+// tensor-core partials (FP32, KP x KP, lower block strips) and the exactly summed rows' partials
+// (FP64, k x k, lower tiles), in unit order; NaN if a tensor-core block timed out.
+__global__ void mixed_units_reduce(const float *__restrict__ part_tc, int KP,
+                                   const double *__restrict__ part64, const int *__restrict__ ubeg,
+                                   int k, const int *__restrict__ active,
+                                   const int *__restrict__ err, double *__restrict__ M,
+                                   int64_t strideM) {
+  const int p = blockIdx.y;
+  if (active && !active[p]) return;
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)k * k) return;
+  const int r = (int)(e / k), c = (int)(e % k);
+  if (c > r) return;
+  double s = r == c ? 1.0 : 0.0;
+  for (int u = ubeg[p]; u < ubeg[p + 1]; ++u)
+    s += (double)part_tc[(int64_t)u * KP * KP + (int64_t)r * KP + c] +
+         part64[(int64_t)u * k * k + (int64_t)r * k + c];
+  if (*err) s = NAN;
+  double *Mp = M + p * strideM;
+  Mp[(int64_t)r * k + c] = s;
+  Mp[(int64_t)c * k + r] = s;
+}
+
 // Stages and shared memory of one streaming pass (see Runner::pass_launch).
 template <int MODE, int R, int CR, int LPR, int CPL>
 void stream_config(int64_t ldz, size_t *stages_out, size_t *smem_out) {
@@ -1768,6 +1836,27 @@ struct BRunner {
   template <class Op>
   tsvm_status zw(const Op &op, const double *w, int stage) {
     return pass<MODE_ZW, Op, Op::R>(op, w, nullptr, stage);
+  }
+  // per problem: w_p = Z_p^T D_p^-1 Z_p g_p for R vectors (R kz entries per problem)
+  template <int R>
+  tsvm_status zgz(const double *g, double *w) {
+    return pass<MODE_ZGZ, GramVecOp, R>(GramVecOp{}, g, w, ST_NONE);
+  }
+  // One refinement sweep of every problem's capacitance solve M_p g_p = h0_p against the exact
+  // operator (M~_p factored in M, one CTA per problem): g_p += M~_p^-1 (h0_p - g_p - w_p).
+  template <int R>
+  tsvm_status refine(const double *M, int64_t strideM, const double *Mdinv, const double *h0,
+                     double *g, double *w, double *c) {
+    TSVM_TRY(zgz<R>(g, w));
+    refine_resid_batched<<<P, 256, 0, ctx->stream>>>(h0, g, w, c, R, geo.kz, k, scal, info,
+                                                      active);
+    TSVM_LAUNCHED(ctx);
+    TSVM_TRY(potrs_fp64_batched(ctx, M, k, k, strideM, Mdinv, strideM, c, R, geo.kz,
+                                (int64_t)R * geo.kz, P, active));
+    kvec_add<<<(unsigned)ceil_div((int64_t)P * R * geo.kz, 256), 256, 0, ctx->stream>>>(
+        g, c, P * R * geo.kz);
+    TSVM_LAUNCHED(ctx);
+    return TSVM_OK;
   }
   template <class Op>
   tsvm_status vec(const Op &op, int stage) {
@@ -1843,9 +1932,27 @@ tsvm_status ipm_solve_batched(tsvm_context *ctx, const tsvm_ipm_problem *pr, int
   int *d_info =
       reinterpret_cast<int *>(tab + al(tb_units) + al(tb_ubeg) + al(tb_z) + al(tb_act));
 
+  // Mixed-precision capacitance matrices (16-bit precisions, k <= 256): per unit, the rows with
+  // dinv <= tau_p through the fused tensor-core SYRK and the others exactly in FP64; every
+  // capacitance solve refined once against the exact operator; tau_p adapted on the device.
+  const bool mixed = opt.precision != TSVM_PREC_FP32 && syrk_tc_supported(k) && k >= 32 &&
+                     k <= 256 && ldz <= syrk_units_kp(k) && ldz % 4 == 0;
+  const int KPs = syrk_units_kp(k);
   double *vec = nullptr, *sbuf = nullptr, *Mall = nullptr, *gpart = nullptr, *part = nullptr;
   TSVM_TRY(scratch_t(ctx, SLOT_B_VEC, (size_t)11 * N + (size_t)N / 2 + 8, &vec));
-  TSVM_TRY(scratch_t(ctx, SLOT_B_SCAL, (size_t)P * (kNScal + 3 * kz), &sbuf));
+  TSVM_TRY(scratch_t(ctx, SLOT_B_SCAL, (size_t)P * (kNScal + (mixed ? 9 : 3) * kz), &sbuf));
+  float *part_tc = nullptr;
+  int *syrk_err = nullptr, *xcounts = nullptr;
+  double *taus = nullptr;
+  int64_t *xidx = nullptr;
+  if (mixed) {
+    const size_t ntc = (size_t)max_units * KPs * KPs;
+    TSVM_TRY(scratch_t(ctx, SLOT_B_SYRK, ntc + 64 + (size_t)max_units + 2 * (size_t)P, &part_tc));
+    syrk_err = reinterpret_cast<int *>(part_tc + ntc);
+    xcounts = syrk_err + 16;
+    taus = reinterpret_cast<double *>(part_tc + ntc + 32 + (((size_t)max_units + 1) & ~(size_t)1));
+    TSVM_TRY(scratch_t(ctx, SLOT_B_IDX, (size_t)N, &xidx));
+  }
   const int64_t strideD = (int64_t)ceil_div(k, 32) * 1024;
   const int64_t strideM = (int64_t)k * k + strideD;
   TSVM_TRY(scratch_t(ctx, SLOT_B_M, (size_t)P * strideM, &Mall));
@@ -1853,6 +1960,8 @@ tsvm_status ipm_solve_batched(tsvm_context *ctx, const tsvm_ipm_problem *pr, int
   TSVM_TRY(scratch_t(ctx, SLOT_B_PART, (size_t)max_units * (2 * kz + 16), &part));
   float *labels = reinterpret_cast<float *>(vec + (size_t)11 * N);
   double *scal = sbuf, *q = sbuf + (size_t)P * kNScal, *h = q + (size_t)P * kz;
+  // mixed: copies of the right-hand sides, Z^T D^-1 Z g and the corrections (2 kz per problem)
+  double *h0 = h + (size_t)P * 2 * kz, *wv = h0 + (size_t)P * 2 * kz, *cv = wv + (size_t)P * 2 * kz;
 
   Vecs V;
   V.x = vec;
@@ -1886,6 +1995,7 @@ tsvm_status ipm_solve_batched(tsvm_context *ctx, const tsvm_ipm_problem *pr, int
   TSVM_CUDA(cudaMemsetAsync(d_info, 0, tb_info, ctx->stream));
   TSVM_CUDA(cudaMemcpyAsync(scal, hsc.data(), sizeof(double) * hsc.size(), cudaMemcpyHostToDevice,
                             ctx->stream));
+  if (mixed) TSVM_CUDA(cudaMemsetAsync(syrk_err, 0, sizeof(int), ctx->stream));
 
   BRunner br;
   br.ctx = ctx;
@@ -1977,20 +2087,42 @@ tsvm_status ipm_solve_batched(tsvm_context *ctx, const tsvm_ipm_problem *pr, int
   double *M = Mall;
   double *Mdinv_base = Mall + (size_t)k * k;
   auto body = [&]() -> tsvm_status {
-    TSVM_TRY(gram_fp64_units(ctx, d_z, ldz, k, d_units, br.nunits, d_active, V.dinv, gpart));
-    gram_units_reduce<<<dim3((unsigned)ceil_div((int64_t)k * k, 256), P), 256, 0, ctx->stream>>>(
-        gpart, d_ubeg, k, d_active, M, strideM);
+    if (mixed) {
+      tau_update_batched<<<(unsigned)ceil_div(P, 128), 128, 0, ctx->stream>>>(scal, taus, P,
+                                                                               d_active);
+      TSVM_LAUNCHED(ctx);
+      TSVM_TRY(big_rows_units(ctx, V.dinv, d_units, br.nunits, d_active, taus, xidx, xcounts));
+      TSVM_TRY(gram_fp64_units(ctx, d_z, ldz, k, d_units, br.nunits, d_active, V.dinv, gpart,
+                               xidx, xcounts));
+      TSVM_TRY(syrk_units_tc(ctx, d_z, ldz, k, d_units, br.nunits, d_active, V.dinv, taus,
+                             part_tc, syrk_err));
+      mixed_units_reduce<<<dim3((unsigned)ceil_div((int64_t)k * k, 256), P), 256, 0,
+                           ctx->stream>>>(part_tc, KPs, gpart, d_ubeg, k, d_active, syrk_err, M,
+                                          strideM);
+    } else {
+      TSVM_TRY(gram_fp64_units(ctx, d_z, ldz, k, d_units, br.nunits, d_active, V.dinv, gpart));
+      gram_units_reduce<<<dim3((unsigned)ceil_div((int64_t)k * k, 256), P), 256, 0,
+                          ctx->stream>>>(gpart, d_ubeg, k, d_active, M, strideM);
+    }
     TSVM_LAUNCHED(ctx);
     TSVM_TRY(chol_fp64_batched(ctx, M, k, k, strideM, d_info, Mdinv_base, strideM, P, d_active));
     TSVM_TRY(br.zt(SmwRhs2Op{V}, h, ST_NONE));
+    if (mixed)
+      TSVM_CUDA(cudaMemcpyAsync(h0, h, sizeof(double) * P * 2 * kz, cudaMemcpyDeviceToDevice,
+                                ctx->stream));
     TSVM_TRY(potrs_fp64_batched(ctx, M, k, k, strideM, Mdinv_base, strideM, h, 2, kz,
                                 (int64_t)2 * kz, P, d_active));
+    if (mixed) TSVM_TRY(br.refine<2>(M, strideM, Mdinv_base, h0, h, wv, cv));
     TSVM_TRY(br.zw(SmwBack2Op{V}, h, ST_DYA));
     TSVM_TRY(br.vec(AffineOp{V, 0.0, 0.0}, ST_ALPHA_AFF));
     TSVM_TRY(br.vec(MuAffOp{V, 0.0, 0.0}, ST_SIGMA));
     TSVM_TRY(br.zt(CorrRhsOp{V, 0.0, 0.0}, h, ST_NONE));
+    if (mixed)
+      TSVM_CUDA(cudaMemcpyAsync(h0, h, sizeof(double) * P * kz, cudaMemcpyDeviceToDevice,
+                                ctx->stream));
     TSVM_TRY(potrs_fp64_batched(ctx, M, k, k, strideM, Mdinv_base, strideM, h, 1, kz, kz, P,
                                 d_active));
+    if (mixed) TSVM_TRY(br.refine<1>(M, strideM, Mdinv_base, h0, h, wv, cv));
     TSVM_TRY(br.zw(CorrBackOp{V}, h, ST_DYC));
     TSVM_TRY(br.vec(CombineOp{V, 0.0, 0.0, 0.0}, ST_ALPHA));
     TSVM_TRY(br.vec(UpdateOp{V, 0.0, true}, ST_NONE));
@@ -2030,7 +2162,10 @@ tsvm_status ipm_solve_batched(tsvm_context *ctx, const tsvm_ipm_problem *pr, int
       const double scale = 1.0 + sqrt((double)pr[p].n);
       const double nrd = sp[I_NORMRD], nrp = fabs(sp[I_RP]);
       int st = -1;
-      if (iter > 0 && sp[I_INFO] != 0.0) st = TSVM_ERR_NOT_SPD;
+      // a failed step (Cholesky, or the refinement of the mixed form) ends the problem, unless
+      // the mixed form can retry it with more rows summed exactly (the step was not taken; the
+      // device divides tau by 64, down to 0)
+      if (iter > 0 && sp[I_INFO] != 0.0 && !(mixed && sp[I_TAU] > 0.0)) st = TSVM_ERR_NOT_SPD;
       if (st < 0 && t_gap[p] < 0 && sp[I_RELGAP] <= 1e-6 && nrd / scale <= 1e-6 &&
           nrp / scale <= 1e-6)
         t_gap[p] = tnow;

@@ -109,10 +109,12 @@ tsvm_status gram_fp64_rows(tsvm_context *ctx, const float *A, int64_t lda, int64
                            double *G);
 // Per-unit partial Gram matrices of a batch: part[u] (k x k, lower 64 x 64 tiles filled) =
 // sum over the unit's rows j of rowscale[goff + j] z_j z_j^T with z_j rows of Zs[p] (lda);
-// units of problems with active[p] == 0 are skipped.
+// units of problems with active[p] == 0 are skipped.  With rowidx and counts, only the
+// counts[u] rows rowidx[goff + i] (indices within the unit) of each unit are summed.
 tsvm_status gram_fp64_units(tsvm_context *ctx, const float *const *Zs, int64_t lda, int k,
                             const WorkUnit *units, int nunits, const int *active,
-                            const double *rowscale, double *part);
+                            const double *rowscale, double *part, const int64_t *rowidx = nullptr,
+                            const int *counts = nullptr);
 // Out (n x kp) = A (n x kp) * R (kp x kp, fp32 row-major). Out may alias A.
 tsvm_status apply_right_fp32(tsvm_context *ctx, const float *A, int64_t n, int kp,
                              const float *R, float *Out);
@@ -160,6 +162,17 @@ tsvm_status big_rows(tsvm_context *ctx, const double *dinv, int64_t n, double ta
 // M (k x k, fp64, full) = I + G64 + sum over rows with dinv <= tau of dinv_j z_j z_j^T, the
 // latter from a `ways`-term BF16 split on the tensor cores with FP32 accumulation.  G64 may be
 // null.  A timed-out tensor-core launch leaves NaN in M (the Cholesky then reports failure).
+// The batched form for k <= 256 (one window, 2-way split, ldz <= 256): per work unit u, the
+// rows with dinv <= taus[p] through the fused tensor-core SYRK into FP32 part_tc[u] (KP x KP,
+// KP = 128 for k <= 128 else 256), and the others listed in index order (rowidx[goff + i],
+// counts[u]) and summed exactly into FP64 part64[u] (k x k).  big_rows_units only lists.
+tsvm_status big_rows_units(tsvm_context *ctx, const double *dinv, const WorkUnit *units,
+                           int nunits, const int *active, const double *taus, int64_t *rowidx,
+                           int *counts);
+tsvm_status syrk_units_tc(tsvm_context *ctx, const float *const *Zs, int64_t ldz, int k,
+                          const WorkUnit *units, int nunits, const int *active,
+                          const double *dinv, const double *taus, float *part_tc, int *err);
+int syrk_units_kp(int k);
 tsvm_status syrk_capacitance_tc(tsvm_context *ctx, const float *Z, int ldz, int64_t n, int k,
                                 const double *dinv, double tau, int ways, const double *G64,
                                 double *M);

@@ -268,12 +268,31 @@ struct FusedCfg {
   static constexpr uint32_t kSmem = kBars + 256 + 1024;
 };
 
+// Work-unit mode (units non-null, the batched interior-point solve): block b sums the rows of
+// unit b alone -- Z = Zs[p] + row0 ldz, its rows, their weights at dinv + goff, the problem's own
+// tau -- into partial b; a block whose problem is inactive returns at once.
 template <int KP>
 __global__ void __launch_bounds__(kSyrkFusedThreads, 1)
 syrk_fused_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, int T,
                   const double *__restrict__ dinv, double tau, float *__restrict__ part,
-                  int *__restrict__ err) {
+                  int *__restrict__ err, const WorkUnit *__restrict__ units,
+                  const float *const *__restrict__ Zs, const double *__restrict__ taus,
+                  const int *__restrict__ active) {
   using Cfg = FusedCfg<KP>;
+  int t0, t1;
+  if (units) {
+    const WorkUnit u = units[blockIdx.x];
+    if (active && !active[u.p]) return;   // the whole block, before any barrier or TMEM
+    Z = Zs[u.p] + u.row0 * ldz;
+    n = u.rows;
+    dinv += u.goff;
+    tau = taus[u.p];
+    t0 = 0;
+    t1 = (int)((n + kSJ - 1) / kSJ);
+  } else {
+    t0 = (int)((int64_t)T * blockIdx.x / gridDim.x);
+    t1 = (int)((int64_t)T * (blockIdx.x + 1) / gridDim.x);
+  }
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   const uint32_t raw = su32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -289,8 +308,6 @@ syrk_fused_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, in
   const float *staging = reinterpret_cast<const float *>(sbase + Cfg::kStaging);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int G = gridDim.x;
-  const int t0 = (int)((int64_t)T * blockIdx.x / G), t1 = (int)((int64_t)T * (blockIdx.x + 1) / G);
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < Cfg::kHalves; ++s) {
@@ -573,6 +590,41 @@ big_rows_index(const double *__restrict__ dinv, int64_t n, double tau,
   }
 }
 
+// Batched form: block u lists the rows of work unit u with dinv > taus[p] (indices within the
+// unit, in index order) at rowidx + goff and their count in counts[u].
+__global__ void __launch_bounds__(256)
+big_rows_units_kernel(const double *__restrict__ dinv, const WorkUnit *__restrict__ units,
+                      const int *__restrict__ active, const double *__restrict__ taus,
+                      int64_t *__restrict__ rowidx, int *__restrict__ counts) {
+  __shared__ int wcnt[8];
+  const WorkUnit u = units[blockIdx.x];
+  if (active && !active[u.p]) {
+    if (threadIdx.x == 0) counts[blockIdx.x] = 0;
+    return;
+  }
+  const double tau = taus[u.p];
+  const double *dv = dinv + u.goff;
+  int64_t *idx = rowidx + u.goff;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int base = 0;   // the same in every thread: updated from the same shared counts
+  for (int b0 = 0; b0 < u.rows; b0 += 256) {
+    const int i = b0 + (int)threadIdx.x;
+    const bool f = i < u.rows && dv[i] > tau;
+    const unsigned bal = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) wcnt[warp] = __popc(bal);
+    __syncthreads();
+    int off = base;
+    for (int w = 0; w < warp; ++w) off += wcnt[w];
+    off += __popc(bal & ((1u << lane) - 1u));
+    if (f) idx[off] = i;
+    int tot = 0;
+    for (int w = 0; w < 8; ++w) tot += wcnt[w];
+    __syncthreads();
+    base += tot;
+  }
+  if (threadIdx.x == 0) counts[blockIdx.x] = base;
+}
+
 // Column windows for k > 256 (see the file comment).
 struct SyrkPlan {
   int ng = 1, nw = 1;
@@ -630,7 +682,23 @@ tsvm_status launch_syrk_fused(tsvm_context *ctx, const float *Z, int64_t ldz, in
   auto kern = syrk_fused_kernel<KP>;
   TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)Cfg::kSmem));
-  kern<<<G, kSyrkFusedThreads, Cfg::kSmem, ctx->stream>>>(Z, ldz, k, n, T, dinv, tau, part, err);
+  kern<<<G, kSyrkFusedThreads, Cfg::kSmem, ctx->stream>>>(Z, ldz, k, n, T, dinv, tau, part, err,
+                                                          nullptr, nullptr, nullptr, nullptr);
+  TSVM_LAUNCHED(ctx);
+  return TSVM_OK;
+}
+
+template <int KP>
+tsvm_status launch_syrk_fused_units(tsvm_context *ctx, const float *const *Zs, int64_t ldz,
+                                    int k, const WorkUnit *units, int nunits, const int *active,
+                                    const double *dinv, const double *taus, float *part,
+                                    int *err) {
+  using Cfg = FusedCfg<KP>;
+  auto kern = syrk_fused_kernel<KP>;
+  TSVM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)Cfg::kSmem));
+  kern<<<nunits, kSyrkFusedThreads, Cfg::kSmem, ctx->stream>>>(
+      nullptr, ldz, k, 0, 0, dinv, 0.0, part, err, units, Zs, taus, active);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;
 }
@@ -649,6 +717,30 @@ tsvm_status big_rows(tsvm_context *ctx, const double *dinv, int64_t n, double ta
   big_rows_index<<<nb, 256, 0, ctx->stream>>>(dinv, n, tau, counts, idx, count_dev);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;
+}
+
+tsvm_status big_rows_units(tsvm_context *ctx, const double *dinv, const WorkUnit *units,
+                           int nunits, const int *active, const double *taus, int64_t *rowidx,
+                           int *counts) {
+  if (nunits < 1) return TSVM_ERR_INVALID_ARGUMENT;
+  big_rows_units_kernel<<<nunits, 256, 0, ctx->stream>>>(dinv, units, active, taus, rowidx,
+                                                         counts);
+  TSVM_LAUNCHED(ctx);
+  return TSVM_OK;
+}
+
+int syrk_units_kp(int k) { return k <= 128 ? 128 : 256; }
+
+tsvm_status syrk_units_tc(tsvm_context *ctx, const float *const *Zs, int64_t ldz, int k,
+                          const WorkUnit *units, int nunits, const int *active,
+                          const double *dinv, const double *taus, float *part_tc, int *err) {
+  const int KP = syrk_units_kp(k);
+  if (!syrk_tc_supported(k) || k > 256 || ldz > KP || ldz % 4 != 0 || nunits < 1)
+    return TSVM_ERR_UNSUPPORTED;
+  return KP == 128 ? launch_syrk_fused_units<128>(ctx, Zs, ldz, k, units, nunits, active, dinv,
+                                                  taus, part_tc, err)
+                   : launch_syrk_fused_units<256>(ctx, Zs, ldz, k, units, nunits, active, dinv,
+                                                  taus, part_tc, err);
 }
 
 tsvm_status syrk_capacitance_tc(tsvm_context *ctx, const float *Z, int ldz, int64_t n, int k,

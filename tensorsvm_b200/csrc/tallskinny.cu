@@ -16,6 +16,27 @@ namespace {
 constexpr int kGT = 64;      // output tile edge
 constexpr int kGRows = 32;   // rows staged per step
 
+// One staged slab into a thread's 4 x 4 block of the tile (rows ty + 16 i, columns tx + 16 j).
+// DIAG (a diagonal tile of a symmetric product, of which only the lower triangle is used): the
+// blocks i < j lie wholly above the diagonal and are skipped, 6 of the 16 products a row.
+template <bool DIAG>
+__device__ __forceinline__ void gram_slab(const double (*As)[kGT], const double (*Bs)[kGT], int tx,
+                                          int ty, double (&acc)[4][4]) {
+#pragma unroll 8
+  for (int rr = 0; rr < kGRows; ++rr) {
+    double av[4], bv[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) av[i] = As[rr][ty + 16 * i];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) bv[j] = Bs[rr][tx + 16 * j];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (!DIAG || i >= j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+  }
+}
+
 // grid: (tile index, split).  Each block accumulates a 64x64 tile over rows [r0, r1).
 // Operands are converted to FP64 once, while staging 32-row slabs into shared memory (with the
 // optional row weight folded into the A side), so the inner loop is pure DFMA: each thread owns
@@ -47,8 +68,12 @@ gram_partial_kernel(const float *__restrict__ A, int64_t lda, const float *__res
     n = u.rows;
     rows_per_split = u.rows;
     rowscale += u.goff;
-  }
-  if (count) {  // row count on the device: split it evenly over gridDim.y
+    if (count) {   // only the unit's listed rows (indices within the unit) at rowidx + goff
+      n = count[blockIdx.y];
+      rows_per_split = n;
+      rowidx += u.goff;
+    }
+  } else if (count) {  // row count on the device: split it evenly over gridDim.y
     n = *count;
     rows_per_split = (n + gridDim.y - 1) / gridDim.y;
     rows_per_split = (rows_per_split + kGRows - 1) / kGRows * kGRows;
@@ -56,6 +81,8 @@ gram_partial_kernel(const float *__restrict__ A, int64_t lda, const float *__res
   const int64_t r0 = units ? 0 : (int64_t)blockIdx.y * rows_per_split;
   const int64_t r1 = min(n, r0 + rows_per_split);
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  // a tile on the diagonal of a symmetric product: only its lower triangle is read back
+  const bool diag = symmetric && ta == tb;
   double acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
@@ -73,18 +100,10 @@ gram_partial_kernel(const float *__restrict__ A, int64_t lda, const float *__res
       Bs[rr][c] = (in && b0 + c < kb) ? (double)B[row * ldb + b0 + c] : 0.0;
     }
     __syncthreads();
-#pragma unroll 8
-    for (int rr = 0; rr < kGRows; ++rr) {
-      double av[4], bv[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) av[i] = As[rr][ty + 16 * i];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) bv[j] = Bs[rr][tx + 16 * j];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
-    }
+    if (diag)
+      gram_slab<true>(As, Bs, tx, ty, acc);
+    else
+      gram_slab<false>(As, Bs, tx, ty, acc);
   }
   // partial layout: [split][ka][kb]
   double *P = part + (int64_t)blockIdx.y * ka * kb;
@@ -109,44 +128,86 @@ __global__ void gram_reduce_kernel(const double *__restrict__ part, int nsplit, 
   if (symmetric && a != b) G[(int64_t)b * kb + a] = s;
 }
 
+// Asynchronous 16-byte global -> shared copies (LDGSTS), grouped and waited on per stage.
+__device__ __forceinline__ void cp_async16(float *dst, const float *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                   (uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Out[I, 0:KP] = A[I, 0:kin] * R[0:kin, 0:KP]; CTA = 128 rows, KP (<= 256) output columns in
-// registers (8 x KPT per thread).  kin is a multiple of 16; R has leading dimension ldr.
+// registers (8 x KPT per thread).  kin is a multiple of 32; A's and R's rows start on 16-byte
+// boundaries (lda, ldr multiples of 4).  32-deep K slabs of A (row-major, padded rows) and R
+// are staged in two shared-memory stages by cp.async, the next slab in flight while the
+// current one is multiplied.  Out may be A itself: a CTA writes its rows after it has read all
+// of them, and no other CTA reads them.
+constexpr int kApTM = 32;            // K slab
+constexpr int kApAP = kApTM + 4;     // padded A row in shared memory (floats)
+template <int KPT>
+constexpr size_t apply_smem() {
+  return sizeof(float) * 2 * ((size_t)128 * kApAP + (size_t)kApTM * KPT * 16);
+}
+
 template <int KPT>
 __global__ void __launch_bounds__(256, 1)
 apply_right_kernel(const float *__restrict__ A, int64_t lda, int kin, int64_t n,
                    const float *__restrict__ R, int64_t ldr, float *Out, int64_t ldo) {
-  constexpr int KP = KPT * 16;
-  constexpr int TM = 16;
-  __shared__ __align__(16) float As[TM][128 + 4];
-  __shared__ __align__(16) float Rs[TM][KP];
+  constexpr int KP = KPT * 16, TM = kApTM, AP = kApAP;
+  extern __shared__ __align__(16) float apsm[];
+  float *const As0 = apsm;                    // [2][128][AP]
+  float *const Rs0 = apsm + 2 * 128 * AP;     // [2][TM][KP]
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   const int64_t i0 = (int64_t)blockIdx.x * 128;
+  auto load = [&](int stage, int m0) {
+    float *As = As0 + stage * 128 * AP;
+    float *Rs = Rs0 + stage * TM * KP;
+    for (int e = tid; e < 128 * (TM / 4); e += 256) {
+      const int r = e / (TM / 4), c4 = e % (TM / 4);
+      const int64_t gi = i0 + r;
+      float *dst = As + r * AP + 4 * c4;
+      if (gi < n)
+        cp_async16(dst, A + gi * lda + m0 + 4 * c4);
+      else
+        *reinterpret_cast<float4 *>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    for (int e = tid; e < TM * (KP / 4); e += 256) {
+      const int r = e / (KP / 4), c4 = e % (KP / 4);
+      cp_async16(Rs + r * KP + 4 * c4, R + (int64_t)(m0 + r) * ldr + 4 * c4);
+    }
+    cp_async_commit();
+  };
   float acc[8][KPT];
 #pragma unroll
   for (int r = 0; r < 8; ++r)
 #pragma unroll
     for (int c = 0; c < KPT; ++c) acc[r][c] = 0.f;
-  for (int m0 = 0; m0 < kin; m0 += TM) {
-    __syncthreads();
-    for (int e = tid; e < 128 * TM; e += 256) {
-      const int r = e / TM, c = e % TM;
-      const int64_t gi = i0 + r;
-      As[c][r] = gi < n ? A[gi * lda + m0 + c] : 0.f;
-    }
-    for (int e = tid; e < TM * KP / 4; e += 256) {
-      const int r = e / (KP / 4), c4 = e % (KP / 4);
-      reinterpret_cast<float4 *>(&Rs[r][0])[c4] =
-          reinterpret_cast<const float4 *>(R + (int64_t)(m0 + r) * ldr)[c4];
+  load(0, 0);
+  for (int m0 = 0, st = 0; m0 < kin; m0 += TM, st ^= 1) {
+    if (m0 + TM < kin) {
+      load(st ^ 1, m0 + TM);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
+    const float *As = As0 + st * 128 * AP;
+    const float *Rs = Rs0 + st * TM * KP;
 #pragma unroll 4
     for (int m = 0; m < TM; ++m) {
       float a[8];
 #pragma unroll
-      for (int r = 0; r < 8; ++r) a[r] = As[m][ty * 8 + r];
+      for (int r = 0; r < 8; ++r) a[r] = As[(ty * 8 + r) * AP + m];
 #pragma unroll
       for (int q = 0; q < KPT / 4; ++q) {
-        const float4 b = reinterpret_cast<const float4 *>(&Rs[m][q * 64])[tx];
+        const float4 b = reinterpret_cast<const float4 *>(Rs + m * KP + q * 64)[tx];
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
           acc[r][4 * q + 0] = fmaf(a[r], b.x, acc[r][4 * q + 0]);
@@ -156,8 +217,8 @@ apply_right_kernel(const float *__restrict__ A, int64_t lda, int kin, int64_t n,
         }
       }
     }
+    __syncthreads();   // this stage is read out before the next iteration refills it
   }
-  __syncthreads();  // all reads of this CTA's rows done before in-place writes
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
     const int64_t gi = i0 + ty * 8 + r;
@@ -172,7 +233,13 @@ apply_right_kernel(const float *__restrict__ A, int64_t lda, int kin, int64_t n,
 template <int KPT>
 tsvm_status launch_apply(tsvm_context *ctx, const float *A, int64_t lda, int kin, int64_t n,
                          const float *R, int64_t ldr, float *Out, int64_t ldo) {
-  apply_right_kernel<KPT><<<(unsigned)ceil_div(n, 128), 256, 0, ctx->stream>>>(
+  if (kin % kApTM != 0 || lda % 4 != 0 || ldr % 4 != 0 ||
+      (reinterpret_cast<uintptr_t>(A) & 15) != 0 || (reinterpret_cast<uintptr_t>(R) & 15) != 0)
+    return TSVM_ERR_UNSUPPORTED;
+  constexpr size_t smem = apply_smem<KPT>();
+  TSVM_CUDA(cudaFuncSetAttribute(apply_right_kernel<KPT>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  apply_right_kernel<KPT><<<(unsigned)ceil_div(n, 128), 256, smem, ctx->stream>>>(
       A, lda, kin, n, R, ldr, Out, ldo);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;
@@ -239,12 +306,14 @@ tsvm_status gram_fp64_rows(tsvm_context *ctx, const float *A, int64_t lda, int64
 
 tsvm_status gram_fp64_units(tsvm_context *ctx, const float *const *Zs, int64_t lda, int k,
                             const WorkUnit *units, int nunits, const int *active,
-                            const double *rowscale, double *part) {
+                            const double *rowscale, double *part, const int64_t *rowidx,
+                            const int *counts) {
   if (nunits < 1 || nunits > 65535) return TSVM_ERR_UNSUPPORTED;
+  if ((rowidx == nullptr) != (counts == nullptr)) return TSVM_ERR_INVALID_ARGUMENT;
   const int tiles = (int)ceil_div(k, kGT);
   const int ntiles = tiles * (tiles + 1) / 2;
   gram_partial_kernel<<<dim3(ntiles, nunits), 256, 0, ctx->stream>>>(
-      nullptr, lda, nullptr, lda, 0, k, k, tiles, 1, 0, rowscale, nullptr, nullptr, units, Zs,
+      nullptr, lda, nullptr, lda, 0, k, k, tiles, 1, 0, rowscale, rowidx, counts, units, Zs,
       active, part);
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;

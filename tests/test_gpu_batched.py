@@ -55,6 +55,31 @@ def test_batched_matches_single(ctx, grid, rel_gap_tol):
         assert len(set(sv.tolist()) ^ set(sv1.tolist())) <= max(1, len(sv1) // 1000)
 
 
+@pytest.mark.parametrize("rel_gap_tol", [0.0, 1e-6])
+def test_batched_mixed_matches_single_mixed(ctx, grid, rel_gap_tol):
+    """The 16-bit precisions' batched solve (per work unit the tensor-core capacitance matrix
+    of the rows with weight <= tau and the other rows exactly in FP64, one refinement sweep per
+    capacitance solve, tau adapted per problem on the device) against the single-problem mixed
+    solver on the same factors."""
+    Zs, ys, Cs, k = grid
+    alphas, stats, info = api.ipm_batched(ctx, Zs, ys, k, Cs, rel_gap_tol=rel_gap_tol,
+                                          precision=_lib.PREC_BF16)
+    assert info["graph_used"] == 1
+    for Z, y, C, a, s in zip(Zs, ys, Cs, alphas, stats):
+        a1, _, _, s1 = api.ipm(ctx, Z, y, k, C, rel_gap_tol=rel_gap_tol, precision=_lib.PREC_BF16)
+        assert s1["mixed_syrk"] == 1
+        assert s["status"] == s1["status_code"]
+        assert abs(s["iters"] - s1["iters"]) <= 1, (s["iters"], s1["iters"])
+        assert abs(s["pobj"] - s1["pobj"]) <= 1e-8 * max(1.0, abs(s1["pobj"]))
+        yh = y.cpu().numpy().astype(np.float64)
+        f = decision(Z, k, a.cpu().numpy(), yh)
+        f1 = decision(Z, k, a1.cpu().numpy(), yh)
+        assert np.max(np.abs(f - f1)) <= 1e-5 * max(1.0, np.max(np.abs(f1)))
+        sv, _ = orc.sv_sets(a.cpu().numpy(), C)
+        sv1, _ = orc.sv_sets(a1.cpu().numpy(), C)
+        assert len(set(sv.tolist()) ^ set(sv1.tolist())) <= max(1, len(sv1) // 1000)
+
+
 def test_batched_single_problem_and_launch_count(ctx, grid):
     Zs, ys, Cs, k = grid
     l0 = ctx.launches
