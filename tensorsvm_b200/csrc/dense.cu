@@ -384,6 +384,99 @@ __global__ void __launch_bounds__(1024) diag_inverse_kernel(const double *__rest
     Dinv[(int64_t)blockIdx.x * kNB * kNB + e] = Di[(e / kNB) * kDP + e % kNB];
 }
 
+// Cholesky of a matrix of at most 128 columns held entirely in shared memory (its lower
+// triangle, rows padded to n + 1 doubles), one CTA: per 32-column panel one warp factors the
+// diagonal block in registers and forms its inverse (diag_block_warp, the same as the general
+// kernels), then all warps form the panel below, L_ij = A_ij Di^T, and update the trailing lower
+// triangle (a warp a row, lane = column, the row's panel entries as broadcasts).  At this size
+// the general kernels' round trips to L2 between the phases cost more than the arithmetic
+// (148 against 187 us for chol_la_kernel at n = 128).  Writes L (lower part) and the Dinv blocks
+// as chol_kernel does; strideA / strideD / active allow one CTA per problem.
+constexpr int kCholSmallN = 128;
+constexpr int kCholSmallThreads = 512;
+__global__ void __launch_bounds__(kCholSmallThreads, 1)
+chol_small_kernel(double *__restrict__ A, int n, int lda, double *__restrict__ Dinv,
+                  int *__restrict__ info, int64_t strideA, int64_t strideD,
+                  const int *__restrict__ active) {
+  if (active && !active[blockIdx.x]) return;
+  A += blockIdx.x * strideA;
+  Dinv += blockIdx.x * strideD;
+  info += blockIdx.x;
+  extern __shared__ __align__(16) double S[];   // [n][n + 1]
+  __shared__ double Dg[kNB * kDP], Di[kNB * kDP], rdiag[kNB];
+  __shared__ int fail;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int kWarps = kCholSmallThreads / 32;
+  const int ld = n + 1;
+  if (tid == 0) fail = 0;
+  for (int e = tid; e < n * n; e += blockDim.x) {
+    const int r = e / n, c = e % n;
+    if (c <= r) S[r * ld + c] = A[(int64_t)r * lda + c];
+  }
+  __syncthreads();
+  for (int jb = 0; jb < n; jb += kNB) {
+    const int nb = min(kNB, n - jb), r0 = jb + nb, m = n - r0;
+    if (warp == 0) {
+#pragma unroll 4
+      for (int c = 0; c < kNB; ++c)
+        Dg[lane * kDP + c] = (lane < nb && c <= lane) ? S[(jb + lane) * ld + jb + c] : 0.0;
+      __syncwarp();
+      const int bad = diag_block_warp(Dg, Di, nb, rdiag);
+      if (bad) {
+        if (lane == 0) fail = jb + bad;
+      } else {
+        if (lane < nb)
+          for (int c = 0; c <= lane; ++c) S[(jb + lane) * ld + jb + c] = Dg[lane * kDP + c];
+        double *Dblk = Dinv + (int64_t)(jb / kNB) * kNB * kNB;
+        for (int r = 0; r < kNB; ++r) Dblk[r * kNB + lane] = Di[r * kDP + lane];
+      }
+    }
+    __syncthreads();
+    if (fail || m <= 0) break;
+    // the panel below: L[r0 + i][jb + c] = sum_{q <= c} A[r0 + i][jb + q] Di[c][q]
+    constexpr int kPer = (kCholSmallN * kNB) / kCholSmallThreads;   // entries a thread, at most
+    double v[kPer];
+#pragma unroll
+    for (int t = 0; t < kPer; ++t) {
+      const int e = tid + t * kCholSmallThreads, i = r0 + e / kNB, c = e % kNB;
+      double a = 0.0;
+      if (e < m * kNB && c < nb)
+        for (int q = 0; q <= c; ++q) a = fma(S[i * ld + jb + q], Di[c * kDP + q], a);
+      v[t] = a;
+    }
+    __syncthreads();   // every panel entry read before any is overwritten
+#pragma unroll
+    for (int t = 0; t < kPer; ++t) {
+      const int e = tid + t * kCholSmallThreads, i = r0 + e / kNB, c = e % kNB;
+      if (e < m * kNB && c < nb) S[i * ld + jb + c] = v[t];
+    }
+    __syncthreads();
+    // trailing lower triangle: A[i][j] -= sum_c L[i][jb + c] L[j][jb + c], r0 <= j <= i
+    for (int i = r0 + warp; i < n; i += kWarps) {
+      double li[kNB];
+#pragma unroll
+      for (int c = 0; c < kNB; ++c) li[c] = c < nb ? S[i * ld + jb + c] : 0.0;
+      for (int j = r0 + lane; j <= i; j += 32) {
+        const double *lj = S + j * ld + jb;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int c = 0; c < kNB; ++c)
+          if (c < nb) acc[c & 3] = fma(li[c], lj[c], acc[c & 3]);
+        S[i * ld + j] -= (acc[0] + acc[1]) + (acc[2] + acc[3]);
+      }
+    }
+    __syncthreads();
+  }
+  if (!fail)
+    for (int e = tid; e < n * n; e += blockDim.x) {
+      const int r = e / n, c = e % n;
+      if (c <= r) A[(int64_t)r * lda + c] = S[r * ld + c];
+    }
+  if (tid == 0) *info = fail;
+}
+
+size_t chol_small_smem(int n) { return sizeof(double) * (size_t)n * (n + 1); }
+
 // Solve L L^T X = B for nrhs (<= 4) right-hand sides (rows of B) with the blocked forward and
 // backward substitutions; the diagonal blocks are applied through their inverses (Dinv, staged
 // in shared memory per block), so every step is a set of independent dot products.  One CTA of
@@ -815,6 +908,15 @@ __global__ void eig_pack_out(const double *__restrict__ A0, const double *__rest
 tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_dev, double *Dinv,
                       cudaStream_t stream) {
   if (n < 1 || n > kMaxDense) return TSVM_ERR_UNSUPPORTED;  // panel must fit shared memory
+  if (n <= kCholSmallN) {   // the whole matrix in shared memory
+    const size_t smem = chol_small_smem(n);
+    TSVM_CUDA(cudaFuncSetAttribute(chol_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+    chol_small_kernel<<<1, kCholSmallThreads, smem, stream ? stream : ctx->stream>>>(
+        A, n, lda, Dinv, info_dev, 0, 0, nullptr);
+    TSVM_LAUNCHED(ctx);
+    return TSVM_OK;
+  }
   // the panel rows padded to an even length, plus the slack the 4-row reads of a ragged last
   // block run into
   const size_t ldp = ((size_t)(n > kNB ? n - kNB : 1) + 1) & ~(size_t)1;
@@ -831,6 +933,8 @@ tsvm_status chol_fp64_batched(tsvm_context *ctx, double *A, int n, int lda, int6
                               int *info_dev, double *Dinv, int64_t strideD, int count,
                               const int *active) {
   if (n < 1 || n > kMaxDense || count < 1) return TSVM_ERR_UNSUPPORTED;
+  // (chol_small_kernel, one CTA a problem, measured slower here: 142 against 124 us for 64
+  // problems at n = 128, its trailing update reading each panel row once per entry)
   const size_t smem = sizeof(double) * (size_t)kNB * (size_t)(n > kNB ? n - kNB : 1);
   TSVM_CUDA(cudaFuncSetAttribute(chol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
