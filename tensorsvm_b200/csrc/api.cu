@@ -23,6 +23,11 @@ tsvm_status cuda_status(cudaError_t e, const char *what, const char *file, int l
   return TSVM_ERR_CUDA;
 }
 
+tsvm_status timeout_status(const char *where) {
+  if (getenv("TSVM_DEBUG")) fprintf(stderr, "tensorsvm: bounded device wait timed out in %s\n", where);
+  return TSVM_ERR_TIMEOUT;
+}
+
 tsvm_status scratch(tsvm_context *ctx, Slot s, size_t bytes, void **out) {
   bytes = (bytes + 255) & ~(size_t)255;
   if (bytes == 0) bytes = 256;

@@ -14,6 +14,8 @@ namespace tsvm {
 // Error plumbing: every internal routine returns tsvm_status; no exit().
 // ---------------------------------------------------------------------------------------
 tsvm_status cuda_status(cudaError_t e, const char *what, const char *file, int line);
+// TSVM_ERR_TIMEOUT, naming the wait that gave up on stderr when TSVM_DEBUG is set.
+tsvm_status timeout_status(const char *where);
 
 #define TSVM_CUDA(call)                                                                   \
   do {                                                                                    \

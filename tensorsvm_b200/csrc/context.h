@@ -59,6 +59,8 @@ enum Slot : int {
   SLOT_PRED_IN,       // tsvm_predict: device copies of the model and the rows
   SLOT_PRED_OUT,      // tsvm_predict: decision values
   SLOT_B_EIG,         // batched factor: projections C, eigenvectors, eigenvalues
+  SLOT_B_FXC,         // batched factor: centred rows and row norms of every problem
+  SLOT_B_FACG,        // batched factor: CholeskyQR Gram matrices / factors, Dinv blocks, status
   SLOT_B_EIGSW,       // batched factor: per-problem sweep counts
   SLOT_COMM,          // row-sharded path: staging of host values for the collectives
   SLOT_SHARD_A,       // row-sharded factor: the all-gathered kernel-block operand (all rows)

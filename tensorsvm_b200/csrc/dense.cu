@@ -929,6 +929,24 @@ tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_de
   return TSVM_OK;
 }
 
+tsvm_status chol_fp64_same(tsvm_context *ctx, double *A, int n, int lda, int64_t strideA,
+                           int *info_dev, double *Dinv, int64_t strideD, int count,
+                           const int *active, const std::vector<int> &pending) {
+  if (n < 1 || n > kMaxDense || count < 1) return TSVM_ERR_UNSUPPORTED;
+  if (n <= kCholSmallN) {   // one CTA per problem, the single-launch kernel's arithmetic
+    const size_t smem = chol_small_smem(n);
+    TSVM_CUDA(cudaFuncSetAttribute(chol_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+    chol_small_kernel<<<count, kCholSmallThreads, smem, ctx->stream>>>(A, n, lda, Dinv, info_dev,
+                                                                       strideA, strideD, active);
+    TSVM_LAUNCHED(ctx);
+    return TSVM_OK;
+  }
+  for (int p : pending)
+    TSVM_TRY(chol_fp64(ctx, A + p * strideA, n, lda, info_dev + p, Dinv + p * strideD));
+  return TSVM_OK;
+}
+
 tsvm_status chol_fp64_batched(tsvm_context *ctx, double *A, int n, int lda, int64_t strideA,
                               int *info_dev, double *Dinv, int64_t strideD, int count,
                               const int *active) {
@@ -1049,7 +1067,7 @@ tsvm_status eig_jacobi_fp64(tsvm_context *ctx, double *A, int n, int lda, double
   TSVM_CUDA(cudaMemcpyAsync(&sweeps, sweeps_dev, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
   if (sweeps_out) *sweeps_out = sweeps;
-  if (sweeps < 0) return TSVM_ERR_TIMEOUT;
+  if (sweeps < 0) return timeout_status("eig_jacobi_fp64 (grid barrier)");
   return TSVM_OK;
 }
 

@@ -13,7 +13,9 @@
 // then two unshifted CholeskyQR steps.  Only range(W) matters for Z Z^T = W C+ W^T, so any
 // orthonormal basis of the same range gives the reference's factor.
 #include <math.h>
+#include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "common.cuh"
@@ -404,29 +406,196 @@ tsvm_status factor_finish(tsvm_context *ctx, float *Z, int64_t n, int k, const d
   return TSVM_OK;
 }
 
+// Shifted CholeskyQR3 of the bases W_p = Zs[p] (ns[p] x kp) of `count` problems, stage by stage:
+// each step forms every problem's Gram matrix (the same kernels as orthonormalise), factors them
+// all in one launch (chol_fp64_same: the single-problem arithmetic), reads all statuses with one
+// host synchronisation, retries the failed ones with a larger shift, then applies R^-1 problem
+// by problem.  The result is that of orthonormalise for each problem.
+static tsvm_status orthonormalise_batched(tsvm_context *ctx, float *const *Zs, const int64_t *ns,
+                                          int count, int k, int kp, bool tc_gram) {
+  const size_t kk = (size_t)k * k;
+  const int64_t strideD = (int64_t)ceil_div(k, 32) * 1024;
+  int64_t n_max = 0;
+  for (int p = 0; p < count; ++p) n_max = std::max(n_max, ns[p]);
+  double *Gall = nullptr, *Linv = nullptr;
+  float *R32 = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_B_FACG, (kk + (size_t)strideD) * count + (size_t)count + 8, &Gall));
+  double *Dall = Gall + kk * count;
+  int *d_info = reinterpret_cast<int *>(Dall + (size_t)strideD * count);
+  int *d_active = d_info + count;
+  TSVM_TRY(scratch_t(ctx, SLOT_SMALL2, kk, &Linv));
+  TSVM_TRY(scratch_t(ctx, SLOT_IPM_M, (size_t)kp * kp, &R32));
+  double *ones = nullptr, *negI = nullptr;
+  const unsigned gk = (unsigned)ceil_div((int64_t)k * k, 256);
+  if (tc_gram) {
+    TSVM_TRY(scratch_t(ctx, SLOT_IPM_VEC, (size_t)n_max, &ones));
+    TSVM_TRY(scratch_t(ctx, SLOT_SMALL3, kk, &negI));
+    fill_value<<<(unsigned)ceil_div(n_max, 256), 256, 0, ctx->stream>>>(ones, n_max, 1.0);
+    TSVM_LAUNCHED(ctx);
+    set_scaled_identity<<<gk, 256, 0, ctx->stream>>>(negI, k, -1.0);
+    TSVM_LAUNCHED(ctx);
+  }
+  const double u = ldexp(1.0, -53);
+  std::vector<double> fac(count);
+  std::vector<int> hinfo(count), act(count);
+  for (int step = 0; step < 3; ++step) {
+    std::vector<int> pending(count);
+    for (int p = 0; p < count; ++p) {
+      pending[p] = p;
+      fac[p] = step == 0 ? 11.0 * ((double)ns[p] * k + (double)k * (k + 1)) * u : 0.0;
+    }
+    for (int attempt = 0; !pending.empty(); ++attempt) {
+      for (int p : pending) {
+        double *G = Gall + kk * p;
+        if (tc_gram && step > 0 && attempt == 0)
+          TSVM_TRY(syrk_capacitance_tc(ctx, Zs[p], kp, ns[p], k, ones, 2.0, 3, negI, G));
+        else
+          TSVM_TRY(gram_fp64(ctx, Zs[p], kp, Zs[p], kp, ns[p], k, k, true, G));
+        if (fac[p] > 0) {
+          shift_by_trace<<<1, 256, 0, ctx->stream>>>(G, k, fac[p]);
+          TSVM_LAUNCHED(ctx);
+        }
+      }
+      std::fill(act.begin(), act.end(), 0);
+      for (int p : pending) act[p] = 1;
+      TSVM_CUDA(cudaMemcpyAsync(d_active, act.data(), sizeof(int) * count, cudaMemcpyHostToDevice,
+                                ctx->stream));
+      TSVM_TRY(chol_fp64_same(ctx, Gall, k, k, (int64_t)kk, d_info, Dall, strideD, count,
+                              d_active, pending));
+      TSVM_CUDA(cudaMemcpyAsync(hinfo.data(), d_info, sizeof(int) * count, cudaMemcpyDeviceToHost,
+                                ctx->stream));
+      TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
+      std::vector<int> failed;
+      for (int p : pending)
+        if (hinfo[p] != 0) failed.push_back(p);
+      if (!failed.empty() && attempt == 3) return TSVM_ERR_NOT_SPD;
+      for (int p : failed)
+        fac[p] = fac[p] > 0 ? fac[p] * 100.0
+                            : 11.0 * ((double)ns[p] * k + (double)k * (k + 1)) * u;
+      pending.swap(failed);
+    }
+    for (int p = 0; p < count; ++p) {
+      TSVM_TRY(trinv_lower_fp64(ctx, Gall + kk * p, k, k, Dall + (size_t)strideD * p, Linv));
+      rinv_to_fp32<<<(unsigned)ceil_div((int64_t)kp * kp, 256), 256, 0, ctx->stream>>>(Linv, k,
+                                                                                        kp, R32);
+      TSVM_LAUNCHED(ctx);
+      TSVM_TRY(apply_right_fp32(ctx, Zs[p], ns[p], kp, R32, Zs[p]));
+    }
+  }
+  return TSVM_OK;
+}
+
+// The factors of `count` problems (tsvm_factor_batched), stage by stage so that the small k x k
+// steps of all problems share launches and host synchronisations: one sketch (the glibc and
+// Philox streams are prefixes of each other, so the first n_p rows of the longest problem's
+// sketch are problem p's), every range-finder pass, one batched CholeskyQR3, every projection
+// pass with C_p = W_p^T (K W_p), all eigenproblems in one launch, then Z_p = W_p V diag(sqrt w)
+// in place.  Every kernel is the one factor_rbf runs for that problem, on the same data: the
+// factors are those of tsvm_factor.
 tsvm_status factor_rbf_batched(tsvm_context *ctx, const tsvm_factor_problem *pr, int count, int d,
                                int k, int precision, int sketch, int ldz,
                                tsvm_factor_info *infos, double *ms_eig) {
   const int kp = (int)round_up(k, 64);
-  if (count < 1 || ldz != kp) return TSVM_ERR_INVALID_ARGUMENT;
-  double *buf = nullptr;   // [count][k][k] C, then [count][k][k] V, then [count][k] w
+  if (count < 1 || ldz != kp || d < 1 || k < 1 || k > 1000) return TSVM_ERR_INVALID_ARGUMENT;
+  int64_t n_max = 0;
+  std::vector<int64_t> ns(count), xo(count + 1, 0);
+  std::vector<float *> Zs(count);
+  for (int p = 0; p < count; ++p) {
+    ns[p] = pr[p].n;
+    if (ns[p] < 2 || k > ns[p] || !(pr[p].gamma > 0)) return TSVM_ERR_INVALID_ARGUMENT;
+    n_max = std::max(n_max, ns[p]);
+    Zs[p] = pr[p].Z;
+    xo[p + 1] = xo[p] + round_up(ns[p] * (d + 1) + 64, 4);   // rows then norms, 16-byte aligned
+  }
+  TraceRange tr_b("factor batched");
   const size_t kk = (size_t)k * k;
+  double *buf = nullptr;   // [count][k][k] C, then [count][k][k] V, then [count][k] w
   TSVM_TRY(scratch_t(ctx, SLOT_B_EIG, (2 * kk + (size_t)k) * count, &buf));
   double *Cb = buf, *Vb = buf + kk * count, *wb = Vb + kk * count;
-  for (int p = 0; p < count; ++p)
-    TSVM_TRY(factor_rbf(ctx, pr[p].X, pr[p].y, pr[p].n, d, pr[p].gamma, k, precision, sketch,
-                        nullptr, pr[p].Z, ldz, infos ? infos + p : nullptr, nullptr, 0, -1,
-                        Cb + kk * p));
+  float *Xall = nullptr, *Q = nullptr, *raw = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_B_FXC, (size_t)xo[count], &Xall));
+  TSVM_TRY(scratch_t(ctx, SLOT_Q, (size_t)n_max * kp, &Q));
+  TSVM_TRY(scratch_t(ctx, SLOT_W2, (size_t)n_max * k, &raw));
+  if (sketch == TSVM_SKETCH_GLIBC)
+    TSVM_TRY(sketch_glibc(ctx, n_max * (int64_t)k, raw));
+  else if (sketch == TSVM_SKETCH_PHILOX)
+    TSVM_TRY(sketch_philox(ctx, ctx->sketch_seed, n_max * (int64_t)k, raw));
+  else
+    return TSVM_ERR_INVALID_ARGUMENT;
+  TSVM_TRY(pad_rows(ctx, raw, k, n_max, k, Q, kp));
+  const bool split = precision_is_split(precision);
+  std::vector<float> km(count, 0.f);
+  // range-finder passes: W_p = Y K Y Q_p into Z_p
+  for (int p = 0; p < count; ++p) {
+    float *Xc = Xall + xo[p], *norms = Xc + ns[p] * d;
+    TSVM_TRY(centre_features(ctx, pr[p].X, ns[p], d, Xc, norms));
+    float km1 = 0.f;
+    TSVM_TRY(kermatmul(ctx, Xc, norms, pr[p].y, ns[p], d, pr[p].gamma, Q, kp, Zs[p], precision,
+                       &km1, nullptr, split ? 1 : 0, 0, -1, k));
+    km[p] += km1;
+  }
+  const bool tc_gram = precision != TSVM_PREC_FP32 && syrk_tc_supported(k) && k >= 32;
+  TSVM_TRY(orthonormalise_batched(ctx, Zs.data(), ns.data(), count, k, kp, tc_gram));
+  // projection passes and C_p (the sketch in Q is no longer needed: Q takes each pass's output)
+  double *sym = nullptr;
+  TSVM_TRY(scratch_t(ctx, SLOT_SMALL, (size_t)kp + 8, &sym));
+  const bool half = precision != TSVM_PREC_FP32;
+  for (int p = 0; p < count; ++p) {
+    float *Xc = Xall + xo[p], *norms = Xc + ns[p] * d, *W = Zs[p];
+    double *Cm = Cb + kk * p;
+    float km2 = 0.f;
+    if (half)
+      TSVM_TRY(kermatmul_tc_half(ctx, Xc, pr[p].y, ns[p], d, pr[p].gamma, W, kp, Q, precision,
+                                 &km2, split ? nullptr : W, split ? 2 : 0, sym, false, k));
+    else
+      TSVM_TRY(kermatmul(ctx, Xc, norms, pr[p].y, ns[p], d, pr[p].gamma, W, kp, Q, precision,
+                         &km2, W, 0, 0, -1, k));
+    km[p] += km2;
+    TSVM_TRY(gram_fp64(ctx, W, kp, Q, kp, ns[p], k, k, false, Cm));
+    if (half) {
+      half_projection_finish<<<(unsigned)ceil_div((int64_t)k * k, 256), 256, 0, ctx->stream>>>(
+          Cm, k, sym);
+      TSVM_LAUNCHED(ctx);
+    } else {
+      TSVM_TRY(small_symmetrize(ctx, Cm, k, k));
+    }
+  }
   cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
   TSVM_CUDA(cudaEventRecord(e0, ctx->stream));
   int sweeps = 0;
   TSVM_TRY(eig_jacobi_fp64_batched(ctx, Cb, k, count, wb, Vb, &sweeps));
   TSVM_CUDA(cudaEventRecord(e1, ctx->stream));
   for (int p = 0; p < count; ++p)
-    TSVM_TRY(factor_finish(ctx, pr[p].Z, pr[p].n, k, Vb + kk * p, wb + (size_t)k * p,
-                           infos ? infos + p : nullptr));
+    TSVM_TRY(factor_finish(ctx, Zs[p], ns[p], k, Vb + kk * p, wb + (size_t)k * p, nullptr));
+  std::vector<double> hw((size_t)k * count);
+  TSVM_CUDA(cudaMemcpyAsync(hw.data(), wb, sizeof(double) * hw.size(), cudaMemcpyDeviceToHost,
+                            ctx->stream));
   TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
   if (ms_eig) *ms_eig = event_ms(e0, e1);
+  if (infos) {
+    for (int p = 0; p < count; ++p) {
+      tsvm_factor_info &in = infos[p];
+      memset(&in, 0, sizeof(in));
+      in.n = ns[p];
+      in.d = d;
+      in.k = k;
+      in.k_padded = kp;
+      in.precision = precision;
+      int realk = 0;
+      double wmax = -INFINITY, wmin = INFINITY;
+      for (int i = 0; i < k; ++i) {
+        const double v = hw[(size_t)k * p + i];
+        realk += v > 0.0;
+        wmax = fmax(wmax, v);
+        wmin = fmin(wmin, v);
+      }
+      in.realk = realk;
+      in.eig_max = wmax;
+      in.eig_min = wmin;
+      in.ms_kermatmul_kernel = km[p];
+      in.flops_kermatmul = 2.0 * (2.0 * (double)ns[p] * ns[p] * k + 2.0 * (double)ns[p] * ns[p] * d);
+    }
+  }
   return TSVM_OK;
 }
 

@@ -1220,9 +1220,9 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
     if (run.shard) {   // a rank whose pass timed out takes the others out with it
       double e = host_info[2] ? 1.0 : 0.0;
       TSVM_TRY(comm_sum_host(ctx, &e));
-      if (e > 0.0) return TSVM_ERR_TIMEOUT;
+      if (e > 0.0) return timeout_status("ipm streaming pass (another rank)");
     }
-    if (host_info[2]) return TSVM_ERR_TIMEOUT;
+    if (host_info[2]) return timeout_status("ipm streaming pass");
     if (pending_events) {
       ms_syrk += event_ms(ev_syrk0, ev_syrk1);
       ms_factor += event_ms(ev_syrk1, ev_chol1);
@@ -1533,7 +1533,7 @@ tsvm_status bias_rbf(tsvm_context *ctx, const float *Z, int ldz, const float *y,
   TSVM_CUDA(cudaMemcpyAsync(hb, out, sizeof(hb), cudaMemcpyDeviceToHost, ctx->stream));
   TSVM_CUDA(cudaMemcpyAsync(&herr, run.err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
-  if (herr) return TSVM_ERR_TIMEOUT;
+  if (herr) return timeout_status("bias pass");
   if (nsv) *nsv = (int32_t)hs[0];
   if (nfree) *nfree = (int32_t)hs[1];
   if (b) *b = hb[0];
@@ -1596,7 +1596,7 @@ tsvm_status check_runner(tsvm_context *ctx, Runner &run) {
   int h[3] = {0, 0, 0};
   TSVM_CUDA(cudaMemcpyAsync(h, run.info, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
   TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
-  if (h[2]) return TSVM_ERR_TIMEOUT;
+  if (h[2]) return timeout_status("ipm runner pass");
   if (h[0]) return TSVM_ERR_NOT_SPD;
   return TSVM_OK;
 }
@@ -2149,7 +2149,7 @@ tsvm_status ipm_solve_batched(tsvm_context *ctx, const tsvm_ipm_problem *pr, int
                               ctx->stream));
     TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
     if (hinfo[P]) {
-      result = TSVM_ERR_TIMEOUT;
+      result = timeout_status("batched ipm streaming pass");
       break;
     }
     const double tnow =

@@ -1131,7 +1131,7 @@ tsvm_status kermatmul_tc_core(tsvm_context *ctx, const float *XI, const float *y
   TSVM_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   TSVM_CUDA(cudaStreamSynchronize(ctx->stream));
   if (kernel_ms) *kernel_ms = event_ms(e0, e1);
-  if (herr) return TSVM_ERR_TIMEOUT;
+  if (herr) return timeout_status("kermatmul_tc_kernel");
   return TSVM_OK;
 }
 

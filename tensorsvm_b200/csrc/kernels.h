@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "context.h"
 #include "tensorsvm.h"
 
@@ -133,6 +135,12 @@ tsvm_status potrs_fp64(tsvm_context *ctx, const double *L, int n, int lda, const
                        double *B, int nrhs, int ldb);
 // Batched forms: `count` independent n x n problems at A + b * strideA (Dinv + b * strideD,
 // info_dev[b], B + b * strideB), problems with active[b] == 0 skipped; one CTA per problem.
+// The factorisations of `count` problems (stride strideA / strideD, info_dev[p]) with the same
+// arithmetic per problem as chol_fp64: one launch of one CTA per problem (those with
+// active[p] != 0) when n <= 128, else chol_fp64 for each problem in `pending`.
+tsvm_status chol_fp64_same(tsvm_context *ctx, double *A, int n, int lda, int64_t strideA,
+                           int *info_dev, double *Dinv, int64_t strideD, int count,
+                           const int *active, const std::vector<int> &pending);
 tsvm_status chol_fp64_batched(tsvm_context *ctx, double *A, int n, int lda, int64_t strideA,
                               int *info_dev, double *Dinv, int64_t strideD, int count,
                               const int *active);
