@@ -662,6 +662,58 @@ def run_workload(args, world, rank, local):
     return line
 
 
+def kernel_table(args, local):
+    """Per-kernel device time of one step (after one warm-up step) through CUPTI (torch.profiler),
+    which also sees the kernels a CUDA graph replays: the two-Gaussian solve (factor + IPM) or the
+    grid (batched factors, then the batched IPM).  Prints a table per phase; no JSON line."""
+    import collections
+    import torch
+    from torch.profiler import profile, ProfilerActivity
+    from tensorsvm_b200 import _lib, api, synth
+    torch.cuda.set_device(local)
+    ctx = _lib.Context(local)
+    prec = args.precision
+    mixed = _lib.PREC_FP32 if prec == "fp32" else _lib.PREC_BF16
+    if args.workload == "grid":
+        probs = synth.grid_problems(count=64)
+        Xs = [torch.from_numpy(X).cuda() for X, _, _, _ in probs]
+        ys = [torch.from_numpy(y).cuda() for _, y, _, _ in probs]
+        gs = [g for _, _, g, _ in probs]
+        Cs = [C for _, _, _, C in probs]
+        state = {}
+        phases = [("factors", lambda: state.__setitem__(
+                      "Z", api.factor_batched(ctx, Xs, ys, gs, 128, prec)[0])),
+                  ("batched ipm", lambda: api.ipm_batched(ctx, state["Z"], ys, 128, Cs,
+                                                          rel_gap_tol=1e-6, precision=mixed))]
+    else:
+        X, y = synth.two_gaussians(args.n, D, seed=replica_seed(0), noise=NOISE)
+        Xd, yd = torch.from_numpy(X).cuda(), torch.from_numpy(y).cuda()
+        state = {}
+        phases = [("factor", lambda: state.__setitem__(
+                      "Z", api.factor(ctx, Xd, yd, GAMMA, K, prec)[0])),
+                  ("ipm", lambda: api.ipm(ctx, state["Z"], yd, K, CPEN, rel_gap_tol=1e-6,
+                                          precision=mixed))]
+    for _, fn in phases:   # warm-up
+        fn()
+    torch.cuda.synchronize()
+    for name, fn in phases:
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            fn()
+            torch.cuda.synchronize()
+        tot, cnt = collections.defaultdict(float), collections.Counter()
+        for e in prof.events():
+            if e.device_type == torch.autograd.DeviceType.CUDA:
+                kn = e.name.replace("(anonymous namespace)::", "").split("(")[0][:110]
+                tot[kn] += e.time_range.elapsed_us()
+                cnt[kn] += 1
+        total = sum(tot.values())
+        print(f"== {name}: {total / 1e3:.1f} ms of kernels over {sum(cnt.values())} launches")
+        for kn, v in sorted(tot.items(), key=lambda x: -x[1])[:30]:
+            print(f"{cnt[kn]:6d} {v / 1e3:9.2f} ms {100 * v / total:6.2f}%  "
+                  f"{v / cnt[kn]:9.1f} us  {kn}")
+    ctx.close()
+
+
 def run_other_workloads(args, local):
     """The wide-feature, batched-grid and hypergradient lines (their full-size workloads, three
     warm-up and up to three timed steps each), nested in the default line so that one run
@@ -795,6 +847,9 @@ def main():
                     help="reference arm: seconds of full-size reference runs (at least one run)")
     ap.add_argument("--factor-threads", type=int, default=4,
                     help="grid workload: host threads (one context each) for the 64 factors")
+    ap.add_argument("--kernel-table", action="store_true",
+                    help="print per-kernel device times of one step (CUPTI) instead of timing; "
+                         "two_gaussians or grid")
     ap.add_argument("--no-workloads", dest="workloads", action="store_false",
                     help="default line at N=1: skip the wide / grid / hypergrad lines that are "
                          "otherwise appended under 'workloads'")
@@ -804,6 +859,10 @@ def main():
                          "hypergradient at n=200k + 50k")
     args = ap.parse_args()
     world, rank, local = dist_setup()
+    if args.kernel_table:
+        if rank == 0:
+            kernel_table(args, local)
+        return
     if args.workload != "two_gaussians" and args.impl == "ours":
         line = run_workload(args, world, rank, local)
     elif args.impl == "reference":
