@@ -271,8 +271,12 @@ tsvm_status tsvm_ipm(tsvm_context *ctx, const float *Z, int32_t ldz, const float
  * of all unconverged problems, the k x k Cholesky and solves are one launch with a CTA per
  * problem, the host synchronises once per iteration for all stopping rules, and from the second
  * iteration on the iteration's launches are replayed from a captured CUDA graph.  The unit
- * size is autotuned on the first pass.  The capacitance matrices are summed in FP64 (the
- * reference's DSYRK numerics); opt->precision is not used.  stats[count] receives each
+ * size is autotuned on the first pass.  opt->precision TSVM_PREC_FP32 sums the capacitance
+ * matrices in FP64 (the reference's DSYRK numerics); the 16-bit precisions (k <= 256, ldz <=
+ * 256) build them as tsvm_ipm does -- per work unit the tensor-core SYRK of the rows with weight
+ * <= tau and the other rows exactly in FP64, every solve refined once against the exact
+ * operator, tau adapted per problem on the device, a failed step retried with more rows exact.
+ * stats[count] receives each
  * problem's statistics (status in stats[i].status); the call returns TSVM_OK when every
  * problem ended with a usable alpha (OK, WARN_*), else the first failing status. */
 tsvm_status tsvm_ipm_batched(tsvm_context *ctx, const tsvm_ipm_problem *problems, int32_t count,
