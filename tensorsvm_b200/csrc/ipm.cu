@@ -1762,7 +1762,7 @@ __global__ void mixed_units_reduce(const float *__restrict__ part_tc, int KP,
                                    const double *__restrict__ part64, const int *__restrict__ ubeg,
                                    int k, const int *__restrict__ active,
                                    const int *__restrict__ err, double *__restrict__ M,
-                                   int64_t strideM) {
+                                   int64_t strideM, const int *__restrict__ counts, int parts) {
   const int p = blockIdx.y;
   if (active && !active[p]) return;
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1770,9 +1770,13 @@ __global__ void mixed_units_reduce(const float *__restrict__ part_tc, int KP,
   const int r = (int)(e / k), c = (int)(e % k);
   if (c > r) return;
   double s = r == c ? 1.0 : 0.0;
-  for (int u = ubeg[p]; u < ubeg[p + 1]; ++u)
-    s += (double)part_tc[(int64_t)u * KP * KP + (int64_t)r * KP + c] +
-         part64[(int64_t)u * k * k + (int64_t)r * k + c];
+  for (int u = ubeg[p]; u < ubeg[p + 1]; ++u) {
+    s += (double)part_tc[(int64_t)u * KP * KP + (int64_t)r * KP + c];
+    const int cnt = counts[u];
+    for (int j = 0; j < parts; ++j)   // the pieces of the unit's exact rows that hold any
+      if (gram_units_piece_rows(cnt, parts, j))
+        s += part64[((int64_t)u * parts + j) * k * k + (int64_t)r * k + c];
+  }
   if (*err) s = NAN;
   double *Mp = M + p * strideM;
   Mp[(int64_t)r * k + c] = s;
@@ -1956,7 +1960,10 @@ tsvm_status ipm_solve_batched(tsvm_context *ctx, const tsvm_ipm_problem *pr, int
   const int64_t strideD = (int64_t)ceil_div(k, 32) * 1024;
   const int64_t strideM = (int64_t)k * k + strideD;
   TSVM_TRY(scratch_t(ctx, SLOT_B_M, (size_t)P * strideM, &Mall));
-  TSVM_TRY(scratch_t(ctx, SLOT_B_GPART, (size_t)max_units * k * k, &gpart));
+  // the exactly summed rows of a unit (mixed) in kExactParts pieces of one partial each
+  constexpr int kExactParts = 4;
+  TSVM_TRY(scratch_t(ctx, SLOT_B_GPART, (size_t)max_units * k * k * (mixed ? kExactParts : 1),
+                     &gpart));
   TSVM_TRY(scratch_t(ctx, SLOT_B_PART, (size_t)max_units * (2 * kz + 16), &part));
   float *labels = reinterpret_cast<float *>(vec + (size_t)11 * N);
   double *scal = sbuf, *q = sbuf + (size_t)P * kNScal, *h = q + (size_t)P * kz;
@@ -2093,12 +2100,12 @@ tsvm_status ipm_solve_batched(tsvm_context *ctx, const tsvm_ipm_problem *pr, int
       TSVM_LAUNCHED(ctx);
       TSVM_TRY(big_rows_units(ctx, V.dinv, d_units, br.nunits, d_active, taus, xidx, xcounts));
       TSVM_TRY(gram_fp64_units(ctx, d_z, ldz, k, d_units, br.nunits, d_active, V.dinv, gpart,
-                               xidx, xcounts));
+                               xidx, xcounts, kExactParts));
       TSVM_TRY(syrk_units_tc(ctx, d_z, ldz, k, d_units, br.nunits, d_active, V.dinv, taus,
                              part_tc, syrk_err));
       mixed_units_reduce<<<dim3((unsigned)ceil_div((int64_t)k * k, 256), P), 256, 0,
                            ctx->stream>>>(part_tc, KPs, gpart, d_ubeg, k, d_active, syrk_err, M,
-                                          strideM);
+                                          strideM, xcounts, kExactParts);
     } else {
       TSVM_TRY(gram_fp64_units(ctx, d_z, ldz, k, d_units, br.nunits, d_active, V.dinv, gpart));
       gram_units_reduce<<<dim3((unsigned)ceil_div((int64_t)k * k, 256), P), 256, 0,

@@ -112,11 +112,18 @@ tsvm_status gram_fp64_rows(tsvm_context *ctx, const float *A, int64_t lda, int64
 // Per-unit partial Gram matrices of a batch: part[u] (k x k, lower 64 x 64 tiles filled) =
 // sum over the unit's rows j of rowscale[goff + j] z_j z_j^T with z_j rows of Zs[p] (lda);
 // units of problems with active[p] == 0 are skipped.  With rowidx and counts, only the
-// counts[u] rows rowidx[goff + i] (indices within the unit) of each unit are summed.
+// counts[u] rows rowidx[goff + i] (indices within the unit) of each unit are summed, the list
+// cut into `parts` pieces of whole 32-row slabs, piece j into part[u * parts + j]; a piece past
+// the end of the list writes nothing (gram_units_piece_rows says which pieces hold rows).
 tsvm_status gram_fp64_units(tsvm_context *ctx, const float *const *Zs, int64_t lda, int k,
                             const WorkUnit *units, int nunits, const int *active,
                             const double *rowscale, double *part, const int64_t *rowidx = nullptr,
-                            const int *counts = nullptr);
+                            const int *counts = nullptr, int parts = 1);
+// Whether piece j of `parts` of a list of cnt rows holds any (the cut of gram_fp64_units).
+__host__ __device__ inline bool gram_units_piece_rows(int cnt, int parts, int j) {
+  const int per = ((cnt + parts - 1) / parts + 31) / 32 * 32;
+  return j * per < cnt;
+}
 // Out (n x kp) = A (n x kp) * R (kp x kp, fp32 row-major). Out may alias A.
 tsvm_status apply_right_fp32(tsvm_context *ctx, const float *A, int64_t n, int kp,
                              const float *R, float *Out);

@@ -60,6 +60,7 @@ gram_partial_kernel(const float *__restrict__ A, int64_t lda, const float *__res
     tb = t % tiles_b;
   }
   const int a0 = ta * kGT, b0 = tb * kGT;
+  int64_t rows_beg = 0;
   if (units) {  // batched: this block sums the rows of one work unit (symmetric, A = B)
     const WorkUnit u = units[blockIdx.y];
     if (active && !active[u.p]) return;
@@ -68,9 +69,16 @@ gram_partial_kernel(const float *__restrict__ A, int64_t lda, const float *__res
     n = u.rows;
     rows_per_split = u.rows;
     rowscale += u.goff;
-    if (count) {   // only the unit's listed rows (indices within the unit) at rowidx + goff
-      n = count[blockIdx.y];
-      rows_per_split = n;
+    if (count) {   // only the unit's listed rows (indices within the unit) at rowidx + goff,
+                   // the list cut into gridDim.z parts of whole slabs; an empty part writes
+                   // nothing (the reduction skips it)
+      const int cnt = count[blockIdx.y], S = (int)gridDim.z;
+      const int per = ((cnt + S - 1) / S + kGRows - 1) / kGRows * kGRows;
+      const int b = (int)blockIdx.z * per;
+      if (b >= cnt) return;
+      rows_beg = b;
+      n = min(cnt, b + per);
+      rows_per_split = n - b;
       rowidx += u.goff;
     }
   } else if (count) {  // row count on the device: split it evenly over gridDim.y
@@ -78,7 +86,7 @@ gram_partial_kernel(const float *__restrict__ A, int64_t lda, const float *__res
     rows_per_split = (n + gridDim.y - 1) / gridDim.y;
     rows_per_split = (rows_per_split + kGRows - 1) / kGRows * kGRows;
   }
-  const int64_t r0 = units ? 0 : (int64_t)blockIdx.y * rows_per_split;
+  const int64_t r0 = units ? rows_beg : (int64_t)blockIdx.y * rows_per_split;
   const int64_t r1 = min(n, r0 + rows_per_split);
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   // a tile on the diagonal of a symmetric product: only its lower triangle is read back
@@ -105,8 +113,8 @@ gram_partial_kernel(const float *__restrict__ A, int64_t lda, const float *__res
     else
       gram_slab<false>(As, Bs, tx, ty, acc);
   }
-  // partial layout: [split][ka][kb]
-  double *P = part + (int64_t)blockIdx.y * ka * kb;
+  // partial layout: [split][ka][kb] (batched: [unit][part][ka][kb])
+  double *P = part + ((int64_t)blockIdx.y * gridDim.z + blockIdx.z) * ka * kb;
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -307,12 +315,13 @@ tsvm_status gram_fp64_rows(tsvm_context *ctx, const float *A, int64_t lda, int64
 tsvm_status gram_fp64_units(tsvm_context *ctx, const float *const *Zs, int64_t lda, int k,
                             const WorkUnit *units, int nunits, const int *active,
                             const double *rowscale, double *part, const int64_t *rowidx,
-                            const int *counts) {
+                            const int *counts, int parts) {
   if (nunits < 1 || nunits > 65535) return TSVM_ERR_UNSUPPORTED;
   if ((rowidx == nullptr) != (counts == nullptr)) return TSVM_ERR_INVALID_ARGUMENT;
+  if (parts < 1 || parts > 64 || (parts > 1 && !counts)) return TSVM_ERR_INVALID_ARGUMENT;
   const int tiles = (int)ceil_div(k, kGT);
   const int ntiles = tiles * (tiles + 1) / 2;
-  gram_partial_kernel<<<dim3(ntiles, nunits), 256, 0, ctx->stream>>>(
+  gram_partial_kernel<<<dim3(ntiles, nunits, parts), 256, 0, ctx->stream>>>(
       nullptr, lda, nullptr, lda, 0, k, k, tiles, 1, 0, rowscale, rowidx, counts, units, Zs,
       active, part);
   TSVM_LAUNCHED(ctx);
