@@ -28,7 +28,7 @@
 // from precomputed descriptors and incremental ring counters.  The exponentials can be split
 // between MUFU ex2 and a polynomial on the FMA pipe (TSVM_TC_POLY); MUFU alone is fastest
 // here.  All waits are bounded: after
-// ~1 s without progress a block records an error and leaves; the host reports
+// ~4 s without progress a block records an error and leaves; the host reports
 // TSVM_ERR_TIMEOUT.  No cluster multicast anywhere.
 #include <cuda.h>
 #include <cuda_bf16.h>

@@ -39,7 +39,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: returns false (and raises the block's abort flag) after ~1 s without progress,
+// Bounded wait: returns false (and raises the block's abort flag) after ~4 s without progress,
 // or as soon as another thread of the block has aborted.  The global timer is slow to read, so
 // it is only consulted every 1024 unsuccessful polls (each poll may itself suspend briefly).
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort) {
@@ -50,7 +50,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
       if (*abort) return false;
       const uint64_t now = gtimer();
       if (deadline == 0) {
-        deadline = now + 1000000000ull;
+        deadline = now + 4000000000ull;   // 4 s: a margin over any stall of a working GPU
       } else if (now > deadline) {
         *abort = 1;
         return false;
