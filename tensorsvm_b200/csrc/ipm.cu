@@ -1946,14 +1946,13 @@ tsvm_status ipm_solve_batched(tsvm_context *ctx, const tsvm_ipm_problem *pr, int
   TSVM_TRY(scratch_t(ctx, SLOT_B_VEC, (size_t)11 * N + (size_t)N / 2 + 8, &vec));
   TSVM_TRY(scratch_t(ctx, SLOT_B_SCAL, (size_t)P * (kNScal + (mixed ? 9 : 3) * kz), &sbuf));
   float *part_tc = nullptr;
-  int *syrk_err = nullptr, *xcounts = nullptr;
+  int *xcounts = nullptr;
   double *taus = nullptr;
   int64_t *xidx = nullptr;
-  if (mixed) {
+  if (mixed) {   // [tensor-core partials | 16 words | exact-row counts | tau per problem]
     const size_t ntc = (size_t)max_units * KPs * KPs;
     TSVM_TRY(scratch_t(ctx, SLOT_B_SYRK, ntc + 64 + (size_t)max_units + 2 * (size_t)P, &part_tc));
-    syrk_err = reinterpret_cast<int *>(part_tc + ntc);
-    xcounts = syrk_err + 16;
+    xcounts = reinterpret_cast<int *>(part_tc + ntc) + 16;
     taus = reinterpret_cast<double *>(part_tc + ntc + 32 + (((size_t)max_units + 1) & ~(size_t)1));
     TSVM_TRY(scratch_t(ctx, SLOT_B_IDX, (size_t)N, &xidx));
   }
@@ -2002,7 +2001,6 @@ tsvm_status ipm_solve_batched(tsvm_context *ctx, const tsvm_ipm_problem *pr, int
   TSVM_CUDA(cudaMemsetAsync(d_info, 0, tb_info, ctx->stream));
   TSVM_CUDA(cudaMemcpyAsync(scal, hsc.data(), sizeof(double) * hsc.size(), cudaMemcpyHostToDevice,
                             ctx->stream));
-  if (mixed) TSVM_CUDA(cudaMemsetAsync(syrk_err, 0, sizeof(int), ctx->stream));
 
   BRunner br;
   br.ctx = ctx;
@@ -2101,10 +2099,12 @@ tsvm_status ipm_solve_batched(tsvm_context *ctx, const tsvm_ipm_problem *pr, int
       TSVM_TRY(big_rows_units(ctx, V.dinv, d_units, br.nunits, d_active, taus, xidx, xcounts));
       TSVM_TRY(gram_fp64_units(ctx, d_z, ldz, k, d_units, br.nunits, d_active, V.dinv, gpart,
                                xidx, xcounts, kExactParts));
+      // a tensor-core block that timed out raises the streaming passes' flag (the host reports
+      // TSVM_ERR_TIMEOUT) and poisons M
       TSVM_TRY(syrk_units_tc(ctx, d_z, ldz, k, d_units, br.nunits, d_active, V.dinv, taus,
-                             part_tc, syrk_err));
+                             part_tc, br.err));
       mixed_units_reduce<<<dim3((unsigned)ceil_div((int64_t)k * k, 256), P), 256, 0,
-                           ctx->stream>>>(part_tc, KPs, gpart, d_ubeg, k, d_active, syrk_err, M,
+                           ctx->stream>>>(part_tc, KPs, gpart, d_ubeg, k, d_active, br.err, M,
                                           strideM, xcounts, kExactParts);
     } else {
       TSVM_TRY(gram_fp64_units(ctx, d_z, ldz, k, d_units, br.nunits, d_active, V.dinv, gpart));
