@@ -58,6 +58,11 @@ tsvm_status tsvm_test_potrs(tsvm_context *ctx, const double *L, int32_t n, doubl
  * (T:2191). */
 tsvm_status tsvm_test_eig(tsvm_context *ctx, double *A, int32_t n, double *w, double *V,
                           int32_t *sweeps_host);
+/* `count` symmetric n x n eigenproblems at once (the batched factor's eigensolver, the
+ * reference's dsyevd, T:2191): A (count x n x n, row-major, overwritten), w (count x n), V
+ * (count x n x n, eigenvectors in columns); *max_sweeps_host = the most sweeps any needed. */
+tsvm_status tsvm_test_eig_batched(tsvm_context *ctx, double *A, int32_t n, int32_t count,
+                                  double *w, double *V, int32_t *max_sweeps_host);
 /* G (ka x kb) = A^T diag(s) B over n rows with FP64 accumulation; s may be NULL. */
 tsvm_status tsvm_test_gram(tsvm_context *ctx, const float *A, int64_t lda, const float *B,
                            int64_t ldb, int64_t n, int32_t ka, int32_t kb, int32_t symmetric,

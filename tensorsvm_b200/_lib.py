@@ -54,7 +54,7 @@ TEST_EXPORTS = [
     "tsvm_test_potrs", "tsvm_test_eig", "tsvm_test_gram", "tsvm_test_syrk_mixed",
     "tsvm_test_grid_barrier", "tsvm_test_fail_alloc", "tsvm_test_sketch_philox",
     "tsvm_test_kprod", "tsvm_test_kermatmul_half", "tsvm_test_kermatmul_cols",
-    "tsvm_test_kermatmul_half_cols",
+    "tsvm_test_kermatmul_half_cols", "tsvm_test_eig_batched",
 ]
 
 
@@ -216,6 +216,7 @@ def load() -> ctypes.CDLL:
         "tsvm_test_kermatmul": [P, P, P, I64, I32, D, P, I32, P, I32, I32],
         "tsvm_test_kermatmul_half": [P, P, P, I64, I32, D, P, I32, P, P, I32, I32],
         "tsvm_test_kermatmul_cols": [P, P, P, I64, I32, D, P, I32, I32, P, I32, I32],
+        "tsvm_test_eig_batched": [P, P, I32, I32, P, P, P],
         "tsvm_test_kermatmul_half_cols": [P, P, P, I64, I32, D, P, I32, I32, P, P, I32, I32],
         "tsvm_test_sketch_philox": [P, ctypes.c_uint64, I64, P],
         "tsvm_test_kprod": [P, P, I64, P, I64, I32, D, P, I32, P, I32, I32],

@@ -145,6 +145,15 @@ tsvm_status tsvm_test_eig(tsvm_context *ctx, double *A, int32_t n, double *w, do
   return st;
 }
 
+tsvm_status tsvm_test_eig_batched(tsvm_context *ctx, double *A, int32_t n, int32_t count,
+                                  double *w, double *V, int32_t *max_sweeps_host) {
+  if (!ctx || !A || !w || !V || n < 1 || count < 1) return TSVM_ERR_INVALID_ARGUMENT;
+  int sweeps = 0;
+  tsvm_status st = eig_jacobi_fp64_batched(ctx, A, n, count, w, V, &sweeps);
+  if (max_sweeps_host) *max_sweeps_host = sweeps;
+  return st;
+}
+
 tsvm_status tsvm_test_gram(tsvm_context *ctx, const float *A, int64_t lda, const float *B,
                            int64_t ldb, int64_t n, int32_t ka, int32_t kb, int32_t symmetric,
                            const double *s, double *G) {

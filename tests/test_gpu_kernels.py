@@ -90,6 +90,28 @@ def test_jacobi_eigensolver(ctx, k):
     assert np.linalg.norm(Vh.T @ Vh - np.eye(k)) < 1e-11
 
 
+@pytest.mark.parametrize("k,count", [(128, 64), (64, 9), (33, 5), (130, 3)])
+def test_jacobi_eigensolver_batched(ctx, k, count):
+    """The batched factor's eigensolver (one CTA per problem in one launch up to k = 128, the
+    grid eigensolver one problem after the other above) against numpy, problem by problem."""
+    rng = np.random.default_rng(300 + k + count)
+    S = rng.standard_normal((count, k, k))
+    S = (S + np.transpose(S, (0, 2, 1))) / 2
+    S *= np.logspace(0, 3, count)[:, None, None]   # problems of different scales
+    w = torch.empty((count, k), dtype=torch.float64, device="cuda")
+    V = torch.empty((count, k, k), dtype=torch.float64, device="cuda")
+    sweeps = ctypes.c_int32(0)
+    _lib.check(ctx.lib.tsvm_test_eig_batched(ctx.handle, P(dev(S.copy())), k, count, P(w), P(V),
+                                             ctypes.byref(sweeps)), "eig_batched")
+    assert 0 < sweeps.value < 40
+    for b in range(count):
+        wh, Vh = w[b].cpu().numpy(), V[b].cpu().numpy()
+        sc = np.abs(S[b]).max()
+        assert np.allclose(np.sort(wh), np.linalg.eigvalsh(S[b]), rtol=1e-10, atol=1e-9 * sc)
+        assert np.linalg.norm(Vh @ np.diag(wh) @ Vh.T - S[b]) / np.linalg.norm(S[b]) < 1e-12
+        assert np.linalg.norm(Vh.T @ Vh - np.eye(k)) < 1e-11
+
+
 def test_grid_barrier_wait_runs_out_and_context_stays_usable(ctx):
     # the cooperative eigensolver's grid barrier with an arrival that never comes: every block
     # gives up after its bounded poll count, the error flag reads back as a status, and the same
