@@ -6,6 +6,7 @@
 // plus a triangular inverse used by the shifted CholeskyQR that replaces the TSQR.
 // Matrices are row-major with leading dimension lda; only lower triangles are referenced
 // where noted.
+#include <cooperative_groups.h>
 #include <math.h>
 
 #include <vector>
@@ -391,7 +392,10 @@ __global__ void __launch_bounds__(1024) diag_inverse_kernel(const double *__rest
 // triangle (a warp a row, lane = column, the row's panel entries as broadcasts).  At this size
 // the general kernels' round trips to L2 between the phases cost more than the arithmetic
 // (148 against 187 us for chol_la_kernel at n = 128).  Writes L (lower part) and the Dinv blocks
-// as chol_kernel does; strideA / strideD / active allow one CTA per problem.
+// as chol_kernel does; strideA / strideD / active allow one CTA per problem: the batched
+// factorisations (chol_fp64_same) run it, one CTA a problem; a single factorisation takes the
+// cluster kernel below, whose per-entry arithmetic is the same (the same panel sums and the same
+// four-chain trailing-update sums, in the same step order).
 constexpr int kCholSmallN = 128;
 constexpr int kCholSmallThreads = 512;
 __global__ void __launch_bounds__(kCholSmallThreads, 1)
@@ -476,6 +480,140 @@ chol_small_kernel(double *__restrict__ A, int n, int lda, double *__restrict__ D
 }
 
 size_t chol_small_smem(int n) { return sizeof(double) * (size_t)n * (n + 1); }
+
+// Cholesky of at most 256 columns by a cluster of 8 CTAs, one 32-row block row each, held in the
+// CTA's shared memory (its lower part, L written in place); the cluster's distributed shared
+// memory carries the panels between the CTAs and its hardware barrier orders the steps.
+// Block column j:
+//  (a) CTA j (warp 0) factors its diagonal block, updated by the steps before, and forms its
+//      inverse Di_j (diag_block_warp); L_jj and Di_j go to global memory;
+//  (b) cluster barrier; every CTA reads CTA j's status (a failure ends all of them together);
+//  (c) every CTA i > j copies Di_j from CTA j and forms L_ij = A_ij Di_j^T in place (and in A);
+//  (d) cluster barrier;
+//  (e) every CTA i > j copies L_cj (j < c <= i) from CTA c and updates its blocks
+//      A_ic -= L_ij L_cj^T; CTA j + 1 goes straight on to (a) of the next column while the others
+//      still update.
+// A one-CTA factorisation waits on L2 round trips between its phases (0.36 ms at k = 256 alone,
+// 0.5-0.6 ms beside a streaming pass); here the block rows stay on chip and the eight CTAs
+// share the updates.  Writes L (lower part), the Dinv blocks and info as chol_la_kernel does.
+constexpr int kClusterCTAs = 8;
+constexpr int kClusterMaxN = kClusterCTAs * kNB;
+constexpr int kClusterThreads = 256;
+constexpr int kRS = kClusterMaxN + 1;   // shared-memory row stride of a block row (doubles)
+struct ClusterSmem {
+  double R[kNB * kRS];                     // this CTA's block row (columns 0 .. 32 (rank + 1))
+  double P[(kClusterCTAs - 1) * kNB * kDP];   // staged L_cj blocks of the update
+  double Dl[kNB * kDP];                    // staged Di_j of the panel
+  double Dg[kNB * kDP], Di[kNB * kDP];     // this CTA's diagonal block: factor and inverse
+  double rdiag[kNB];
+  int status;                              // 0, or 1 + the failing column (global index)
+};
+__global__ void __cluster_dims__(kClusterCTAs, 1, 1) __launch_bounds__(kClusterThreads, 1)
+chol_cluster_kernel(double *__restrict__ A, int n, int lda, double *__restrict__ Dinv,
+                    int *__restrict__ info) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ __align__(16) uint8_t cl_raw[];
+  ClusterSmem &sm = *reinterpret_cast<ClusterSmem *>(cl_raw);
+  const int rank = (int)cl.block_rank();
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nblk = (n + kNB - 1) / kNB;
+  const int row0 = rank * kNB;
+  const bool mine = rank < nblk;   // CTAs past the last block row only keep the barriers
+  // this CTA's block row: the lower part of rows row0 .. row0 + 31, zero past n
+  for (int e = tid; e < kNB * kClusterMaxN; e += kClusterThreads) {
+    const int r = e / kClusterMaxN, c = e % kClusterMaxN, gr = row0 + r;
+    sm.R[r * kRS + c] = (mine && gr < n && c <= gr) ? A[(int64_t)gr * lda + c] : 0.0;
+  }
+  if (tid == 0) sm.status = 0;
+  __syncthreads();
+  // entries of a 32 x 32 block per thread: row tid / 8, columns tid % 8 + 8 u
+  const int er = tid >> 3, ec = tid & 7;
+  int fail = 0;
+  for (int j = 0; j < nblk; ++j) {
+    const int jb = j * kNB;
+    if (rank == j && warp == 0) {   // (a)
+      const int nb = min(kNB, n - jb);
+#pragma unroll 4
+      for (int c = 0; c < kNB; ++c)
+        sm.Dg[lane * kDP + c] = (lane < nb && c <= lane) ? sm.R[lane * kRS + jb + c] : 0.0;
+      __syncwarp();
+      const int bad = diag_block_warp(sm.Dg, sm.Di, nb, sm.rdiag);
+      if (bad) {
+        if (lane == 0) sm.status = jb + bad;
+      } else {
+        double *Dblk = Dinv + (int64_t)j * kNB * kNB;
+        for (int r = 0; r < kNB; ++r) {
+          Dblk[r * kNB + lane] = sm.Di[r * kDP + lane];
+          if (r < nb && lane <= r) {
+            const double l = sm.Dg[r * kDP + lane];
+            sm.R[r * kRS + jb + lane] = l;
+            A[(int64_t)(jb + r) * lda + jb + lane] = l;
+          }
+        }
+      }
+    }
+    cl.sync();   // (b)
+    fail = *cl.map_shared_rank(&sm.status, j);
+    if (fail) break;
+    const bool below = mine && rank > j;
+    if (below) {   // (c)
+      const double *Dj = cl.map_shared_rank(sm.Di, j);
+      for (int e = tid; e < kNB * kNB; e += kClusterThreads) {
+        const int r = e >> 5, c = e & 31;
+        sm.Dl[r * kDP + c] = Dj[r * kDP + c];
+      }
+      __syncthreads();
+      double v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int c = ec + 8 * u;
+        double a = 0.0;
+        for (int q = 0; q <= c; ++q) a = fma(sm.R[er * kRS + jb + q], sm.Dl[c * kDP + q], a);
+        v[u] = a;
+      }
+      __syncthreads();   // the block read by every thread before any entry is replaced
+      const int gr = row0 + er;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int c = ec + 8 * u;
+        sm.R[er * kRS + jb + c] = v[u];
+        if (gr < n) A[(int64_t)gr * lda + jb + c] = v[u];
+      }
+    }
+    cl.sync();   // (d)
+    if (below) {   // (e)
+      const int nc = rank - j;   // blocks c = j + 1 .. rank
+      for (int t = 0; t < nc; ++t) {
+        const double *Lc = cl.map_shared_rank(sm.R, j + 1 + t);
+        double *Pt = sm.P + (size_t)t * kNB * kDP;
+        for (int e = tid; e < kNB * kNB; e += kClusterThreads) {
+          const int r = e >> 5, c = e & 31;
+          Pt[r * kDP + c] = Lc[r * kRS + jb + c];
+        }
+      }
+      __syncthreads();
+      double li[kNB];
+#pragma unroll
+      for (int q = 0; q < kNB; ++q) li[q] = sm.R[er * kRS + jb + q];
+      for (int t = 0; t < nc; ++t) {
+        const double *Pt = sm.P + (size_t)t * kNB * kDP;
+        const int cb = (j + 1 + t) * kNB;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int s = ec + 8 * u;
+          double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+          for (int q = 0; q < kNB; ++q) acc[q & 3] = fma(li[q], Pt[s * kDP + q], acc[q & 3]);
+          sm.R[er * kRS + cb + s] -= (acc[0] + acc[1]) + (acc[2] + acc[3]);
+        }
+      }
+      __syncthreads();
+    }
+  }
+  cl.sync();   // no CTA leaves while another may still read its shared memory
+  if (rank == 0 && tid == 0) *info = fail;
+}
 
 // Solve L L^T X = B for nrhs (<= 4) right-hand sides (rows of B) with the blocked forward and
 // backward substitutions; the diagonal blocks are applied through their inverses (Dinv, staged
@@ -908,12 +1046,12 @@ __global__ void eig_pack_out(const double *__restrict__ A0, const double *__rest
 tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_dev, double *Dinv,
                       cudaStream_t stream) {
   if (n < 1 || n > kMaxDense) return TSVM_ERR_UNSUPPORTED;  // panel must fit shared memory
-  if (n <= kCholSmallN) {   // the whole matrix in shared memory
-    const size_t smem = chol_small_smem(n);
-    TSVM_CUDA(cudaFuncSetAttribute(chol_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem));
-    chol_small_kernel<<<1, kCholSmallThreads, smem, stream ? stream : ctx->stream>>>(
-        A, n, lda, Dinv, info_dev, 0, 0, nullptr);
+  if (n <= kClusterMaxN) {   // one block row per CTA of a cluster, all of it on chip
+    const size_t smem = sizeof(ClusterSmem);
+    TSVM_CUDA(cudaFuncSetAttribute(chol_cluster_kernel,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    chol_cluster_kernel<<<kClusterCTAs, kClusterThreads, smem, stream ? stream : ctx->stream>>>(
+        A, n, lda, Dinv, info_dev);
     TSVM_LAUNCHED(ctx);
     return TSVM_OK;
   }
@@ -928,6 +1066,8 @@ tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_de
   TSVM_LAUNCHED(ctx);
   return TSVM_OK;
 }
+
+int chol_fp64_sms(int n) { return n <= kClusterMaxN ? kClusterCTAs : 1; }
 
 tsvm_status chol_fp64_same(tsvm_context *ctx, double *A, int n, int lda, int64_t strideA,
                            int *info_dev, double *Dinv, int64_t strideD, int count,

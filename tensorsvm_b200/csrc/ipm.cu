@@ -512,21 +512,23 @@ stream_kernel(const float *__restrict__ Z, int64_t ldz, int k, int64_t n, Op op,
          q += (int64_t)kSConsumers * qs, j += kSConsumers) {
       const int st = (int)(j % stages);
       const uint32_t ph = (uint32_t)((j / stages) & 1);
-      if (!tc::mbar_wait(b_full + 8 * st, ph, abort)) break;
-      const float *S = stage0 + (size_t)st * CR * ldz;
       const int64_t r0 = q * CR;   // first row of the chunk
+      // The per-row work that does not read the chunk goes before its wait, so that its vector
+      // loads overlap the chunk's arrival: the right-hand side of Z^T v (lane = row) ...
       double v[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) v[r] = 0.0;
       if constexpr (MODE == MODE_ZT) {
         if (lane < RW && r0 + lane < n) op.rhs(goff + r0 + lane, v, sums, mins);
       }
-      // Z^T D^-1 Z g: the chunk's D^-1 values, loaded once per chunk (lane = row) and passed to
-      // each row's lanes by a shuffle, off the per-row dependency chain
+      // ... and, for Z^T D^-1 Z g, the chunk's D^-1 values (lane = row), passed to each row's
+      // lanes by a shuffle off the per-row dependency chain
       double dch = 0.0;
       if constexpr (MODE == MODE_ZGZ) {
         if (lane < RW && r0 + lane < n) dch = dinv[goff + r0 + lane];
       }
+      if (!tc::mbar_wait(b_full + 8 * st, ph, abort)) break;
+      const float *S = stage0 + (size_t)st * CR * ldz;
       double mine[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) mine[r] = 0.0;
@@ -1301,14 +1303,15 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
     }
     TSVM_CUDA(cudaEventRecord(ev_syrk1, ctx->stream));
     // predictor: r7 = SMW(r5), b = SMW(a) in one pair of passes.  The right-hand sides
-    // Z^T [r5/D, a/D] do not need M: the Cholesky (one CTA, latency-bound) runs on the side
-    // stream on one SM while that pass streams Z on the others.
+    // Z^T [r5/D, a/D] do not need M: the Cholesky (latency-bound; a cluster of 8 CTAs up to
+    // k = 256) runs on the high-priority side stream, its SMs left out of that pass, while the
+    // pass streams Z on the others.
     if (!run.shard) {
       TSVM_CUDA(cudaEventRecord(ctx->fork_ev, ctx->stream));
       TSVM_CUDA(cudaStreamWaitEvent(ctx->side_stream, ctx->fork_ev, 0));
       TSVM_TRY(chol_fp64(ctx, M, k, k, run.info, Mdinv, ctx->side_stream));
       TSVM_CUDA(cudaEventRecord(ev_chol1, ctx->side_stream));
-      run.sm_reserve = 1;
+      run.sm_reserve = chol_fp64_sms(k);
       const tsvm_status st_rhs = run.zt(SmwRhs2Op{V}, h, ST_NONE);
       run.sm_reserve = 0;
       TSVM_CUDA(cudaStreamWaitEvent(ctx->stream, ev_chol1, 0));

@@ -135,6 +135,8 @@ tsvm_status apply_right_fp32(tsvm_context *ctx, const float *A, int64_t n, int k
 // The upper triangle is left untouched.
 tsvm_status chol_fp64(tsvm_context *ctx, double *A, int n, int lda, int *info_dev, double *Dinv,
                       cudaStream_t stream = nullptr);
+// SMs one chol_fp64 of order n occupies (a cluster of 8 CTAs up to n = 256, else one CTA).
+int chol_fp64_sms(int n);
 // Dinv of an existing lower factor L (as chol_fp64 writes it).
 tsvm_status tri_diag_inverse(tsvm_context *ctx, const double *L, int n, int lda, double *Dinv);
 // Solve (L L^T) X = B for nrhs (<= 4) right-hand sides stored as rows of B (nrhs x ldb).

@@ -59,9 +59,11 @@ def test_cholesky_and_solve(ctx, k):
     assert np.allclose(Bd.cpu().numpy(), np.linalg.solve(M, B.T).T, rtol=1e-8, atol=1e-10)
 
 
-@pytest.mark.parametrize("n,bad", [(40, 17), (100, 70), (100, 0), (65, 64)])
+@pytest.mark.parametrize("n,bad", [(40, 17), (100, 70), (100, 0), (65, 64), (160, 32), (200, 150),
+                                   (256, 255), (300, 290)])
 def test_cholesky_reports_indefinite(ctx, n, bad):
-    # the first failing pivot's 1-based column, in the first panel and in later ones
+    # the first failing pivot's 1-based column, in the first panel and in later ones (n <= 256:
+    # the cluster kernel, a failure in any of its CTAs; 300: the one-CTA kernel)
     M = np.eye(n)
     M[bad, bad] = -1.0
     L = dev(M)
