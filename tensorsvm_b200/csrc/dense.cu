@@ -499,10 +499,12 @@ size_t chol_small_smem(int n) { return sizeof(double) * (size_t)n * (n + 1); }
 constexpr int kClusterCTAs = 8;
 constexpr int kClusterMaxN = kClusterCTAs * kNB;
 constexpr int kClusterThreads = 256;
-constexpr int kRS = kClusterMaxN + 1;   // shared-memory row stride of a block row (doubles)
+constexpr int kRS = kClusterMaxN + 2;   // row stride of a block row (doubles): rows on 16-byte
+                                        // boundaries, 4 banks apart
+constexpr int kPS = kNB + 2;            // row stride of a staged 32 x 32 block, likewise
 struct ClusterSmem {
   double R[kNB * kRS];                     // this CTA's block row (columns 0 .. 32 (rank + 1))
-  double P[(kClusterCTAs - 1) * kNB * kDP];   // staged L_cj blocks of the update
+  double P[(kClusterCTAs - 1) * kNB * kPS];   // staged L_cj blocks of the update
   double Dl[kNB * kDP];                    // staged Di_j of the panel
   double Dg[kNB * kDP], Di[kNB * kDP];     // this CTA's diagonal block: factor and inverse
   double rdiag[kNB];
@@ -520,8 +522,11 @@ chol_cluster_kernel(double *__restrict__ A, int n, int lda, double *__restrict__
   const int nblk = (n + kNB - 1) / kNB;
   const int row0 = rank * kNB;
   const bool mine = rank < nblk;   // CTAs past the last block row only keep the barriers
-  // this CTA's block row: the lower part of rows row0 .. row0 + 31, zero past n
-  for (int e = tid; e < kNB * kClusterMaxN; e += kClusterThreads) {
+  // this CTA's block row: the lower part of rows row0 .. row0 + 31, zero past n (eight loads
+  // in flight a thread)
+#pragma unroll 8
+  for (int m = 0; m < kNB * kClusterMaxN / kClusterThreads; ++m) {
+    const int e = tid + m * kClusterThreads;
     const int r = e / kClusterMaxN, c = e % kClusterMaxN, gr = row0 + r;
     sm.R[r * kRS + c] = (mine && gr < n && c <= gr) ? A[(int64_t)gr * lda + c] : 0.0;
   }
@@ -559,9 +564,16 @@ chol_cluster_kernel(double *__restrict__ A, int n, int lda, double *__restrict__
     const bool below = mine && rank > j;
     if (below) {   // (c)
       const double *Dj = cl.map_shared_rank(sm.Di, j);
-      for (int e = tid; e < kNB * kNB; e += kClusterThreads) {
-        const int r = e >> 5, c = e & 31;
-        sm.Dl[r * kDP + c] = Dj[r * kDP + c];
+      double dv[kNB * kNB / kClusterThreads];   // every remote load issued before the stores
+#pragma unroll
+      for (int m = 0; m < kNB * kNB / kClusterThreads; ++m) {
+        const int e = tid + m * kClusterThreads;
+        dv[m] = Dj[(e >> 5) * kDP + (e & 31)];
+      }
+#pragma unroll
+      for (int m = 0; m < kNB * kNB / kClusterThreads; ++m) {
+        const int e = tid + m * kClusterThreads;
+        sm.Dl[(e >> 5) * kDP + (e & 31)] = dv[m];
       }
       __syncthreads();
       double v[4];
@@ -584,27 +596,43 @@ chol_cluster_kernel(double *__restrict__ A, int n, int lda, double *__restrict__
     cl.sync();   // (d)
     if (below) {   // (e)
       const int nc = rank - j;   // blocks c = j + 1 .. rank
-      for (int t = 0; t < nc; ++t) {
-        const double *Lc = cl.map_shared_rank(sm.R, j + 1 + t);
-        double *Pt = sm.P + (size_t)t * kNB * kDP;
-        for (int e = tid; e < kNB * kNB; e += kClusterThreads) {
-          const int r = e >> 5, c = e & 31;
-          Pt[r * kDP + c] = Lc[r * kRS + jb + c];
+      // every remote 16-byte load of the step issued before the stores: thread tid moves
+      // entries (r, 2 p) and (r, 2 p + 1) of each block, r = e / 16, p = e % 16, e = tid, tid + 256
+      constexpr int kH = kNB * kNB / 2 / kClusterThreads;   // 16-byte pieces a thread per block
+      double2 pv[kClusterCTAs - 1][kH];
+#pragma unroll
+      for (int t = 0; t < kClusterCTAs - 1; ++t)
+        if (t < nc) {
+          const double *Lc = cl.map_shared_rank(sm.R, j + 1 + t);
+#pragma unroll
+          for (int h = 0; h < kH; ++h) {
+            const int e = tid + h * kClusterThreads;
+            pv[t][h] = *reinterpret_cast<const double2 *>(Lc + (e >> 4) * kRS + jb + 2 * (e & 15));
+          }
         }
-      }
+#pragma unroll
+      for (int t = 0; t < kClusterCTAs - 1; ++t)
+        if (t < nc) {
+          double *Pt = sm.P + (size_t)t * kNB * kPS;
+#pragma unroll
+          for (int h = 0; h < kH; ++h) {
+            const int e = tid + h * kClusterThreads;
+            *reinterpret_cast<double2 *>(Pt + (e >> 4) * kPS + 2 * (e & 15)) = pv[t][h];
+          }
+        }
       __syncthreads();
       double li[kNB];
 #pragma unroll
       for (int q = 0; q < kNB; ++q) li[q] = sm.R[er * kRS + jb + q];
       for (int t = 0; t < nc; ++t) {
-        const double *Pt = sm.P + (size_t)t * kNB * kDP;
+        const double *Pt = sm.P + (size_t)t * kNB * kPS;
         const int cb = (j + 1 + t) * kNB;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int s = ec + 8 * u;
           double acc[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-          for (int q = 0; q < kNB; ++q) acc[q & 3] = fma(li[q], Pt[s * kDP + q], acc[q & 3]);
+          for (int q = 0; q < kNB; ++q) acc[q & 3] = fma(li[q], Pt[s * kPS + q], acc[q & 3]);
           sm.R[er * kRS + cb + s] -= (acc[0] + acc[1]) + (acc[2] + acc[3]);
         }
       }

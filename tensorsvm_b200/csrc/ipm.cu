@@ -1303,15 +1303,16 @@ tsvm_status ipm_solve(tsvm_context *ctx, const float *Z, int ldz, const float *y
     }
     TSVM_CUDA(cudaEventRecord(ev_syrk1, ctx->stream));
     // predictor: r7 = SMW(r5), b = SMW(a) in one pair of passes.  The right-hand sides
-    // Z^T [r5/D, a/D] do not need M: the Cholesky (latency-bound; a cluster of 8 CTAs up to
-    // k = 256) runs on the high-priority side stream, its SMs left out of that pass, while the
-    // pass streams Z on the others.
-    if (!run.shard) {
+    // Z^T [r5/D, a/D] do not need M.  Above k = 256 the Cholesky (one CTA, latency-bound) runs
+    // on the high-priority side stream on one SM while that pass streams Z on the others.  Up to
+    // k = 256 it is the cluster kernel, which needs eight free SMs of one GPC: beside the
+    // persistent pass it only started once the pass had ended, so it runs in line before it.
+    if (!run.shard && chol_fp64_sms(k) == 1) {
       TSVM_CUDA(cudaEventRecord(ctx->fork_ev, ctx->stream));
       TSVM_CUDA(cudaStreamWaitEvent(ctx->side_stream, ctx->fork_ev, 0));
       TSVM_TRY(chol_fp64(ctx, M, k, k, run.info, Mdinv, ctx->side_stream));
       TSVM_CUDA(cudaEventRecord(ev_chol1, ctx->side_stream));
-      run.sm_reserve = chol_fp64_sms(k);
+      run.sm_reserve = 1;
       const tsvm_status st_rhs = run.zt(SmwRhs2Op{V}, h, ST_NONE);
       run.sm_reserve = 0;
       TSVM_CUDA(cudaStreamWaitEvent(ctx->stream, ev_chol1, 0));

@@ -42,6 +42,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
 // Bounded wait: returns false (and raises the block's abort flag) after ~4 s without progress,
 // or as soon as another thread of the block has aborted.  The global timer is slow to read, so
 // it is only consulted every 1024 unsuccessful polls (each poll may itself suspend briefly).
+// A wait gives up once 4 s have passed on the global timer AND it has polled at least 2^22
+// times (each poll a try_wait that may suspend the thread for a while), so that a jump of the
+// timer cannot end a short wait; 2^30 polls end it whatever the timer says.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort) {
   uint64_t deadline = 0;
   for (uint32_t spin = 1;; ++spin) {
@@ -51,7 +54,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
       const uint64_t now = gtimer();
       if (deadline == 0) {
         deadline = now + 4000000000ull;   // 4 s: a margin over any stall of a working GPU
-      } else if (now > deadline) {
+      } else if ((now > deadline && spin >= (1u << 22)) || spin >= (1u << 30)) {
         *abort = 1;
         return false;
       }
